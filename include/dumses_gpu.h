@@ -1,0 +1,155 @@
+/*
+ * dumses_gpu.h -- C-ABI of libdumses_gpu, the sm_100a implementation of the
+ * DUMSES-Hybrid (v2.2.0) second-order Godunov MHD step.
+ *
+ * The reference exposes this path as argument-less Fortran subroutines that
+ * work on module globals (uin, dt, time, input_params).  Each entry point below
+ * replaces one of them; the Fortran driver keeps its loop and calls these
+ * through ISO_C_BINDING shims:
+ *
+ *   dg_init          <- init_param/allocate_workspace   src/subroutines/init.f90:18-71, 348-419
+ *   dg_upload        <- !$acc data copy(uin)            src/dumses.f90:59
+ *   dg_download      <- !$acc update host(uin)          src/dumses.f90:62,122,133,138,144
+ *   dg_compute_dt    <- compute_dt(dt)                  src/subroutines/physics.f90:18-132
+ *   dg_godunov       <- godunov                         src/subroutines/scheme.f90:104-189
+ *   dg_fargo_update  <- fargo_update                    src/subroutines/fargo.f90:17-124
+ *   dg_boundary      <- boundary                        src/subroutines/boundary.f90:18-92
+ *   dg_history       <- history (MRI problem variant)   src/problem/mri/history.f90:19-174
+ *   dg_step          <- one pass of the loop body       src/dumses.f90:82-120
+ *   dg_finalize      <- deallocate_workspace            src/subroutines/finalize.f90
+ *
+ * Conventions
+ *  - All host arrays use the reference's own layout: Fortran column-major
+ *    uin(iu1:iu2, ju1:ju2, ku1:ku2, 1:11) with nghost = 3 ghost cells on each
+ *    side of every active dimension (ju1=ju2=1 when ndim<2, ku1=ku2=1 when
+ *    ndim<3).  Variables: 1 rho, 2-4 rho*v, 5 total energy, 6-8 B on the left
+ *    x/y/z faces, 9-11 B on the right faces.
+ *  - Every function returns DG_OK (0) or a negative DG_ERR_* code; the text of
+ *    the last error of the calling thread is available from dg_last_error().
+ *  - Calls are ordered on the context's CUDA stream.  dg_compute_dt,
+ *    dg_download, dg_history and dg_sync wait for the stream with a bounded
+ *    poll and return DG_ERR_TIMEOUT rather than block forever.
+ *  - One host thread per context (the reference runs MPI_THREAD_FUNNELED).
+ */
+#ifndef DUMSES_GPU_H
+#define DUMSES_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define DG_OK              0
+#define DG_ERR_ARG        -1   /* invalid argument or parameter combination   */
+#define DG_ERR_CUDA       -2   /* a CUDA runtime call failed                   */
+#define DG_ERR_NOMEM      -3   /* device allocation failed                    */
+#define DG_ERR_TIMEOUT    -4   /* a bounded wait on the device ran out        */
+#define DG_ERR_STATE      -5   /* non-finite or non-physical state detected   */
+#define DG_ERR_DT         -6   /* the CFL reduction gave dt <= 0 or non-finite */
+#define DG_ERR_NODEVICE   -7   /* no CUDA device is visible                   */
+#define DG_ERR_UNSUPPORTED -8  /* option the library does not implement       */
+
+/* Riemann solver ids: the reference's own numbering (src/modules/commons.f90:98-105) */
+#define DG_RIEMANN_LLF     2
+#define DG_RIEMANN_HLL     3
+#define DG_RIEMANN_HLLD    4
+#define DG_RIEMANN_UPWIND  5
+#define DG_RIEMANN_HLLA    8   /* 2D (EMF) solver only */
+
+/* boundary types, one per direction (input_params bdtypex/y/z, commons.f90:123-126) */
+#define DG_BC_PERIODIC      0
+#define DG_BC_ZERO_GRADIENT 1
+#define DG_BC_SHEARINGBOX   2  /* x only, ndim == 3 (boundary.f90:40-52) */
+
+/* arithmetic of the step */
+#define DG_PREC_FP64   0   /* plain path: bit-identical to the FP64 reference arithmetic */
+#define DG_PREC_FP32   1   /* FP32 trace/Riemann/CT, compensated FP32 hi/lo state        */
+
+/* POD mirror of the reference's &scheme_params / &model_params namelists
+ * (src/subroutines/init.f90:153-173) plus the compile-time switches NDIM/ISO. */
+typedef struct dg_params {
+    int    ndim;             /* 2 or 3 (reference NDIM)                                */
+    int    iso;              /* 1: isothermal EOS (reference ISO=1), 0: adiabatic      */
+    int    nx, ny, nz;       /* active cells (nz = 1 when ndim = 2)                    */
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double gamma;            /* ratio of specific heats                                */
+    double ciso;             /* isothermal sound speed                                 */
+    double omega0;           /* rotation rate; > 0 enables Coriolis + shear terms      */
+    double courant;          /* CFL number                                             */
+    int    slope_type;       /* 0 none, 1 minmod, 2 MC, 3 multi-D (scheme.f90:253-656) */
+    int    iriemann;         /* 1D solver: LLF, HLL, HLLD, UPWIND                      */
+    int    iriemann2d;       /* 2D solver: LLF, HLLD, UPWIND, HLLA                     */
+    int    bc[3];            /* DG_BC_* per direction                                  */
+    int    fargo;            /* 1: FARGO orbital advection after the Godunov step      */
+    int    precision;        /* DG_PREC_*                                              */
+    int    surrogate;        /* 1: learned flux surrogate with HLLD fallback (FP32)    */
+    int    device;           /* CUDA device ordinal                                    */
+    int    reserved[6];
+} dg_params;
+
+typedef struct dg_ctx dg_ctx;
+
+/* fill *p with the reference's default_parameters (init.f90:244-302) */
+void dg_default_params(dg_params *p);
+
+/* number of doubles in one host uin array: (nx+6)(ny+6)(nz+6) * 11 for ndim=3 */
+long long dg_uin_size(const dg_params *p);
+
+int  dg_init(const dg_params *p, dg_ctx **ctx);
+int  dg_finalize(dg_ctx *ctx);
+int  dg_upload(dg_ctx *ctx, const double *uin);
+int  dg_download(dg_ctx *ctx, double *uin);
+
+/* CFL step (physics.f90:18-132); returns dt to the host */
+int  dg_compute_dt(dg_ctx *ctx, double *dt);
+/* one Godunov update of the active cells with the given dt, at the given time (scheme.f90:104-189) */
+int  dg_godunov(dg_ctx *ctx, double dt, double time);
+/* FARGO shift of the state after the Godunov update (fargo.f90:17-124) */
+int  dg_fargo_update(dg_ctx *ctx, double dt);
+/* ghost fill, shear-periodic remap at time+dt (boundary.f90:18-92) */
+int  dg_boundary(dg_ctx *ctx, double time, double dt);
+
+/* Loop body of dumses.f90:82-120: compute_dt, godunov, fargo (if on), boundary,
+ * time += dt.  dt and time stay on the device; nsteps steps are enqueued without
+ * any host synchronisation.  On return *time and *dt hold the values after the
+ * last step (this waits for the stream). */
+int  dg_run(dg_ctx *ctx, int nsteps, double *time, double *dt);
+/* one step, as dg_run(ctx, 1, ...) */
+int  dg_step(dg_ctx *ctx, double *time, double *dt);
+
+/* MRI history sums (src/problem/mri/history.f90:60-125) of the current state:
+ * out[0] mass, out[1] maxwell, out[2] reynolds, out[3] maxwell+reynolds,
+ * out[4] magp, out[5..7] <B>, out[8] divB.  FP64 sums in a fixed tree order. */
+int  dg_history(dg_ctx *ctx, double out[9]);
+
+/* wait for all work of the context (bounded) */
+int  dg_sync(dg_ctx *ctx);
+
+/* number of kernels the library launched on this context since dg_init */
+long long dg_kernel_launches(const dg_ctx *ctx);
+
+/* the context's CUDA stream (a cudaStream_t), so a caller can order its own work */
+void *dg_stream(dg_ctx *ctx);
+
+/* message of the last failing call on this thread ("" if none) */
+const char *dg_last_error(void);
+
+/* Host-side initial conditions written straight into a reference-layout uin
+ * (11 variables, ghosts included), followed by the reference's first boundary
+ * call being the caller's job (dg_upload + dg_boundary(ctx, 0, 0)).
+ *   DG_IC_FIELD_LOOP  2D field-loop advection (magnetic_loop/condinit.f90 form)
+ *   DG_IC_ORSZAG_TANG 3D Orszag-Tang-type vortex
+ *   DG_IC_MRI         shearing-box MRI, net vertical field, seeded velocity kicks
+ *   DG_IC_MRI_TEST    the reference's deterministic MRI "Test" setup
+ *                     (mri/condinit.f90:73-105 with type='Test', amp=0) */
+#define DG_IC_FIELD_LOOP  1
+#define DG_IC_ORSZAG_TANG 2
+#define DG_IC_MRI         3
+#define DG_IC_MRI_TEST    4
+int  dg_condinit(const dg_params *p, int ic, double beta, double amp,
+                 unsigned long long seed, double *uin);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DUMSES_GPU_H */
