@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Benchmark of the DUMSES Godunov MHD step on B200.
+
+Headline workload: the 3D Orszag-Tang-type vortex on a 256^3 periodic grid,
+plain FP64 path, HLLD face fluxes and HLLD edge EMFs, MC slopes, CFL 0.8.
+A step is one pass of the reference loop body (compute_dt, godunov,
+boundary; src/dumses.f90:82-120) over the whole grid.
+
+  value  zone-cycles/s with the state resident in HBM: K steps enqueued back to
+         back (dg_run), timed with CUDA events on the library's stream.
+  e2e    the same metric through the reference-facing C-ABI as the Fortran
+         driver calls it: the state uploaded from pinned host memory, then per
+         step dg_compute_dt (dt read back to the host), dg_godunov,
+         dg_boundary, and the state downloaded at the end -- all inside the
+         timed region.
+  roofline  the dominant kernel's algorithmic HBM bytes (128 B per zone-cycle:
+         read + write of the 8 conserved FP64 variables) per launch over its
+         average CUDA-event duration, against the measured copy bandwidth.
+  cpu_baseline  the CPU restatement of the reference (oracle/, C + OpenMP,
+         FP64) on all host cores, on a bounded 128^3 sample of the same setup.
+
+--impl reference times that CPU implementation alone (the reference itself is
+Fortran and no Fortran compiler exists on this image).
+With torchrun and N > 1 every rank runs an independent replica of the
+workload (the step is not decomposed across GPUs in this build).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "zone-cycles/s at 256³: plain FP64 vs FP32+NN-flux at stated L1 vs FP64"
+ALGO_BYTES_PER_ZONE = 128  # read + write of 8 conserved FP64 variables per zone-cycle
+
+
+def workload_params(n: int, device: int = 0):
+    from dumses_hybrid_b200 import Params
+    return Params(ndim=3, nx=n, ny=n, nz=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
+                  gamma=5.0 / 3.0, courant=0.8, slope_type=2, riemann="hlld", riemann2d="hlld", device=device)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            pass
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = ROOT / f".clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        try:
+            self.f.close()
+        except Exception:
+            pass
+
+    def summary(self) -> dict:
+        try:
+            lines = self.path.read_text().strip().splitlines()
+            self.path.unlink()
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            if self.uuid and f[0] != self.uuid:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(steps: int, warmup: int, n: int = 128) -> dict:
+    """The CPU restatement (oracle) on all host cores, n^3 sample of the workload."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from _oracle import Oracle, lib as oracle_lib
+    from dumses_hybrid_b200 import condinit
+    cores = os.cpu_count() or 1
+    oracle_lib().or_set_threads(cores)
+    P = workload_params(n)
+    o = Oracle(P)
+    o.set_state(condinit(P, "orszag_tang"))
+    o.boundary(0.0, 0.0)
+    t = 0.0
+    for _ in range(warmup):
+        t, _ = o.step(t)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        t, _ = o.step(t)
+    el = time.perf_counter() - t0
+    o.close()
+    return {"value": n ** 3 * steps / el, "unit": "zone-cycles/s", "cores": cores, "kind": "port",
+            "sample": f"{n}^3 Orszag-Tang (same setup, 1/{(256 // n) ** 3} of the 256^3 grid), {steps} timed steps "
+                      f"after {warmup} warm-up, C restatement of the reference with OpenMP (FP64)",
+            "seconds": el}
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    cb = cpu_baseline(max(args.steps, 1), max(args.warmup, 0), n=128)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "zone-cycles/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds"] / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "orszag_tang_3d_256^3 (timed on a 128^3 sample per step)", "grid": [128, 128, 128],
+                       "solver": "hlld/hlld", "slope": "mc", "courant": 0.8},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256, help="grid edge (the headline workload is 256)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import datetime
+
+    import numpy as np
+    import torch
+
+    import dumses_hybrid_b200 as dg
+    from dumses_hybrid_b200 import build as dgbuild
+
+    if rank == 0:
+        dgbuild.build()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.barrier()
+        dgbuild.build()
+
+    P = workload_params(args.n, device=local_rank)
+    u0 = dg.condinit(P, "orszag_tang")
+    ncell = args.n ** 3
+    ctx = dg.Context(P)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timed region (value + roofline) ----
+    ctx.upload(u0)
+    ctx.boundary(0.0, 0.0)
+    t_sim, _ = ctx.run(args.warmup, 0.0)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.profile(True)
+    ctx.profile_read()
+    launches0 = ctx.kernel_launches
+    with ClockSampler(uuid) as clk:
+        ev0.record(stream)
+        t_sim, dt_last = ctx.run(args.steps, t_sim)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    launches = ctx.kernel_launches - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * ncell * args.steps / (ms / 1e3)
+
+    # ---- end-to-end through the reference-facing C-ABI ----
+    nt = (args.n + 6) ** 3
+    pinned = torch.empty((11, args.n + 6, args.n + 6, args.n + 6), dtype=torch.float64, pin_memory=True)
+    host = pinned.numpy().T  # Fortran-ordered view (nx+6, ny+6, nz+6, 11)
+    host[...] = u0
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.upload(host)
+    ctx.boundary(0.0, 0.0)
+    te = 0.0
+    for _ in range(args.steps):
+        dt = ctx.compute_dt()
+        ctx.godunov(dt, te)
+        ctx.boundary(te, dt)
+        te = te + dt
+    got = ctx.download()
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * ncell * args.steps / (ms_e2e / 1e3)
+    ok = bool(np.isfinite(got[..., :8]).all())
+    ctx.close()
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm_peak else "fallback"
+    hbm_peak = hbm_peak or 6650.0
+    kernels = {k: {"ms_total": v[0], "launches": v[1], "ms_per_launch": v[0] / max(v[1], 1)} for k, v in prof.items()}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"]) if kernels else None
+    roof = None
+    if dom:
+        per_launch_s = kernels[dom]["ms_per_launch"] / 1e3
+        achieved = ALGO_BYTES_PER_ZONE * ncell / per_launch_s / 1e9
+        traffic = None
+        tpath = ROOT / "profiles" / f"ncu_traffic_ot{args.n}_fp64.json"
+        if tpath.exists():
+            try:
+                traffic = json.loads(tpath.read_text()).get(dom)
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_ZONE * ncell,
+                "step_achieved": ALGO_BYTES_PER_ZONE * ncell * args.steps / (ms / 1e3) / 1e9 / world,
+                "step_frac": ALGO_BYTES_PER_ZONE * ncell * args.steps / (ms / 1e3) / 1e9 / world / hbm_peak}
+    line = {"metric": METRIC, "value": value, "unit": "zone-cycles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"orszag_tang_3d_{args.n}^3_fp64", "grid": [args.n] * 3, "precision": "fp64",
+                       "solver": "hlld/hlld", "slope": "mc", "courant": 0.8, "parallelism": f"replicas x{world}",
+                       "l2": "working set ~13 GB per step >> 126 MB L2, no flush needed"},
+            "e2e": {"value": e2e_value, "unit": "zone-cycles/s", "h2d_bytes_per_step": 8 * nt * 8 / args.steps,
+                    "d2h_bytes_per_step": (11 * nt * 8) / args.steps + 8 * 2, "finite": ok},
+            "gpu_launches": launches, "roofline": roof, "kernels": kernels, "clocks": clk.summary(),
+            "sim_time": t_sim}
+    if world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(2, 1, n=128)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,293 @@
+"""dumses_hybrid_b200: the DUMSES-Hybrid Godunov MHD step on B200 (sm_100a).
+
+Python mirror of the reference's operator interface for the hot path.  The
+reference calls argument-less Fortran subroutines on module globals from its
+driver loop (src/dumses.f90:82-120); the same calls exist here as methods of
+:class:`Context`, which wraps one context of the C-ABI library
+``libdumses_gpu.so`` (include/dumses_gpu.h):
+
+    reference                         here
+    ---------------------------------  ------------------------------------
+    call compute_dt(dt)                dt = ctx.compute_dt()
+    call godunov                       ctx.godunov(dt, time)
+    if (fargo) call fargo_update       ctx.fargo_update(dt)
+    call boundary                      ctx.boundary(time, dt)
+    call history (MRI problem)         ctx.history()
+    !$acc update host(uin)             uin = ctx.download()
+
+Arrays use the reference layout: numpy arrays of shape
+(nx+6, ny+6, nz+6, 11) in Fortran order (uin(iu1:iu2,ju1:ju2,ku1:ku2,1:11)).
+
+There is no CPU fallback: if the library is missing or no GPU is visible the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import re
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "libdumses_gpu.so"
+
+DG_OK = 0
+ERRORS = {-1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -4: "DG_ERR_TIMEOUT", -5: "DG_ERR_STATE",
+          -6: "DG_ERR_DT", -7: "DG_ERR_NODEVICE", -8: "DG_ERR_UNSUPPORTED"}
+RIEMANN = {"llf": 2, "hll": 3, "hlld": 4, "upwind": 5, "hlla": 8}
+BC = {"periodic": 0, "zero_gradient": 1, "shearingbox": 2}
+IC = {"field_loop": 1, "orszag_tang": 2, "mri": 3, "mri_test": 4}
+PREC = {"fp64": 0, "fp32": 1}
+
+
+class DgParams(ctypes.Structure):
+    """ctypes mirror of ``dg_params`` (include/dumses_gpu.h)."""
+    _fields_ = [("ndim", ctypes.c_int), ("iso", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("nz", ctypes.c_int), ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double), ("zmin", ctypes.c_double),
+                ("zmax", ctypes.c_double), ("gamma", ctypes.c_double), ("ciso", ctypes.c_double),
+                ("omega0", ctypes.c_double), ("courant", ctypes.c_double), ("slope_type", ctypes.c_int),
+                ("iriemann", ctypes.c_int), ("iriemann2d", ctypes.c_int), ("bc", ctypes.c_int * 3),
+                ("fargo", ctypes.c_int), ("precision", ctypes.c_int), ("surrogate", ctypes.c_int),
+                ("device", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
+class DumsesError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
+    """Load libdumses_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: build it with `python -m dumses_hybrid_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    c_p = ctypes.POINTER(DgParams)
+    vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "dg_default_params": (None, [c_p]),
+        "dg_uin_size": (ctypes.c_longlong, [c_p]),
+        "dg_init": (ctypes.c_int, [c_p, ctypes.POINTER(vp)]),
+        "dg_finalize": (ctypes.c_int, [vp]),
+        "dg_upload": (ctypes.c_int, [vp, dp]),
+        "dg_download": (ctypes.c_int, [vp, dp]),
+        "dg_compute_dt": (ctypes.c_int, [vp, dp]),
+        "dg_godunov": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double]),
+        "dg_fargo_update": (ctypes.c_int, [vp, ctypes.c_double]),
+        "dg_boundary": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double]),
+        "dg_run": (ctypes.c_int, [vp, ctypes.c_int, dp, dp]),
+        "dg_step": (ctypes.c_int, [vp, dp, dp]),
+        "dg_history": (ctypes.c_int, [vp, dp]),
+        "dg_sync": (ctypes.c_int, [vp]),
+        "dg_kernel_launches": (ctypes.c_longlong, [vp]),
+        "dg_stream": (vp, [vp]),
+        "dg_last_error": (ctypes.c_char_p, []),
+        "dg_profile": (ctypes.c_int, [vp, ctypes.c_int]),
+        "dg_profile_read": (ctypes.c_int, [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+        "dg_profile_slot_name": (ctypes.c_char_p, [ctypes.c_int]),
+        "dg_debug_copy": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
+        "dg_condinit": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong, dp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != DG_OK:
+        raise DumsesError(rc, load_library().dg_last_error().decode())
+
+
+@dataclass
+class Params:
+    """The reference's &scheme_params / &model_params plus NDIM and ISO."""
+    ndim: int = 3
+    iso: int = 0
+    nx: int = 256
+    ny: int = 256
+    nz: int = 256
+    xmin: float = 0.0
+    xmax: float = 1.0
+    ymin: float = -0.5
+    ymax: float = 0.5
+    zmin: float = 0.0
+    zmax: float = 1.0
+    gamma: float = 5.0 / 3.0
+    ciso: float = 0.0
+    omega0: float = 0.0
+    courant: float = 0.7
+    slope_type: int = 2
+    riemann: str = "hlld"
+    riemann2d: str = "hlld"
+    bdtypex: str = "periodic"
+    bdtypey: str = "periodic"
+    bdtypez: str = "periodic"
+    fargo: bool = False
+    precision: str = "fp64"
+    surrogate: bool = False
+    device: int = 0
+
+    def to_c(self) -> DgParams:
+        p = DgParams()
+        p.ndim, p.iso, p.nx, p.ny, p.nz = self.ndim, int(self.iso), self.nx, self.ny, self.nz
+        p.xmin, p.xmax, p.ymin, p.ymax, p.zmin, p.zmax = self.xmin, self.xmax, self.ymin, self.ymax, self.zmin, self.zmax
+        p.gamma, p.ciso, p.omega0, p.courant = self.gamma, self.ciso, self.omega0, self.courant
+        p.slope_type = self.slope_type
+        p.iriemann, p.iriemann2d = RIEMANN[self.riemann], RIEMANN[self.riemann2d]
+        p.bc[0], p.bc[1], p.bc[2] = BC[self.bdtypex], BC[self.bdtypey], BC[self.bdtypez]
+        p.fargo, p.precision, p.surrogate, p.device = int(self.fargo), PREC[self.precision], int(self.surrogate), self.device
+        return p
+
+    @property
+    def shape(self) -> tuple[int, int, int, int]:
+        return (self.nx + 6, self.ny + 6 if self.ndim > 1 else 1, self.nz + 6 if self.ndim == 3 else 1, 11)
+
+
+def read_namelist(path: str | pathlib.Path, ndim: int = 3, iso: int = 0) -> Params:
+    """Build :class:`Params` from a reference ``input`` namelist file
+    (&scheme_params, &model_params; init.f90:153-173), applying the reference
+    defaults (init.f90:244-302) for keys the file does not set."""
+    text = pathlib.Path(path).read_text()
+    kv = {}
+    for m in re.finditer(r"([A-Za-z0-9_]+)\s*=\s*('[^']*'|\"[^\"]*\"|[^,\s/]+)", text):
+        kv[m.group(1).lower()] = m.group(2).strip("'\"")
+
+    def num(s: str) -> float:
+        return float(s.lower().replace("d", "e"))
+
+    p = Params(ndim=ndim, iso=iso)
+    for key in ("nx", "ny", "nz", "slope_type"):
+        if key in kv:
+            setattr(p, key, int(kv[key]))
+    for key in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "gamma", "ciso", "courant"):
+        if key in kv:
+            setattr(p, key, num(kv[key]))
+    if "omega0" in kv:
+        p.omega0 = num(kv["omega0"])
+    for key in ("riemann", "riemann2d", "bdtypex", "bdtypey", "bdtypez"):
+        if key in kv:
+            setattr(p, key, kv[key].strip().lower())
+    if "fargo" in kv:
+        p.fargo = kv["fargo"].strip(".").lower().startswith("t")
+    if ndim < 3:
+        p.nz = 1
+    return p
+
+
+def condinit(params: Params, ic: str, beta: float = 1000.0, amp: float = 0.0, seed: int = 0) -> np.ndarray:
+    """Initial conditions in the reference layout (host-side, no GPU needed)."""
+    lib = load_library()
+    cp = params.to_c()
+    u = np.zeros(params.shape, dtype=np.float64, order="F")
+    _check(lib.dg_condinit(ctypes.byref(cp), IC[ic], beta, amp, seed, u.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return u
+
+
+class Context:
+    """One device state of the MHD step (a dg_ctx of the C-ABI)."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        self.lib = load_library()
+        self._cp = params.to_c()
+        h = ctypes.c_void_p()
+        _check(self.lib.dg_init(ctypes.byref(self._cp), ctypes.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.dg_finalize(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _ptr(a: np.ndarray):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    def upload(self, uin: np.ndarray) -> None:
+        if uin.shape != self.params.shape or uin.dtype != np.float64 or not uin.flags.f_contiguous:
+            raise ValueError(f"uin must be a Fortran-ordered float64 array of shape {self.params.shape}")
+        _check(self.lib.dg_upload(self.h, self._ptr(uin)))
+
+    def download(self) -> np.ndarray:
+        u = np.zeros(self.params.shape, dtype=np.float64, order="F")
+        _check(self.lib.dg_download(self.h, self._ptr(u)))
+        return u
+
+    def compute_dt(self) -> float:
+        dt = ctypes.c_double()
+        _check(self.lib.dg_compute_dt(self.h, ctypes.byref(dt)))
+        return dt.value
+
+    def godunov(self, dt: float, time: float) -> None:
+        _check(self.lib.dg_godunov(self.h, dt, time))
+
+    def fargo_update(self, dt: float) -> None:
+        _check(self.lib.dg_fargo_update(self.h, dt))
+
+    def boundary(self, time: float, dt: float) -> None:
+        _check(self.lib.dg_boundary(self.h, time, dt))
+
+    def run(self, nsteps: int, time: float) -> tuple[float, float]:
+        t, dt = ctypes.c_double(time), ctypes.c_double(0.0)
+        _check(self.lib.dg_run(self.h, nsteps, ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
+
+    def history(self) -> np.ndarray:
+        out = np.zeros(9)
+        _check(self.lib.dg_history(self.h, self._ptr(out)))
+        return out
+
+    def sync(self) -> None:
+        _check(self.lib.dg_sync(self.h))
+
+    def debug_array(self, which: int, size: int) -> np.ndarray:
+        """Copy a device work array of the last step (see dg_debug_copy)."""
+        out = np.zeros(size)
+        n = ctypes.c_longlong()
+        _check(self.lib.dg_debug_copy(self.h, which, self._ptr(out), size, ctypes.byref(n)))
+        return out[: n.value]
+
+    def profile(self, on: bool = True) -> None:
+        """Record CUDA events around every kernel of this context."""
+        _check(self.lib.dg_profile(self.h, int(on)))
+
+    def profile_read(self) -> dict[str, tuple[float, int]]:
+        """{kernel slot: (total ms, launches)} since the last read."""
+        n = 11
+        ms = np.zeros(n)
+        cnt = (ctypes.c_longlong * n)()
+        _check(self.lib.dg_profile_read(self.h, self._ptr(ms), cnt, n))
+        return {self.lib.dg_profile_slot_name(k).decode(): (float(ms[k]), int(cnt[k])) for k in range(n) if cnt[k]}
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.dg_stream(self.h) or 0)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.dg_kernel_launches(self.h))

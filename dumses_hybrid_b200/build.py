@@ -1,0 +1,88 @@
+"""Build libdumses_gpu.so in-tree for sm_100a.
+
+nvcc compiles each CUDA translation unit with
+  -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo --fmad=false
+(no multiply-add contraction: the FP64 path is bit-identical to the CPU
+reference arithmetic) and links them, with the host-side initial conditions,
+into dumses_hybrid_b200/libdumses_gpu.so against the static CUDA runtime.
+Objects are rebuilt only when a source or header is newer than the library.
+
+Usage: python -m dumses_hybrid_b200.build [--force] [--verbose]
+"""
+from __future__ import annotations
+
+import os
+import pathlib
+import shutil
+import subprocess
+import sys
+
+PKG = pathlib.Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = PKG / "_build"
+LIB = PKG / "libdumses_gpu.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
+                     "-I", str(INCLUDE), "-I", str(CSRC)]
+CU_SOURCES = ["mhd_kernels.cu", "dg_api.cu"]
+CXX_SOURCES = ["condinit.cpp"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and pathlib.Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _cxx() -> str:
+    # the environment's CC/CXX may point at a wrapper; the system compiler is enough here
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and pathlib.Path(cand).exists():
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def _newest_input() -> float:
+    files = list(CSRC.glob("*")) + list(INCLUDE.glob("*.h")) + [pathlib.Path(__file__)]
+    return max(f.stat().st_mtime for f in files if f.is_file())
+
+
+def _run(cmd: list[str], verbose: bool) -> None:
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose and (res.stdout or res.stderr):
+        print(res.stdout + res.stderr, flush=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"command failed ({res.returncode}): {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> pathlib.Path:
+    if LIB.exists() and not force and LIB.stat().st_mtime >= _newest_input():
+        return LIB
+    BUILD.mkdir(exist_ok=True)
+    nvcc, cxx = _nvcc(), _cxx()
+    objs = []
+    for src in CU_SOURCES:
+        obj = BUILD / (src + ".o")
+        extra = ["-Xptxas", "-v"] if ptxas_info else []
+        _run([nvcc, *NVCC_FLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)], verbose or ptxas_info)
+        objs.append(str(obj))
+    for src in CXX_SOURCES:
+        obj = BUILD / (src + ".o")
+        _run([cxx, "-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-I", str(INCLUDE), "-c", str(CSRC / src),
+              "-o", str(obj)], verbose)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", *objs, "-o", str(tmp)], verbose)
+    tmp.replace(LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

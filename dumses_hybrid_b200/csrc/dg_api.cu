@@ -1,0 +1,463 @@
+// C-ABI of libdumses_gpu (declarations and reference mapping in include/dumses_gpu.h).
+//
+// One context owns the device state of one grid: two state buffers used in
+// ping-pong (each step reads one and writes the other), the work arrays of the
+// step, and a CUDA stream.  Device scalars (dt, time, CFL minimum, error word)
+// stay on the device so that whole steps can be enqueued back to back.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+
+#include <vector>
+
+#include "dumses_gpu.h"
+#include "mhd_kernels.cuh"
+
+namespace {
+// CUDA-event timing of every kernel the context enqueues, on the context's stream
+struct EventTimer : dg::KernelTimer {
+    struct Rec { int slot; cudaEvent_t a, b; };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Rec> recs;
+    cudaEvent_t pending = nullptr;
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int, cudaStream_t st) override { pending = get(); cudaEventRecord(pending, st); }
+    void end(int slot, cudaStream_t st) override {
+        cudaEvent_t b = get();
+        cudaEventRecord(b, st);
+        recs.push_back({slot, pending, b});
+        pending = nullptr;
+    }
+    ~EventTimer() override {
+        for (auto &r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+const char *kSlotNames[dg::KS_COUNT] = {"scalars", "cfl_dt", "primitive", "trace", "riemann_flux_emf", "update_ct",
+                                       "fargo_emf", "fargo_update", "boundary", "history", "right_faces"};
+}  // namespace
+
+struct dg_ctx {
+    dg_params p;
+    dg::Geo G;
+    dg::Bufs B;
+    int cur = 0;
+    int nv = 8;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+    dg::Scalars *h_scal = nullptr;  // pinned read-back of the device scalars
+    double *h_hist = nullptr;       // pinned read-back of history sums
+    size_t bytes = 0;
+    EventTimer *timer = nullptr;    // non-null while per-kernel profiling is on
+};
+
+namespace {
+// attach the context's timer (if any) to the launches of the current call
+struct TimerScope {
+    explicit TimerScope(dg_ctx *c) { dg::g_timer = c ? c->timer : nullptr; }
+    ~TimerScope() { dg::g_timer = nullptr; }
+};
+}  // namespace
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define DG_CUDA(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+double sync_timeout_s() {
+    const char *e = std::getenv("DG_SYNC_TIMEOUT_S");
+    if (e) {
+        double v = std::atof(e);
+        if (v > 0) return v;
+    }
+    return 300.0;
+}
+
+// wait for the stream with a wall-clock bound instead of blocking forever
+int bounded_sync(cudaStream_t s) {
+    const double limit = sync_timeout_s();
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess) return DG_OK;
+        if (e != cudaErrorNotReady) return fail(DG_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) return fail(DG_ERR_TIMEOUT, "device work did not finish within DG_SYNC_TIMEOUT_S");
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
+    }
+}
+
+int check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(DG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return DG_OK;
+}
+
+int validate(const dg_params *p) {
+    if (!p) return fail(DG_ERR_ARG, "null parameters");
+    if (p->ndim != 2 && p->ndim != 3) return fail(DG_ERR_UNSUPPORTED, "ndim must be 2 or 3");
+    if (p->nx < 3 || p->ny < 3) return fail(DG_ERR_ARG, "nx and ny must be >= 3 (three ghost layers are copied)");
+    if (p->ndim == 3 && p->nz < 3) return fail(DG_ERR_ARG, "nz must be >= 3 when ndim = 3");
+    if (p->ndim == 2 && p->nz != 1) return fail(DG_ERR_ARG, "nz must be 1 when ndim = 2");
+    if (!(p->xmax > p->xmin) || !(p->ymax > p->ymin) || !(p->zmax > p->zmin)) return fail(DG_ERR_ARG, "empty domain");
+    if (!(p->courant > 0)) return fail(DG_ERR_ARG, "courant must be > 0");
+    if (p->iso && !(p->ciso > 0)) return fail(DG_ERR_ARG, "isothermal EOS needs ciso > 0");
+    if (!p->iso && !(p->gamma > 1)) return fail(DG_ERR_ARG, "adiabatic EOS needs gamma > 1");
+    if (p->slope_type < 0 || p->slope_type > 3) return fail(DG_ERR_ARG, "slope_type must be 0..3");
+    if (p->iriemann != DG_RIEMANN_LLF && p->iriemann != DG_RIEMANN_HLL && p->iriemann != DG_RIEMANN_HLLD &&
+        p->iriemann != DG_RIEMANN_UPWIND)
+        return fail(DG_ERR_UNSUPPORTED, "iriemann must be llf, hll, hlld or upwind");
+    if (p->iriemann2d != DG_RIEMANN_LLF && p->iriemann2d != DG_RIEMANN_HLLD && p->iriemann2d != DG_RIEMANN_UPWIND &&
+        p->iriemann2d != DG_RIEMANN_HLLA)
+        return fail(DG_ERR_UNSUPPORTED, "iriemann2d must be llf, hlld, upwind or hlla");
+    for (int d = 0; d < 3; d++)
+        if (p->bc[d] < DG_BC_PERIODIC || p->bc[d] > DG_BC_SHEARINGBOX) return fail(DG_ERR_ARG, "unknown boundary type");
+    if (p->bc[1] == DG_BC_SHEARINGBOX || p->bc[2] == DG_BC_SHEARINGBOX)
+        return fail(DG_ERR_UNSUPPORTED, "the shearing box is an x boundary");
+    if (p->bc[0] == DG_BC_SHEARINGBOX && p->ndim != 3)
+        return fail(DG_ERR_UNSUPPORTED, "the shearing-box boundary exists for ndim = 3 only (boundary.f90:40)");
+    if (p->bc[0] == DG_BC_SHEARINGBOX && p->bc[1] != DG_BC_PERIODIC)
+        return fail(DG_ERR_UNSUPPORTED, "the shearing box needs a periodic y direction");
+    if (p->fargo && (p->ndim != 3 || p->bc[1] != DG_BC_PERIODIC))
+        return fail(DG_ERR_UNSUPPORTED, "FARGO needs ndim = 3 and a periodic y direction");
+    if (p->precision != DG_PREC_FP64) return fail(DG_ERR_UNSUPPORTED, "this build implements the FP64 path only");
+    if (p->surrogate) return fail(DG_ERR_UNSUPPORTED, "the flux surrogate needs the FP32 path");
+    return DG_OK;
+}
+
+dg::Geo make_geo(const dg_params &p) {
+    dg::Geo G{};
+    G.ndim = p.ndim; G.nx = p.nx; G.ny = p.ny; G.nz = p.nz;
+    G.NX = p.nx + 6;
+    G.NY = p.ndim > 1 ? p.ny + 6 : 1;
+    G.NZ = p.ndim == 3 ? p.nz + 6 : 1;
+    G.gy = p.ndim > 1 ? 3 : 0;
+    G.gz = p.ndim == 3 ? 3 : 0;
+    G.sy = G.NX;
+    G.sz = (long long)G.NX * G.NY;
+    G.sv = G.sz * G.NZ;
+    G.CX = p.nx + 2; G.CY = p.ny + 2;
+    G.CZ = p.ndim == 3 ? p.nz + 2 : 1;
+    G.kc0 = p.ndim == 3 ? 0 : 1;
+    G.csz = (long long)G.CX * G.CY * G.CZ;
+    G.FX = p.nx + 1; G.FY = p.ny + 1;
+    G.FZ = p.ndim == 3 ? p.nz + 1 : 1;
+    G.fsz = (long long)G.FX * G.FY * G.FZ;
+    // init_grid (init.f90:447-449), single rank
+    G.dx = (p.xmax - p.xmin) / p.nx;
+    G.dy = (p.ymax - p.ymin) / p.ny;
+    G.dz = (p.zmax - p.zmin) / p.nz;
+    G.xmin = p.xmin; G.xmax = p.xmax; G.ymin = p.ymin; G.ymax = p.ymax; G.zmin = p.zmin; G.zmax = p.zmax;
+    G.gamma = p.gamma; G.ciso = p.ciso; G.omega0 = p.omega0; G.courant = p.courant;
+    G.iso = p.iso; G.slope_type = p.slope_type; G.iriemann = p.iriemann; G.iriemann2d = p.iriemann2d;
+    G.fargo = p.fargo;
+    G.shearing = (p.bc[0] == DG_BC_SHEARINGBOX);
+    for (int d = 0; d < 3; d++) G.bc[d] = p.bc[d];
+    // ndim_act, init.f90:203-213
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    if ((nx == 1 && ny == 1) || (nx == 1 && nz == 1) || (ny == 1 && nz == 1)) G.ndim_act = 1;
+    else if ((nx == 1 && ny > 1 && nz > 1) || (nx > 1 && ny == 1 && nz > 1) || (nx > 1 && ny > 1 && nz == 1)) G.ndim_act = 2;
+    else G.ndim_act = 3;
+    return G;
+}
+
+int alloc(dg_ctx *c, double **p, size_t n) {
+    size_t b = n * sizeof(double);
+    cudaError_t e = cudaMalloc((void **)p, b);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(DG_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(b) + " bytes: " + cudaGetErrorString(e));
+    }
+    c->bytes += b;
+    DG_CUDA(cudaMemsetAsync(*p, 0, b, c->stream));
+    return DG_OK;
+}
+
+int read_scalars(dg_ctx *c) {
+    DG_CUDA(cudaMemcpyAsync(c->h_scal, c->B.S, sizeof(dg::Scalars), cudaMemcpyDeviceToHost, c->stream));
+    int rc = bounded_sync(c->stream);
+    if (rc) return rc;
+    if (c->h_scal->err) {
+        int e = c->h_scal->err;
+        c->h_scal->err = 0;
+        DG_CUDA(cudaMemsetAsync(&c->B.S->err, 0, sizeof(int), c->stream));
+        if (e == DG_ERR_DT) return fail(e, "CFL reduction produced dt <= 0 or a non-finite dt");
+        return fail(e, "non-finite or non-physical state met in the CFL reduction");
+    }
+    return DG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void dg_default_params(dg_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    // default_parameters, init.f90:244-302
+    p->ndim = 3; p->iso = 0;
+    p->nx = 256; p->ny = 256; p->nz = 256;
+    p->xmin = 0.0; p->xmax = 1.0; p->ymin = -0.5; p->ymax = 0.5; p->zmin = 0.0; p->zmax = 1.0;
+    p->gamma = 5.0 / 3.0; p->ciso = 0.0; p->omega0 = 0.0; p->courant = 0.7;
+    p->slope_type = 2; p->iriemann = DG_RIEMANN_HLLD; p->iriemann2d = DG_RIEMANN_HLLD;
+    p->bc[0] = p->bc[1] = p->bc[2] = DG_BC_PERIODIC;
+    p->fargo = 0; p->precision = DG_PREC_FP64; p->surrogate = 0; p->device = 0;
+}
+
+long long dg_uin_size(const dg_params *p) {
+    if (!p) return 0;
+    long long nx = p->nx + 6, ny = p->ndim > 1 ? p->ny + 6 : 1, nz = p->ndim == 3 ? p->nz + 6 : 1;
+    return nx * ny * nz * 11;
+}
+
+const char *dg_last_error(void) { return g_last_error.c_str(); }
+
+int dg_init(const dg_params *p, dg_ctx **out) {
+    if (!out) return fail(DG_ERR_ARG, "null context pointer");
+    *out = nullptr;
+    int rc = validate(p);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(DG_ERR_NODEVICE, "no CUDA device visible");
+    if (p->device < 0 || p->device >= ndev) return fail(DG_ERR_ARG, "device ordinal out of range");
+    DG_CUDA(cudaSetDevice(p->device));
+    dg_ctx *c = new dg_ctx();
+    c->p = *p;
+    c->G = make_geo(*p);
+    c->nv = dg::nstate_vars(c->G);
+    std::memset(&c->B, 0, sizeof(c->B));
+    auto bail = [&](int code) { dg_finalize(c); return code; };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(DG_ERR_CUDA, "cudaStreamCreate failed"));
+    const dg::Geo &G = c->G;
+    const size_t nt = (size_t)G.sv;
+    if ((rc = alloc(c, &c->B.U[0], nt * c->nv))) return bail(rc);
+    if ((rc = alloc(c, &c->B.U[1], nt * c->nv))) return bail(rc);
+    if ((rc = alloc(c, &c->B.Q, nt * 8))) return bail(rc);
+    const int ncore = p->ndim == 3 ? dg::kCore3 : dg::kCore2;
+    if ((rc = alloc(c, &c->B.core, (size_t)G.csz * ncore))) return bail(rc);
+    for (int d = 0; d < p->ndim; d++)
+        if ((rc = alloc(c, &c->B.flx[d], (size_t)G.fsz * dg::kFluxComp))) return bail(rc);
+    for (int d = 0; d < 3; d++) {
+        if (p->ndim == 2 && d < 2) continue;
+        if ((rc = alloc(c, &c->B.emf[d], (size_t)G.fsz))) return bail(rc);
+    }
+    if (p->fargo)
+        for (int d = 0; d < 2; d++)
+            if ((rc = alloc(c, &c->B.femf[d], (size_t)G.fsz))) return bail(rc);
+    if ((rc = alloc(c, &c->B.part, (size_t)(2 * p->nx + 8 * 296 + 64)))) return bail(rc);
+    if ((rc = alloc(c, &c->B.hist, 16))) return bail(rc);
+    {
+        cudaError_t e = cudaMalloc((void **)&c->B.S, sizeof(dg::Scalars));
+        if (e != cudaSuccess) return bail(fail(DG_ERR_NOMEM, "cudaMalloc of the device scalars failed"));
+        cudaMemsetAsync(c->B.S, 0, sizeof(dg::Scalars), c->stream);
+    }
+    if (cudaMallocHost((void **)&c->h_scal, sizeof(dg::Scalars)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->h_hist, 16 * sizeof(double)) != cudaSuccess)
+        return bail(fail(DG_ERR_NOMEM, "cudaMallocHost failed"));
+    if ((rc = bounded_sync(c->stream))) return bail(rc);
+    *out = c;
+    return DG_OK;
+}
+
+int dg_finalize(dg_ctx *c) {
+    if (!c) return DG_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    double *bufs[] = {c->B.U[0], c->B.U[1], c->B.Q, c->B.core, c->B.flx[0], c->B.flx[1], c->B.flx[2], c->B.emf[0],
+                      c->B.emf[1], c->B.emf[2], c->B.femf[0], c->B.femf[1], c->B.part, c->B.hist};
+    for (double *b : bufs)
+        if (b) cudaFree(b);
+    if (c->B.S) cudaFree(c->B.S);
+    if (c->h_scal) cudaFreeHost(c->h_scal);
+    if (c->h_hist) cudaFreeHost(c->h_hist);
+    delete c->timer;
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DG_OK;
+}
+
+int dg_upload(dg_ctx *c, const double *uin) {
+    if (!c || !uin) return fail(DG_ERR_ARG, "null argument");
+    DG_CUDA(cudaSetDevice(c->p.device));
+    const size_t nt = (size_t)c->G.sv;
+    // uin(:,:,:,1:8) is contiguous in the reference layout
+    DG_CUDA(cudaMemcpyAsync(c->B.U[c->cur], uin, nt * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (c->nv == 9) {
+        // ndim = 2: the right z-face B (uin var 11) is never refreshed by the reference and
+        // stays at its initial value; both state buffers carry it
+        for (int b = 0; b < 2; b++)
+            DG_CUDA(cudaMemcpyAsync(c->B.U[b] + nt * 8, uin + nt * 10, nt * sizeof(double), cudaMemcpyHostToDevice,
+                                    c->stream));
+    }
+    return bounded_sync(c->stream);
+}
+
+int dg_download(dg_ctx *c, double *uin) {
+    TimerScope ts_(c);
+    if (!c || !uin) return fail(DG_ERR_ARG, "null argument");
+    DG_CUDA(cudaSetDevice(c->p.device));
+    const size_t nt = (size_t)c->G.sv;
+    DG_CUDA(cudaMemcpyAsync(uin, c->B.U[c->cur], nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->launches += dg::launch_right_faces(c->G, c->B.U[c->cur], c->B.Q, c->stream);
+    int rc = check_launch();
+    if (rc) return rc;
+    DG_CUDA(cudaMemcpyAsync(uin + nt * 8, c->B.Q, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return bounded_sync(c->stream);
+}
+
+int dg_compute_dt(dg_ctx *c, double *dt) {
+    TimerScope ts_(c);
+    if (!c || !dt) return fail(DG_ERR_ARG, "null argument");
+    c->launches += dg::launch_dt(c->G, c->B, c->cur, c->stream);
+    int rc = check_launch();
+    if (rc) return rc;
+    if ((rc = read_scalars(c))) return rc;
+    *dt = c->h_scal->dt;
+    return DG_OK;
+}
+
+int dg_godunov(dg_ctx *c, double dt, double time) {
+    TimerScope ts_(c);
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    if (!(dt > 0) || !std::isfinite(dt)) return fail(DG_ERR_DT, "dt must be positive and finite");
+    c->launches += dg::launch_set_scalars(c->B, dt, time, 1, 1, c->stream);
+    c->launches += dg::launch_godunov(c->G, c->B, c->cur, c->stream);
+    c->cur ^= 1;
+    return check_launch();
+}
+
+int dg_fargo_update(dg_ctx *c, double dt) {
+    TimerScope ts_(c);
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    if (!c->p.fargo) return fail(DG_ERR_ARG, "context was created with fargo = 0");
+    c->launches += dg::launch_set_scalars(c->B, dt, 0.0, 1, 0, c->stream);
+    c->launches += dg::launch_fargo(c->G, c->B, c->cur, c->stream);
+    c->cur ^= 1;
+    return check_launch();
+}
+
+int dg_boundary(dg_ctx *c, double time, double dt) {
+    TimerScope ts_(c);
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    c->launches += dg::launch_set_scalars(c->B, dt, time, 1, 1, c->stream);
+    c->launches += dg::launch_boundary(c->G, c->B, c->cur, c->stream);
+    return check_launch();
+}
+
+int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
+    TimerScope ts_(c);
+    if (!c || !time) return fail(DG_ERR_ARG, "null argument");
+    if (nsteps < 0) return fail(DG_ERR_ARG, "nsteps < 0");
+    c->launches += dg::launch_set_scalars(c->B, 0.0, *time, 0, 1, c->stream);
+    for (int n = 0; n < nsteps; n++) {
+        c->launches += dg::launch_dt(c->G, c->B, c->cur, c->stream);
+        c->launches += dg::launch_godunov(c->G, c->B, c->cur, c->stream);
+        c->cur ^= 1;
+        if (c->p.fargo) {
+            c->launches += dg::launch_fargo(c->G, c->B, c->cur, c->stream);
+            c->cur ^= 1;
+        }
+        c->launches += dg::launch_boundary(c->G, c->B, c->cur, c->stream);
+        c->launches += dg::launch_advance_time(c->B, c->stream);
+    }
+    int rc = check_launch();
+    if (rc) return rc;
+    if ((rc = read_scalars(c))) return rc;
+    *time = c->h_scal->time;
+    if (dt) *dt = c->h_scal->dt;
+    return DG_OK;
+}
+
+int dg_step(dg_ctx *c, double *time, double *dt) { return dg_run(c, 1, time, dt); }
+
+int dg_history(dg_ctx *c, double out[9]) {
+    TimerScope ts_(c);
+    if (!c || !out) return fail(DG_ERR_ARG, "null argument");
+    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the MRI history is defined for ndim = 3");
+    c->launches += dg::launch_history(c->G, c->B, c->cur, c->stream);
+    int rc = check_launch();
+    if (rc) return rc;
+    DG_CUDA(cudaMemcpyAsync(c->h_hist, c->B.hist, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = bounded_sync(c->stream))) return rc;
+    std::memcpy(out, c->h_hist, 9 * sizeof(double));
+    return DG_OK;
+}
+
+int dg_sync(dg_ctx *c) {
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    return bounded_sync(c->stream);
+}
+
+int dg_debug_copy(dg_ctx *c, int which, double *host, long long count, long long *copied) {
+    if (!c || !host) return fail(DG_ERR_ARG, "null argument");
+    const double *src = nullptr;
+    long long n = 0;
+    if (which >= 0 && which <= 2) { src = c->B.flx[which]; n = c->G.fsz * dg::kFluxComp; }
+    else if (which >= 3 && which <= 5) { src = c->B.emf[which - 3]; n = c->G.fsz; }
+    else if (which == 6) { src = c->B.Q; n = c->G.sv * 8; }
+    if (!src) return fail(DG_ERR_ARG, "no such array for this context");
+    if (count < n) return fail(DG_ERR_ARG, "host buffer too small");
+    DG_CUDA(cudaMemcpyAsync(host, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    int rc = bounded_sync(c->stream);
+    if (rc) return rc;
+    if (copied) *copied = n;
+    return DG_OK;
+}
+
+long long dg_kernel_launches(const dg_ctx *c) { return c ? c->launches : 0; }
+
+int dg_profile(dg_ctx *c, int on) {
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    if (on && !c->timer) c->timer = new EventTimer();
+    if (!on && c->timer) {
+        cudaStreamSynchronize(c->stream);
+        delete c->timer;
+        c->timer = nullptr;
+    }
+    return DG_OK;
+}
+
+int dg_profile_read(dg_ctx *c, double *ms, long long *count, int nslots) {
+    if (!c || !ms || !count) return fail(DG_ERR_ARG, "null argument");
+    for (int k = 0; k < nslots; k++) { ms[k] = 0.0; count[k] = 0; }
+    if (!c->timer) return DG_OK;
+    int rc = bounded_sync(c->stream);
+    if (rc) return rc;
+    for (auto &r : c->timer->recs) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        if (r.slot < nslots) { ms[r.slot] += t; count[r.slot] += 1; }
+        c->timer->pool.push_back(r.a);
+        c->timer->pool.push_back(r.b);
+    }
+    c->timer->recs.clear();
+    return DG_OK;
+}
+
+const char *dg_profile_slot_name(int slot) {
+    return (slot >= 0 && slot < dg::KS_COUNT) ? kSlotNames[slot] : "";
+}
+
+void *dg_stream(dg_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+}  // extern "C"

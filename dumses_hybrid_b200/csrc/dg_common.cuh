@@ -1,0 +1,80 @@
+// Shared definitions of the sm_100a MHD step kernels.
+//
+// Arithmetic rule for the FP64 path: every expression keeps the operation
+// order of the reference Fortran (and of the CPU oracle that restates it),
+// the translation units are compiled with --fmad=false so no multiply-add is
+// contracted, division and sqrt are IEEE round-to-nearest, and Fortran
+// MIN/MAX/SIGN map to the ternaries below.  Under those rules the GPU results
+// are bit-identical to a gfortran x86-64 build of the reference.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dumses_gpu.h"
+
+namespace dg {
+
+// variable slots of the device state (the reference's uin(:,:,:,1:8))
+enum { IR = 0, IU = 1, IV = 2, IW = 3, IP = 4, IA = 5, IB = 6, IC = 7, NVAR = 8 };
+
+constexpr double kSmallr = 1.0e-10;  // commons.f90:48
+constexpr double kSmallc = 1.0e-10;  // commons.f90:49
+
+template <typename T> __host__ __device__ __forceinline__ T mn(T a, T b) { return a < b ? a : b; }
+template <typename T> __host__ __device__ __forceinline__ T mx(T a, T b) { return a > b ? a : b; }
+__device__ __forceinline__ double sgn1(double x) { return copysign(1.0, x); }
+__device__ __forceinline__ float sgn1(float x) { return copysignf(1.0f, x); }
+__device__ __forceinline__ double fab(double x) { return fabs(x); }
+__device__ __forceinline__ float fab(float x) { return fabsf(x); }
+__device__ __forceinline__ double sqr(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqr(float x) { return sqrtf(x); }
+
+// Geometry of one context, passed to every kernel by value.
+struct Geo {
+    int ndim, nx, ny, nz;
+    int NX, NY, NZ;           // ghosted extents (nx+6, ny+6 or 1, nz+6 or 1)
+    int gy, gz;               // ghost layers in y and z (3 or 0)
+    long long sy, sz, sv;     // strides of j, k and variable in the state arrays
+    // trace-core index space: cells [0, nx+1] x [0, ny+1] x [kc0, kc1]
+    int CX, CY, CZ, kc0;
+    long long csz;            // cells in the core index space
+    // face index space: [1, nx+1] x [1, ny+1] x [1, nz+1] (z extent 1 for ndim = 2)
+    int FX, FY, FZ;
+    long long fsz;
+    double dx, dy, dz;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double gamma, ciso, omega0, courant;
+    int iso, slope_type, iriemann, iriemann2d, fargo, shearing;
+    int bc[3];
+    int ndim_act;
+
+    __host__ __device__ __forceinline__ long long idx(int i, int j, int k) const {
+        return (long long)(i + 2) + sy * (long long)(j + gy - 1) + sz * (long long)(k + gz - 1);
+    }
+    __host__ __device__ __forceinline__ long long cidx(int i, int j, int k) const {
+        return (long long)i + (long long)CX * ((long long)j + (long long)CY * (long long)(k - kc0));
+    }
+    __host__ __device__ __forceinline__ long long fidx(int i, int j, int k) const {
+        return (long long)(i - 1) + (long long)FX * ((long long)(j - 1) + (long long)FY * (long long)(k - 1));
+    }
+    // cell centre x(i) = xmin + dx/2 + (i-1) dx (init.f90:461-468)
+    __host__ __device__ __forceinline__ double xc(int i) const { return xmin + dx / 2 + (i - 1) * dx; }
+};
+
+// Scalars that stay on the device across steps (dt, time, CFL reduction).
+struct Scalars {
+    double dt;
+    double time;
+    unsigned long long red;   // bits of the running CFL minimum (positive doubles order as integers)
+    int err;                  // DG_ERR_* raised by a kernel (0 = none)
+    int pad;
+};
+
+// number of trace-core fields per cell
+constexpr int kCore3 = 47;
+constexpr int kCore2 = 30;
+
+// face flux components stored per face: rho, E, normal momentum, t1, t2, p*_tot, Bz (2D only)
+constexpr int kFluxComp = 7;
+
+}  // namespace dg

@@ -1,0 +1,379 @@
+// Riemann solvers of the MHD step as device functions, templated on the
+// arithmetic type T (double for the plain path, float for the mixed path).
+//
+// 1D interface solvers (face fluxes), src/modules/solvers/solver.f90:
+//   llf :393-498, hll :504-612, hlld :618-836, upwind :842-935.
+//   State order: 0 rho, 1 P, 2 u_n, 3 B_n, 4 v_t1, 5 B_t1, 6 v_t2, 7 B_t2.
+//   HLLD returns the normal-momentum flux without total pressure and the star
+//   total pressure p*_T separately (solver.f90:818-833); the other solvers put
+//   the pressure in the flux and report p*_T = 0 (pgstar is zeroed, :94-99).
+// 2D edge solvers (EMFs), src/modules/solvers/solver_magnetic.f90:
+//   llf :241-356, hlld :362-548, upwind :554-600, hlla :688-727.
+//   Corner order LL, LR, RL, RR as set by solver_magnetic_utils (:32-49).
+#pragma once
+#include "dg_common.cuh"
+
+namespace dg {
+
+template <typename T>
+__device__ __forceinline__ T cfast(T gamma, T ploc, T rho, T a, T b, T c) {
+    const T half = T(0.5);
+    T c2 = gamma * ploc / rho;
+    T b2 = a * a + b * b + c * c;
+    T d2 = half * (c2 + b2 / rho);
+    return sqr(d2 + sqr(d2 * d2 - c2 * a * a / rho));
+}
+
+// left/right physical fluxes and conserved states shared by llf, hll, upwind
+template <typename T>
+__device__ __forceinline__ void lr_fluxes(const T *ql, const T *qr, T gamma, T ciso, int iso,
+                                          T *fl, T *cl, T *fr, T *cr, T &ploc, T &proc, T &a) {
+    const T one = T(1), half = T(0.5);
+    const T rl = ql[0], ul = ql[2], vl = ql[4], bl = ql[5], wl = ql[6], clv = ql[7];
+    const T rr = qr[0], ur = qr[2], vr = qr[4], br = qr[5], wr = qr[6], crv = qr[7];
+    const T entho = one / (gamma - one);
+    a = half * (ql[3] + qr[3]);
+    const T al = a, ar = a;
+    if (iso) { ploc = rl * (ciso * ciso); proc = rr * (ciso * ciso); }
+    else { ploc = ql[1]; proc = qr[1]; }
+    T ecin = half * (ul * ul + vl * vl + wl * wl) * rl;
+    T emag = half * (a * a + bl * bl + clv * clv);
+    T etot = ploc * entho + ecin + emag;
+    T ptot = ploc + emag;
+    fl[0] = rl * ul;
+    fl[1] = (etot + ptot) * ul - al * (ul * al + vl * bl + wl * clv);
+    fl[2] = rl * ul * ul + ptot - al * al;
+    fl[3] = T(0);
+    fl[4] = rl * ul * vl - al * bl;
+    fl[5] = bl * ul - al * vl;
+    fl[6] = rl * ul * wl - al * clv;
+    fl[7] = clv * ul - al * wl;
+    cl[0] = rl; cl[1] = etot; cl[2] = rl * ul; cl[3] = al; cl[4] = rl * vl; cl[5] = bl; cl[6] = rl * wl; cl[7] = clv;
+    ecin = half * (ur * ur + vr * vr + wr * wr) * rr;
+    emag = half * (a * a + br * br + crv * crv);
+    etot = proc * entho + ecin + emag;
+    ptot = proc + emag;
+    fr[0] = rr * ur;
+    fr[1] = (etot + ptot) * ur - ar * (ur * ar + vr * br + wr * crv);
+    fr[2] = rr * ur * ur + ptot - ar * ar;
+    fr[3] = T(0);
+    fr[4] = rr * ur * vr - ar * br;
+    fr[5] = br * ur - ar * vr;
+    fr[6] = rr * ur * wr - ar * crv;
+    fr[7] = crv * ur - ar * wr;
+    cr[0] = rr; cr[1] = etot; cr[2] = rr * ur; cr[3] = ar; cr[4] = rr * vr; cr[5] = br; cr[6] = rr * wr; cr[7] = crv;
+}
+
+template <typename T>
+__device__ void llf1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int iso) {
+    const T half = T(0.5);
+    T fl[8], cl[8], fr[8], cr[8], ploc, proc, a;
+    lr_fluxes(ql, qr, gamma, ciso, iso, fl, cl, fr, cr, ploc, proc, a);
+    T vleft = cfast(gamma, ploc, ql[0], a, ql[5], ql[7]) + fab(ql[2]);
+    T vright = cfast(gamma, proc, qr[0], a, qr[5], qr[7]) + fab(qr[2]);
+    T vel_info = mx(vleft, vright);
+#pragma unroll
+    for (int n = 0; n < 8; n++) f[n] = half * (fl[n] + fr[n]) - vel_info * half * (cr[n] - cl[n]);
+}
+
+template <typename T>
+__device__ void hll1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int iso) {
+    T fl[8], cl[8], fr[8], cr[8], ploc, proc, a;
+    lr_fluxes(ql, qr, gamma, ciso, iso, fl, cl, fr, cr, ploc, proc, a);
+    T vleft = cfast(gamma, ploc, ql[0], a, ql[5], ql[7]);
+    T vright = cfast(gamma, proc, qr[0], a, qr[5], qr[7]);
+    T ul = ql[2], ur = qr[2];
+    T sl = mn(mn(ul, ur) - mx(vleft, vright), T(0));
+    T sr = mx(mx(ul, ur) + mx(vleft, vright), T(0));
+#pragma unroll
+    for (int n = 0; n < 8; n++) f[n] = (sr * fl[n] - sl * fr[n] + sr * sl * (cr[n] - cl[n])) / (sr - sl);
+}
+
+template <typename T>
+__device__ void upwind1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int iso) {
+    const T half = T(0.5);
+    T fl[8], cl[8], fr[8], cr[8], ploc, proc, a;
+    lr_fluxes(ql, qr, gamma, ciso, iso, fl, cl, fr, cr, ploc, proc, a);
+    T vleft = half * (ql[2] + qr[2]);
+#pragma unroll
+    for (int n = 0; n < 8; n++) f[n] = half * (fl[n] + fr[n]) - fab(vleft) * half * (cr[n] - cl[n]);
+}
+
+// HLLD; returns p*_T in pg
+template <typename T>
+__device__ void hlld1d(const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso, int iso) {
+    const T one = T(1), half = T(0.5), zero = T(0);
+    const T rl = ql[0], ul = ql[2], vl = ql[4], bl = ql[5], wl = ql[6], cl = ql[7];
+    const T rr = qr[0], ur = qr[2], vr = qr[4], br = qr[5], wr = qr[6], cr = qr[7];
+    const T entho = one / (gamma - one);
+    const T a = half * (ql[3] + qr[3]);
+    const T sgnm = sgn1(a);
+    T ploc, proc;
+    if (iso) { ploc = rl * (ciso * ciso); proc = rr * (ciso * ciso); }
+    else { ploc = ql[1]; proc = qr[1]; }
+    const T ecinl = half * (ul * ul + vl * vl + wl * wl) * rl;
+    const T emagl = half * (a * a + bl * bl + cl * cl);
+    const T etotl = ploc * entho + ecinl + emagl;
+    const T ptotl = ploc + emagl;
+    const T vdotbl = ul * a + vl * bl + wl * cl;
+    const T ecinr = half * (ur * ur + vr * vr + wr * wr) * rr;
+    const T emagr = half * (a * a + br * br + cr * cr);
+    const T etotr = proc * entho + ecinr + emagr;
+    const T ptotr = proc + emagr;
+    const T vdotbr = ur * a + vr * br + wr * cr;
+    const T cfastl = cfast(gamma, ploc, rl, a, bl, cl);
+    const T cfastr = cfast(gamma, proc, rr, a, br, cr);
+    const T sl = mn(ul, ur) - mx(cfastl, cfastr);
+    const T sr = mx(ul, ur) + mx(cfastl, cfastr);
+    const T rcl = rl * (ul - sl);
+    const T rcr = rr * (sr - ur);
+    const T ustar = (rcr * ur + rcl * ul + (ptotl - ptotr)) / (rcr + rcl);
+    const T ptotstar = (rcr * ptotl + rcl * ptotr + rcl * rcr * (ul - ur)) / (rcr + rcl);
+    // left star region
+    const T rstarl = rl * (sl - ul) / (sl - ustar);
+    T estar = rl * (sl - ul) * (sl - ustar) - a * a;
+    const T el = rl * (sl - ul) * (sl - ul) - a * a;
+    T vstarl, bstarl, wstarl, cstarl;
+    if (estar == zero) { vstarl = vl; bstarl = bl; wstarl = wl; cstarl = cl; }
+    else {
+        vstarl = vl - a * bl * (ustar - ul) / estar;
+        bstarl = bl * el / estar;
+        wstarl = wl - a * cl * (ustar - ul) / estar;
+        cstarl = cl * el / estar;
+    }
+    const T vdotbstarl = ustar * a + vstarl * bstarl + wstarl * cstarl;
+    const T etotstarl = ((sl - ul) * etotl - ptotl * ul + ptotstar * ustar + a * (vdotbl - vdotbstarl)) / (sl - ustar);
+    const T sqrrstarl = sqr(rstarl);
+    const T calfvenl = fab(a) / sqrrstarl;
+    const T sal = ustar - calfvenl;
+    // right star region
+    const T rstarr = rr * (sr - ur) / (sr - ustar);
+    estar = rr * (sr - ur) * (sr - ustar) - a * a;
+    const T er = rr * (sr - ur) * (sr - ur) - a * a;
+    T vstarr, bstarr, wstarr, cstarr;
+    if (estar == zero) { vstarr = vr; bstarr = br; wstarr = wr; cstarr = cr; }
+    else {
+        vstarr = vr - a * br * (ustar - ur) / estar;
+        bstarr = br * er / estar;
+        wstarr = wr - a * cr * (ustar - ur) / estar;
+        cstarr = cr * er / estar;
+    }
+    const T vdotbstarr = ustar * a + vstarr * bstarr + wstarr * cstarr;
+    const T etotstarr = ((sr - ur) * etotr - ptotr * ur + ptotstar * ustar + a * (vdotbr - vdotbstarr)) / (sr - ustar);
+    const T sqrrstarr = sqr(rstarr);
+    const T calfvenr = fab(a) / sqrrstarr;
+    const T sar = ustar + calfvenr;
+    // double star region
+    const T vstarstar = (sqrrstarl * vstarl + sqrrstarr * vstarr + sgnm * (bstarr - bstarl)) / (sqrrstarl + sqrrstarr);
+    const T wstarstar = (sqrrstarl * wstarl + sqrrstarr * wstarr + sgnm * (cstarr - cstarl)) / (sqrrstarl + sqrrstarr);
+    const T bstarstar = (sqrrstarl * bstarr + sqrrstarr * bstarl + sgnm * sqrrstarl * sqrrstarr * (vstarr - vstarl))
+                      / (sqrrstarl + sqrrstarr);
+    const T cstarstar = (sqrrstarl * cstarr + sqrrstarr * cstarl + sgnm * sqrrstarl * sqrrstarr * (wstarr - wstarl))
+                      / (sqrrstarl + sqrrstarr);
+    const T vdotbstarstar = ustar * a + vstarstar * bstarstar + wstarstar * cstarstar;
+    const T etotstarstarl = etotstarl - sgnm * sqrrstarl * (vdotbstarl - vdotbstarstar);
+    const T etotstarstarr = etotstarr + sgnm * sqrrstarr * (vdotbstarr - vdotbstarstar);
+    // sample at x/t = 0
+    T ro, uo, vo, wo, bo, co, ptoto, etoto, vdotbo;
+    if (sl > zero) {
+        ro = rl; uo = ul; vo = vl; wo = wl; bo = bl; co = cl; ptoto = ptotl; etoto = etotl; vdotbo = vdotbl;
+    } else if (sal > zero) {
+        ro = rstarl; uo = ustar; vo = vstarl; wo = wstarl; bo = bstarl; co = cstarl;
+        ptoto = ptotstar; etoto = etotstarl; vdotbo = vdotbstarl;
+    } else if (ustar > zero) {
+        ro = rstarl; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
+        ptoto = ptotstar; etoto = etotstarstarl; vdotbo = vdotbstarstar;
+    } else if (sar > zero) {
+        ro = rstarr; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
+        ptoto = ptotstar; etoto = etotstarstarr; vdotbo = vdotbstarstar;
+    } else if (sr > zero) {
+        ro = rstarr; uo = ustar; vo = vstarr; wo = wstarr; bo = bstarr; co = cstarr;
+        ptoto = ptotstar; etoto = etotstarr; vdotbo = vdotbstarr;
+    } else {
+        ro = rr; uo = ur; vo = vr; wo = wr; bo = br; co = cr; ptoto = ptotr; etoto = etotr; vdotbo = vdotbr;
+    }
+    f[0] = ro * uo;
+    f[1] = (etoto + ptoto) * uo - a * vdotbo;
+    f[2] = ro * uo * uo - a * a;
+    f[3] = zero;
+    f[4] = ro * uo * vo - a * bo;
+    f[5] = bo * uo - a * vo;
+    f[6] = ro * uo * wo - a * co;
+    f[7] = co * uo - a * wo;
+    pg = ptoto;
+}
+
+// the four corner states of an edge after solver_magnetic_utils
+template <typename T>
+struct Corners {
+    T rLL, rLR, rRL, rRR, pLL, pLR, pRL, pRR, uLL, uLR, uRL, uRR;
+    T vLL, vLR, vRL, vRR, ALL, ALR, ARL, ARR, BLL, BLR, BRL, BRR;
+    T CLL, CLR, CRL, CRR, ELL, ELR, ERL, ERR;
+};
+
+template <typename T> __device__ __forceinline__ T mn4(T a, T b, T c, T d) { return mn(mn(mn(a, b), c), d); }
+template <typename T> __device__ __forceinline__ T mx4(T a, T b, T c, T d) { return mx(mx(mx(a, b), c), d); }
+
+template <typename T>
+__device__ T llf2d(const Corners<T> &c, T dt, T gamma, T ciso, int iso) {
+    const T half = T(0.5), forth = T(0.25);
+    T E = forth * (c.ELL + c.ERL + c.ELR + c.ERR);
+    T rl = half * (c.rLL + c.rLR), pl = half * (c.pLL + c.pLR), ul = half * (c.uLL + c.uLR);
+    T al = half * (c.ALL + c.ALR), bl = half * (c.BLL + c.BLR), cl = half * (c.CLL + c.CLR);
+    T rr = half * (c.rRR + c.rRL), pr = half * (c.pRR + c.pRL), ur = half * (c.uRR + c.uRL);
+    T ar = half * (c.ARR + c.ARL), br = half * (c.BRR + c.BRL), cr = half * (c.CRR + c.CRL);
+    T ploc, proc;
+    if (iso) { ploc = rl * (ciso * ciso); proc = rr * (ciso * ciso); } else { ploc = pl; proc = pr; }
+    al = half * (al + ar); ar = al;
+    T vleft = cfast(gamma, ploc, rl, al, bl, cl) + fab(ul);
+    T vright = cfast(gamma, proc, rr, ar, br, cr) + fab(ur);
+    T vel_info = mx(vleft, vright);
+    T flux_x = -vel_info * half * (br - bl);
+    rl = half * (c.rLL + c.rRL); pl = half * (c.pLL + c.pRL); ul = half * (c.vLL + c.vRL);
+    al = half * (c.BLL + c.BRL); bl = half * (c.ALL + c.ARL); cl = half * (c.CLL + c.CRL);
+    rr = half * (c.rRR + c.rLR); pr = half * (c.pRR + c.pLR); ur = half * (c.vRR + c.vLR);
+    ar = half * (c.BRR + c.BLR); br = half * (c.ARR + c.ALR); cr = half * (c.CRR + c.CLR);
+    if (iso) { ploc = rl * (ciso * ciso); proc = rr * (ciso * ciso); } else { ploc = pl; proc = pr; }
+    al = half * (al + ar); ar = al;
+    vleft = cfast(gamma, ploc, rl, al, bl, cl) + fab(ul);
+    vright = cfast(gamma, proc, rr, ar, br, cr) + fab(ur);
+    vel_info = mx(vleft, vright);
+    T flux_y = -vel_info * half * (br - bl);
+    T emf = E + (flux_x - flux_y);
+    return emf * dt;
+}
+
+template <typename T>
+__device__ T hlld2d(const Corners<T> &c, T dt, T gamma) {
+    const T one = T(1), half = T(0.5), zero = T(0), smallc = T(kSmallc);
+    const T cfastLLx = cfast(gamma, c.pLL, c.rLL, c.ALL, c.BLL, c.CLL);
+    const T cfastLRx = cfast(gamma, c.pLR, c.rLR, c.ALR, c.BLR, c.CLR);
+    const T cfastRLx = cfast(gamma, c.pRL, c.rRL, c.ARL, c.BRL, c.CRL);
+    const T cfastRRx = cfast(gamma, c.pRR, c.rRR, c.ARR, c.BRR, c.CRR);
+    const T cfastLLy = cfast(gamma, c.pLL, c.rLL, c.BLL, c.ALL, c.CLL);
+    const T cfastLRy = cfast(gamma, c.pLR, c.rLR, c.BLR, c.ALR, c.CLR);
+    const T cfastRLy = cfast(gamma, c.pRL, c.rRL, c.BRL, c.ARL, c.CRL);
+    const T cfastRRy = cfast(gamma, c.pRR, c.rRR, c.BRR, c.ARR, c.CRR);
+    const T SL = mn4(c.uLL, c.uLR, c.uRL, c.uRR) - mx4(cfastLLx, cfastLRx, cfastRLx, cfastRRx);
+    const T SR = mx4(c.uLL, c.uLR, c.uRL, c.uRR) + mx4(cfastLLx, cfastLRx, cfastRLx, cfastRRx);
+    const T SB = mn4(c.vLL, c.vLR, c.vRL, c.vRR) - mx4(cfastLLy, cfastLRy, cfastRLy, cfastRRy);
+    const T ST = mx4(c.vLL, c.vLR, c.vRL, c.vRR) + mx4(cfastLLy, cfastLRy, cfastRLy, cfastRRy);
+    const T PtotLL = c.pLL + half * (c.ALL * c.ALL + c.BLL * c.BLL + c.CLL * c.CLL);
+    const T PtotLR = c.pLR + half * (c.ALR * c.ALR + c.BLR * c.BLR + c.CLR * c.CLR);
+    const T PtotRL = c.pRL + half * (c.ARL * c.ARL + c.BRL * c.BRL + c.CRL * c.CRL);
+    const T PtotRR = c.pRR + half * (c.ARR * c.ARR + c.BRR * c.BRR + c.CRR * c.CRR);
+    const T rcLLx = c.rLL * (c.uLL - SL), rcRLx = c.rRL * (SR - c.uRL);
+    const T rcLRx = c.rLR * (c.uLR - SL), rcRRx = c.rRR * (SR - c.uRR);
+    const T rcLLy = c.rLL * (c.vLL - SB), rcLRy = c.rLR * (ST - c.vLR);
+    const T rcRLy = c.rRL * (c.vRL - SB), rcRRy = c.rRR * (ST - c.vRR);
+    const T ustar = (rcLLx * c.uLL + rcLRx * c.uLR + rcRLx * c.uRL + rcRRx * c.uRR + (PtotLL - PtotRL + PtotLR - PtotRR))
+                  / (rcLLx + rcLRx + rcRLx + rcRRx);
+    const T vstar = (rcLLy * c.vLL + rcLRy * c.vLR + rcRLy * c.vRL + rcRRy * c.vRR + (PtotLL - PtotLR + PtotRL - PtotRR))
+                  / (rcLLy + rcLRy + rcRLy + rcRRy);
+    const T SLustar = one / (SL - ustar), SRustar = one / (SR - ustar);
+    const T SBvstar = one / (SB - vstar), STvstar = one / (ST - vstar);
+    const T rstarLLx = c.rLL * (SL - c.uLL) * SLustar;
+    const T BstarLL = c.BLL * (SL - c.uLL) * SLustar;
+    const T rstarLLy = c.rLL * (SB - c.vLL) * SBvstar;
+    const T AstarLL = c.ALL * (SB - c.vLL) * SBvstar;
+    const T rstarLL = c.rLL * (SL - c.uLL) * SLustar * (SB - c.vLL) * SBvstar;
+    const T EstarLLx = ustar * BstarLL - c.vLL * c.ALL;
+    const T EstarLLy = c.uLL * c.BLL - vstar * AstarLL;
+    const T EstarLL = ustar * BstarLL - vstar * AstarLL;
+    const T rstarLRx = c.rLR * (SL - c.uLR) * SLustar;
+    const T BstarLR = c.BLR * (SL - c.uLR) * SLustar;
+    const T rstarLRy = c.rLR * (ST - c.vLR) * STvstar;
+    const T AstarLR = c.ALR * (ST - c.vLR) * STvstar;
+    const T rstarLR = c.rLR * (SL - c.uLR) * SLustar * (ST - c.vLR) * STvstar;
+    const T EstarLRx = ustar * BstarLR - c.vLR * c.ALR;
+    const T EstarLRy = c.uLR * c.BLR - vstar * AstarLR;
+    const T EstarLR = ustar * BstarLR - vstar * AstarLR;
+    const T rstarRLx = c.rRL * (SR - c.uRL) * SRustar;
+    const T BstarRL = c.BRL * (SR - c.uRL) * SRustar;
+    const T rstarRLy = c.rRL * (SB - c.vRL) * SBvstar;
+    const T AstarRL = c.ARL * (SB - c.vRL) * SBvstar;
+    const T rstarRL = c.rRL * (SR - c.uRL) * SRustar * (SB - c.vRL) * SBvstar;
+    const T EstarRLx = ustar * BstarRL - c.vRL * c.ARL;
+    const T EstarRLy = c.uRL * c.BRL - vstar * AstarRL;
+    const T EstarRL = ustar * BstarRL - vstar * AstarRL;
+    const T rstarRRx = c.rRR * (SR - c.uRR) * SRustar;
+    const T BstarRR = c.BRR * (SR - c.uRR) * SRustar;
+    const T rstarRRy = c.rRR * (ST - c.vRR) * STvstar;
+    const T AstarRR = c.ARR * (ST - c.vRR) * STvstar;
+    const T rstarRR = c.rRR * (SR - c.uRR) * SRustar * (ST - c.vRR) * STvstar;
+    const T EstarRRx = ustar * BstarRR - c.vRR * c.ARR;
+    const T EstarRRy = c.uRR * c.BRR - vstar * AstarRR;
+    const T EstarRR = ustar * BstarRR - vstar * AstarRR;
+    const T sqrtrstarLR = one / sqr(rstarLR);
+    const T sqrtrstarRL = one / sqr(rstarRL);
+    const T sqrtrstarRR = one / sqr(rstarRR);
+    const T sqrtrstarLL = one / sqr(rstarLL);
+    const T calfvenL = mx(mx(mx(mx(fab(c.ALR) / sqr(rstarLRx), fab(AstarLR) * sqrtrstarLR),
+                                fab(c.ALL) / sqr(rstarLLx)), fab(AstarLL) * sqrtrstarLL), smallc);
+    const T calfvenR = mx(mx(mx(mx(fab(c.ARR) / sqr(rstarRRx), fab(AstarRR) * sqrtrstarRR),
+                                fab(c.ARL) / sqr(rstarRLx)), fab(AstarRL) * sqrtrstarRL), smallc);
+    const T calfvenB = mx(mx(mx(mx(fab(c.BLL) / sqr(rstarLLy), fab(BstarLL) * sqrtrstarLL),
+                                fab(c.BRL) / sqr(rstarRLy)), fab(BstarRL) * sqrtrstarRL), smallc);
+    const T calfvenT = mx(mx(mx(mx(fab(c.BLR) / sqr(rstarLRy), fab(BstarLR) * sqrtrstarLR),
+                                fab(c.BRR) / sqr(rstarRRy)), fab(BstarRR) * sqrtrstarRR), smallc);
+    const T SAL = mn(ustar - calfvenL, zero), SAR = mx(ustar + calfvenR, zero);
+    const T SAB = mn(vstar - calfvenB, zero), SAT = mx(vstar + calfvenT, zero);
+    const T SARSAL = one / (SAR - SAL);
+    const T SATSAB = one / (SAT - SAB);
+    const T AstarT = (SAR * AstarRR - SAL * AstarLR) * SARSAL;
+    const T AstarB = (SAR * AstarRL - SAL * AstarLL) * SARSAL;
+    const T BstarR = (SAT * BstarRR - SAB * BstarRL) * SATSAB;
+    const T BstarL = (SAT * BstarLR - SAB * BstarLL) * SATSAB;
+    T E;
+    if (SB > zero) {
+        if (SL > zero) E = c.ELL;
+        else if (SR < zero) E = c.ERL;
+        else E = (SAR * EstarLLx - SAL * EstarRLx + SAR * SAL * (c.BRL - c.BLL)) * SARSAL;
+    } else if (ST < zero) {
+        if (SL > zero) E = c.ELR;
+        else if (SR < zero) E = c.ERR;
+        else E = (SAR * EstarLRx - SAL * EstarRRx + SAR * SAL * (c.BRR - c.BLR)) * SARSAL;
+    } else if (SL > zero) {
+        E = (SAT * EstarLLy - SAB * EstarLRy - SAT * SAB * (c.ALR - c.ALL)) * SATSAB;
+    } else if (SR < zero) {
+        E = (SAT * EstarRLy - SAB * EstarRRy - SAT * SAB * (c.ARR - c.ARL)) * SATSAB;
+    } else {
+        E = (SAL * SAB * EstarRR - SAL * SAT * EstarRL - SAR * SAB * EstarLR + SAR * SAT * EstarLL) * SARSAL * SATSAB
+          - SAT * SAB * SATSAB * (AstarT - AstarB) + SAR * SAL * SARSAL * (BstarR - BstarL);
+    }
+    return E * dt;
+}
+
+template <typename T>
+__device__ T upwind2d(const Corners<T> &c, T dt) {
+    const T half = T(0.5), forth = T(0.25);
+    T E = forth * (c.ELL + c.ERL + c.ELR + c.ERR);
+    T ul = half * (c.uLL + c.uLR), bl = half * (c.BLL + c.BLR);
+    T ur = half * (c.uRR + c.uRL), br = half * (c.BRR + c.BRL);
+    T vel_info = half * (ul + ur);
+    T flux_x = -fab(vel_info) * half * (br - bl);
+    ul = half * (c.vLL + c.vRL); bl = half * (c.ALL + c.ARL);
+    ur = half * (c.vRR + c.vLR); br = half * (c.ARR + c.ALR);
+    vel_info = half * (ul + ur);
+    T flux_y = -fab(vel_info) * half * (br - bl);
+    T emf = E + (flux_x - flux_y);
+    return emf * dt;
+}
+
+template <typename T>
+__device__ T hlla2d(const Corners<T> &c, T dt) {
+    const T zero = T(0), smallc = T(kSmallc);
+    const T cLLx = sqr(c.ALL * c.ALL / c.rLL), cLRx = sqr(c.ALR * c.ALR / c.rLR);
+    const T cRLx = sqr(c.ARL * c.ARL / c.rRL), cRRx = sqr(c.ARR * c.ARR / c.rRR);
+    const T cLLy = sqr(c.BLL * c.BLL / c.rLL), cLRy = sqr(c.BLR * c.BLR / c.rLR);
+    const T cRLy = sqr(c.BRL * c.BRL / c.rRL), cRRy = sqr(c.BRR * c.BRR / c.rRR);
+    const T SL = mn(mn4(c.uLL, c.uLR, c.uRL, c.uRR) - mx(mx4(cLLx, cLRx, cRLx, cRRx), smallc), zero);
+    const T SR = mx(mx4(c.uLL, c.uLR, c.uRL, c.uRR) + mx(mx4(cLLx, cLRx, cRLx, cRRx), smallc), zero);
+    const T SB = mn(mn4(c.vLL, c.vLR, c.vRL, c.vRR) - mx(mx4(cLLy, cLRy, cRLy, cRRy), smallc), zero);
+    const T ST = mx(mx4(c.vLL, c.vLR, c.vRL, c.vRR) + mx(mx4(cLLy, cLRy, cRLy, cRRy), smallc), zero);
+    T emf = (SL * SB * c.ERR - SL * ST * c.ERL - SR * SB * c.ELR + SR * ST * c.ELL) / (SR - SL) / (ST - SB)
+          - ST * SB / (ST - SB) * (c.ARR - c.ALL) + SR * SL / (SR - SL) * (c.BRR - c.BLL);
+    return emf * dt;
+}
+
+}  // namespace dg

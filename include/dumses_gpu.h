@@ -125,11 +125,33 @@ int  dg_history(dg_ctx *ctx, double out[9]);
 /* wait for all work of the context (bounded) */
 int  dg_sync(dg_ctx *ctx);
 
+/* Per-kernel CUDA-event timing on the context's stream (no counterpart in the
+ * reference, whose timers are host system_clock calls inserted by its
+ * preprocessor, utils/pyutils/preproc/preprocess.py:330-355).
+ * dg_profile(ctx, 1) starts recording an event pair around every kernel;
+ * dg_profile_read fills ms[slot] and count[slot] for the launches since the
+ * last read (slots named by dg_profile_slot_name) and resets them. */
+#define DG_PROFILE_SLOTS 11
+int  dg_profile(dg_ctx *ctx, int on);
+int  dg_profile_read(dg_ctx *ctx, double *ms, long long *count, int nslots);
+const char *dg_profile_slot_name(int slot);
+
 /* number of kernels the library launched on this context since dg_init */
 long long dg_kernel_launches(const dg_ctx *ctx);
 
 /* the context's CUDA stream (a cudaStream_t), so a caller can order its own work */
 void *dg_stream(dg_ctx *ctx);
+
+/* Test hook: copy one device work array of the last step to the host.
+ *   which 0..2  face fluxes of direction x/y/z, 7 components (rho, E, rho u,
+ *               rho v, rho w scaled by area*dt as compflux does, then p*_T and
+ *               the 2D B_z flux) over faces [1,nx+1]x[1,ny+1]x[1,nz+1]
+ *   which 3..5  edge EMFs x/y/z (already multiplied by dt) over the same index space
+ *   which 6     primitive variables (8) on the ghosted grid
+ * count is the number of doubles the host buffer holds; returns the number of
+ * doubles copied in *copied.  No counterpart in the reference (its arrays are
+ * module globals). */
+int  dg_debug_copy(dg_ctx *ctx, int which, double *host, long long count, long long *copied);
 
 /* message of the last failing call on this thread ("" if none) */
 const char *dg_last_error(void);

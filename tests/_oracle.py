@@ -1,0 +1,104 @@
+"""ctypes loader of the CPU oracle (oracle/liboracle.so) -- test infrastructure.
+
+The oracle restates the reference's Fortran routines in C; tests use it only as
+the checker of the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import subprocess
+
+import numpy as np
+
+from dumses_hybrid_b200 import DgParams, Params
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+ORACLE_DIR = ROOT / "oracle"
+LIB = ORACLE_DIR / "liboracle.so"
+
+_lib = None
+
+
+def build_oracle() -> pathlib.Path:
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "liboracle.so"], check=True)
+    return LIB
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build_oracle()
+        L = ctypes.CDLL(str(LIB))
+        vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+        L.or_create.restype, L.or_create.argtypes = vp, [ctypes.POINTER(DgParams)]
+        L.or_destroy.restype, L.or_destroy.argtypes = None, [vp]
+        L.or_uin.restype, L.or_uin.argtypes = dp, [vp]
+        L.or_uin_size.restype, L.or_uin_size.argtypes = ctypes.c_longlong, [vp]
+        L.or_compute_dt.restype, L.or_compute_dt.argtypes = ctypes.c_double, [vp]
+        L.or_godunov.restype, L.or_godunov.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
+        L.or_fargo_update.restype, L.or_fargo_update.argtypes = None, [vp, ctypes.c_double]
+        L.or_boundary.restype, L.or_boundary.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
+        L.or_history_mri.restype, L.or_history_mri.argtypes = None, [vp, dp]
+        L.or_step.restype, L.or_step.argtypes = ctypes.c_double, [vp, dp]
+        L.or_run_history.restype = ctypes.c_int
+        L.or_run_history.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, ctypes.c_int]
+        L.or_array.restype, L.or_array.argtypes = dp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+        L.or_set_threads.restype, L.or_set_threads.argtypes = None, [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """One oracle state, driven like the reference's module globals."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        self._cp = params.to_c()
+        self.L = lib()
+        self.h = self.L.or_create(ctypes.byref(self._cp))
+        n = self.L.or_uin_size(self.h)
+        self.uin = np.ctypeslib.as_array(self.L.or_uin(self.h), shape=(n,)).reshape(params.shape, order="F")
+
+    def close(self):
+        if self.h:
+            self.L.or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_state(self, u: np.ndarray) -> None:
+        self.uin[...] = u
+
+    def compute_dt(self) -> float:
+        return self.L.or_compute_dt(self.h)
+
+    def godunov(self, dt: float, time: float) -> None:
+        self.L.or_godunov(self.h, dt, time)
+
+    def fargo_update(self, dt: float) -> None:
+        self.L.or_fargo_update(self.h, dt)
+
+    def boundary(self, time: float, dt: float) -> None:
+        self.L.or_boundary(self.h, time, dt)
+
+    def step(self, time: float) -> tuple[float, float]:
+        t = ctypes.c_double(time)
+        dt = self.L.or_step(self.h, ctypes.byref(t))
+        return t.value, dt
+
+    def history(self) -> np.ndarray:
+        out = np.zeros(9)
+        self.L.or_history_mri(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
+    def run_history(self, tlim: float, dthist: float, max_rows: int) -> np.ndarray:
+        rows = np.zeros((max_rows, 11))
+        n = self.L.or_run_history(self.h, tlim, dthist, rows.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), max_rows)
+        return rows[:n]
+
+    def array(self, which: int) -> np.ndarray:
+        n = ctypes.c_longlong()
+        p = self.L.or_array(self.h, which, ctypes.byref(n))
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()

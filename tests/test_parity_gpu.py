@@ -1,0 +1,194 @@
+"""Parity of the CUDA library with the CPU oracle (bit-exact, FP64).
+
+Both sides start from the same initial state; after every step dt must be
+identical and after the run the whole reference-layout state must be identical:
+variables 1-8 in every cell (ghosts included) and the right-face B (9-11)
+everywhere except the last ghost layer of its direction, which the reference
+never refreshes and never reads.
+"""
+import numpy as np
+import pytest
+
+from dumses_hybrid_b200 import Context, Params, condinit
+from _oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def compare_states(ug, uo, params):
+    assert np.isfinite(ug[..., :8]).all()
+    d = ug[..., :8] != uo[..., :8]
+    if d.any():
+        idx = np.argwhere(d)[:5]
+        diff = np.max(np.abs(ug[..., :8] - uo[..., :8]))
+        raise AssertionError(f"{int(d.sum())} values differ (max abs {diff:.3e}); first (i,j,k,v): {idx.tolist()}")
+    nx, ny, nz, _ = ug.shape
+    assert np.array_equal(ug[:-1, :, :, 8], uo[:-1, :, :, 8])
+    if params.ndim > 1:
+        assert np.array_equal(ug[:, :-1, :, 9], uo[:, :-1, :, 9])
+    if params.ndim == 3:
+        assert np.array_equal(ug[:, :, :-1, 10], uo[:, :, :-1, 10])
+    else:
+        assert np.array_equal(ug[..., 10], uo[..., 10])
+
+
+def run_pair(params, ic, nsteps, use_run=False, **ickw):
+    u0 = condinit(params, ic, **ickw)
+    o = Oracle(params)
+    o.set_state(u0)
+    o.boundary(0.0, 0.0)
+    t_o = 0.0
+    dts_o = []
+    for _ in range(nsteps):
+        t_o, dt = o.step(t_o)
+        dts_o.append(dt)
+    with Context(params) as g:
+        g.upload(u0)
+        g.boundary(0.0, 0.0)
+        t_g = 0.0
+        dts_g = []
+        if use_run:
+            t_g, _ = g.run(nsteps, t_g)
+        else:
+            for _ in range(nsteps):
+                dt = g.compute_dt()
+                g.godunov(dt, t_g)
+                if params.fargo:
+                    g.fargo_update(dt)
+                g.boundary(t_g, dt)
+                t_g = t_g + dt
+                dts_g.append(dt)
+        ug = g.download()
+    if not use_run:
+        assert dts_g == dts_o
+    assert t_g == t_o
+    compare_states(ug, o.uin, params)
+    return ug
+
+
+OT16 = Params(ndim=3, nx=16, ny=16, nz=16, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, gamma=5 / 3, courant=0.8)
+MRI_TEST = Params(ndim=3, iso=1, nx=16, ny=32, nz=16, xmin=-0.5, xmax=0.5, ymin=0.0, ymax=4.0, zmin=-0.5, zmax=0.5,
+                  gamma=1.001, ciso=1e-3, omega0=1e-3, courant=0.8, bdtypex="shearingbox")
+MRI_FARGO = Params(ndim=3, iso=1, nx=16, ny=32, nz=16, xmin=-0.25, xmax=0.25, ymin=-0.5, ymax=0.5, zmin=-0.25,
+                   zmax=0.25, ciso=1.0, omega0=1.0, courant=0.8, bdtypex="shearingbox", fargo=True)
+LOOP2D = Params(ndim=2, nx=32, ny=16, nz=1, xmin=-1, xmax=1, ymin=-0.5, ymax=0.5, courant=0.7)
+
+
+def test_orszag_tang_3d_steps():
+    run_pair(OT16, "orszag_tang", 6)
+
+
+def test_orszag_tang_3d_device_loop():
+    run_pair(OT16, "orszag_tang", 6, use_run=True)
+
+
+def test_field_loop_2d():
+    run_pair(LOOP2D, "field_loop", 8)
+
+
+def test_field_loop_2d_device_loop():
+    run_pair(LOOP2D, "field_loop", 8, use_run=True)
+
+
+def test_mri_shearing_box():
+    run_pair(MRI_TEST, "mri_test", 6, beta=1000.0, amp=0.0)
+
+
+def test_mri_shearing_box_kicks():
+    p = Params(**{**MRI_TEST.__dict__, "ciso": 1.0, "omega0": 1.0, "gamma": 5 / 3, "xmin": -0.25, "xmax": 0.25,
+                  "ymin": -0.5, "ymax": 0.5, "zmin": -0.25, "zmax": 0.25})
+    run_pair(p, "mri", 6, beta=1000.0, amp=0.1, seed=3)
+
+
+def test_mri_fargo():
+    run_pair(MRI_FARGO, "mri", 6, beta=1000.0, amp=0.1, seed=5)
+
+
+def test_mri_fargo_device_loop():
+    run_pair(MRI_FARGO, "mri", 6, use_run=True, beta=1000.0, amp=0.1, seed=5)
+
+
+@pytest.mark.parametrize("riemann,riemann2d,slope", [
+    ("hll", "llf", 2), ("llf", "upwind", 1), ("upwind", "hlla", 2), ("hlld", "hlld", 3), ("hlld", "llf", 0),
+])
+def test_solver_and_limiter_variants_3d(riemann, riemann2d, slope):
+    p = Params(**{**OT16.__dict__, "riemann": riemann, "riemann2d": riemann2d, "slope_type": slope})
+    run_pair(p, "orszag_tang", 4)
+
+
+@pytest.mark.parametrize("riemann,riemann2d,slope", [("hll", "upwind", 2), ("llf", "hlla", 3), ("hlld", "llf", 1)])
+def test_solver_and_limiter_variants_2d(riemann, riemann2d, slope):
+    p = Params(**{**LOOP2D.__dict__, "riemann": riemann, "riemann2d": riemann2d, "slope_type": slope})
+    run_pair(p, "field_loop", 4)
+
+
+def test_zero_gradient_boundaries():
+    p = Params(**{**OT16.__dict__, "bdtypex": "zero_gradient", "bdtypez": "zero_gradient"})
+    run_pair(p, "orszag_tang", 4)
+
+
+def test_isothermal_rotating_periodic():
+    # Coriolis + shear source terms without the shearing boundary
+    p = Params(**{**MRI_TEST.__dict__, "bdtypex": "periodic", "ciso": 1.0, "omega0": 1.0, "gamma": 5 / 3,
+                  "xmin": -0.25, "xmax": 0.25, "ymin": -0.5, "ymax": 0.5, "zmin": -0.25, "zmax": 0.25})
+    run_pair(p, "mri", 4, beta=400.0, amp=0.1, seed=11)
+
+
+def test_uneven_grid_orszag_tang():
+    p = Params(**{**OT16.__dict__, "nx": 24, "ny": 12, "nz": 20})
+    run_pair(p, "orszag_tang", 3)
+
+
+def test_stage_fluxes_and_emfs():
+    """Face fluxes and edge EMFs of one Godunov step against the oracle's arrays."""
+    P = OT16
+    u0 = condinit(P, "orszag_tang")
+    o = Oracle(P)
+    o.set_state(u0)
+    o.boundary(0.0, 0.0)
+    dt = o.compute_dt()
+    o.godunov(dt, 0.0)
+    nx, ny, nz = P.nx, P.ny, P.nz
+    F = (nx + 1) * (ny + 1) * (nz + 1)
+    flux = o.array(0).reshape((nx + 1, ny + 1, nz + 1, 8, 3), order="F")
+    emf = [o.array(w).reshape((nx + 6, ny + 6, nz + 6), order="F") for w in (1, 2, 3)]
+    with Context(P) as g:
+        g.upload(u0)
+        g.boundary(0.0, 0.0)
+        assert g.compute_dt() == dt
+        g.godunov(dt, 0.0)
+        for d in range(3):
+            gf = g.debug_array(d, F * 7).reshape((7, nz + 1, ny + 1, nx + 1))
+            hi = [nx + 1 if d == 0 else nx, ny + 1 if d == 1 else ny, nz + 1 if d == 2 else nz]
+            for comp, var in ((0, 0), (1, 4), (2, 1), (3, 2), (4, 3)):
+                a = gf[comp, : hi[2], : hi[1], : hi[0]].transpose(2, 1, 0)
+                b = flux[: hi[0], : hi[1], : hi[2], var, d]
+                assert np.array_equal(a, b), f"flux dir {d} var {var}: max diff {np.max(np.abs(a - b))}"
+        for e in range(3):
+            ge = g.debug_array(3 + e, F).reshape((nz + 1, ny + 1, nx + 1)).transpose(2, 1, 0)
+            hi = [nx if e == 0 else nx + 1, ny if e == 1 else ny + 1, nz if e == 2 else nz + 1]
+            a = ge[: hi[0], : hi[1], : hi[2]]
+            b = emf[e][3: 3 + hi[0], 3: 3 + hi[1], 3: 3 + hi[2]]
+            assert np.array_equal(a, b), f"emf {e}: max diff {np.max(np.abs(a - b))}"
+
+
+def test_history_sums_match_oracle():
+    p = Params(**{**MRI_FARGO.__dict__})
+    u0 = condinit(p, "mri", beta=1000.0, amp=0.1, seed=5)
+    o = Oracle(p)
+    o.set_state(u0)
+    o.boundary(0.0, 0.0)
+    with Context(p) as g:
+        g.upload(u0)
+        g.boundary(0.0, 0.0)
+        t, _ = g.run(3, 0.0)
+        h_g = g.history()
+    t_o = 0.0
+    for _ in range(3):
+        t_o, _ = o.step(t_o)
+    h_o = o.history()
+    scale = np.maximum(np.abs(h_o), 1e-300)
+    # FP64 sums in a different (tree) order: relative 1e-12, div B at round-off
+    for q in (0, 1, 2, 3, 4, 5, 6, 7):
+        assert abs(h_g[q] - h_o[q]) <= 1e-12 * scale[q] + 1e-18, (q, h_g[q], h_o[q])
+    assert abs(h_g[8]) < 1e-9 and abs(h_o[8]) < 1e-9
