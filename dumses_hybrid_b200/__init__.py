@@ -92,6 +92,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_kernel_launches": (ctypes.c_longlong, [vp]),
         "dg_stream": (vp, [vp]),
         "dg_last_error": (ctypes.c_char_p, []),
+        "dg_history_noalloc": (ctypes.c_int, [c_p, vp, vp, vp]),
         "dg_profile": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_profile_read": (ctypes.c_int, [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
         "dg_profile_slot_name": (ctypes.c_char_p, [ctypes.c_int]),

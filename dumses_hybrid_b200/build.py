@@ -27,7 +27,7 @@ LIB = PKG / "libdumses_gpu.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-I", str(INCLUDE), "-I", str(CSRC)]
-CU_SOURCES = ["mhd_kernels.cu", "dg_api.cu"]
+CU_SOURCES = ["mhd_kernels.cu", "dg_api.cu", "dg_noalloc.cu"]
 CXX_SOURCES = ["condinit.cpp"]
 
 

@@ -145,7 +145,9 @@ int validate(const dg_params *p) {
     return DG_OK;
 }
 
-dg::Geo make_geo(const dg_params &p) {
+}  // namespace
+
+dg::Geo dg::make_geo(const dg_params &p) {
     dg::Geo G{};
     G.ndim = p.ndim; G.nx = p.nx; G.ny = p.ny; G.nz = p.nz;
     G.NX = p.nx + 6;
@@ -180,6 +182,10 @@ dg::Geo make_geo(const dg_params &p) {
     else G.ndim_act = 3;
     return G;
 }
+
+int dg::set_error(int code, const char *msg) { return fail(code, msg); }
+
+namespace {
 
 int alloc(dg_ctx *c, double **p, size_t n) {
     size_t b = n * sizeof(double);
@@ -243,7 +249,7 @@ int dg_init(const dg_params *p, dg_ctx **out) {
     DG_CUDA(cudaSetDevice(p->device));
     dg_ctx *c = new dg_ctx();
     c->p = *p;
-    c->G = make_geo(*p);
+    c->G = dg::make_geo(*p);
     c->nv = dg::nstate_vars(c->G);
     std::memset(&c->B, 0, sizeof(c->B));
     auto bail = [&](int code) { dg_finalize(c); return code; };

@@ -1,0 +1,61 @@
+// History sums of a caller-owned device state without any device allocation.
+//
+// Who needs it: a Fortran driver that keeps uin in its OpenACC runtime's
+// present table hands the library device pointers from
+// `!$acc host_data use_device(uin)`; it must not create a library context, which
+// would cudaMalloc a second copy of the state plus the work arrays of a step, and
+// some production jobs run under a device-memory budget that forbids allocation
+// after start-up.  For them this entry point computes the MRI history sums of
+// src/problem/mri/history.f90:60-125 directly from their array, with the caller's
+// output buffer, and keeps its reduction scratch (per-column yz means and
+// per-block partial sums) in the file-scope array below.
+#include <mutex>
+
+#include "dumses_gpu.h"
+#include "mhd_kernels.cuh"
+
+namespace {
+
+// Largest nx accepted; the scratch holds 2*nx column means and the block partials.
+constexpr int kNoAllocMaxNx = DG_HISTORY_NOALLOC_MAX_NX;
+constexpr long long kScratchDoubles = 2LL * kNoAllocMaxNx + 8LL * 296 + 64;
+
+// One copy per GPU that loads the library, kept until the process exits.
+static __device__ __align__(256) double g_history_scratch[kScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+double *g_scratch_ptr[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" int dg_history_noalloc(const dg_params *p, const double *uin_dev, double *out_dev, void *stream) {
+    if (!p || !uin_dev || !out_dev) return dg::set_error(DG_ERR_ARG, "null argument");
+    if (p->ndim != 3) return dg::set_error(DG_ERR_UNSUPPORTED, "the MRI history is defined for ndim = 3");
+    if (p->nx < 3 || p->ny < 3 || p->nz < 3) return dg::set_error(DG_ERR_ARG, "nx, ny and nz must be >= 3");
+    if (p->nx > kNoAllocMaxNx)
+        return dg::set_error(DG_ERR_ARG, "dg_history_noalloc: nx exceeds DG_HISTORY_NOALLOC_MAX_NX");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return dg::set_error(DG_ERR_NODEVICE, "dg_history_noalloc: no usable current CUDA device");
+    double *scratch = nullptr;
+    {
+        // set-up, once per device, on the caller's current device
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (!g_scratch_ptr[dev]) {
+            cudaError_t e = cudaGetSymbolAddress((void **)&g_scratch_ptr[dev], g_history_scratch);
+            if (e != cudaSuccess) {
+                g_scratch_ptr[dev] = nullptr;
+                return dg::set_error(DG_ERR_CUDA, cudaGetErrorString(e));
+            }
+        }
+        scratch = g_scratch_ptr[dev];
+    }
+    const dg::Geo G = dg::make_geo(*p);
+    if (dg::history_scratch_doubles(G) > kScratchDoubles)
+        return dg::set_error(DG_ERR_ARG, "dg_history_noalloc: scratch too small for this grid");
+    dg::launch_history_ptrs(G, uin_dev, scratch, out_dev, (cudaStream_t)stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return dg::set_error(DG_ERR_CUDA, cudaGetErrorString(e));
+    return DG_OK;
+}

@@ -1361,12 +1361,20 @@ int launch_right_faces(const Geo &G, const double *U, double *out, cudaStream_t 
     return 1;
 }
 
-int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st) {
-    TIMED(KS_HISTORY, st, (k_hist_yzmean<<<G.nx, 256, 0, st>>>(G, B.U[cur], B.part)));
-    const int nb = 296;
-    TIMED(KS_HISTORY, st, (k_hist_sums<<<nb, 256, 0, st>>>(G, B.U[cur], B.part, B.part + 2 * G.nx)));
-    TIMED(KS_HISTORY, st, (k_hist_final<<<1, 32, 0, st>>>(G, B.part + 2 * G.nx, nb, B.hist)));
+constexpr int kHistBlocks = 296;
+
+long long history_scratch_doubles(const Geo &G) { return 2LL * G.nx + 8LL * kHistBlocks; }
+
+int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t st) {
+    // every scratch entry read below is written earlier in the same launch sequence
+    TIMED(KS_HISTORY, st, (k_hist_yzmean<<<G.nx, 256, 0, st>>>(G, U, scratch)));
+    TIMED(KS_HISTORY, st, (k_hist_sums<<<kHistBlocks, 256, 0, st>>>(G, U, scratch, scratch + 2 * G.nx)));
+    TIMED(KS_HISTORY, st, (k_hist_final<<<1, 32, 0, st>>>(G, scratch + 2 * G.nx, kHistBlocks, out)));
     return 3;
+}
+
+int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st) {
+    return launch_history_ptrs(G, B.U[cur], B.part, B.hist, st);
 }
 
 }  // namespace dg

@@ -37,6 +37,14 @@ int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t st);  // 
 int launch_set_scalars(const Bufs &B, double dt, double time, int set_dt, int set_time, cudaStream_t st);
 int launch_advance_time(const Bufs &B, cudaStream_t st);
 int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st);
+// history of any state array U (8 leading variables in the reference layout) with explicit
+// scratch (>= history_scratch_doubles(G) doubles) and a 9-double output, all device pointers
+int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t st);
+long long history_scratch_doubles(const Geo &G);
+
+// shared host helpers (dg_api.cu)
+Geo make_geo(const dg_params &p);
+int set_error(int code, const char *msg);
 int launch_right_faces(const Geo &G, const double *U, double *out, cudaStream_t st);  // vars 9-11 for download
 
 }  // namespace dg

@@ -122,6 +122,24 @@ int  dg_step(dg_ctx *ctx, double *time, double *dt);
  * out[4] magp, out[5..7] <B>, out[8] divB.  FP64 sums in a fixed tree order. */
 int  dg_history(dg_ctx *ctx, double out[9]);
 
+/* MRI history sums of a state that the caller keeps on the device, with no
+ * device allocation.  No counterpart in the reference: it is for callers that
+ * cannot let the library allocate, e.g. a Fortran driver whose uin lives in
+ * its OpenACC runtime (device pointers from `host_data use_device`) or a job
+ * under a fixed device-memory budget.
+ *   uin_dev  device array in the reference layout uin(iu1:iu2,ju1:ju2,ku1:ku2,1:11)
+ *            (only variables 1-8 are read), on the calling thread's current device
+ *   out_dev  9 device doubles, the same quantities as dg_history
+ *   stream   cudaStream_t to enqueue on (NULL: the legacy default stream)
+ * Needs ndim = 3 and nx <= DG_HISTORY_NOALLOC_MAX_NX (DG_ERR_ARG otherwise).
+ * The reduction scratch is one file-scope device array per GPU, held until the
+ * process exits; its address is looked up the first time the call runs on a
+ * device, so make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU (different streams, no ordering)
+ * race.  The call is asynchronous; out_dev is valid once the stream reaches it. */
+#define DG_HISTORY_NOALLOC_MAX_NX 16384
+int  dg_history_noalloc(const dg_params *p, const double *uin_dev, double *out_dev, void *stream);
+
 /* wait for all work of the context (bounded) */
 int  dg_sync(dg_ctx *ctx);
 
