@@ -42,10 +42,11 @@ METRIC = "zone-cycles/s at 256³: plain FP64 vs FP32+NN-flux at stated L1 vs FP6
 ALGO_BYTES_PER_ZONE = 128  # read + write of 8 conserved FP64 variables per zone-cycle
 
 
-def workload_params(n: int, device: int = 0):
+def workload_params(n: int, device: int = 0, precision: str = "fp64"):
     from dumses_hybrid_b200 import Params
     return Params(ndim=3, nx=n, ny=n, nz=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
-                  gamma=5.0 / 3.0, courant=0.8, slope_type=2, riemann="hlld", riemann2d="hlld", device=device)
+                  gamma=5.0 / 3.0, courant=0.8, slope_type=2, riemann="hlld", riemann2d="hlld", device=device,
+                  precision=precision)
 
 
 def measured_peaks() -> dict:
@@ -166,6 +167,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="grid edge (the headline workload is 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -193,7 +195,7 @@ def main() -> None:
         dist.barrier()
         dgbuild.build()
 
-    P = workload_params(args.n, device=local_rank)
+    P = workload_params(args.n, device=local_rank, precision=args.precision)
     u0 = dg.condinit(P, "orszag_tang")
     ncell = args.n ** 3
     ctx = dg.Context(P)

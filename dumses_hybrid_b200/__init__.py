@@ -279,7 +279,7 @@ class Context:
 
     def profile_read(self) -> dict[str, tuple[float, int]]:
         """{kernel slot: (total ms, launches)} since the last read."""
-        n = 11
+        n = 12
         ms = np.zeros(n)
         cnt = (ctypes.c_longlong * n)()
         _check(self.lib.dg_profile_read(self.h, self._ptr(ms), cnt, n))

@@ -1,9 +1,10 @@
 """Build libdumses_gpu.so in-tree for sm_100a.
 
 nvcc compiles each CUDA translation unit with
-  -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo --fmad=false
-(no multiply-add contraction: the FP64 path is bit-identical to the CPU
-reference arithmetic) and links them, with the host-side initial conditions,
+  -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo
+plus --fmad=false for the FP64 path and the host code (no multiply-add
+contraction: the FP64 path is bit-identical to the CPU reference arithmetic)
+and --use_fast_math for the FP32 mixed path, and links them, with the host-side initial conditions,
 into dumses_hybrid_b200/libdumses_gpu.so against the static CUDA runtime.
 Objects are rebuilt only when a source or header is newer than the library.
 
@@ -25,9 +26,12 @@ BUILD = PKG / "_build"
 LIB = PKG / "libdumses_gpu.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-                     "-I", str(INCLUDE), "-I", str(CSRC)]
-CU_SOURCES = ["mhd_kernels.cu", "dg_api.cu", "dg_noalloc.cu"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(INCLUDE), "-I", str(CSRC)]
+# FP64 path and host code: no multiply-add contraction (bit-identical arithmetic);
+# FP32 mixed path: fast FP32 math (contraction, approximate division and sqrt, FTZ)
+EXACT = ["--fmad=false"]
+FAST = ["--use_fast_math"]
+CU_SOURCES = {"step_fp64.cu": EXACT, "step_fp32.cu": FAST, "dg_api.cu": EXACT, "dg_noalloc.cu": EXACT}
 CXX_SOURCES = ["condinit.cpp"]
 
 
@@ -67,10 +71,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     BUILD.mkdir(exist_ok=True)
     nvcc, cxx = _nvcc(), _cxx()
     objs = []
-    for src in CU_SOURCES:
+    for src, flags in CU_SOURCES.items():
         obj = BUILD / (src + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_info else []
-        _run([nvcc, *NVCC_FLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)], verbose or ptxas_info)
+        _run([nvcc, *NVCC_FLAGS, *flags, *extra, "-c", str(CSRC / src), "-o", str(obj)], verbose or ptxas_info)
         objs.append(str(obj))
     for src in CXX_SOURCES:
         obj = BUILD / (src + ".o")

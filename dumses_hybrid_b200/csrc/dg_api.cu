@@ -43,13 +43,42 @@ struct EventTimer : dg::KernelTimer {
     }
 };
 const char *kSlotNames[dg::KS_COUNT] = {"scalars", "cfl_dt", "primitive", "trace", "riemann_flux_emf", "update_ct",
-                                       "fargo_emf", "fargo_update", "boundary", "history", "right_faces"};
+                                       "fargo_emf", "fargo_update", "boundary", "history", "right_faces", "edge_efield"};
 }  // namespace
+
+namespace {
+// the launch set of one arithmetic
+struct Launches {
+    int (*set_scalars)(const dg::Bufs &, double, double, int, int, cudaStream_t);
+    int (*advance_time)(const dg::Bufs &, cudaStream_t);
+    int (*dt)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*godunov)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*fargo)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*boundary)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*history)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*right_faces)(const dg::Geo &, const dg::Bufs &, int, double *, cudaStream_t);
+    int (*to_f64)(const dg::Geo &, const dg::Bufs &, int, double *, cudaStream_t);
+    int (*from_f64)(const dg::Geo &, const dg::Bufs &, int, const double *, int, cudaStream_t);
+};
+#define DG_LAUNCH_TABLE(ns)                                                                                  \
+    Launches{ns::launch_set_scalars, ns::launch_advance_time, ns::launch_dt, ns::launch_godunov, ns::launch_fargo, \
+             ns::launch_boundary, ns::launch_history, ns::launch_right_faces, ns::launch_state_to_f64,        \
+             ns::launch_f64_to_state}
+const Launches kLaunchF64 = DG_LAUNCH_TABLE(dg::f64);
+const Launches kLaunchF32 = DG_LAUNCH_TABLE(dg::f32);
+}  // namespace
+
+namespace dg {
+thread_local KernelTimer *g_timer = nullptr;
+int nstate_vars(const Geo &G) { return G.ndim == 2 ? 9 : 8; }
+}  // namespace dg
 
 struct dg_ctx {
     dg_params p;
     dg::Geo G;
     dg::Bufs B;
+    const Launches *L = &kLaunchF64;
+    size_t es = 8;  // bytes per element of the work arrays
     int cur = 0;
     int nv = 8;
     cudaStream_t stream = nullptr;
@@ -140,7 +169,7 @@ int validate(const dg_params *p) {
         return fail(DG_ERR_UNSUPPORTED, "the shearing box needs a periodic y direction");
     if (p->fargo && (p->ndim != 3 || p->bc[1] != DG_BC_PERIODIC))
         return fail(DG_ERR_UNSUPPORTED, "FARGO needs ndim = 3 and a periodic y direction");
-    if (p->precision != DG_PREC_FP64) return fail(DG_ERR_UNSUPPORTED, "this build implements the FP64 path only");
+    if (p->precision != DG_PREC_FP64 && p->precision != DG_PREC_FP32) return fail(DG_ERR_ARG, "unknown precision");
     if (p->surrogate) return fail(DG_ERR_UNSUPPORTED, "the flux surrogate needs the FP32 path");
     return DG_OK;
 }
@@ -165,6 +194,10 @@ dg::Geo dg::make_geo(const dg_params &p) {
     G.FX = p.nx + 1; G.FY = p.ny + 1;
     G.FZ = p.ndim == 3 ? p.nz + 1 : 1;
     G.fsz = (long long)G.FX * G.FY * G.FZ;
+    G.EX = p.nx + 3; G.EY = p.ny + 3;
+    G.EZ = p.ndim == 3 ? p.nz + 3 : 1;
+    G.ke0 = p.ndim == 3 ? 0 : 1;
+    G.esz = (long long)G.EX * G.EY * G.EZ;
     // init_grid (init.f90:447-449), single rank
     G.dx = (p.xmax - p.xmin) / p.nx;
     G.dy = (p.ymax - p.ymin) / p.ny;
@@ -187,9 +220,8 @@ int dg::set_error(int code, const char *msg) { return fail(code, msg); }
 
 namespace {
 
-int alloc(dg_ctx *c, double **p, size_t n) {
-    size_t b = n * sizeof(double);
-    cudaError_t e = cudaMalloc((void **)p, b);
+int alloc_bytes(dg_ctx *c, void **p, size_t b) {
+    cudaError_t e = cudaMalloc(p, b);
     if (e != cudaSuccess) {
         *p = nullptr;
         return fail(DG_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(b) + " bytes: " + cudaGetErrorString(e));
@@ -198,6 +230,8 @@ int alloc(dg_ctx *c, double **p, size_t n) {
     DG_CUDA(cudaMemsetAsync(*p, 0, b, c->stream));
     return DG_OK;
 }
+int alloc(dg_ctx *c, double **p, size_t n) { return alloc_bytes(c, (void **)p, n * sizeof(double)); }
+int alloc_w(dg_ctx *c, void **p, size_t n) { return alloc_bytes(c, p, n * c->es); }
 
 int read_scalars(dg_ctx *c) {
     DG_CUDA(cudaMemcpyAsync(c->h_scal, c->B.S, sizeof(dg::Scalars), cudaMemcpyDeviceToHost, c->stream));
@@ -252,21 +286,30 @@ int dg_init(const dg_params *p, dg_ctx **out) {
     c->G = dg::make_geo(*p);
     c->nv = dg::nstate_vars(c->G);
     std::memset(&c->B, 0, sizeof(c->B));
+    c->B.nv = c->nv;
+    c->B.sv = c->G.sv;
+    if (p->precision == DG_PREC_FP32) { c->L = &kLaunchF32; c->es = 4; }
     auto bail = [&](int code) { dg_finalize(c); return code; };
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(DG_ERR_CUDA, "cudaStreamCreate failed"));
     const dg::Geo &G = c->G;
     const size_t nt = (size_t)G.sv;
-    if ((rc = alloc(c, &c->B.U[0], nt * c->nv))) return bail(rc);
-    if ((rc = alloc(c, &c->B.U[1], nt * c->nv))) return bail(rc);
-    if ((rc = alloc(c, &c->B.Q, nt * 8))) return bail(rc);
+    // the state takes 8 bytes per variable and cell in both paths (FP64, or an FP32 hi/lo pair)
+    if ((rc = alloc(c, (double **)&c->B.U[0], nt * c->nv))) return bail(rc);
+    if ((rc = alloc(c, (double **)&c->B.U[1], nt * c->nv))) return bail(rc);
+    if (p->precision == DG_PREC_FP32 && (rc = alloc(c, &c->B.stage, nt * c->nv))) return bail(rc);
+    if ((rc = alloc_w(c, &c->B.Q, nt * 8))) return bail(rc);
     const int ncore = p->ndim == 3 ? dg::kCore3 : dg::kCore2;
-    if ((rc = alloc(c, &c->B.core, (size_t)G.csz * ncore))) return bail(rc);
+    if ((rc = alloc_w(c, &c->B.core, (size_t)G.csz * ncore))) return bail(rc);
     for (int d = 0; d < p->ndim; d++)
-        if ((rc = alloc(c, &c->B.flx[d], (size_t)G.fsz * dg::kFluxComp))) return bail(rc);
+        if ((rc = alloc_w(c, &c->B.flx[d], (size_t)G.fsz * dg::kFluxComp))) return bail(rc);
     for (int d = 0; d < 3; d++) {
         if (p->ndim == 2 && d < 2) continue;
-        if ((rc = alloc(c, &c->B.emf[d], (size_t)G.fsz))) return bail(rc);
+        if ((rc = alloc_w(c, &c->B.emf[d], (size_t)G.fsz))) return bail(rc);
+    }
+    for (int d = 0; d < 3; d++) {
+        if (p->ndim == 2 && d < 2) continue;
+        if ((rc = alloc_w(c, &c->B.E[d], (size_t)G.esz))) return bail(rc);
     }
     if (p->fargo)
         for (int d = 0; d < 2; d++)
@@ -289,9 +332,10 @@ int dg_init(const dg_params *p, dg_ctx **out) {
 int dg_finalize(dg_ctx *c) {
     if (!c) return DG_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    double *bufs[] = {c->B.U[0], c->B.U[1], c->B.Q, c->B.core, c->B.flx[0], c->B.flx[1], c->B.flx[2], c->B.emf[0],
-                      c->B.emf[1], c->B.emf[2], c->B.femf[0], c->B.femf[1], c->B.part, c->B.hist};
-    for (double *b : bufs)
+    void *bufs[] = {c->B.U[0], c->B.U[1], c->B.Q, c->B.core, c->B.flx[0], c->B.flx[1], c->B.flx[2], c->B.emf[0],
+                    c->B.emf[1], c->B.emf[2], c->B.femf[0], c->B.femf[1], c->B.part, c->B.hist,
+                    c->B.E[0], c->B.E[1], c->B.E[2], c->B.stage};
+    for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->B.S) cudaFree(c->B.S);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -304,37 +348,58 @@ int dg_finalize(dg_ctx *c) {
 
 int dg_upload(dg_ctx *c, const double *uin) {
     if (!c || !uin) return fail(DG_ERR_ARG, "null argument");
+    TimerScope ts_(c);
     DG_CUDA(cudaSetDevice(c->p.device));
     const size_t nt = (size_t)c->G.sv;
-    // uin(:,:,:,1:8) is contiguous in the reference layout
-    DG_CUDA(cudaMemcpyAsync(c->B.U[c->cur], uin, nt * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    if (c->nv == 9) {
-        // ndim = 2: the right z-face B (uin var 11) is never refreshed by the reference and
-        // stays at its initial value; both state buffers carry it
-        for (int b = 0; b < 2; b++)
-            DG_CUDA(cudaMemcpyAsync(c->B.U[b] + nt * 8, uin + nt * 10, nt * sizeof(double), cudaMemcpyHostToDevice,
+    if (c->p.precision == DG_PREC_FP64) {
+        // uin(:,:,:,1:8) is contiguous in the reference layout
+        DG_CUDA(cudaMemcpyAsync(c->B.U[c->cur], uin, nt * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if (c->nv == 9) {
+            // ndim = 2: the right z-face B (uin var 11) is never refreshed by the reference and
+            // stays at its initial value; both state buffers carry it
+            for (int b = 0; b < 2; b++)
+                DG_CUDA(cudaMemcpyAsync((double *)c->B.U[b] + nt * 8, uin + nt * 10, nt * sizeof(double),
+                                        cudaMemcpyHostToDevice, c->stream));
+        }
+    } else {
+        DG_CUDA(cudaMemcpyAsync(c->B.stage, uin, nt * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if (c->nv == 9)
+            DG_CUDA(cudaMemcpyAsync(c->B.stage + nt * 8, uin + nt * 10, nt * sizeof(double), cudaMemcpyHostToDevice,
                                     c->stream));
+        c->launches += c->L->from_f64(c->G, c->B, c->cur, c->B.stage, c->nv, c->stream);
+        if (c->nv == 9) c->launches += c->L->from_f64(c->G, c->B, c->cur ^ 1, c->B.stage, c->nv, c->stream);
+        int rc = check_launch();
+        if (rc) return rc;
     }
     return bounded_sync(c->stream);
 }
 
 int dg_download(dg_ctx *c, double *uin) {
-    TimerScope ts_(c);
     if (!c || !uin) return fail(DG_ERR_ARG, "null argument");
+    TimerScope ts_(c);
     DG_CUDA(cudaSetDevice(c->p.device));
     const size_t nt = (size_t)c->G.sv;
-    DG_CUDA(cudaMemcpyAsync(uin, c->B.U[c->cur], nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    c->launches += dg::launch_right_faces(c->G, c->B.U[c->cur], c->B.Q, c->stream);
+    double *scratch;
+    if (c->p.precision == DG_PREC_FP64) {
+        DG_CUDA(cudaMemcpyAsync(uin, c->B.U[c->cur], nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        scratch = (double *)c->B.Q;  // 8 planes of doubles, recomputed by every step
+    } else {
+        c->launches += c->L->to_f64(c->G, c->B, c->cur, c->B.stage, c->stream);
+        DG_CUDA(cudaMemcpyAsync(uin, c->B.stage, nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        DG_CUDA(cudaStreamSynchronize(c->stream));
+        scratch = c->B.stage;
+    }
+    c->launches += c->L->right_faces(c->G, c->B, c->cur, scratch, c->stream);
     int rc = check_launch();
     if (rc) return rc;
-    DG_CUDA(cudaMemcpyAsync(uin + nt * 8, c->B.Q, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DG_CUDA(cudaMemcpyAsync(uin + nt * 8, scratch, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return bounded_sync(c->stream);
 }
 
 int dg_compute_dt(dg_ctx *c, double *dt) {
     TimerScope ts_(c);
     if (!c || !dt) return fail(DG_ERR_ARG, "null argument");
-    c->launches += dg::launch_dt(c->G, c->B, c->cur, c->stream);
+    c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
     int rc = check_launch();
     if (rc) return rc;
     if ((rc = read_scalars(c))) return rc;
@@ -346,8 +411,8 @@ int dg_godunov(dg_ctx *c, double dt, double time) {
     TimerScope ts_(c);
     if (!c) return fail(DG_ERR_ARG, "null context");
     if (!(dt > 0) || !std::isfinite(dt)) return fail(DG_ERR_DT, "dt must be positive and finite");
-    c->launches += dg::launch_set_scalars(c->B, dt, time, 1, 1, c->stream);
-    c->launches += dg::launch_godunov(c->G, c->B, c->cur, c->stream);
+    c->launches += c->L->set_scalars(c->B, dt, time, 1, 1, c->stream);
+    c->launches += c->L->godunov(c->G, c->B, c->cur, c->stream);
     c->cur ^= 1;
     return check_launch();
 }
@@ -356,8 +421,8 @@ int dg_fargo_update(dg_ctx *c, double dt) {
     TimerScope ts_(c);
     if (!c) return fail(DG_ERR_ARG, "null context");
     if (!c->p.fargo) return fail(DG_ERR_ARG, "context was created with fargo = 0");
-    c->launches += dg::launch_set_scalars(c->B, dt, 0.0, 1, 0, c->stream);
-    c->launches += dg::launch_fargo(c->G, c->B, c->cur, c->stream);
+    c->launches += c->L->set_scalars(c->B, dt, 0.0, 1, 0, c->stream);
+    c->launches += c->L->fargo(c->G, c->B, c->cur, c->stream);
     c->cur ^= 1;
     return check_launch();
 }
@@ -365,8 +430,8 @@ int dg_fargo_update(dg_ctx *c, double dt) {
 int dg_boundary(dg_ctx *c, double time, double dt) {
     TimerScope ts_(c);
     if (!c) return fail(DG_ERR_ARG, "null context");
-    c->launches += dg::launch_set_scalars(c->B, dt, time, 1, 1, c->stream);
-    c->launches += dg::launch_boundary(c->G, c->B, c->cur, c->stream);
+    c->launches += c->L->set_scalars(c->B, dt, time, 1, 1, c->stream);
+    c->launches += c->L->boundary(c->G, c->B, c->cur, c->stream);
     return check_launch();
 }
 
@@ -374,17 +439,17 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
     TimerScope ts_(c);
     if (!c || !time) return fail(DG_ERR_ARG, "null argument");
     if (nsteps < 0) return fail(DG_ERR_ARG, "nsteps < 0");
-    c->launches += dg::launch_set_scalars(c->B, 0.0, *time, 0, 1, c->stream);
+    c->launches += c->L->set_scalars(c->B, 0.0, *time, 0, 1, c->stream);
     for (int n = 0; n < nsteps; n++) {
-        c->launches += dg::launch_dt(c->G, c->B, c->cur, c->stream);
-        c->launches += dg::launch_godunov(c->G, c->B, c->cur, c->stream);
+        c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
+        c->launches += c->L->godunov(c->G, c->B, c->cur, c->stream);
         c->cur ^= 1;
         if (c->p.fargo) {
-            c->launches += dg::launch_fargo(c->G, c->B, c->cur, c->stream);
+            c->launches += c->L->fargo(c->G, c->B, c->cur, c->stream);
             c->cur ^= 1;
         }
-        c->launches += dg::launch_boundary(c->G, c->B, c->cur, c->stream);
-        c->launches += dg::launch_advance_time(c->B, c->stream);
+        c->launches += c->L->boundary(c->G, c->B, c->cur, c->stream);
+        c->launches += c->L->advance_time(c->B, c->stream);
     }
     int rc = check_launch();
     if (rc) return rc;
@@ -400,7 +465,7 @@ int dg_history(dg_ctx *c, double out[9]) {
     TimerScope ts_(c);
     if (!c || !out) return fail(DG_ERR_ARG, "null argument");
     if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the MRI history is defined for ndim = 3");
-    c->launches += dg::launch_history(c->G, c->B, c->cur, c->stream);
+    c->launches += c->L->history(c->G, c->B, c->cur, c->stream);
     int rc = check_launch();
     if (rc) return rc;
     DG_CUDA(cudaMemcpyAsync(c->h_hist, c->B.hist, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -416,16 +481,24 @@ int dg_sync(dg_ctx *c) {
 
 int dg_debug_copy(dg_ctx *c, int which, double *host, long long count, long long *copied) {
     if (!c || !host) return fail(DG_ERR_ARG, "null argument");
-    const double *src = nullptr;
+    const void *src = nullptr;
     long long n = 0;
     if (which >= 0 && which <= 2) { src = c->B.flx[which]; n = c->G.fsz * dg::kFluxComp; }
     else if (which >= 3 && which <= 5) { src = c->B.emf[which - 3]; n = c->G.fsz; }
     else if (which == 6) { src = c->B.Q; n = c->G.sv * 8; }
     if (!src) return fail(DG_ERR_ARG, "no such array for this context");
     if (count < n) return fail(DG_ERR_ARG, "host buffer too small");
-    DG_CUDA(cudaMemcpyAsync(host, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    int rc = bounded_sync(c->stream);
-    if (rc) return rc;
+    if (c->es == sizeof(double)) {
+        DG_CUDA(cudaMemcpyAsync(host, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        int rc = bounded_sync(c->stream);
+        if (rc) return rc;
+    } else {
+        std::vector<float> tmp((size_t)n);
+        DG_CUDA(cudaMemcpyAsync(tmp.data(), src, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        int rc = bounded_sync(c->stream);
+        if (rc) return rc;
+        for (long long k = 0; k < n; k++) host[k] = tmp[(size_t)k];
+    }
     if (copied) *copied = n;
     return DG_OK;
 }

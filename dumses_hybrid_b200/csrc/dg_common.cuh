@@ -41,6 +41,9 @@ struct Geo {
     // face index space: [1, nx+1] x [1, ny+1] x [1, nz+1] (z extent 1 for ndim = 2)
     int FX, FY, FZ;
     long long fsz;
+    // edge electric-field index space of the trace: [0, nx+2] x [0, ny+2] x [ke0, ke1]
+    int EX, EY, EZ, ke0;
+    long long esz;
     double dx, dy, dz;
     double xmin, xmax, ymin, ymax, zmin, zmax;
     double gamma, ciso, omega0, courant;
@@ -56,6 +59,9 @@ struct Geo {
     }
     __host__ __device__ __forceinline__ long long fidx(int i, int j, int k) const {
         return (long long)(i - 1) + (long long)FX * ((long long)(j - 1) + (long long)FY * (long long)(k - 1));
+    }
+    __host__ __device__ __forceinline__ long long eidx(int i, int j, int k) const {
+        return (long long)i + (long long)EX * ((long long)j + (long long)EY * (long long)(k - ke0));
     }
     // cell centre x(i) = xmin + dx/2 + (i-1) dx (init.f90:461-468)
     __host__ __device__ __forceinline__ double xc(int i) const { return xmin + dx / 2 + (i - 1) * dx; }

@@ -52,9 +52,9 @@ extern "C" int dg_history_noalloc(const dg_params *p, const double *uin_dev, dou
         scratch = g_scratch_ptr[dev];
     }
     const dg::Geo G = dg::make_geo(*p);
-    if (dg::history_scratch_doubles(G) > kScratchDoubles)
+    if (dg::f64::history_scratch_doubles(G) > kScratchDoubles)
         return dg::set_error(DG_ERR_ARG, "dg_history_noalloc: scratch too small for this grid");
-    dg::launch_history_ptrs(G, uin_dev, scratch, out_dev, (cudaStream_t)stream);
+    dg::f64::launch_history_ptrs(G, uin_dev, scratch, out_dev, (cudaStream_t)stream);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return dg::set_error(DG_ERR_CUDA, cudaGetErrorString(e));
     return DG_OK;

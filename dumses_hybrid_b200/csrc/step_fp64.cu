@@ -1,0 +1,292 @@
+// FP64 plain path: the step kernels of step_impl.cuh instantiated for T = double
+// on an FP64 state, compiled with --fmad=false.  Bit-identical to the reference
+// arithmetic (see dg_common.cuh).
+#define DG_NS f64
+#include "step_impl.cuh"
+
+namespace dg {
+namespace f64 {
+namespace {
+
+// update + constrained_transport of the FP64 state (scheme.f90:1764-1993), in the
+// reference's statement order
+__global__ void __launch_bounds__(kThreads) k_update3d(Geo G, const double *__restrict__ U, double *__restrict__ Un,
+                                                       const double *__restrict__ fx, const double *__restrict__ fy,
+                                                       const double *__restrict__ fz, const double *__restrict__ ex,
+                                                       const double *__restrict__ ey, const double *__restrict__ ez,
+                                                       const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const double dt = S->dt;
+    const double one = 1.0, two = 2.0, half = 0.5;
+    const long long sv = G.sv, fs = G.fsz;
+    const long long c = G.idx(i, j, k);
+    const bool shear = G.shearing != 0;
+    ShearRemap sr{0.0, 0};
+    if (shear) sr = shear_offset(G, S->time + half * dt);
+
+    if (i <= nx && j <= ny && k <= nz) {
+        // hydro update, scheme.f90:1783-1907
+        const double Omega0 = G.omega0;
+        double lambda = 0.0, ratio = 0.0;
+        if (Omega0 > 0.0) {
+            lambda = Omega0 * dt; lambda = 2.5e-1 * lambda * lambda;
+            ratio = (one - lambda) / (one + lambda);
+        }
+        const double dv = G.dx * G.dy * G.dz;
+        const double dvloc = one / dv;
+        double ur = ld(U + c), uu = ld(U + sv * IU + c), uv = ld(U + sv * IV + c), uw = ld(U + sv * IW + c);
+        double up = ld(U + sv * IP + c);
+        if (Omega0 > 0.0) {
+            const double dsx = two * Omega0 * dt * uv / (one + lambda);
+            const double dsy = -(half * Omega0 * dt * uu) / (one + lambda);
+            uu = uu * ratio + dsx;
+            uv = uv * ratio + dsy;
+        }
+        const long long f0 = t;
+        const long long fxr = G.fidx(i + 1, j, k), fyr = G.fidx(i, j + 1, k), fzr = G.fidx(i, j, k + 1);
+        const double *FA[3] = {fx, fy, fz};
+        const long long FR[3] = {fxr, fyr, fzr};
+        double pre[3];
+        for (int d = 0; d < 3; d++) {
+            const double *F = FA[d];
+            double rl = ld(F + f0), rr = ld(F + FR[d]);
+            if (d == 0 && shear) {
+                if (i == 1) rl = shear_avg(G, sr, fx, 0, 0, j, k);
+                if (i == nx) rr = shear_avg(G, sr, fx, 0, 1, j, k);
+            }
+            const double ds = (d == 0) ? G.dy * G.dz : (d == 1 ? G.dx * G.dz : G.dx * G.dy);
+            pre[d] = -(ld(F + 5 * fs + FR[d]) * ds - ld(F + 5 * fs + f0) * ds) * dt;
+            ur = ur + (rl - rr) * dvloc;
+            uw = uw + (ld(F + 4 * fs + f0) * one - ld(F + 4 * fs + FR[d]) * one) * dvloc / one;
+            up = up + (ld(F + 1 * fs + f0) - ld(F + 1 * fs + FR[d])) * dvloc;
+            if (Omega0 > 0.0) {
+                double dfn2 = (ld(F + 2 * fs + f0) - ld(F + 2 * fs + FR[d])) * dvloc;
+                if (d == 0) dfn2 = dfn2 + pre[0] * dvloc;
+                double dfn3 = (ld(F + 3 * fs + f0) - ld(F + 3 * fs + FR[d])) * dvloc;
+                if (d == 1) dfn3 = dfn3 + pre[1] * dvloc;
+                uu = uu + dfn2 / (one + lambda) + Omega0 * dt / (one + lambda) * dfn3;
+                uv = uv + dfn3 / (one + lambda) - 2.5e-1 * Omega0 * dt / (one + lambda) * dfn2;
+            } else {
+                uu = uu + (ld(F + 2 * fs + f0) * one - ld(F + 2 * fs + FR[d]) * one) * dvloc / one;
+                uv = uv + (ld(F + 3 * fs + f0) * one - ld(F + 3 * fs + FR[d]) * one) * dvloc / one;
+            }
+        }
+        if (Omega0 == 0.0) {
+            uu = uu + pre[0] * dvloc;
+            uv = uv + pre[1] * dvloc;
+        }
+        uw = uw + pre[2] * dvloc;
+        Un[c] = ur; Un[sv * IU + c] = uu; Un[sv * IV + c] = uv; Un[sv * IW + c] = uw; Un[sv * IP + c] = up;
+    }
+    // constrained transport of the left faces, scheme.f90:1957-1993 (ranges 1..n+1)
+    auto EYc = [&](int ii, int jj, int kk) -> double {
+        if (shear && (ii == 1 || ii == nx + 1) && jj <= ny && kk <= nz + 1)
+            return shear_avg(G, sr, ey, 0, ii == 1 ? 0 : 1, jj, kk);
+        return ld(ey + G.fidx(ii, jj, kk));
+    };
+    const double dx = G.dx, dy = G.dy, dz = G.dz;
+    const bool ct = G.ndim_act > 1;
+    if (j <= ny && k <= nz) {  // B_x at face i (i = 1..nx+1)
+        double b = ld(U + sv * IA + c);
+        if (ct) {
+            b = b + (ld(ez + G.fidx(i, j + 1, k)) - ld(ez + t)) / dy;
+            b = b - (EYc(i, j, k + 1) - EYc(i, j, k)) / dz;
+        }
+        Un[sv * IA + c] = b;
+    }
+    if (i <= nx && k <= nz) {  // B_y at face j
+        double b = ld(U + sv * IB + c);
+        if (ct) {
+            b = b - (ld(ez + G.fidx(i + 1, j, k)) - ld(ez + t)) / dx;
+            b = b + (ld(ex + G.fidx(i, j, k + 1)) - ld(ex + t)) / dz;
+        }
+        Un[sv * IB + c] = b;
+    }
+    if (i <= nx && j <= ny) {  // B_z at face k
+        double b = ld(U + sv * IC + c);
+        if (ct) b = b + (EYc(i + 1, j, k) - EYc(i, j, k)) / dx - (ld(ex + G.fidx(i, j + 1, k)) - ld(ex + t)) / dy;
+        Un[sv * IC + c] = b;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_update2d(Geo G, const double *__restrict__ U, double *__restrict__ Un,
+                                                       const double *__restrict__ fx, const double *__restrict__ fy,
+                                                       const double *__restrict__ ez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const int j = (int)(t / G.FX) + 1;
+    const int k = 1;
+    const int nx = G.nx, ny = G.ny;
+    const double dt = S->dt;
+    const double one = 1.0, two = 2.0, half = 0.5;
+    const long long sv = G.sv, fs = G.fsz;
+    const long long c = G.idx(i, j, k);
+    if (i <= nx && j <= ny) {
+        const double Omega0 = G.omega0;
+        double lambda = 0.0, ratio = 0.0;
+        if (Omega0 > 0.0) {
+            lambda = Omega0 * dt; lambda = 2.5e-1 * lambda * lambda;
+            ratio = (one - lambda) / (one + lambda);
+        }
+        const double dv = G.dx * G.dy * G.dz;
+        const double dvloc = one / dv;
+        double ur = ld(U + c), uu = ld(U + sv * IU + c), uv = ld(U + sv * IV + c), uw = ld(U + sv * IW + c);
+        double up = ld(U + sv * IP + c), uc = ld(U + sv * IC + c);
+        if (Omega0 > 0.0) {
+            const double dsx = two * Omega0 * dt * uv / (one + lambda);
+            const double dsy = -(half * Omega0 * dt * uu) / (one + lambda);
+            uu = uu * ratio + dsx;
+            uv = uv * ratio + dsy;
+        }
+        const long long FR[2] = {G.fidx(i + 1, j, k), G.fidx(i, j + 1, k)};
+        const double *FA[2] = {fx, fy};
+        double pre[2];
+        for (int d = 0; d < 2; d++) {
+            const double *F = FA[d];
+            const double ds = (d == 0) ? G.dy * G.dz : G.dx * G.dz;
+            pre[d] = -(ld(F + 5 * fs + FR[d]) * ds - ld(F + 5 * fs + t) * ds) * dt;
+            ur = ur + (ld(F + t) - ld(F + FR[d])) * dvloc;
+            uw = uw + (ld(F + 4 * fs + t) * one - ld(F + 4 * fs + FR[d]) * one) * dvloc / one;
+            up = up + (ld(F + 1 * fs + t) - ld(F + 1 * fs + FR[d])) * dvloc;
+            uc = uc + (ld(F + 6 * fs + t) - ld(F + 6 * fs + FR[d])) * dvloc;
+            if (Omega0 > 0.0) {
+                double dfn2 = (ld(F + 2 * fs + t) - ld(F + 2 * fs + FR[d])) * dvloc;
+                if (d == 0) dfn2 = dfn2 + pre[0] * dvloc;
+                double dfn3 = (ld(F + 3 * fs + t) - ld(F + 3 * fs + FR[d])) * dvloc;
+                if (d == 1) dfn3 = dfn3 + pre[1] * dvloc;
+                uu = uu + dfn2 / (one + lambda) + Omega0 * dt / (one + lambda) * dfn3;
+                uv = uv + dfn3 / (one + lambda) - 2.5e-1 * Omega0 * dt / (one + lambda) * dfn2;
+            } else {
+                uu = uu + (ld(F + 2 * fs + t) * one - ld(F + 2 * fs + FR[d]) * one) * dvloc / one;
+                uv = uv + (ld(F + 3 * fs + t) * one - ld(F + 3 * fs + FR[d]) * one) * dvloc / one;
+            }
+        }
+        if (Omega0 == 0.0) {
+            uu = uu + pre[0] * dvloc;
+            uv = uv + pre[1] * dvloc;
+        }
+        Un[c] = ur; Un[sv * IU + c] = uu; Un[sv * IV + c] = uv; Un[sv * IW + c] = uw; Un[sv * IP + c] = up;
+        Un[sv * IC + c] = uc;
+    }
+    const bool ct = G.ndim_act > 1;
+    if (j <= ny) {
+        double b = ld(U + sv * IA + c);
+        if (ct) b = b + (ld(ez + G.fidx(i, j + 1, k)) - ld(ez + t)) / G.dy;
+        Un[sv * IA + c] = b;
+    }
+    if (i <= nx) {
+        double b = ld(U + sv * IB + c);
+        if (ct) b = b - (ld(ez + G.fidx(i + 1, j, k)) - ld(ez + t)) / G.dx;
+        Un[sv * IB + c] = b;
+    }
+}
+
+
+StoreD st(const Bufs &B, int b) { return StoreD{(double *)B.U[b]}; }
+
+}  // namespace
+
+#define TIMED(slot, st, launch)                          \
+    do {                                                 \
+        if (g_timer) g_timer->begin(slot, st);           \
+        launch;                                          \
+        if (g_timer) g_timer->end(slot, st);             \
+    } while (0)
+
+int launch_set_scalars(const Bufs &B, double dt, double time, int set_dt, int set_time, cudaStream_t s) {
+    TIMED(KS_SCALARS, s, (k_set_scalars<<<1, 1, 0, s>>>(B.S, dt, time, set_dt, set_time)));
+    return 1;
+}
+
+int launch_advance_time(const Bufs &B, cudaStream_t s) {
+    TIMED(KS_SCALARS, s, (k_advance_time<<<1, 1, 0, s>>>(B.S)));
+    return 1;
+}
+
+int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    TIMED(KS_DT, s, (k_dt_reset<<<1, 1, 0, s>>>(G, B.S)));
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    long long nb = (n + kThreads - 1) / kThreads;
+    if (nb > 148 * 16) nb = 148 * 16;
+    TIMED(KS_DT, s, (k_dt<StoreD><<<(unsigned)nb, kThreads, 0, s>>>(G, st(B, cur), B.S)));
+    TIMED(KS_DT, s, (k_dt_final<<<1, 1, 0, s>>>(G, B.S)));
+    return 3;
+}
+
+int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    const StoreD U = st(B, cur);
+    double *Un = (double *)B.U[cur ^ 1];
+    double *Q = (double *)B.Q, *core = (double *)B.core;
+    double *E0 = (double *)B.E[0], *E1 = (double *)B.E[1], *E2 = (double *)B.E[2];
+    double *fx = (double *)B.flx[0], *fy = (double *)B.flx[1], *fz = (double *)B.flx[2];
+    double *ex = (double *)B.emf[0], *ey = (double *)B.emf[1], *ez = (double *)B.emf[2];
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    TIMED(KS_PRIM, s, (k_prim<double, StoreD><<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    if (G.ndim == 3) {
+        TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
+        TIMED(KS_TRACE, s, (k_trace3d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
+        TIMED(KS_RIEMANN, s, (k_riemann3d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S)));
+        TIMED(KS_UPDATE, s, (k_update3d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, fz, ex, ey, ez, B.S)));
+    } else {
+        TIMED(KS_EFIELD, s, (k_efield2d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2)));
+        TIMED(KS_TRACE, s, (k_trace2d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2, core, B.S)));
+        TIMED(KS_RIEMANN, s, (k_riemann2d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S)));
+        TIMED(KS_UPDATE, s, (k_update2d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, ez, B.S)));
+    }
+    return 5;
+}
+
+int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    TIMED(KS_FARGO_EMF, s, (k_fargo_emf<StoreD><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), B.femf[0], B.femf[1], B.S)));
+    TIMED(KS_FARGO_UPDATE, s, (k_fargo_update<StoreD><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), B.femf[0], B.femf[1], B.S)));
+    return 2;
+}
+
+int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    const long long n = (long long)G.NX * G.NY * G.NZ;
+    TIMED(KS_BOUNDARY, s, (k_boundary<StoreD><<<nblocks(n, kThreads), kThreads, 0, s>>>(G, st(B, cur), B.nv, B.S)));
+    return 1;
+}
+
+int launch_right_faces(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t s) {
+    const long long n = (long long)G.NX * G.NY * G.NZ;
+    TIMED(KS_RIGHT_FACES, s, (k_right_faces<StoreD><<<nblocks(n, 256), 256, 0, s>>>(G, st(B, cur), out)));
+    return 1;
+}
+
+int launch_state_to_f64(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t s) {
+    TIMED(KS_RIGHT_FACES, s, (k_state_to_f64<StoreD><<<nblocks(G.sv * B.nv, 256), 256, 0, s>>>(G, st(B, cur), B.nv, out)));
+    return 1;
+}
+
+int launch_f64_to_state(const Geo &G, const Bufs &B, int b, const double *in, int nv, cudaStream_t s) {
+    TIMED(KS_RIGHT_FACES, s, (k_f64_to_state<StoreD><<<nblocks(G.sv * nv, 256), 256, 0, s>>>(G, in, nv, st(B, b))));
+    return 1;
+}
+
+constexpr int kHistBlocks = 296;
+
+long long history_scratch_doubles(const Geo &G) { return 2LL * G.nx + 8LL * kHistBlocks; }
+
+int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t s) {
+    // every scratch entry read below is written earlier in the same launch sequence
+    const StoreD S{(double *)U};
+    TIMED(KS_HISTORY, s, (k_hist_yzmean<StoreD><<<G.nx, 256, 0, s>>>(G, S, scratch)));
+    TIMED(KS_HISTORY, s, (k_hist_sums<StoreD><<<kHistBlocks, 256, 0, s>>>(G, S, scratch, scratch + 2 * G.nx)));
+    TIMED(KS_HISTORY, s, (k_hist_final<<<1, 32, 0, s>>>(G, scratch + 2 * G.nx, kHistBlocks, out)));
+    return 3;
+}
+
+int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    return launch_history_ptrs(G, (const double *)B.U[cur], B.part, B.hist, s);
+}
+
+}  // namespace f64
+}  // namespace dg

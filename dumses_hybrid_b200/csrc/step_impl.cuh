@@ -1,0 +1,1245 @@
+// Kernels of the DUMSES Godunov MHD step, written once and instantiated for two
+// arithmetics (this header is included by step_fp64.cu and step_fp32.cu):
+//
+//   FP64 plain path   T = double, state StoreD (8 FP64 planes), --fmad=false:
+//                     bit-identical to the reference arithmetic.
+//   FP32 mixed path   T = float, state StoreHL (compensated FP32 hi/lo planes),
+//                     fast FP32 math; FP64 only where the state is turned into
+//                     primitives (pressure recovery from total energy), in the
+//                     CFL reduction, FARGO's remap and the history sums.
+//
+// Pipeline of one step (the call order of src/dumses.f90:82-120):
+//   k_dt          compute_dt  (physics.f90:18-132)      primitive + CFL min-reduction
+//   k_prim        primitive   (scheme.f90:20-91)        Q on the ghosted grid
+//   k_efield      edge E of trace3d/trace2d (scheme.f90:1194-1239, 856-872), once per edge
+//   k_trace       slope + trace3d/trace2d (scheme.f90:253-656, 807-1711)
+//                 -> per-cell "trace core": predicted cell state, half slopes,
+//                    predicted face B and its transverse half slopes; every
+//                    face and corner state of the reference is one add (and a
+//                    floor) away from these values.
+//   k_riemann     riemann_solver + riemann_solver_magnetic + compflux
+//                 (solver.f90:65-387, solver_magnetic.f90:55-235, scheme.f90:1716-1760)
+//                 one thread per cell: its three left faces and three lower edges.
+//   k_update      update + constrained_transport (scheme.f90:1764-1993), with the
+//                 shearing-box averaging of the boundary mass flux and emfy
+//                 (shearingbox.f90:207-390) applied on the fly.
+//   k_fargo_*     fargo_update (fargo.f90:17-288)
+//   k_boundary    boundary (boundary.f90:18-92) incl. shearing_boundary (shearingbox.f90:19-203)
+#pragma once
+#include "mhd_kernels.cuh"
+#include "solvers.cuh"
+
+#ifndef DG_NS
+#error "define DG_NS (f64 or f32) before including step_impl.cuh"
+#endif
+
+namespace dg {
+namespace DG_NS {
+namespace {
+
+constexpr int kThreads = 128;
+
+template <typename X> __device__ __forceinline__ X ld(const X *p) { return __ldg(p); }
+
+inline unsigned nblocks(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// ---------------------------------------------------------------------------
+// state storage policies
+// ---------------------------------------------------------------------------
+// FP64 state: nv planes of doubles, plane v at p + v*sv
+struct StoreD {
+    double *p;
+    __device__ __forceinline__ double get(const Geo &G, int v, long long c) const { return p[G.sv * v + c]; }
+    __device__ __forceinline__ double getr(const Geo &G, int v, long long c) const { return ld(p + G.sv * v + c); }
+    __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const { p[G.sv * v + c] = x; }
+    __device__ __forceinline__ const double *faces() const { return p; }
+};
+
+// Compensated FP32 state: value = hi + lo with |lo| <= ulp(hi)/2 (renormalised on
+// every write), hi planes at hi + v*sv and lo planes at lo + v*sv.
+struct StoreHL {
+    float *hi, *lo;
+    __device__ __forceinline__ double get(const Geo &G, int v, long long c) const {
+        return (double)hi[G.sv * v + c] + (double)lo[G.sv * v + c];
+    }
+    __device__ __forceinline__ double getr(const Geo &G, int v, long long c) const {
+        return (double)ld(hi + G.sv * v + c) + (double)ld(lo + G.sv * v + c);
+    }
+    __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const {
+        const float h = (float)x;
+        hi[G.sv * v + c] = h;
+        lo[G.sv * v + c] = (float)(x - (double)h);
+    }
+    __device__ __forceinline__ const float *faces() const { return hi; }
+};
+
+// ---------------------------------------------------------------------------
+// small scalar kernels
+// ---------------------------------------------------------------------------
+__global__ void k_set_scalars(Scalars *S, double dt, double time, int set_dt, int set_time) {
+    if (set_dt) S->dt = dt;
+    if (set_time) S->time = time;
+}
+
+__global__ void k_advance_time(Scalars *S) { S->time = S->time + S->dt; }
+
+__global__ void k_dt_reset(Geo G, Scalars *S) {
+    // dt = courant*dx/smallc before the minimum (physics.f90:40)
+    double d0 = G.courant * G.dx / kSmallc;
+    S->red = (unsigned long long)__double_as_longlong(d0);
+}
+
+__global__ void k_dt_final(Geo G, Scalars *S) {
+    double m = __longlong_as_double((long long)S->red);
+    double dt = G.courant * m;
+    S->dt = dt;
+    if (!(dt > 0.0) || !isfinite(dt)) S->err = DG_ERR_DT;
+}
+
+// primitive variables of one cell in FP64 (scheme.f90:44-86); the right faces are the
+// neighbour's left faces (the frozen right z-face when ndim = 2)
+template <class Store>
+__device__ __forceinline__ void prim_cell(const Geo &G, const Store &U, long long c, double dt, double q[8]) {
+    const double one = 1.0, half = 0.5, two = 2.0;
+    const double d = U.getr(G, IR, c);
+    q[IR] = mx(d, kSmallr);
+    q[IU] = U.getr(G, IU, c) / d;
+    q[IV] = U.getr(G, IV, c) / d;
+    q[IW] = U.getr(G, IW, c) / d;
+    q[IA] = half * (U.getr(G, IA, c) + U.getr(G, IA, c + 1));
+    q[IB] = half * (U.getr(G, IB, c) + U.getr(G, IB, c + G.sy));
+    if (G.ndim == 3) q[IC] = half * (U.getr(G, IC, c) + U.getr(G, IC, c + G.sz));
+    else q[IC] = half * (U.getr(G, IC, c) + U.getr(G, 8, c));
+    if (G.iso) {
+        q[IP] = d * (G.ciso * G.ciso);
+    } else {
+        const double smallp = kSmallr * (kSmallc * kSmallc) / G.gamma;
+        double eken = half * (q[IU] * q[IU] + q[IV] * q[IV] + q[IW] * q[IW]);
+        double emag = half * (q[IA] * q[IA] + q[IB] * q[IB] + q[IC] * q[IC]);
+        double eint = (U.getr(G, IP, c) - emag) / d - eken;
+        q[IP] = mx((G.gamma - one) * q[IR] * eint, smallp);
+    }
+    if (G.omega0 > 0.0) {
+        double dvx = two * G.omega0 * q[IV];
+        double dvy = -(half * G.omega0 * q[IU]);
+        q[IU] = q[IU] + dvx * dt * half;
+        q[IV] = q[IV] + dvy * dt * half;
+    }
+}
+
+// comp_speed, physics.f90:148-164
+__device__ __forceinline__ double comp_speed(double gamma, double rho, double p, double v, double bn, double bt1,
+                                             double bt2) {
+    const double half = 0.5;
+    double c2 = gamma * p / rho;
+    double b2 = bn * bn + bt1 * bt1 + bt2 * bt2;
+    double d2 = half * (c2 + b2 / rho);
+    double cf = sqrt(d2 + sqrt(d2 * d2 - c2 * bn * bn / rho));
+    return cf + fabs(v);
+}
+
+// compute_dt reduction over the active cells (physics.f90:42-121), FP64 in both paths
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_dt(Geo G, Store U, Scalars *S) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    double best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    int bad = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t % G.nx) + 1;
+        long long r = t / G.nx;
+        int j = (int)(r % G.ny) + 1;
+        int k = (int)(r / G.ny) + 1;
+        double q[8];
+        prim_cell(G, U, G.idx(i, j, k), 0.0, q);
+        double velx = comp_speed(G.gamma, q[IR], q[IP], q[IU], q[IA], q[IB], q[IC]);
+        if (G.nx == 1) velx = 0.0;
+        double vely = comp_speed(G.gamma, q[IR], q[IP], q[IV], q[IB], q[IC], q[IA]);
+        if ((G.omega0 > 0.0) && !G.fargo) vely = vely + 1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5;
+        if (G.ny == 1) vely = 0.0;
+        double c;
+        if (G.ndim == 3) {
+            double velz = comp_speed(G.gamma, q[IR], q[IP], q[IW], q[IC], q[IA], q[IB]);
+            if (G.nz == 1) velz = 0.0;
+            c = 1.0 / (velx / G.dx + vely / G.dy + velz / G.dz);
+        } else {
+            c = 1.0 / (velx / G.dx + vely / G.dy);
+        }
+        if (!(c > 0.0)) bad = 1;  // NaN or non-positive
+        else best = mn(best, c);
+    }
+    // warp then block minimum on the bit patterns (positive doubles order as integers)
+    unsigned long long b = (unsigned long long)__double_as_longlong(best);
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+        b = ob < b ? ob : b;
+    }
+    __shared__ unsigned long long sb[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = b;
+    if (bad) S->err = DG_ERR_STATE;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = sb[0];
+        for (int w = 1; w < kThreads / 32; w++) m = sb[w] < m ? sb[w] : m;
+        atomicMin(&S->red, m);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// primitive variables on the ghosted grid (cells with a right neighbour)
+// ---------------------------------------------------------------------------
+template <typename T, class Store>
+__global__ void __launch_bounds__(kThreads) k_prim(Geo G, Store U, T *__restrict__ Q, const Scalars *S) {
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    const long long n = (long long)ni * nj * nk;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int i = (int)(t % ni) - 2;
+    long long r = t / ni;
+    int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
+    int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+    const long long c = G.idx(i, j, k);
+    double q[8];
+    prim_cell(G, U, c, S->dt, q);
+#pragma unroll
+    for (int v = 0; v < 8; v++) Q[G.sv * v + c] = (T)q[v];
+}
+
+// the slope limiter of slope() for slope_type 1 and 2 (scheme.f90:450-458)
+template <typename T>
+__device__ __forceinline__ T limit1(T st, T qm1, T q0, T qp1) {
+    const T half = T(0.5);
+    T dlft = st * (q0 - qm1);
+    T drgt = st * (qp1 - q0);
+    T dcen = half * (dlft + drgt) / st;
+    T dsgn = sgn1(dcen);
+    T slop = mn(fab(dlft), fab(drgt));
+    T dlim = slop;
+    if ((dlft * drgt) <= T(0)) dlim = T(0);
+    return dsgn * mn(dlim, fab(dcen));
+}
+
+// ---------------------------------------------------------------------------
+// edge electric fields and trace
+// ---------------------------------------------------------------------------
+template <typename T>
+struct QV {
+    const T *Q;
+    const T *B;  // face-B planes (IA..IC) of the state, left faces
+    Geo G;
+    __device__ __forceinline__ T q(int v, int i, int j, int k) const { return ld(Q + G.sv * v + G.idx(i, j, k)); }
+    __device__ __forceinline__ T bf(int c, int i, int j, int k) const { return ld(B + G.sv * (IA + c) + G.idx(i, j, k)); }
+};
+
+// edge electric fields of trace3d (scheme.f90:1194-1239)
+template <typename T>
+__device__ __forceinline__ T Ex_at(const QV<T> &a, int i, int j, int k) {
+    const T forth = T(0.25), half = T(0.5);
+    T v = forth * (a.q(IV, i, j - 1, k - 1) + a.q(IV, i, j - 1, k) + a.q(IV, i, j, k - 1) + a.q(IV, i, j, k));
+    T w = forth * (a.q(IW, i, j - 1, k - 1) + a.q(IW, i, j - 1, k) + a.q(IW, i, j, k - 1) + a.q(IW, i, j, k));
+    T B = half * (a.bf(1, i, j, k - 1) + a.bf(1, i, j, k));
+    T C = half * (a.bf(2, i, j - 1, k) + a.bf(2, i, j, k));
+    T e = v * C - w * B;
+    if ((a.G.omega0 > 0.0) && !a.G.fargo) {
+        T shear = (T)(-1.5 * a.G.omega0 * a.G.xc(i));
+        e = e + shear * C;
+    }
+    return e;
+}
+template <typename T>
+__device__ __forceinline__ T Ey_at(const QV<T> &a, int i, int j, int k) {
+    const T forth = T(0.25), half = T(0.5);
+    T u = forth * (a.q(IU, i - 1, j, k - 1) + a.q(IU, i - 1, j, k) + a.q(IU, i, j, k - 1) + a.q(IU, i, j, k));
+    T w = forth * (a.q(IW, i - 1, j, k - 1) + a.q(IW, i - 1, j, k) + a.q(IW, i, j, k - 1) + a.q(IW, i, j, k));
+    T A = half * (a.bf(0, i, j, k - 1) + a.bf(0, i, j, k));
+    T C = half * (a.bf(2, i - 1, j, k) + a.bf(2, i, j, k));
+    return w * A - u * C;
+}
+template <typename T>
+__device__ __forceinline__ T Ez_at(const QV<T> &a, int i, int j, int k) {
+    const T forth = T(0.25), half = T(0.5);
+    T u = forth * (a.q(IU, i - 1, j - 1, k) + a.q(IU, i - 1, j, k) + a.q(IU, i, j - 1, k) + a.q(IU, i, j, k));
+    T v = forth * (a.q(IV, i - 1, j - 1, k) + a.q(IV, i - 1, j, k) + a.q(IV, i, j - 1, k) + a.q(IV, i, j, k));
+    T A = half * (a.bf(0, i, j - 1, k) + a.bf(0, i, j, k));
+    T B = half * (a.bf(1, i - 1, j, k) + a.bf(1, i, j, k));
+    T e = u * B - v * A;
+    if ((a.G.omega0 > 0.0) && !a.G.fargo) {
+        T shear = (T)(-1.5 * a.G.omega0 * 0.5 * (a.G.xc(i) + a.G.xc(i - 1)));
+        e = e - shear * A;
+    }
+    return e;
+}
+// trace2d's edge field (scheme.f90:856-872)
+template <typename T>
+__device__ __forceinline__ T Ez2_at(const QV<T> &a, int i, int j) {
+    const int k = 1;
+    T u = T(0.25) * (a.q(IU, i - 1, j - 1, k) + a.q(IU, i - 1, j, k) + a.q(IU, i, j - 1, k) + a.q(IU, i, j, k));
+    T v = T(0.25) * (a.q(IV, i - 1, j - 1, k) + a.q(IV, i - 1, j, k) + a.q(IV, i, j - 1, k) + a.q(IV, i, j, k));
+    T A = T(0.5) * (a.bf(0, i, j - 1, k) + a.bf(0, i, j, k));
+    T B = T(0.5) * (a.bf(1, i - 1, j, k) + a.bf(1, i, j, k));
+    return u * B - v * A;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_efield3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf,
+                                                       T *__restrict__ Ex, T *__restrict__ Ey, T *__restrict__ Ez) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.esz) return;
+    const int i = (int)(t % G.EX);
+    const long long rr = t / G.EX;
+    const int j = (int)(rr % G.EY);
+    const int k = (int)(rr / G.EY) + G.ke0;
+    const QV<T> a{Q, Bf, G};
+    Ex[t] = Ex_at(a, i, j, k);
+    Ey[t] = Ey_at(a, i, j, k);
+    Ez[t] = Ez_at(a, i, j, k);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_efield2d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf,
+                                                       T *__restrict__ Ez) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.esz) return;
+    const int i = (int)(t % G.EX);
+    const int j = (int)(t / G.EX);
+    const QV<T> a{Q, Bf, G};
+    Ez[t] = Ez2_at(a, i, j);
+}
+
+// limited cell slopes of one variable in the three directions (slope_type 1..3)
+template <typename T>
+__device__ __forceinline__ void cell_slopes3(const QV<T> &a, int v, int i, int j, int k, T d[3]) {
+    const int st = a.G.slope_type;
+    if (st == 0) { d[0] = d[1] = d[2] = T(0); return; }
+    const T c = a.q(v, i, j, k);
+    if (st < 3) {
+        const T s = (T)st;
+        d[0] = limit1(s, a.q(v, i - 1, j, k), c, a.q(v, i + 1, j, k));
+        d[1] = limit1(s, a.q(v, i, j - 1, k), c, a.q(v, i, j + 1, k));
+        d[2] = limit1(s, a.q(v, i, j, k - 1), c, a.q(v, i, j, k + 1));
+        return;
+    }
+    // multidimensional limiter, scheme.f90:484-557
+    const T half = T(0.5), one = T(1);
+    T vmin = T(0), vmax = T(0);
+    bool first = true;
+    for (int dk = -1; dk <= 1; dk++)
+        for (int di = -1; di <= 1; di++)
+            for (int dj = -1; dj <= 1; dj++) {
+                T e = a.q(v, i + di, j + dj, k + dk) - c;
+                if (first) { vmin = e; vmax = e; first = false; }
+                else { vmin = mn(vmin, e); vmax = mx(vmax, e); }
+            }
+    T dfx = half * (a.q(v, i + 1, j, k) - a.q(v, i - 1, j, k));
+    T dfy = half * (a.q(v, i, j + 1, k) - a.q(v, i, j - 1, k));
+    T dfz = half * (a.q(v, i, j, k + 1) - a.q(v, i, j, k - 1));
+    T dff = half * (fab(dfx) + fab(dfy) + fab(dfz));
+    T slop = (dff > T(0)) ? mn(one, mn(fab(vmin), fab(vmax)) / dff) : one;
+    d[0] = slop * dfx; d[1] = slop * dfy; d[2] = slop * dfz;
+}
+
+template <typename T>
+__device__ __forceinline__ void cell_slopes2(const QV<T> &a, int v, int i, int j, T d[2]) {
+    const int st = a.G.slope_type, k = 1;
+    if (st == 0) { d[0] = d[1] = T(0); return; }
+    const T c = a.q(v, i, j, k);
+    if (st < 3) {
+        const T s = (T)st;
+        d[0] = limit1(s, a.q(v, i - 1, j, k), c, a.q(v, i + 1, j, k));
+        d[1] = limit1(s, a.q(v, i, j - 1, k), c, a.q(v, i, j + 1, k));
+        return;
+    }
+    // scheme.f90:355-391, including its choice of neighbours
+    const T half = T(0.5), one = T(1);
+    T e[9] = {a.q(v, i - 1, j - 1, k) - c, a.q(v, i - 1, j, k) - c, a.q(v, i, j - 1, k) - c,
+              a.q(v, i, j - 1, k) - c,     a.q(v, i, j, k) - c,     a.q(v, i, j + 1, k) - c,
+              a.q(v, i + 1, j - 1, k) - c, a.q(v, i + 1, j, k) - c, a.q(v, i + 1, j + 1, k) - c};
+    T vmin = e[0], vmax = e[0];
+#pragma unroll
+    for (int n = 1; n < 9; n++) { vmin = mn(vmin, e[n]); vmax = mx(vmax, e[n]); }
+    T dfx = half * (a.q(v, i + 1, j, k) - a.q(v, i - 1, j, k));
+    T dfy = half * (a.q(v, i, j + 1, k) - a.q(v, i, j - 1, k));
+    T dff = half * (fab(dfx) + fab(dfy));
+    T slop = (dff > T(0)) ? mn(one, mn(fab(vmin), fab(vmax)) / dff) : one;
+    d[0] = slop * dfx; d[1] = slop * dfy;
+}
+
+// transverse slope of a face-B component c (0,1,2) at face (i,j,k) along direction dir
+template <typename T>
+__device__ __forceinline__ T face_slope(const QV<T> &a, int c, int dir, int i, int j, int k) {
+    const int st = a.G.slope_type;
+    if (st == 0) return T(0);
+    const T s = (T)mn(st, 2);
+    int di = dir == 0, dj = dir == 1, dk = dir == 2;
+    return limit1(s, a.bf(c, i - di, j - dj, k - dk), a.bf(c, i, j, k), a.bf(c, i + di, j + dj, k + dk));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? 3 : 4))
+k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
+          const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.csz) return;
+    const int i = (int)(t % G.CX);
+    const long long rr = t / G.CX;
+    const int j = (int)(rr % G.CY);
+    const int k = (int)(rr / G.CY) + G.kc0;
+    const QV<T> a{Q, Bf, G};
+    const double dtd = S->dt;
+    const T dt = (T)dtd;
+    const T half = T(0.5), gamma = (T)G.gamma;
+    const T dtdx = (T)(dtd / G.dx), dtdy = (T)(dtd / G.dy), dtdz = (T)(dtd / G.dz), dx = (T)G.dx;
+    (void)dt;
+
+    const T r = a.q(IR, i, j, k), u = a.q(IU, i, j, k), v = a.q(IV, i, j, k), w = a.q(IW, i, j, k);
+    const T p = a.q(IP, i, j, k), A = a.q(IA, i, j, k), B = a.q(IB, i, j, k), C = a.q(IC, i, j, k);
+    T d3[3];
+    cell_slopes3(a, IR, i, j, k, d3); const T drx = half * d3[0], dry = half * d3[1], drz = half * d3[2];
+    cell_slopes3(a, IU, i, j, k, d3); const T dux = half * d3[0], duy = half * d3[1], duz = half * d3[2];
+    cell_slopes3(a, IV, i, j, k, d3); const T dvx = half * d3[0], dvy = half * d3[1], dvz = half * d3[2];
+    cell_slopes3(a, IW, i, j, k, d3); const T dwx = half * d3[0], dwy = half * d3[1], dwz = half * d3[2];
+    cell_slopes3(a, IP, i, j, k, d3); const T dpx = half * d3[0], dpy = half * d3[1], dpz = half * d3[2];
+    cell_slopes3(a, IA, i, j, k, d3); const T dAy = half * d3[1], dAz = half * d3[2];
+    cell_slopes3(a, IB, i, j, k, d3); const T dBx = half * d3[0], dBz = half * d3[2];
+    cell_slopes3(a, IC, i, j, k, d3); const T dCx = half * d3[0], dCy = half * d3[1];
+
+    const T AL = a.bf(0, i, j, k), AR = a.bf(0, i + 1, j, k);
+    const T BL = a.bf(1, i, j, k), BR = a.bf(1, i, j + 1, k);
+    const T CL = a.bf(2, i, j, k), CR = a.bf(2, i, j, k + 1);
+    const T dAx = half * (AR - AL), dBy = half * (BR - BL), dCz = half * (CR - CL);
+
+    const T dALy = half * face_slope(a, 0, 1, i, j, k), dARy = half * face_slope(a, 0, 1, i + 1, j, k);
+    const T dALz = half * face_slope(a, 0, 2, i, j, k), dARz = half * face_slope(a, 0, 2, i + 1, j, k);
+    const T dBLx = half * face_slope(a, 1, 0, i, j, k), dBRx = half * face_slope(a, 1, 0, i, j + 1, k);
+    const T dBLz = half * face_slope(a, 1, 2, i, j, k), dBRz = half * face_slope(a, 1, 2, i, j + 1, k);
+    const T dCLx = half * face_slope(a, 2, 0, i, j, k), dCRx = half * face_slope(a, 2, 0, i, j, k + 1);
+    const T dCLy = half * face_slope(a, 2, 1, i, j, k), dCRy = half * face_slope(a, 2, 1, i, j, k + 1);
+
+    const T ELL = ld(Exa + G.eidx(i, j, k)), ELR = ld(Exa + G.eidx(i, j, k + 1));
+    const T ERL = ld(Exa + G.eidx(i, j + 1, k)), ERR = ld(Exa + G.eidx(i, j + 1, k + 1));
+    const T FLL = ld(Eya + G.eidx(i, j, k)), FLR = ld(Eya + G.eidx(i, j, k + 1));
+    const T FRL = ld(Eya + G.eidx(i + 1, j, k)), FRR = ld(Eya + G.eidx(i + 1, j, k + 1));
+    const T GLL = ld(Eza + G.eidx(i, j, k)), GLR = ld(Eza + G.eidx(i, j + 1, k));
+    const T GRL = ld(Eza + G.eidx(i + 1, j, k)), GRR = ld(Eza + G.eidx(i + 1, j + 1, k));
+
+    // source terms, scheme.f90:1351-1389
+    T sr0 = (-u * drx - dux * r) * dtdx + (-v * dry - dvy * r) * dtdy + (-w * drz - dwz * r) * dtdz;
+    T su0 = (-u * dux - (dpx + B * dBx + C * dCx) / r) * dtdx + (-v * duy + B * dAy / r) * dtdy
+          + (-w * duz + C * dAz / r) * dtdz;
+    T sv0 = (-u * dvx + A * dBx / r) * dtdx + (-v * dvy - (dpy + A * dAy + C * dCy) / r) * dtdy
+          + (-w * dvz + C * dBz / r) * dtdz;
+    T sw0 = (-u * dwx + A * dCx / r) * dtdx + (-v * dwy + B * dCy / r) * dtdy
+          + (-w * dwz - (dpz + A * dAz + B * dBz) / r) * dtdz;
+    T sp0 = (-u * dpx - dux * gamma * p) * dtdx + (-v * dpy - dvy * gamma * p) * dtdy
+          + (-w * dpz - dwz * gamma * p) * dtdz;
+    T sA0 = (u * dBy + B * duy - v * dAy - A * dvy) * dtdy + (u * dCz + C * duz - w * dAz - A * dwz) * dtdz;
+    T sB0 = (v * dAx + A * dvx - u * dBx - B * dux) * dtdx + (v * dCz + C * dvz - w * dBz - B * dwz) * dtdz;
+    T sC0 = (w * dAx + A * dwx - u * dCx - C * dux) * dtdx + (w * dBy + B * dwy - v * dCy - C * dvy) * dtdy;
+    if ((G.omega0 > 0.0) && !G.fargo) {
+        const T Omega0 = (T)G.omega0;
+        const T shear = (T)(-1.5 * G.omega0 * G.xc(i));
+        sr0 = sr0 - shear * dry * dtdy;
+        su0 = su0 - shear * duy * dtdy;
+        sv0 = sv0 - shear * dvy * dtdy;
+        sw0 = sw0 - shear * dwy * dtdy;
+        sp0 = sp0 - shear * dpy * dtdy;
+        sA0 = sA0 - shear * dAy * dtdy;
+        sB0 = sB0 + (shear * dAx - T(1.5) * Omega0 * A * dx) * dtdx + shear * dBz * dtdz;
+        sC0 = sC0 - shear * dCy * dtdy;
+    }
+    const T sAL0 = +(GLR - GLL) * dtdy * half - (FLR - FLL) * dtdz * half;
+    const T sAR0 = +(GRR - GRL) * dtdy * half - (FRR - FRL) * dtdz * half;
+    const T sBL0 = -(GRL - GLL) * dtdx * half + (ELR - ELL) * dtdz * half;
+    const T sBR0 = -(GRR - GLR) * dtdx * half + (ERR - ERL) * dtdz * half;
+    const T sCL0 = +(FRL - FLL) * dtdx * half - (ERL - ELL) * dtdy * half;
+    const T sCR0 = +(FRR - FLR) * dtdx * half - (ERR - ELR) * dtdy * half;
+
+    T *o = core + t;
+    const long long cs = G.csz;
+    o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
+    o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
+    o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
+    o[15 * cs] = dry; o[16 * cs] = duy; o[17 * cs] = dvy; o[18 * cs] = dwy; o[19 * cs] = dpy; o[20 * cs] = dAy; o[21 * cs] = dCy;
+    o[22 * cs] = drz; o[23 * cs] = duz; o[24 * cs] = dvz; o[25 * cs] = dwz; o[26 * cs] = dpz; o[27 * cs] = dAz; o[28 * cs] = dBz;
+    o[29 * cs] = AL + sAL0; o[30 * cs] = AR + sAR0; o[31 * cs] = BL + sBL0; o[32 * cs] = BR + sBR0;
+    o[33 * cs] = CL + sCL0; o[34 * cs] = CR + sCR0;
+    o[35 * cs] = dALy; o[36 * cs] = dARy; o[37 * cs] = dALz; o[38 * cs] = dARz;
+    o[39 * cs] = dBLx; o[40 * cs] = dBRx; o[41 * cs] = dBLz; o[42 * cs] = dBRz;
+    o[43 * cs] = dCLx; o[44 * cs] = dCRx; o[45 * cs] = dCLy; o[46 * cs] = dCRy;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_trace2d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf,
+                                                      const T *__restrict__ Eza, T *__restrict__ core,
+                                                      const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.csz) return;
+    const int i = (int)(t % G.CX);
+    const int j = (int)(t / G.CX);
+    const int k = 1;
+    const QV<T> a{Q, Bf, G};
+    const double dtd = S->dt;
+    const T half = T(0.5), gamma = (T)G.gamma;
+    const T dtdx = (T)(dtd / G.dx), dtdy = (T)(dtd / G.dy);
+
+    const T r = a.q(IR, i, j, k), u = a.q(IU, i, j, k), v = a.q(IV, i, j, k), w = a.q(IW, i, j, k);
+    const T p = a.q(IP, i, j, k), A = a.q(IA, i, j, k), B = a.q(IB, i, j, k), C = a.q(IC, i, j, k);
+    const T AL = a.bf(0, i, j, k), AR = a.bf(0, i + 1, j, k);
+    const T BL = a.bf(1, i, j, k), BR = a.bf(1, i, j + 1, k);
+    const T ELL = ld(Eza + G.eidx(i, j, 1)), ELR = ld(Eza + G.eidx(i, j + 1, 1));
+    const T ERL = ld(Eza + G.eidx(i + 1, j, 1)), ERR = ld(Eza + G.eidx(i + 1, j + 1, 1));
+    T d2[2];
+    cell_slopes2(a, IR, i, j, d2); const T drx = half * d2[0], dry = half * d2[1];
+    cell_slopes2(a, IU, i, j, d2); const T dux = half * d2[0], duy = half * d2[1];
+    cell_slopes2(a, IV, i, j, d2); const T dvx = half * d2[0], dvy = half * d2[1];
+    cell_slopes2(a, IW, i, j, d2); const T dwx = half * d2[0], dwy = half * d2[1];
+    cell_slopes2(a, IP, i, j, d2); const T dpx = half * d2[0], dpy = half * d2[1];
+    cell_slopes2(a, IA, i, j, d2); const T dAy = half * d2[1];
+    cell_slopes2(a, IB, i, j, d2); const T dBx = half * d2[0];
+    cell_slopes2(a, IC, i, j, d2); const T dCx = half * d2[0], dCy = half * d2[1];
+    const T dALy = half * face_slope(a, 0, 1, i, j, k), dARy = half * face_slope(a, 0, 1, i + 1, j, k);
+    const T dBLx = half * face_slope(a, 1, 0, i, j, k), dBRx = half * face_slope(a, 1, 0, i, j + 1, k);
+    const T dAx = half * (AR - AL), dBy = half * (BR - BL);
+
+    // scheme.f90:946-967
+    const T sr0 = (-u * drx - dux * r) * dtdx + (-v * dry - dvy * r) * dtdy;
+    const T su0 = (-u * dux - dpx / r - B * dBx / r - C * dCx / r) * dtdx + (-v * duy + B * dAy / r) * dtdy;
+    const T sv0 = (-u * dvx + A * dBx / r) * dtdx + (-v * dvy - dpy / r - A * dAy / r - C * dCy / r) * dtdy;
+    const T sw0 = (-u * dwx + A * dCx / r) * dtdx + (-v * dwy + B * dCy / r) * dtdy;
+    const T sp0 = (-u * dpx - dux * gamma * p) * dtdx + (-v * dpy - dvy * gamma * p) * dtdy;
+    const T sA0 = (u * dBy + B * duy - v * dAy - A * dvy) * dtdy;
+    const T sB0 = (-u * dBx - B * dux + v * dAx + A * dvx) * dtdx;
+    T sC0 = (w * dAx + A * dwx - u * dCx - C * dux) * dtdx + (-v * dCy - C * dvy + w * dBy + B * dwy) * dtdy;
+    if (G.omega0 > 0.0) {
+        const T Omega0 = (T)G.omega0;
+        const T shear = (T)(-1.5 * G.omega0 * G.xc(i));
+        sC0 = sC0 + (shear * dAx - T(1.5) * Omega0 * A) * dtdx + shear * dBy * dtdy;
+    }
+    const T sAL0 = +(ELR - ELL) * half * dtdy;
+    const T sAR0 = +(ERR - ERL) * half * dtdy;
+    const T sBL0 = -(ERL - ELL) * half * dtdx;
+    const T sBR0 = -(ERR - ELR) * half * dtdx;
+
+    T *o = core + t;
+    const long long cs = G.csz;
+    o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
+    o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
+    o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
+    o[15 * cs] = dry; o[16 * cs] = duy; o[17 * cs] = dvy; o[18 * cs] = dwy; o[19 * cs] = dpy; o[20 * cs] = dAy; o[21 * cs] = dCy;
+    o[22 * cs] = AL + sAL0; o[23 * cs] = AR + sAR0; o[24 * cs] = BL + sBL0; o[25 * cs] = BR + sBR0;
+    o[26 * cs] = dALy; o[27 * cs] = dARy; o[28 * cs] = dBLx; o[29 * cs] = dBRx;
+}
+
+// ---------------------------------------------------------------------------
+// Riemann fluxes and edge EMFs from the core
+// ---------------------------------------------------------------------------
+// core field slots, 3D
+enum {
+    C_R = 0, C_U, C_V, C_W, C_P, C_A, C_B, C_C,
+    C_DRX = 8, C_DUX, C_DVX, C_DWX, C_DPX, C_DBX, C_DCX,
+    C_DRY = 15, C_DUY, C_DVY, C_DWY, C_DPY, C_DAY, C_DCY,
+    C_DRZ = 22, C_DUZ, C_DVZ, C_DWZ, C_DPZ, C_DAZ, C_DBZ,
+    C_AL = 29, C_AR, C_BL, C_BR, C_CL, C_CR,
+    C_DALY = 35, C_DARY, C_DALZ, C_DARZ, C_DBLX, C_DBRX, C_DBLZ, C_DBRZ, C_DCLX, C_DCRX, C_DCLY, C_DCRY
+};
+// core field slots, 2D
+enum {
+    D_R = 0, D_U, D_V, D_W, D_P, D_A, D_B, D_C,
+    D_DRX = 8, D_DUX, D_DVX, D_DWX, D_DPX, D_DBX, D_DCX,
+    D_DRY = 15, D_DUY, D_DVY, D_DWY, D_DPY, D_DAY, D_DCY,
+    D_AL = 22, D_AR, D_BL, D_BR, D_DALY, D_DARY, D_DBLX, D_DBRX
+};
+
+template <typename T>
+struct CoreView {
+    const T *core;
+    long long cs;
+    __device__ __forceinline__ T f(int field, long long c) const { return ld(core + cs * field + c); }
+};
+
+// face state (uin order r,u,v,w,p,A,B,C) of a cell on its minus (sgn=-1, "qp")
+// or plus (sgn=+1, "qm") side in direction d (scheme.f90:1489-1553, 1062-1100)
+template <typename T>
+__device__ __forceinline__ void face_state(const CoreView<T> &cv, long long c, int d, int sgn, int ndim, T smallp,
+                                           T s[8]) {
+    const T r = cv.f(C_R, c), u = cv.f(C_U, c), v = cv.f(C_V, c), w = cv.f(C_W, c), p = cv.f(C_P, c);
+    const int base = (d == 0) ? C_DRX : (ndim == 3 ? (d == 1 ? C_DRY : C_DRZ) : D_DRY);
+    const T dr = cv.f(base + 0, c), du = cv.f(base + 1, c), dv = cv.f(base + 2, c), dw = cv.f(base + 3, c);
+    const T dp = cv.f(base + 4, c);
+    const T smallr = T(kSmallr);
+    if (sgn > 0) {
+        s[IR] = mx(smallr, r + dr); s[IU] = u + du; s[IV] = v + dv; s[IW] = w + dw; s[IP] = mx(smallp, p + dp);
+    } else {
+        s[IR] = mx(smallr, r - dr); s[IU] = u - du; s[IV] = v - dv; s[IW] = w - dw; s[IP] = mx(smallp, p - dp);
+    }
+    const int fAL = ndim == 3 ? C_AL : D_AL;
+    if (d == 0) {
+        const T B = cv.f(C_B, c), C = cv.f(C_C, c), dB = cv.f(base + 5, c), dC = cv.f(base + 6, c);
+        s[IA] = cv.f(sgn > 0 ? fAL + 1 : fAL, c);
+        s[IB] = sgn > 0 ? B + dB : B - dB;
+        s[IC] = sgn > 0 ? C + dC : C - dC;
+    } else if (d == 1) {
+        const T A = cv.f(C_A, c), C = cv.f(C_C, c), dA = cv.f(base + 5, c), dC = cv.f(base + 6, c);
+        s[IA] = sgn > 0 ? A + dA : A - dA;
+        s[IB] = cv.f(sgn > 0 ? fAL + 3 : fAL + 2, c);
+        s[IC] = sgn > 0 ? C + dC : C - dC;
+    } else {
+        const T A = cv.f(C_A, c), B = cv.f(C_B, c), dA = cv.f(base + 5, c), dB = cv.f(base + 6, c);
+        s[IA] = sgn > 0 ? A + dA : A - dA;
+        s[IB] = sgn > 0 ? B + dB : B - dB;
+        s[IC] = cv.f(sgn > 0 ? C_CR : C_CL, c);
+    }
+}
+
+// corner state qXY(c, e) of edge direction e (0 x, 1 y, 2 z); sa/sb = +1/-1 are the
+// signs of the first/second transverse directions (R/L and T/B of the reference names:
+// RT = (+,+), RB = (+,-), LT = (-,+), LB = (-,-)).  scheme.f90:1555-1697 (3D), 1102-1139 (2D)
+template <typename T>
+__device__ __forceinline__ void corner_state(const CoreView<T> &cv, long long c, int e, int sa, int sb, int ndim,
+                                             T smallp, T s[8]) {
+    int b1, b2;
+    if (ndim == 2) { b1 = D_DRX; b2 = D_DRY; }
+    else if (e == 0) { b1 = C_DRY; b2 = C_DRZ; }
+    else if (e == 1) { b1 = C_DRX; b2 = C_DRZ; }
+    else { b1 = C_DRX; b2 = C_DRY; }
+    T x[5];
+#pragma unroll
+    for (int n = 0; n < 5; n++) {
+        const T d1 = cv.f(b1 + n, c), d2 = cv.f(b2 + n, c);
+        const T comb = (sa > 0 ? (sb > 0 ? (+d1 + d2) : (+d1 - d2)) : (sb > 0 ? (-d1 + d2) : (-d1 - d2)));
+        x[n] = cv.f(C_R + n, c) + comb;
+    }
+    s[IR] = mx(T(kSmallr), x[0]); s[IU] = x[1]; s[IV] = x[2]; s[IW] = x[3]; s[IP] = mx(smallp, x[4]);
+    if (ndim == 2) {
+        // qRT: AR+dARy, BR+dBRx ; qRB: AR-dARy, BL+dBLx ; qLT: AL+dALy, BR-dBRx ; qLB: AL-dALy, BL-dBLx
+        const T Af = cv.f(sa > 0 ? D_AR : D_AL, c), dAf = cv.f(sa > 0 ? D_DARY : D_DALY, c);
+        const T Bf = cv.f(sb > 0 ? D_BR : D_BL, c), dBf = cv.f(sb > 0 ? D_DBRX : D_DBLX, c);
+        s[IA] = Af + (sb > 0 ? +dAf : -dAf);
+        s[IB] = Bf + (sa > 0 ? +dBf : -dBf);
+        const T C = cv.f(D_C, c), dCx = cv.f(D_DCX, c), dCy = cv.f(D_DCY, c);
+        s[IC] = C + (sa > 0 ? (sb > 0 ? (+dCx + dCy) : (+dCx - dCy)) : (sb > 0 ? (-dCx + dCy) : (-dCx - dCy)));
+        return;
+    }
+    if (e == 0) {
+        const T A = cv.f(C_A, c), dAy = cv.f(C_DAY, c), dAz = cv.f(C_DAZ, c);
+        s[IA] = A + (sa > 0 ? (sb > 0 ? (+dAy + dAz) : (+dAy - dAz)) : (sb > 0 ? (-dAy + dAz) : (-dAy - dAz)));
+        const T Bf = cv.f(sa > 0 ? C_BR : C_BL, c), dBf = cv.f(sa > 0 ? C_DBRZ : C_DBLZ, c);
+        const T Cf = cv.f(sb > 0 ? C_CR : C_CL, c), dCf = cv.f(sb > 0 ? C_DCRY : C_DCLY, c);
+        s[IB] = sb > 0 ? Bf + dBf : Bf - dBf;
+        s[IC] = sa > 0 ? Cf + dCf : Cf - dCf;
+    } else if (e == 1) {
+        const T Af = cv.f(sa > 0 ? C_AR : C_AL, c), dAf = cv.f(sa > 0 ? C_DARZ : C_DALZ, c);
+        s[IA] = sb > 0 ? Af + dAf : Af - dAf;
+        const T B = cv.f(C_B, c), dBx = cv.f(C_DBX, c), dBz = cv.f(C_DBZ, c);
+        s[IB] = B + (sa > 0 ? (sb > 0 ? (+dBx + dBz) : (+dBx - dBz)) : (sb > 0 ? (-dBx + dBz) : (-dBx - dBz)));
+        const T Cf = cv.f(sb > 0 ? C_CR : C_CL, c), dCf = cv.f(sb > 0 ? C_DCRX : C_DCLX, c);
+        s[IC] = sa > 0 ? Cf + dCf : Cf - dCf;
+    } else {
+        const T Af = cv.f(sa > 0 ? C_AR : C_AL, c), dAf = cv.f(sa > 0 ? C_DARY : C_DALY, c);
+        s[IA] = sb > 0 ? Af + dAf : Af - dAf;
+        const T Bf = cv.f(sb > 0 ? C_BR : C_BL, c), dBf = cv.f(sb > 0 ? C_DBRX : C_DBLX, c);
+        s[IB] = sa > 0 ? Bf + dBf : Bf - dBf;
+        const T C = cv.f(C_C, c), dCx = cv.f(C_DCX, c), dCy = cv.f(C_DCY, c);
+        s[IC] = C + (sa > 0 ? (sb > 0 ? (+dCx + dCy) : (+dCx - dCy)) : (sb > 0 ? (-dCx + dCy) : (-dCx - dCy)));
+    }
+}
+
+// the 1D solver for one interface (solver.f90:163-187)
+template <typename T>
+__device__ __forceinline__ void solve1d(int iriemann, const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso,
+                                        int iso) {
+    switch (iriemann) {
+        case DG_RIEMANN_HLLD: hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso); break;
+        case DG_RIEMANN_HLL: hll1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
+        case DG_RIEMANN_LLF: llf1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
+        default: upwind1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
+    }
+}
+
+#ifdef DG_FACE_SOLVER_HOOK
+// the mixed path may route selected faces to another solver (learned surrogate)
+DG_FACE_SOLVER_HOOK
+#endif
+
+// one face flux in direction d between cells cl (minus side) and cr (plus side);
+// writes the compflux-scaled fluxes in uin order plus p*_T (solver.f90:116-262, scheme.f90:1740-1753)
+template <typename T>
+__device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d, int i, double dtd,
+                          T *__restrict__ out, long long fo, long long fsz) {
+    const T half = T(0.5), one = T(1);
+    const T gamma = (T)G.gamma;
+    const T smallp = (T)(kSmallr * (kSmallc * kSmallc) / G.gamma);
+    T sm[8], sp[8];
+    face_state(cv, cl, d, +1, G.ndim, smallp, sm);
+    face_state(cv, cr, d, -1, G.ndim, smallp, sp);
+    int ln, lt1, lt2, bn, bt1, bt2;
+    if (d == 0) { ln = IU; lt1 = IV; lt2 = IW; bn = IA; bt1 = IB; bt2 = IC; }
+    else if (d == 1) { ln = IV; lt1 = IU; lt2 = IW; bn = IB; bt1 = IA; bt2 = IC; }
+    else { ln = IW; lt1 = IU; lt2 = IV; bn = IC; bt1 = IA; bt2 = IB; }
+    const T bn_mean = half * (sm[bn] + sp[bn]);
+    T ql[8] = {sm[IR], sm[IP], sm[ln], bn_mean, sm[lt1], sm[bt1], sm[lt2], sm[bt2]};
+    T qr[8] = {sp[IR], sp[IP], sp[ln], bn_mean, sp[lt1], sp[bt1], sp[lt2], sp[bt2]};
+    T f[8], pg = T(0);
+#ifdef DG_FACE_SOLVER_HOOK
+    face_solver_hook<T>(G, ql, qr, f, pg, d);
+#else
+    solve1d<T>(G.iriemann, ql, qr, f, pg, gamma, (T)G.ciso, G.iso);
+#endif
+    // shearing-box upwind terms (solver.f90:199-241)
+    if (G.ndim == 2) {
+        if (G.omega0 > 0.0) {
+            double shear = -1.5 * G.omega0 * G.xc(i);
+            if (d == 0) shear = -1.5 * G.omega0 * (G.xc(i) + G.xc(i - 1));
+            if (d == 1) shear = -1.5 * G.omega0 * G.xc(i);
+            f[7] = f[7] + (T)shear * bn_mean;
+        }
+    } else if ((G.omega0 > 0.0) && (d == 1) && !G.fargo) {
+        const T shear = (T)(-1.5 * G.omega0 * G.xc(i));
+        const T *qs = (shear > T(0)) ? ql : qr;
+        const T rs = qs[0], ps = qs[1], us = qs[2], as = qs[3], vs = qs[4], bs = qs[5], ws = qs[6], cs = qs[7];
+        const T Emag = half * (as * as + bs * bs + cs * cs);
+        const T Ekin = half * (us * us + vs * vs + ws * ws);
+        const T Etot = Ekin + Emag + ps / (gamma - one);
+        f[0] = f[0] + shear * rs;
+        f[1] = f[1] + shear * (Etot + Emag - bn_mean * bn_mean);
+        f[2] = f[2] + shear * rs * us;
+        f[4] = f[4] + shear * rs * vs;
+        f[6] = f[6] + shear * rs * ws;
+    }
+    // compflux: flux = fgodunov*ds*dt, reordered to uin variables
+    double dsd;
+    if (d == 0) dsd = G.dy * G.dz; else if (d == 1) dsd = G.dx * G.dz; else dsd = G.dx * G.dy;
+    const T ds = (T)dsd, dt = (T)dtd;
+    T *o = out + fo;
+    o[0 * fsz] = f[0] * ds * dt;                 // rho
+    o[1 * fsz] = f[1] * ds * dt;                 // E
+    o[(2 + ln - IU) * fsz] = f[2] * ds * dt;      // normal momentum
+    o[(2 + lt1 - IU) * fsz] = f[4] * ds * dt;     // first tangential momentum
+    o[(2 + lt2 - IU) * fsz] = f[6] * ds * dt;     // second tangential momentum
+    o[5 * fsz] = pg;                             // p*_T (zero unless HLLD)
+    if (G.ndim == 2) o[6 * fsz] = f[7] * ds * dt;  // B_t2 = B_z
+}
+
+// one edge EMF (riemann_solver_magnetic, solver_magnetic.f90:79-230); e = edge direction
+template <typename T>
+__device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long long cRL, long long cLR, long long cRR,
+                      int e, int i, double dtd) {
+    const T half = T(0.5);
+    const T smallp = (T)(kSmallr * (kSmallc * kSmallc) / G.gamma);
+    T sLL[8], sRL[8], sLR[8], sRR[8];
+    int lt1, lt2, bn, bt1, bt2;
+    if (e == 0) {
+        // qLL <- qRT(i,j-1,k-1), qRL <- qLT(i,j,k-1), qLR <- qRB(i,j-1,k), qRR <- qLB(i,j,k)
+        corner_state(cv, cLL, 0, +1, +1, G.ndim, smallp, sLL);
+        corner_state(cv, cRL, 0, -1, +1, G.ndim, smallp, sRL);
+        corner_state(cv, cLR, 0, +1, -1, G.ndim, smallp, sLR);
+        corner_state(cv, cRR, 0, -1, -1, G.ndim, smallp, sRR);
+        lt1 = IV; lt2 = IW; bn = IA; bt1 = IB; bt2 = IC;
+    } else if (e == 1) {
+        // call site passes (qRT, qLT, qRB, qLB): qLL <- qRT(i-1,j,k-1), qRL <- qRB(i-1,j,k),
+        // qLR <- qLT(i,j,k-1), qRR <- qLB(i,j,k)
+        corner_state(cv, cLL, 1, +1, +1, G.ndim, smallp, sLL);
+        corner_state(cv, cRL, 1, +1, -1, G.ndim, smallp, sRL);
+        corner_state(cv, cLR, 1, -1, +1, G.ndim, smallp, sLR);
+        corner_state(cv, cRR, 1, -1, -1, G.ndim, smallp, sRR);
+        lt1 = IW; lt2 = IU; bn = IB; bt1 = IC; bt2 = IA;
+    } else {
+        // qLL <- qRT(i-1,j-1,k), qRL <- qLT(i,j-1,k), qLR <- qRB(i-1,j,k), qRR <- qLB(i,j,k)
+        corner_state(cv, cLL, 2, +1, +1, G.ndim, smallp, sLL);
+        corner_state(cv, cRL, 2, -1, +1, G.ndim, smallp, sRL);
+        corner_state(cv, cLR, 2, +1, -1, G.ndim, smallp, sLR);
+        corner_state(cv, cRR, 2, -1, -1, G.ndim, smallp, sRR);
+        lt1 = IU; lt2 = IV; bn = IC; bt1 = IA; bt2 = IB;
+    }
+    T qLL[8], qRL[8], qLR[8], qRR[8];
+    qLL[0] = sLL[IR]; qRL[0] = sRL[IR]; qLR[0] = sLR[IR]; qRR[0] = sRR[IR];
+    if (G.iso) {
+        const T c2 = (T)(G.ciso * G.ciso);
+        qLL[1] = qLL[0] * c2; qRL[1] = qRL[0] * c2; qLR[1] = qLR[0] * c2; qRR[1] = qRR[0] * c2;
+    } else {
+        qLL[1] = sLL[IP]; qRL[1] = sRL[IP]; qLR[1] = sLR[IP]; qRR[1] = sRR[IP];
+    }
+    qLL[2] = sLL[lt1]; qRL[2] = sRL[lt1]; qLR[2] = sLR[lt1]; qRR[2] = sRR[lt1];
+    qLL[3] = sLL[lt2]; qRL[3] = sRL[lt2]; qLR[3] = sLR[lt2]; qRR[3] = sRR[lt2];
+    qLL[4] = half * (sLL[bt1] + sRL[bt1]);
+    qRL[4] = half * (sLL[bt1] + sRL[bt1]);
+    qLR[4] = half * (sLR[bt1] + sRR[bt1]);
+    qRR[4] = half * (sLR[bt1] + sRR[bt1]);
+    qLL[5] = half * (sLL[bt2] + sLR[bt2]);
+    qRL[5] = half * (sRL[bt2] + sRR[bt2]);
+    qLR[5] = half * (sLL[bt2] + sLR[bt2]);
+    qRR[5] = half * (sRL[bt2] + sRR[bt2]);
+    qLL[6] = sLL[bn]; qRL[6] = sRL[bn]; qLR[6] = sLR[bn]; qRR[6] = sRR[bn];
+    qLL[7] = qLL[2] * qLL[5] - qLL[3] * qLL[4];
+    qRL[7] = qRL[2] * qRL[5] - qRL[3] * qRL[4];
+    qLR[7] = qLR[2] * qLR[5] - qLR[3] * qLR[4];
+    qRR[7] = qRR[2] * qRR[5] - qRR[3] * qRR[4];
+    Corners<T> c;
+    c.rLL = qLL[0]; c.uLL = qLL[2]; c.ALL = qLL[4]; c.CLL = qLL[6];
+    c.rRL = qRL[0]; c.uRL = qRL[2]; c.ARL = qRL[4]; c.CRL = qRL[6];
+    c.rLR = qLR[0]; c.uLR = qLR[2]; c.ALR = qLR[4]; c.CLR = qLR[6];
+    c.rRR = qRR[0]; c.uRR = qRR[2]; c.ARR = qRR[4]; c.CRR = qRR[6];
+    c.pLL = qLL[1]; c.vLL = qLL[3]; c.BLL = qLL[5]; c.ELL = qLL[7];
+    c.pRL = qRL[1]; c.vRL = qRL[3]; c.BRL = qRL[5]; c.ERL = qRL[7];
+    c.pLR = qLR[1]; c.vLR = qLR[3]; c.BLR = qLR[5]; c.ELR = qLR[7];
+    c.pRR = qRR[1]; c.vRR = qRR[3]; c.BRR = qRR[5]; c.ERR = qRR[7];
+    const T dt = (T)dtd, gamma = (T)G.gamma;
+    T emf;
+    switch (G.iriemann2d) {
+        case DG_RIEMANN_HLLD: emf = hlld2d<T>(c, dt, gamma); break;
+        case DG_RIEMANN_LLF: emf = llf2d<T>(c, dt, gamma, (T)G.ciso, G.iso); break;
+        case DG_RIEMANN_HLLA: emf = hlla2d<T>(c, dt); break;
+        default: emf = upwind2d<T>(c, dt); break;
+    }
+    if ((G.omega0 > 0.0) && !G.fargo) {
+        if (e == 0) {
+            const T shear = (T)(-1.5 * G.omega0 * G.xc(i));
+            if (shear > T(0)) emf = emf + shear * c.BLL * dt;
+            else emf = emf + shear * c.BRR * dt;
+        } else if (e == 2) {
+            const T shear = (T)(-1.5 * G.omega0 * 0.5 * (G.xc(i) + G.xc(i - 1)));
+            if (shear > T(0)) emf = emf - shear * c.ALL * dt;
+            else emf = emf - shear * c.ARR * dt;
+        }
+    }
+    return emf;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
+                                                           T *__restrict__ fy, T *__restrict__ fz, T *__restrict__ ex,
+                                                           T *__restrict__ ey, T *__restrict__ ez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const double dt = S->dt;
+    const CoreView<T> cv{core, G.csz};
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const long long c = G.cidx(i, j, k);
+    if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t, G.fsz);
+    if (i <= nx && k <= nz) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t, G.fsz);
+    if (i <= nx && j <= ny) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t, G.fsz);
+    if (k <= nz) ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
+    if (j <= ny) ey[t] = edge_emf(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
+    if (i <= nx) ex[t] = edge_emf(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
+                                                        T *__restrict__ fy, T *__restrict__ ez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const int j = (int)(t / G.FX) + 1;
+    const double dt = S->dt;
+    const CoreView<T> cv{core, G.csz};
+    const long long c = G.cidx(i, j, 1);
+    if (j <= G.ny) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t, G.fsz);
+    if (i <= G.nx) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t, G.fsz);
+    ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, 1), G.cidx(i, j - 1, 1), G.cidx(i - 1, j, 1), c, 2, i, dt);
+}
+
+// ---------------------------------------------------------------------------
+// update + constrained transport
+// ---------------------------------------------------------------------------
+struct ShearRemap {
+    double epsi;
+    int jp;
+};
+// shear offset of the x boundaries at time itime (shearingbox.f90:34-37)
+__device__ __forceinline__ ShearRemap shear_offset(const Geo &G, double itime) {
+    double deltay = 1.5 * G.omega0 * (G.xmax - G.xmin) * itime;
+    deltay = fmod(deltay, (G.ymax - G.ymin));
+    ShearRemap s;
+    s.epsi = fmod(deltay, G.dy);
+    s.jp = (int)(deltay / G.dy);
+    return s;
+}
+
+// Any y index into [1, n].  Equal to the reference's single "+/- ny" wrap whenever
+// that wrap lands inside the active range; the reference reads a ghost row or
+// unallocated memory otherwise (a shift of a full box or more), which this guard
+// keeps inside the array.
+__device__ __forceinline__ int wrap1(int j, int n) {
+    if (j >= 1 && j <= n) return j;
+    int m = (j - 1) % n;
+    return (m < 0 ? m + n : m) + 1;
+}
+
+// shearing_flux / shearing_emf average of a face quantity on the inner (side 0)
+// or outer (side 1) x boundary (shearingbox.f90:250-280, 339-380)
+template <typename T>
+__device__ __forceinline__ T shear_avg(const Geo &G, const ShearRemap &sr, const T *a, long long comp_off, int side,
+                                       int j, int k) {
+    const int ny = G.ny;
+    const T one = T(1), half = T(0.5);
+    if (side == 0) {
+        int jremap = j - sr.jp - 1, jremapp = jremap + 1;
+        if (jremap <= 0) jremap = jremap + ny;
+        if (jremapp <= 0) jremapp = jremapp + ny;
+        jremap = wrap1(jremap, ny);
+        jremapp = wrap1(jremapp, ny);
+        const T eps = (T)(1.0 - sr.epsi / G.dy);
+        T v = ld(a + comp_off + G.fidx(1, j, k)) + (one - eps) * ld(a + comp_off + G.fidx(G.nx + 1, jremap, k))
+            + eps * ld(a + comp_off + G.fidx(G.nx + 1, jremapp, k));
+        return half * v;
+    } else {
+        int jremap = j + sr.jp, jremapp = jremap + 1;
+        if (jremap > ny) jremap = jremap - ny;
+        if (jremapp > ny) jremapp = jremapp - ny;
+        jremap = wrap1(jremap, ny);
+        jremapp = wrap1(jremapp, ny);
+        const T eps = (T)(sr.epsi / G.dy);
+        T v = ld(a + comp_off + G.fidx(G.nx + 1, j, k)) + (one - eps) * ld(a + comp_off + G.fidx(1, jremap, k))
+            + eps * ld(a + comp_off + G.fidx(1, jremapp, k));
+        return half * v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// boundary: every ghost value written from active values in one pass
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int map_bc(int type, int i, int n) {
+    if (i >= 1 && i <= n) return i;
+    if (type == DG_BC_ZERO_GRADIENT) return i < 1 ? 1 : n;
+    // periodic (and y/z of the shearing box)
+    return i < 1 ? i + n : i - n;
+}
+
+// the limiter of shearing_slope (shearingbox.f90:415-430), at y index j, FP64
+template <class Store>
+__device__ __forceinline__ double sslope(const Geo &G, const Store &U, int v, int i, int j, int k) {
+    const int st = mn(G.slope_type, 2);
+    if (st == 0) return 0.0;
+    auto val = [&](int jj) { return U.get(G, v, G.idx(i, map_bc(G.bc[1], jj, G.ny), k)); };
+    if (v == IB) return val(j + 1) - val(j);  // By: one-sided difference (shearingbox.f90:493-499)
+    return limit1<double>((double)st, val(j - 1), val(j), val(j + 1));
+}
+
+// shear-periodic x ghost value of variable v at ghost cell i, active (j,k) (shearingbox.f90:62-147)
+template <class Store>
+__device__ double shear_ghost(const Geo &G, const Store &U, const ShearRemap &sr, int v, int i, int j, int k) {
+    const int nx = G.nx, ny = G.ny;
+    const double one = 1.0, half = 0.5;
+    auto val = [&](int ii, int jj) { return U.get(G, v, G.idx(ii, map_bc(G.bc[1], jj, ny), k)); };
+    if (i < 1) {
+        const int src = nx + i;  // outer(1:3) = uin(nx-2:nx) feeds ghosts iu1..iu1+2
+        int jremap = j - sr.jp - 1, jremapp = jremap + 1;
+        if (jremap <= 0) jremap = jremap + ny;
+        if (jremapp <= 0) jremapp = jremapp + ny;
+        const double eps = one - sr.epsi / G.dy;
+        const double lambda = half * eps * (eps - one);
+        if (v == IB) return val(src, jremap) + eps * sslope(G, U, v, src, jremap, k);
+        return (one - eps) * val(src, jremap) + eps * val(src, jremapp)
+             + lambda * (sslope(G, U, v, src, jremap, k) - sslope(G, U, v, src, jremapp, k));
+    }
+    const int src = i - nx;  // inner(1:3) = uin(1:3) feeds ghosts iu2-2..iu2
+    int jremap = j + sr.jp, jremapp = jremap + 1;
+    if (jremap > ny) jremap = jremap - ny;
+    if (jremapp > ny) jremapp = jremapp - ny;
+    const double eps = sr.epsi / G.dy;
+    const double lambda = half * eps * (eps - one);
+    if (v == IB) return val(src, jremap) + eps * sslope(G, U, v, src, jremap, k);
+    return (one - eps) * val(src, jremap) + eps * val(src, jremapp)
+         + lambda * (sslope(G, U, v, src, jremapp, k) - sslope(G, U, v, src, jremap, k));
+}
+
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, const Scalars *S) {
+    const long long n = (long long)G.NX * G.NY * G.NZ;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)(t % G.NX) - 2;
+    const long long r = t / G.NX;
+    const int j = (G.ndim > 1) ? (int)(r % G.NY) - 2 : 1;
+    const int k = (G.ndim == 3) ? (int)(r / G.NY) - 2 : 1;
+    const bool gx = (i < 1 || i > G.nx), gy = (G.ndim > 1) && (j < 1 || j > G.ny), gz = (G.ndim == 3) && (k < 1 || k > G.nz);
+    if (!gx && !gy && !gz) return;
+    const int jj = (G.ndim > 1) ? map_bc(G.bc[1], j, G.ny) : 1;
+    const int kk = (G.ndim == 3) ? map_bc(G.bc[2], k, G.nz) : 1;
+    const long long c = t;
+    if (!gx || G.bc[0] != DG_BC_SHEARINGBOX) {
+        const int ii = map_bc(G.bc[0], i, G.nx);
+        const long long src = G.idx(ii, jj, kk);
+        for (int v = 0; v < nv; v++) U.set(G, v, c, U.get(G, v, src));
+        return;
+    }
+    // shear-periodic x ghost (only with ndim = 3)
+    const ShearRemap sr = shear_offset(G, S->time + S->dt);
+    for (int v = 0; v < nv; v++) {
+        if (v == IA && i == G.nx + 1) {
+            // the outer face keeps its own (CT-updated) value; ghost j/k copy it
+            if (jj != j || kk != k) U.set(G, v, c, U.get(G, v, G.idx(i, jj, kk)));
+            continue;
+        }
+        U.set(G, v, c, shear_ghost(G, U, sr, v, i, jj, kk));
+    }
+}
+
+// right-face B (uin vars 9-11) of the reference layout, from the stored left faces
+template <class Store>
+__global__ void k_right_faces(Geo G, Store U, double *__restrict__ out) {
+    const long long n = (long long)G.NX * G.NY * G.NZ;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)(t % G.NX);
+    const long long r = t / G.NX;
+    const int j = (int)(r % G.NY);
+    const int k = (int)(r / G.NY);
+    // last layer of each direction: no neighbour, keep the left-face value
+    out[t] = (i + 1 < G.NX) ? U.get(G, IA, t + 1) : U.get(G, IA, t);
+    out[n + t] = (G.ndim > 1 && j + 1 < G.NY) ? U.get(G, IB, t + G.sy) : U.get(G, IB, t);
+    if (G.ndim == 3) out[2 * n + t] = (k + 1 < G.NZ) ? U.get(G, IC, t + G.sz) : U.get(G, IC, t);
+    else out[2 * n + t] = U.get(G, 8, t);
+}
+
+// state <-> FP64 planes (upload/download of the compensated state)
+template <class Store>
+__global__ void k_state_to_f64(Geo G, Store U, int nv, double *__restrict__ out) {
+    const long long n = G.sv * nv;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    out[t] = U.get(G, (int)(t / G.sv), t % G.sv);
+}
+template <class Store>
+__global__ void k_f64_to_state(Geo G, const double *__restrict__ in, int nv, Store U) {
+    const long long n = G.sv * nv;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    U.set(G, (int)(t / G.sv), t % G.sv, in[t]);
+}
+
+// ---------------------------------------------------------------------------
+// FARGO, fargo.f90:17-288 (FP64 arithmetic on the state in both paths)
+// ---------------------------------------------------------------------------
+struct FargoShift {
+    double vK, eps;
+    int nshft;
+};
+__device__ __forceinline__ FargoShift fargo_shift(const Geo &G, double xpos, double dt) {
+    FargoShift f;
+    f.vK = -1.5 * G.omega0 * xpos;
+    f.nshft = (int)(fabs(f.vK * dt) / G.dy);
+    f.eps = fmod(fabs(f.vK * dt), G.dy);
+    f.eps = f.eps / G.dy;
+    return f;
+}
+
+// uin_slope of variable v at (i, j, k) with y wrap (fargo.f90:266-280)
+template <class Store>
+__device__ __forceinline__ double fslope(const Geo &G, const Store &U, int v, int i, int j, int k) {
+    const int st = mn(G.slope_type, 2);
+    if (st == 0) return 0.0;
+    auto val = [&](int jj) { return U.getr(G, v, G.idx(i, map_bc(G.bc[1], jj, G.ny), k)); };
+    return limit1<double>((double)st, val(j - 1), val(j), val(j + 1));
+}
+
+// emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_fargo_emf(Geo G, Store U, double *__restrict__ fex,
+                                                        double *__restrict__ fez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const double dt = S->dt, dy = G.dy, half = 0.5, one = 1.0;
+    const int ny = G.ny;
+    const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
+    auto B = [&](int v, int ii, int jj) { return U.getr(G, v, G.idx(ii, jj, kw)); };
+    if (i <= G.nx) {  // get_emfx, fargo.f90:146-177
+        const FargoShift f = fargo_shift(G, G.xc(i), dt);
+        double e = 0.0;
+        if (f.vK > 0.0) {
+            const double lambda = half * f.eps * (one - f.eps);
+            for (int jj = 1; jj <= f.nshft; jj++) {
+                int js = j - jj;
+                if (js < 1) js = js + ny;
+                e = e + B(IC, i, wrap1(js, ny)) * dy;
+            }
+            int js = j - f.nshft - 1;
+            if (js < 1) js = js + ny;
+            js = wrap1(js, ny);
+            const double demf = f.eps * B(IC, i, js) + lambda * fslope(G, U, IC, i, js, kw);
+            e = e + demf * dy;
+        } else {
+            const double lambda = half * f.eps * (f.eps - one);
+            for (int jj = 0; jj <= f.nshft - 1; jj++) {
+                int js = j + jj;
+                if (js > ny) js = js - ny;
+                e = e - B(IC, i, wrap1(js, ny)) * dy;
+            }
+            int js = j + f.nshft;
+            if (js > ny) js = js - ny;
+            js = wrap1(js, ny);
+            const double demf = -f.eps * B(IC, i, js) - lambda * fslope(G, U, IC, i, js, kw);
+            e = e + demf * dy;
+        }
+        fex[t] = e;
+    }
+    if (k <= G.nz) {  // get_emfz, fargo.f90:204-235
+        const FargoShift f = fargo_shift(G, half * (G.xc(i) + G.xc(i - 1)), dt);
+        double e = 0.0;
+        if (f.vK > 0.0) {
+            const double lambda = half * f.eps * (one - f.eps);
+            for (int jj = 1; jj <= f.nshft; jj++) {
+                int js = j - jj;
+                if (js < 1) js = js + ny;
+                e = e - B(IA, i, wrap1(js, ny)) * dy;
+            }
+            int js = j - f.nshft - 1;
+            if (js < 1) js = js + ny;
+            js = wrap1(js, ny);
+            const double demf = f.eps * B(IA, i, js) + lambda * fslope(G, U, IA, i, js, kw);
+            e = e - demf * dy;
+        } else {
+            const double lambda = half * f.eps * (f.eps - one);
+            for (int jj = 0; jj <= f.nshft - 1; jj++) {
+                int js = j + jj;
+                if (js > ny) js = js - ny;
+                e = e + B(IA, i, wrap1(js, ny)) * dy;
+            }
+            int js = j + f.nshft;
+            if (js > ny) js = js - ny;
+            js = wrap1(js, ny);
+            const double demf = -f.eps * B(IA, i, js) - lambda * fslope(G, U, IA, i, js, kw);
+            e = e - demf * dy;
+        }
+        fez[t] = e;
+    }
+}
+
+// remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119)
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_fargo_update(Geo G, Store U, Store Un, const double *__restrict__ fex,
+                                                           const double *__restrict__ fez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const double dt = S->dt, half = 0.5, forth = 0.25, one = 1.0;
+    const long long c = G.idx(i, j, k);
+    if (i <= nx && j <= ny && k <= nz) {
+        const FargoShift f = fargo_shift(G, G.xc(i), dt);
+        int js, jsp;
+        if (f.vK > 0.0) {
+            js = j - f.nshft - 1;
+            if (js < 1) js = js + ny;
+            jsp = js + 1;
+            if (jsp > ny) jsp = jsp - ny;
+        } else {
+            js = j + f.nshft;
+            if (js > ny) js = js - ny;
+            jsp = js + 1;
+            if (jsp > ny) jsp = jsp - ny;
+        }
+        js = wrap1(js, ny);
+        jsp = wrap1(jsp, ny);
+        const double hme = half - f.eps;
+        for (int v = IR; v <= IP; v++) {
+            const double a0 = U.getr(G, v, G.idx(i, js, k)), a1 = U.getr(G, v, G.idx(i, jsp, k));
+            double val = (f.vK > 0.0) ? a0 * f.eps + a1 * (one - f.eps) : a0 * (one - f.eps) + a1 * f.eps;
+            val = val + half * fslope(G, U, v, i, js, k) * (forth - hme * hme)
+                      + half * fslope(G, U, v, i, jsp, k) * (hme * hme - forth);
+            Un.set(G, v, c, val);
+        }
+    }
+    const double dx = G.dx, dy = G.dy, dz = G.dz;
+    auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, jj, kk)); };
+    auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, jj, kk)) : 0.0; };
+    if (j <= ny && k <= nz) {
+        Un.set(G, IA, c, U.getr(G, IA, c) + (EZ(i, j + 1, k) - EZ(i, j, k)) / dy);
+    }
+    if (i <= nx && k <= nz) {
+        Un.set(G, IB, c, U.getr(G, IB, c) - (EZ(i + 1, j, k) - EZ(i, j, k)) / dx + (EX(i, j, k + 1) - EX(i, j, k)) / dz);
+    }
+    if (i <= nx && j <= ny) {
+        Un.set(G, IC, c, U.getr(G, IC, c) - (EX(i, j + 1, k) - EX(i, j, k)) / dy);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MRI history sums (src/problem/mri/history.f90:60-125), FP64
+// ---------------------------------------------------------------------------
+// pass 1: per-x-column yz sums of vx and vy (compute_yz_mean)
+template <class Store>
+__global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m) {
+    const int i = blockIdx.x + 1;
+    double a = 0.0, b = 0.0;
+    const long long n = (long long)G.ny * G.nz;
+    for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+        const int j = (int)(t % G.ny) + 1, k = (int)(t / G.ny) + 1;
+        const long long c = G.idx(i, j, k);
+        const double d = U.get(G, IR, c);
+        a += U.get(G, IU, c) / d;
+        b += U.get(G, IV, c) / d;
+    }
+    __shared__ double sa[256], sb[256];
+    sa[threadIdx.x] = a; sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) { sa[threadIdx.x] += sa[threadIdx.x + s]; sb[threadIdx.x] += sb[threadIdx.x + s]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        m[2 * (i - 1)] = sa[0] / G.ny / G.nz;
+        m[2 * (i - 1) + 1] = sb[0] / G.ny / G.nz;
+    }
+}
+
+// pass 2: per-block partial sums of the 9 quantities
+template <class Store>
+__global__ void k_hist_sums(Geo G, Store U, const double *__restrict__ m, double *__restrict__ part) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    const double forth = 0.25;
+    const double dtau = G.dx * G.dy * G.dz / (G.xmax - G.xmin) / (G.ymax - G.ymin) / (G.zmax - G.zmin);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // mass, magp, maxwell, Bx, By, Bz, reynolds, divB
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % G.nx) + 1;
+        const long long r = t / G.nx;
+        const int j = (int)(r % G.ny) + 1, k = (int)(r / G.ny) + 1;
+        const long long c = G.idx(i, j, k);
+        const double bxl = U.get(G, IA, c), bxr = U.get(G, IA, c + 1);
+        const double byl = U.get(G, IB, c), byr = U.get(G, IB, c + G.sy);
+        const double bzl = U.get(G, IC, c), bzr = U.get(G, IC, c + G.sz);
+        const double bxc = bxl + bxr, byc = byl + byr, bzc = bzl + bzr;
+        const double d = U.get(G, IR, c);
+        acc[0] += d;
+        acc[1] += forth * (bxc * bxc) + forth * (byc * byc) + forth * (bzc * bzc);
+        acc[2] += -(forth * bxc * byc);
+        acc[3] += bxl; acc[4] += byl; acc[5] += bzl;
+        acc[6] += d * dtau * (U.get(G, IU, c) / d - m[2 * (i - 1)]) * (U.get(G, IV, c) / d - m[2 * (i - 1) + 1]);
+        acc[7] += (bxr - bxl) / G.dx + (byr - byl) / G.dy + (bzr - bzl) / G.dz;
+    }
+    __shared__ double sh[8][256];
+    for (int q = 0; q < 8; q++) sh[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int q = 0; q < 8; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 8; q++) part[8 * blockIdx.x + q] = sh[q][0];
+}
+
+__global__ void k_hist_final(Geo G, const double *__restrict__ part, int nb, double *__restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < nb; b++)
+        for (int q = 0; q < 8; q++) s[q] += part[8 * b + q];
+    const double dtau = G.dx * G.dy * G.dz / (G.xmax - G.xmin) / (G.ymax - G.ymin) / (G.zmax - G.zmin);
+    const double mass = s[0] * dtau, magp = 0.5 * s[1] * dtau, maxwell = s[2] * dtau;
+    out[0] = mass; out[1] = maxwell; out[2] = s[6]; out[3] = maxwell + s[6]; out[4] = magp;
+    out[5] = s[3] * dtau; out[6] = s[4] * dtau; out[7] = s[5] * dtau; out[8] = s[7];
+}
+
+}  // namespace
+}  // namespace DG_NS
+}  // namespace dg

@@ -1,0 +1,87 @@
+"""The mixed-precision path (FP32 trace/Riemann/CT, compensated FP32 hi/lo state,
+FP64 pressure recovery, dt and diagnostics) against the bit-exact FP64 path.
+
+Tolerance: relative L1 error per variable over the active cells,
+sum |u32 - u64| / sum |u64|, below 1e-4 after the stated number of steps (the
+mixed path's goal is <= 1e-3 in rho, E and B after one orbit of the shearing box).
+"""
+import numpy as np
+import pytest
+
+from dumses_hybrid_b200 import Context, Params, condinit
+
+pytestmark = pytest.mark.gpu
+
+
+def l1_rel(a, b):
+    den = np.sum(np.abs(b))
+    return float(np.sum(np.abs(a - b)) / den) if den > 0 else float(np.sum(np.abs(a - b)))
+
+
+def active(u, p):
+    if p.ndim == 3:
+        return u[3:-3, 3:-3, 3:-3]
+    return u[3:-3, 3:-3, :]
+
+
+def run(p, ic, nsteps, **kw):
+    u0 = condinit(p, ic, **kw)
+    with Context(p) as g:
+        g.upload(u0)
+        g.boundary(0.0, 0.0)
+        t, dt = g.run(nsteps, 0.0)
+        return g.download(), t, g.history() if p.ndim == 3 else None
+
+
+def compare(p, ic, nsteps, tol=1e-4, **kw):
+    p64 = Params(**{**p.__dict__, "precision": "fp64"})
+    p32 = Params(**{**p.__dict__, "precision": "fp32"})
+    u64, t64, h64 = run(p64, ic, nsteps, **kw)
+    u32, t32, h32 = run(p32, ic, nsteps, **kw)
+    a64, a32 = active(u64, p), active(u32, p)
+    errs = {v: l1_rel(a32[..., v], a64[..., v]) for v in range(8) if np.sum(np.abs(a64[..., v])) > 0}
+    print(ic, "L1 rel", {k: f"{e:.2e}" for k, e in errs.items()}, "t", t32, t64)
+    assert np.isfinite(u32[..., :8]).all()
+    assert abs(t32 - t64) <= 1e-5 * t64
+    for v in (0, 4, 5, 6, 7):
+        if v in errs:
+            assert errs[v] < tol, (v, errs[v])
+    return u32, u64, h32, h64
+
+
+def test_fp32_orszag_tang_3d():
+    p = Params(ndim=3, nx=32, ny=32, nz=32, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, gamma=5 / 3, courant=0.8)
+    compare(p, "orszag_tang", 20)
+
+
+def test_fp32_mri_fargo():
+    p = Params(ndim=3, iso=1, nx=16, ny=32, nz=16, xmin=-0.25, xmax=0.25, ymin=-0.5, ymax=0.5, zmin=-0.25,
+               zmax=0.25, ciso=1.0, omega0=1.0, courant=0.8, bdtypex="shearingbox", fargo=True)
+    u32, u64, h32, h64 = compare(p, "mri", 20, beta=1000.0, amp=0.1, seed=5)
+    # history sums agree to FP32 working precision
+    assert abs(h32[0] - h64[0]) <= 1e-6 * abs(h64[0])
+    assert abs(h32[4] - h64[4]) <= 1e-3 * abs(h64[4])
+
+
+def test_fp32_shearing_box_no_fargo():
+    p = Params(ndim=3, iso=1, nx=16, ny=32, nz=16, xmin=-0.25, xmax=0.25, ymin=-0.5, ymax=0.5, zmin=-0.25,
+               zmax=0.25, ciso=1.0, omega0=1.0, courant=0.8, bdtypex="shearingbox")
+    compare(p, "mri", 10, beta=400.0, amp=0.1, seed=2)
+
+
+def test_fp32_field_loop_2d():
+    p = Params(ndim=2, nx=64, ny=32, nz=1, xmin=-1, xmax=1, ymin=-0.5, ymax=0.5, courant=0.7)
+    compare(p, "field_loop", 20, tol=1e-4)
+
+
+def test_fp32_divergence_free():
+    p = Params(ndim=3, nx=32, ny=32, nz=32, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, gamma=5 / 3,
+               courant=0.8, precision="fp32")
+    u, _, _ = run(p, "orszag_tang", 20)
+    dx = 1 / 32
+    bx, by, bz = u[..., 5], u[..., 6], u[..., 7]
+    # div B of the active cells from their left faces and the left faces of the next cells
+    div = ((bx[4:-2, 3:-3, 3:-3] - bx[3:-3, 3:-3, 3:-3]) + (by[3:-3, 4:-2, 3:-3] - by[3:-3, 3:-3, 3:-3])
+           + (bz[3:-3, 3:-3, 4:-2] - bz[3:-3, 3:-3, 3:-3])) / dx
+    bmax = np.max(np.abs(u[..., 5:8]))
+    assert np.max(np.abs(div)) * dx / bmax < 1e-6
