@@ -2,9 +2,13 @@
 """Benchmark of the DUMSES Godunov MHD step on B200.
 
 Headline workload: the 3D Orszag-Tang-type vortex on a 256^3 periodic grid,
-plain FP64 path, HLLD face fluxes and HLLD edge EMFs, MC slopes, CFL 0.8.
-A step is one pass of the reference loop body (compute_dt, godunov,
-boundary; src/dumses.f90:82-120) over the whole grid.
+HLLD face fluxes and HLLD edge EMFs, MC slopes, CFL 0.8 (--workload mri: the
+256^3 shearing-box MRI with FARGO).  A step is one pass of the reference loop
+body (compute_dt, godunov, fargo_update, boundary; src/dumses.f90:82-120)
+over the whole grid.  By default both arithmetics run: the FP64 plain path
+(bit-identical to the reference arithmetic) and the FP32 mixed path (the
+headline), and the line reports the FP32 path's relative L1 error against the
+FP64 path after the same steps.
 
   value  zone-cycles/s with the state resident in HBM: K steps enqueued back to
          back (dg_run), timed with CUDA events on the library's stream.
@@ -42,11 +46,29 @@ METRIC = "zone-cycles/s at 256³: plain FP64 vs FP32+NN-flux at stated L1 vs FP6
 ALGO_BYTES_PER_ZONE = 128  # read + write of 8 conserved FP64 variables per zone-cycle
 
 
-def workload_params(n: int, device: int = 0, precision: str = "fp64"):
+WORKLOADS = {"ot": "orszag_tang_3d", "mri": "shearing_box_mri_fargo"}
+
+
+def workload_params(n: int, device: int = 0, precision: str = "fp64", kind: str = "ot"):
+    """ot: the 3D Orszag-Tang-type vortex on the periodic unit cube (adiabatic).
+    mri: the unstratified isothermal shearing box of the MRI set-up at n^3 with cubic cells on
+    [-0.5,0.5]^3 H, Omega = 1, q = 1.5, c_s = 1, shear-periodic x, FARGO on."""
     from dumses_hybrid_b200 import Params
+    if kind == "mri":
+        return Params(ndim=3, iso=1, nx=n, ny=n, nz=n, xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5, zmin=-0.5,
+                      zmax=0.5, gamma=5.0 / 3.0, ciso=1.0, omega0=1.0, courant=0.8, slope_type=2, riemann="hlld",
+                      riemann2d="hlld", bdtypex="shearingbox", fargo=True, device=device, precision=precision)
     return Params(ndim=3, nx=n, ny=n, nz=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
                   gamma=5.0 / 3.0, courant=0.8, slope_type=2, riemann="hlld", riemann2d="hlld", device=device,
                   precision=precision)
+
+
+def initial_state(P, kind: str):
+    from dumses_hybrid_b200 import condinit
+    if kind == "mri":
+        # net vertical field, beta = 1000, velocity kicks uniform in +-0.05 c_s, seed 2024
+        return condinit(P, "mri", beta=1000.0, amp=0.1, seed=2024)
+    return condinit(P, "orszag_tang")
 
 
 def measured_peaks() -> dict:
@@ -120,16 +142,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(steps: int, warmup: int, n: int = 128) -> dict:
+def cpu_baseline(steps: int, warmup: int, n: int = 128, kind: str = "ot") -> dict:
     """The CPU restatement (oracle) on all host cores, n^3 sample of the workload."""
     sys.path.insert(0, str(ROOT / "tests"))
     from _oracle import Oracle, lib as oracle_lib
     from dumses_hybrid_b200 import condinit
     cores = os.cpu_count() or 1
     oracle_lib().or_set_threads(cores)
-    P = workload_params(n)
+    P = workload_params(n, kind=kind)
     o = Oracle(P)
-    o.set_state(condinit(P, "orszag_tang"))
+    o.set_state(initial_state(P, kind))
     o.boundary(0.0, 0.0)
     t = 0.0
     for _ in range(warmup):
@@ -140,7 +162,7 @@ def cpu_baseline(steps: int, warmup: int, n: int = 128) -> dict:
     el = time.perf_counter() - t0
     o.close()
     return {"value": n ** 3 * steps / el, "unit": "zone-cycles/s", "cores": cores, "kind": "port",
-            "sample": f"{n}^3 Orszag-Tang (same setup, 1/{(256 // n) ** 3} of the 256^3 grid), {steps} timed steps "
+            "sample": f"{n}^3 {WORKLOADS[kind]} (same setup, 1/{(256 // n) ** 3} of the 256^3 grid), {steps} timed steps "
                       f"after {warmup} warm-up, C restatement of the reference with OpenMP (FP64)",
             "seconds": el}
 
@@ -148,11 +170,11 @@ def cpu_baseline(steps: int, warmup: int, n: int = 128) -> dict:
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
-    cb = cpu_baseline(max(args.steps, 1), max(args.warmup, 0), n=128)
+    cb = cpu_baseline(max(args.steps, 1), max(args.warmup, 0), n=128, kind=args.workload)
     line = {"metric": METRIC, "value": cb["value"], "unit": "zone-cycles/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds"] / max(args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "orszag_tang_3d_256^3 (timed on a 128^3 sample per step)", "grid": [128, 128, 128],
+            "config": {"workload": f"{WORKLOADS[args.workload]}_256^3 (timed on a 128^3 sample per step)", "grid": [128, 128, 128],
                        "solver": "hlld/hlld", "slope": "mc", "courant": 0.8},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": "zone-cycles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -167,7 +189,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256, help="grid edge (the headline workload is 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "fp32", "both"], default="both",
+                    help="both: time the FP64 plain path and the FP32 mixed path (headline) in one run")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ot")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -195,11 +219,11 @@ def main() -> None:
         dist.barrier()
         dgbuild.build()
 
-    P = workload_params(args.n, device=local_rank, precision=args.precision)
-    u0 = dg.condinit(P, "orszag_tang")
-    ncell = args.n ** 3
-    ctx = dg.Context(P)
-    stream = torch.cuda.ExternalStream(ctx.stream)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
 
     def barrier():
         if dist is not None:
@@ -213,56 +237,68 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident timed region (value + roofline) ----
-    ctx.upload(u0)
-    ctx.boundary(0.0, 0.0)
-    t_sim, _ = ctx.run(args.warmup, 0.0)
-    uuid = None
-    try:
-        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
-    except Exception:
-        pass
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ctx.profile(True)
-    ctx.profile_read()
-    launches0 = ctx.kernel_launches
-    with ClockSampler(uuid) as clk:
-        ev0.record(stream)
-        t_sim, dt_last = ctx.run(args.steps, t_sim)
-        ev1.record(stream)
-        ev1.synchronize()
-    barrier()
-    launches = ctx.kernel_launches - launches0
-    prof = ctx.profile_read()
-    ctx.profile(False)
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * ncell * args.steps / (ms / 1e3)
+    ncell = args.n ** 3
 
-    # ---- end-to-end through the reference-facing C-ABI ----
-    nt = (args.n + 6) ** 3
-    pinned = torch.empty((11, args.n + 6, args.n + 6, args.n + 6), dtype=torch.float64, pin_memory=True)
-    host = pinned.numpy().T  # Fortran-ordered view (nx+6, ny+6, nz+6, 11)
-    host[...] = u0
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    ctx.upload(host)
-    ctx.boundary(0.0, 0.0)
-    te = 0.0
-    for _ in range(args.steps):
-        dt = ctx.compute_dt()
-        ctx.godunov(dt, te)
-        ctx.boundary(te, dt)
-        te = te + dt
-    got = ctx.download()
-    e1.record(stream)
-    e1.synchronize()
-    barrier()
-    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * ncell * args.steps / (ms_e2e / 1e3)
-    ok = bool(np.isfinite(got[..., :8]).all())
-    ctx.close()
+    def measure(precision: str, with_e2e: bool) -> dict:
+        P = workload_params(args.n, device=local_rank, precision=precision, kind=args.workload)
+        u0 = initial_state(P, args.workload)
+        ctx = dg.Context(P)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        # device-resident timed region (value + per-kernel events for the roofline)
+        ctx.upload(u0)
+        ctx.boundary(0.0, 0.0)
+        t_sim, _ = ctx.run(args.warmup, 0.0)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.profile(True)
+        ctx.profile_read()
+        launches0 = ctx.kernel_launches
+        with ClockSampler(uuid) as clk:
+            ev0.record(stream)
+            t_sim, _ = ctx.run(args.steps, t_sim)
+            ev1.record(stream)
+            ev1.synchronize()
+        barrier()
+        out = {"launches": ctx.kernel_launches - launches0, "prof": ctx.profile_read(), "clocks": clk.summary()}
+        ctx.profile(False)
+        out["ms"] = max_over_ranks(ev0.elapsed_time(ev1))
+        out["value"] = world * ncell * args.steps / (out["ms"] / 1e3)
+        out["state"] = ctx.download() if rank == 0 else None
+        out["sim_time"] = t_sim
+        if with_e2e:
+            # end-to-end through the reference-facing C-ABI, as the Fortran driver calls it
+            nt = (args.n + 6) ** 3
+            pinned = torch.empty((11, args.n + 6, args.n + 6, args.n + 6), dtype=torch.float64, pin_memory=True)
+            host = pinned.numpy().T  # Fortran-ordered view (nx+6, ny+6, nz+6, 11)
+            host[...] = u0
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.upload(host)
+            ctx.boundary(0.0, 0.0)
+            te = 0.0
+            for _ in range(args.steps):
+                dt = ctx.compute_dt()
+                ctx.godunov(dt, te)
+                if P.fargo:
+                    ctx.fargo_update(dt)
+                ctx.boundary(te, dt)
+                te = te + dt
+            ctx.download_into(host)
+            e1.record(stream)
+            e1.synchronize()
+            barrier()
+            ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+            out["e2e"] = {"value": world * ncell * args.steps / (ms_e2e / 1e3), "unit": "zone-cycles/s",
+                          "h2d_bytes_per_step": 8 * nt * 8 / args.steps,
+                          "d2h_bytes_per_step": (11 * nt * 8) / args.steps + 8,
+                          "finite": bool(np.isfinite(host[..., :8]).all())}
+        ctx.close()
+        return out
+
+    precisions = ["fp64", "fp32"] if args.precision == "both" else [args.precision]
+    head = precisions[-1]
+    res = {pr: measure(pr, with_e2e=(pr == head)) for pr in precisions}
 
     if dist is not None:
         dist.barrier()
@@ -274,36 +310,55 @@ def main() -> None:
     hbm_peak = peaks.get("hbm_gbs")
     peak_src = "measured" if hbm_peak else "fallback"
     hbm_peak = hbm_peak or 6650.0
-    kernels = {k: {"ms_total": v[0], "launches": v[1], "ms_per_launch": v[0] / max(v[1], 1)} for k, v in prof.items()}
-    dom = max(kernels, key=lambda k: kernels[k]["ms_total"]) if kernels else None
-    roof = None
-    if dom:
+
+    def kernel_table(r):
+        return {k: {"ms_total": v[0], "launches": v[1], "ms_per_launch": v[0] / max(v[1], 1)}
+                for k, v in r["prof"].items()}
+
+    def roofline(r, precision):
+        kernels = kernel_table(r)
+        dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
         per_launch_s = kernels[dom]["ms_per_launch"] / 1e3
         achieved = ALGO_BYTES_PER_ZONE * ncell / per_launch_s / 1e9
         traffic = None
-        tpath = ROOT / "profiles" / f"ncu_traffic_ot{args.n}_fp64.json"
+        tpath = ROOT / "profiles" / f"ncu_traffic_{args.workload}{args.n}_{precision}.json"
         if tpath.exists():
             try:
                 traffic = json.loads(tpath.read_text()).get(dom)
             except Exception:
                 traffic = None
-        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+        step = ALGO_BYTES_PER_ZONE * ncell * args.steps / (r["ms"] / 1e3) / 1e9 / world
+        return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_ZONE * ncell,
-                "step_achieved": ALGO_BYTES_PER_ZONE * ncell * args.steps / (ms / 1e3) / 1e9 / world,
-                "step_frac": ALGO_BYTES_PER_ZONE * ncell * args.steps / (ms / 1e3) / 1e9 / world / hbm_peak}
-    line = {"metric": METRIC, "value": value, "unit": "zone-cycles/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"orszag_tang_3d_{args.n}^3_fp64", "grid": [args.n] * 3, "precision": "fp64",
+                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_ZONE * ncell, "step_achieved": step,
+                "step_frac": step / hbm_peak}
+
+    h = res[head]
+    line = {"metric": METRIC, "value": h["value"], "unit": "zone-cycles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": h["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+            "config": {"workload": f"{WORKLOADS[args.workload]}_{args.n}^3", "grid": [args.n] * 3,
+                       "arithmetic": ("fp32 trace/Riemann/CT, compensated fp32 hi/lo state, fp64 primitive "
+                                      "recovery/dt/FARGO/diagnostics") if head == "fp32" else "fp64 (bit-exact)",
                        "solver": "hlld/hlld", "slope": "mc", "courant": 0.8, "parallelism": f"replicas x{world}",
-                       "l2": "working set ~13 GB per step >> 126 MB L2, no flush needed"},
-            "e2e": {"value": e2e_value, "unit": "zone-cycles/s", "h2d_bytes_per_step": 8 * nt * 8 / args.steps,
-                    "d2h_bytes_per_step": (11 * nt * 8) / args.steps + 8 * 2, "finite": ok},
-            "gpu_launches": launches, "roofline": roof, "kernels": kernels, "clocks": clk.summary(),
-            "sim_time": t_sim}
+                       "l2": "working set 8-13 GB per step >> 126 MB L2, no flush needed"},
+            "e2e": h["e2e"], "gpu_launches": h["launches"], "roofline": roofline(h, head),
+            "kernels": kernel_table(h), "clocks": h["clocks"], "sim_time": h["sim_time"]}
+    if "fp64" in res and head != "fp64":
+        f = res["fp64"]
+        a64, a32 = f["state"][3:-3, 3:-3, 3:-3], h["state"][3:-3, 3:-3, 3:-3]
+        names = ["rho", "rho_vx", "rho_vy", "rho_vz", "E", "Bx", "By", "Bz"]
+        l1 = {}
+        for v, nm in enumerate(names):
+            den = float(np.sum(np.abs(a64[..., v])))
+            if den > 0:
+                l1[nm] = float(np.sum(np.abs(a32[..., v] - a64[..., v])) / den)
+        line["fp64_plain_path"] = {"value": f["value"], "ms_per_step": f["ms"] / args.steps,
+                                   "roofline": roofline(f, "fp64"), "kernels": kernel_table(f), "clocks": f["clocks"]}
+        line["speedup_vs_fp64"] = h["value"] / f["value"]
+        line["l1_rel_vs_fp64"] = {"after_steps": args.steps + args.warmup, **l1}
     if world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(2, 1, n=128)
+        cb = cpu_baseline(2, 1, n=128, kind=args.workload)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
 

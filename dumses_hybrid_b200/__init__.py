@@ -239,6 +239,12 @@ class Context:
         _check(self.lib.dg_download(self.h, self._ptr(u)))
         return u
 
+    def download_into(self, uin: np.ndarray) -> None:
+        """Download into a caller-owned Fortran-ordered float64 array (e.g. pinned memory)."""
+        if uin.shape != self.params.shape or uin.dtype != np.float64 or not uin.flags.f_contiguous:
+            raise ValueError(f"uin must be a Fortran-ordered float64 array of shape {self.params.shape}")
+        _check(self.lib.dg_download(self.h, self._ptr(uin)))
+
     def compute_dt(self) -> float:
         dt = ctypes.c_double()
         _check(self.lib.dg_compute_dt(self.h, ctypes.byref(dt)))
