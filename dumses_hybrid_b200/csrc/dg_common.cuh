@@ -73,14 +73,16 @@ struct Scalars {
     double time;
     unsigned long long red;   // bits of the running CFL minimum (positive doubles order as integers)
     int err;                  // DG_ERR_* raised by a kernel (0 = none)
-    int pad;
+    int sh_jp;                // shear offset of the x boundaries: whole cells ...
+    double sh_epsi;           // ... and remainder, for the time of the last k_shear_offset launch
 };
 
 // number of trace-core fields per cell
 constexpr int kCore3 = 47;
 constexpr int kCore2 = 30;
 
-// face flux components stored per face: rho, E, normal momentum, t1, t2, p*_tot, Bz (2D only)
-constexpr int kFluxComp = 7;
+// face flux components, stored face-major (8 contiguous values per face): rho, E,
+// rho u, rho v, rho w (scaled by area*dt as compflux does), p*_tot, Bz (2D only), pad
+constexpr int kFluxComp = 8;
 
 }  // namespace dg

@@ -1,12 +1,12 @@
 // FP32 mixed path: the step kernels of step_impl.cuh instantiated for T = float on a
 // compensated FP32 (hi, lo) state, compiled with fast FP32 math.
 //
-// FP64 is used only where it carries accuracy: turning the state into primitive
-// variables (pressure from total energy, which cancels in low-beta zones), the CFL
-// reduction, FARGO's remap of the state and the history sums.  Trace, Riemann
-// solvers, fluxes, EMFs and the constrained-transport increments are FP32; the
-// state update adds each FP32 increment to the (hi, lo) pair with an error-free
-// two-sum, so the state carries about 48 significant bits across steps.
+// FP64 is used only where it carries accuracy: the gas pressure from the total
+// energy (which cancels in low-beta zones), the CFL
+// reduction, the orbital-advection shift of each x column and the history sums.
+// Trace, Riemann solvers, fluxes, EMFs, FARGO's remap and the constrained-transport
+// increments are FP32; every update adds an FP32 increment to a (hi, lo) pair with
+// an error-free two-sum, so the state carries about 48 significant bits across steps.
 #define DG_NS f32
 #include "step_impl.cuh"
 
@@ -47,11 +47,10 @@ __global__ void __launch_bounds__(kThreads) k_update3d_hl(Geo G, StoreHL U, Stor
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const double dtd = S->dt;
     const float dt = (float)dtd;
-    const long long fs = G.fsz;
     const long long c = G.idx(i, j, k);
     const bool shear = G.shearing != 0;
     ShearRemap sr{0.0, 0};
-    if (shear) sr = shear_offset(G, S->time + 0.5 * dtd);
+    if (shear) sr = ShearRemap{S->sh_epsi, S->sh_jp};  // time + dt/2, from k_shear_offset
 
     if (i <= nx && j <= ny && k <= nz) {
         const float dvloc = (float)(1.0 / (G.dx * G.dy * G.dz));
@@ -72,26 +71,28 @@ __global__ void __launch_bounds__(kThreads) k_update3d_hl(Geo G, StoreHL U, Stor
         const float ds[3] = {(float)(G.dy * G.dz), (float)(G.dx * G.dz), (float)(G.dx * G.dy)};
         float pre[3];
         for (int d = 0; d < 3; d++) {
-            const float *F = FA[d];
-            float rl = ld(F + t), rr = ld(F + FR[d]);
+            float L[8], R[8];
+            load8(FA[d] + t * kFluxComp, L);
+            load8(FA[d] + FR[d] * kFluxComp, R);
+            float rl = L[0], rr = R[0];
             if (d == 0 && shear) {
-                if (i == 1) rl = shear_avg(G, sr, fx, 0, 0, j, k);
-                if (i == nx) rr = shear_avg(G, sr, fx, 0, 1, j, k);
+                if (i == 1) rl = shear_avg(G, sr, fx, kFluxComp, 0, j, k);
+                if (i == nx) rr = shear_avg(G, sr, fx, kFluxComp, 1, j, k);
             }
-            pre[d] = -(ld(F + 5 * fs + FR[d]) * ds[d] - ld(F + 5 * fs + t) * ds[d]) * dt;
+            pre[d] = -(R[5] * ds[d] - L[5] * ds[d]) * dt;
             dr += (rl - rr) * dvloc;
-            dw += (ld(F + 4 * fs + t) - ld(F + 4 * fs + FR[d])) * dvloc;
-            dp += (ld(F + 1 * fs + t) - ld(F + 1 * fs + FR[d])) * dvloc;
+            dw += (L[4] - R[4]) * dvloc;
+            dp += (L[1] - R[1]) * dvloc;
             if (G.omega0 > 0.0) {
-                float dfn2 = (ld(F + 2 * fs + t) - ld(F + 2 * fs + FR[d])) * dvloc;
+                float dfn2 = (L[2] - R[2]) * dvloc;
                 if (d == 0) dfn2 = dfn2 + pre[0] * dvloc;
-                float dfn3 = (ld(F + 3 * fs + t) - ld(F + 3 * fs + FR[d])) * dvloc;
+                float dfn3 = (L[3] - R[3]) * dvloc;
                 if (d == 1) dfn3 = dfn3 + pre[1] * dvloc;
                 du += dfn2 / opl + Om * dt / opl * dfn3;
                 dv += dfn3 / opl - 0.25f * Om * dt / opl * dfn2;
             } else {
-                du += (ld(F + 2 * fs + t) - ld(F + 2 * fs + FR[d])) * dvloc;
-                dv += (ld(F + 3 * fs + t) - ld(F + 3 * fs + FR[d])) * dvloc;
+                du += (L[2] - R[2]) * dvloc;
+                dv += (L[3] - R[3]) * dvloc;
             }
         }
         if (G.omega0 == 0.0) {
@@ -107,7 +108,7 @@ __global__ void __launch_bounds__(kThreads) k_update3d_hl(Geo G, StoreHL U, Stor
     }
     auto EYc = [&](int ii, int jj, int kk) -> float {
         if (shear && (ii == 1 || ii == nx + 1) && jj <= ny && kk <= nz + 1)
-            return shear_avg(G, sr, ey, 0, ii == 1 ? 0 : 1, jj, kk);
+            return shear_avg(G, sr, ey, 1, ii == 1 ? 0 : 1, jj, kk);
         return ld(ey + G.fidx(ii, jj, kk));
     };
     const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
@@ -140,7 +141,6 @@ __global__ void __launch_bounds__(kThreads) k_update2d_hl(Geo G, StoreHL U, Stor
     const int nx = G.nx, ny = G.ny;
     const double dtd = S->dt;
     const float dt = (float)dtd;
-    const long long fs = G.fsz;
     const long long c = G.idx(i, j, k);
     if (i <= nx && j <= ny) {
         const float dvloc = (float)(1.0 / (G.dx * G.dy * G.dz));
@@ -160,22 +160,24 @@ __global__ void __launch_bounds__(kThreads) k_update2d_hl(Geo G, StoreHL U, Stor
         const float ds[2] = {(float)(G.dy * G.dz), (float)(G.dx * G.dz)};
         float pre[2];
         for (int d = 0; d < 2; d++) {
-            const float *F = FA[d];
-            pre[d] = -(ld(F + 5 * fs + FR[d]) * ds[d] - ld(F + 5 * fs + t) * ds[d]) * dt;
-            dr += (ld(F + t) - ld(F + FR[d])) * dvloc;
-            dw += (ld(F + 4 * fs + t) - ld(F + 4 * fs + FR[d])) * dvloc;
-            dp += (ld(F + 1 * fs + t) - ld(F + 1 * fs + FR[d])) * dvloc;
-            dc += (ld(F + 6 * fs + t) - ld(F + 6 * fs + FR[d])) * dvloc;
+            float L[8], R[8];
+            load8(FA[d] + t * kFluxComp, L);
+            load8(FA[d] + FR[d] * kFluxComp, R);
+            pre[d] = -(R[5] * ds[d] - L[5] * ds[d]) * dt;
+            dr += (L[0] - R[0]) * dvloc;
+            dw += (L[4] - R[4]) * dvloc;
+            dp += (L[1] - R[1]) * dvloc;
+            dc += (L[6] - R[6]) * dvloc;
             if (G.omega0 > 0.0) {
-                float dfn2 = (ld(F + 2 * fs + t) - ld(F + 2 * fs + FR[d])) * dvloc;
+                float dfn2 = (L[2] - R[2]) * dvloc;
                 if (d == 0) dfn2 = dfn2 + pre[0] * dvloc;
-                float dfn3 = (ld(F + 3 * fs + t) - ld(F + 3 * fs + FR[d])) * dvloc;
+                float dfn3 = (L[3] - R[3]) * dvloc;
                 if (d == 1) dfn3 = dfn3 + pre[1] * dvloc;
                 du += dfn2 / opl + Om * dt / opl * dfn3;
                 dv += dfn3 / opl - 0.25f * Om * dt / opl * dfn2;
             } else {
-                du += (ld(F + 2 * fs + t) - ld(F + 2 * fs + FR[d])) * dvloc;
-                dv += (ld(F + 3 * fs + t) - ld(F + 3 * fs + FR[d])) * dvloc;
+                du += (L[2] - R[2]) * dvloc;
+                dv += (L[3] - R[3]) * dvloc;
             }
         }
         if (G.omega0 == 0.0) {
@@ -199,6 +201,183 @@ __global__ void __launch_bounds__(kThreads) k_update2d_hl(Geo G, StoreHL U, Stor
         float inc = ct ? -(ld(ez + G.fidx(i + 1, j, k)) - ld(ez + t)) * rdx : 0.f;
         apply(U, Un, G, IB, c, inc);
     }
+}
+
+// primitive variables (scheme.f90:44-86) from the compensated state: velocities and
+// cell-centred B in FP32, the pressure in FP64 as (gamma-1) (E - emag - rho eken), which
+// is (gamma-1) rho eint of the reference without its division when rho >= smallr
+__global__ void __launch_bounds__(kThreads) k_prim_hl(Geo G, StoreHL U, float *__restrict__ Q, const Scalars *S) {
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    const long long n = (long long)ni * nj * nk;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)(t % ni) - 2;
+    const long long r = t / ni;
+    const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
+    const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+    const long long c = G.idx(i, j, k);
+    auto f = [&](int v, long long cc) { return ld(U.hi + G.sv * v + cc) + ld(U.lo + G.sv * v + cc); };
+    const double d = (double)ld(U.hi + G.sv * IR + c) + (double)ld(U.lo + G.sv * IR + c);
+    const float rho = (float)mx(d, kSmallr);
+    const float ri = 1.0f / (float)d;
+    float u = f(IU, c) * ri, v = f(IV, c) * ri, w = f(IW, c) * ri;
+    const float bx = 0.5f * (f(IA, c) + f(IA, c + 1));
+    const float by = 0.5f * (f(IB, c) + f(IB, c + G.sy));
+    const float bz = 0.5f * (f(IC, c) + ((G.ndim == 3) ? f(IC, c + G.sz) : f(8, c)));
+    float p;
+    if (G.iso) {
+        p = (float)(d * (G.ciso * G.ciso));
+    } else {
+        const double E = (double)ld(U.hi + G.sv * IP + c) + (double)ld(U.lo + G.sv * IP + c);
+        const double emag = 0.5 * ((double)bx * bx + (double)by * by + (double)bz * bz);
+        const double eken = 0.5 * ((double)u * u + (double)v * v + (double)w * w);
+        double pe = (G.gamma - 1.0) * (E - emag - d * eken);
+        if (d < kSmallr) pe = pe * (kSmallr / d);
+        const double smallp = kSmallr * (kSmallc * kSmallc) / G.gamma;
+        p = (float)mx(pe, smallp);
+    }
+    if (G.omega0 > 0.0) {
+        const float om = (float)G.omega0, hdt = 0.5f * (float)S->dt;
+        const float dvx = 2.0f * om * v, dvy = -(0.5f * om * u);
+        u = u + dvx * hdt;
+        v = v + dvy * hdt;
+    }
+    float *q = Q + c;
+    q[G.sv * IR] = rho; q[G.sv * IU] = u; q[G.sv * IV] = v; q[G.sv * IW] = w;
+    q[G.sv * IP] = p; q[G.sv * IA] = bx; q[G.sv * IB] = by; q[G.sv * IC] = bz;
+}
+
+// ---------------------------------------------------------------------------
+// FARGO (fargo.f90:17-288) on the compensated state: the shift of each x column is
+// computed in FP64 exactly as in the FP64 path; the remapped value is written as the
+// donor cell's (hi, lo) plus an FP32 increment, and the face-B CT as FP32 increments.
+// ---------------------------------------------------------------------------
+struct HL {
+    float h, l;
+};
+__device__ __forceinline__ HL hl_at(const Geo &G, const StoreHL &U, int v, long long c) {
+    return HL{ld(U.hi + G.sv * v + c), ld(U.lo + G.sv * v + c)};
+}
+// a - b from two (hi, lo) pairs; the hi difference is exact for nearby values
+__device__ __forceinline__ float hl_diff(HL a, HL b) { return (a.h - b.h) + (a.l - b.l); }
+
+// uin_slope (fargo.f90:266-280) from the (hi, lo) values at j-1, j, j+1, on differences
+__device__ __forceinline__ float slope_hl(int ist, HL m, HL c, HL p) {
+    if (ist == 0) return 0.0f;
+    const float sl = (float)ist;
+    const float dlft = sl * hl_diff(c, m), drgt = sl * hl_diff(p, c);
+    const float dcen = 0.5f * (dlft + drgt) / sl;
+    const float dlim = (dlft * drgt <= 0.0f) ? 0.0f : fminf(fabsf(dlft), fabsf(drgt));
+    return copysignf(fminf(dlim, fabsf(dcen)), dcen);
+}
+// uin_slope of variable v at (i, j, k) with y wrap
+__device__ __forceinline__ float fslope_hl(const Geo &G, const StoreHL &U, int v, int i, int j, int k) {
+    auto at = [&](int jj) { return hl_at(G, U, v, G.idx(i, map_bc(G.bc[1], jj, G.ny), k)); };
+    return slope_hl(mn(G.slope_type, 2), at(j - 1), at(j), at(j + 1));
+}
+
+// emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1
+__global__ void __launch_bounds__(kThreads) k_fargo_emf_hl(Geo G, StoreHL U, float *__restrict__ fex,
+                                                           float *__restrict__ fez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const double dt = S->dt;
+    const float dy = (float)G.dy;
+    const int ny = G.ny;
+    const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
+    auto B = [&](int v, int jj) {
+        const HL b = hl_at(G, U, v, G.idx(i, jj, kw));
+        return b.h + b.l;
+    };
+    // sum over the shifted-through cells and the fractional donor (get_emfx / get_emfz)
+    auto emf = [&](int v, const FargoShift &f) {
+        const float eps = (float)f.eps;
+        float e = 0.0f;
+        if (f.vK > 0.0) {
+            const float lambda = 0.5f * eps * (1.0f - eps);
+            for (int jj = 1; jj <= f.nshft; jj++) {
+                int js = j - jj;
+                if (js < 1) js = js + ny;
+                e += B(v, wrap1(js, ny)) * dy;
+            }
+            int js = j - f.nshft - 1;
+            if (js < 1) js = js + ny;
+            js = wrap1(js, ny);
+            e += (eps * B(v, js) + lambda * fslope_hl(G, U, v, i, js, kw)) * dy;
+        } else {
+            const float lambda = 0.5f * eps * (eps - 1.0f);
+            for (int jj = 0; jj <= f.nshft - 1; jj++) {
+                int js = j + jj;
+                if (js > ny) js = js - ny;
+                e -= B(v, wrap1(js, ny)) * dy;
+            }
+            int js = j + f.nshft;
+            if (js > ny) js = js - ny;
+            js = wrap1(js, ny);
+            e += (-eps * B(v, js) - lambda * fslope_hl(G, U, v, i, js, kw)) * dy;
+        }
+        return e;
+    };
+    if (i <= G.nx) fex[t] = emf(IC, fargo_shift(G, G.xc(i), dt));                        // fargo.f90:146-177
+    if (k <= G.nz) fez[t] = -emf(IA, fargo_shift(G, 0.5 * (G.xc(i) + G.xc(i - 1)), dt));  // fargo.f90:204-235
+}
+
+// remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119)
+__global__ void __launch_bounds__(kThreads) k_fargo_update_hl(Geo G, StoreHL U, StoreHL Un,
+                                                              const float *__restrict__ fex,
+                                                              const float *__restrict__ fez, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const long long c = G.idx(i, j, k);
+    if (i <= nx && j <= ny && k <= nz) {
+        const FargoShift f = fargo_shift(G, G.xc(i), S->dt);
+        int js, jsp;
+        if (f.vK > 0.0) {
+            js = j - f.nshft - 1;
+            if (js < 1) js = js + ny;
+        } else {
+            js = j + f.nshft;
+            if (js > ny) js = js - ny;
+        }
+        jsp = js + 1;
+        if (jsp > ny) jsp = jsp - ny;
+        js = wrap1(js, ny);
+        jsp = wrap1(jsp, ny);
+        const float eps = (float)f.eps;
+        const float w = (f.vK > 0.0) ? 1.0f - eps : eps;  // weight of the upper donor
+        const float hme = 0.5f - eps;
+        const float q = 0.5f * (0.25f - hme * hme);
+        const int ist = mn(G.slope_type, 2);
+        const long long cm = G.idx(i, map_bc(G.bc[1], js - 1, ny), k), c0 = G.idx(i, js, k);
+        const long long c1 = G.idx(i, map_bc(G.bc[1], js + 1, ny), k), d0 = G.idx(i, map_bc(G.bc[1], jsp - 1, ny), k);
+        const long long d1 = G.idx(i, jsp, k), dp = G.idx(i, map_bc(G.bc[1], jsp + 1, ny), k);
+        for (int v = IR; v <= IP; v++) {
+            HL a0 = hl_at(G, U, v, c0);
+            const HL a1 = hl_at(G, U, v, d1);
+            const float s0 = slope_hl(ist, hl_at(G, U, v, cm), a0, hl_at(G, U, v, c1));
+            const float s1 = slope_hl(ist, hl_at(G, U, v, d0), a1, hl_at(G, U, v, dp));
+            const float inc = hl_diff(a1, a0) * w + (s0 - s1) * q;
+            add_hl(a0.h, a0.l, inc);
+            Un.hi[G.sv * v + c] = a0.h;
+            Un.lo[G.sv * v + c] = a0.l;
+        }
+    }
+    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
+    auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, jj, kk)); };
+    auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, jj, kk)) : 0.0f; };
+    if (j <= ny && k <= nz) apply(U, Un, G, IA, c, (EZ(i, j + 1, k) - EZ(i, j, k)) * rdy);
+    if (i <= nx && k <= nz)
+        apply(U, Un, G, IB, c, -(EZ(i + 1, j, k) - EZ(i, j, k)) * rdx + (EX(i, j, k + 1) - EX(i, j, k)) * rdz);
+    if (i <= nx && j <= ny) apply(U, Un, G, IC, c, -(EX(i, j + 1, k) - EX(i, j, k)) * rdy);
 }
 
 StoreHL st(const Bufs &B, int b) {
@@ -242,7 +421,8 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     float *fx = (float *)B.flx[0], *fy = (float *)B.flx[1], *fz = (float *)B.flx[2];
     float *ex = (float *)B.emf[0], *ey = (float *)B.emf[1], *ez = (float *)B.emf[2];
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
-    TIMED(KS_PRIM, s, (k_prim<float, StoreHL><<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
         TIMED(KS_TRACE, s, (k_trace3d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
@@ -254,19 +434,24 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S)));
         TIMED(KS_UPDATE, s, (k_update2d_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U, Un, fx, fy, ez, B.S)));
     }
-    return 5;
+    return 5 + (G.shearing ? 1 : 0);
 }
 
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
-    TIMED(KS_FARGO_EMF, s, (k_fargo_emf<StoreHL><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), B.femf[0], B.femf[1], B.S)));
-    TIMED(KS_FARGO_UPDATE, s, (k_fargo_update<StoreHL><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), B.femf[0], B.femf[1], B.S)));
+    float *fex = (float *)B.femf[0], *fez = (float *)B.femf[1];
+    TIMED(KS_FARGO_EMF, s, (k_fargo_emf_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), fex, fez, B.S)));
+    TIMED(KS_FARGO_UPDATE, s, (k_fargo_update_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), fex, fez, B.S)));
     return 2;
 }
 
 int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
-    const long long n = (long long)G.NX * G.NY * G.NZ;
-    TIMED(KS_BOUNDARY, s, (k_boundary<StoreHL><<<nblocks(n, kThreads), kThreads, 0, s>>>(G, st(B, cur), B.nv, B.S)));
-    return 1;
+    int n = 1;
+    if (G.shearing) {
+        TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 1.0)));
+        n++;
+    }
+    TIMED(KS_BOUNDARY, s, (k_boundary<StoreHL><<<nblocks(ghost_cells(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), B.nv, B.S)));
+    return n;
 }
 
 int launch_right_faces(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t s) {

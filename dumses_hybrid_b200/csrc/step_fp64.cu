@@ -24,11 +24,11 @@ __global__ void __launch_bounds__(kThreads) k_update3d(Geo G, const double *__re
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const double dt = S->dt;
     const double one = 1.0, two = 2.0, half = 0.5;
-    const long long sv = G.sv, fs = G.fsz;
+    const long long sv = G.sv;
     const long long c = G.idx(i, j, k);
     const bool shear = G.shearing != 0;
     ShearRemap sr{0.0, 0};
-    if (shear) sr = shear_offset(G, S->time + half * dt);
+    if (shear) sr = ShearRemap{S->sh_epsi, S->sh_jp};  // time + dt/2, from k_shear_offset
 
     if (i <= nx && j <= ny && k <= nz) {
         // hydro update, scheme.f90:1783-1907
@@ -54,27 +54,29 @@ __global__ void __launch_bounds__(kThreads) k_update3d(Geo G, const double *__re
         const long long FR[3] = {fxr, fyr, fzr};
         double pre[3];
         for (int d = 0; d < 3; d++) {
-            const double *F = FA[d];
-            double rl = ld(F + f0), rr = ld(F + FR[d]);
+            double L[8], R[8];
+            load8(FA[d] + f0 * kFluxComp, L);
+            load8(FA[d] + FR[d] * kFluxComp, R);
+            double rl = L[0], rr = R[0];
             if (d == 0 && shear) {
-                if (i == 1) rl = shear_avg(G, sr, fx, 0, 0, j, k);
-                if (i == nx) rr = shear_avg(G, sr, fx, 0, 1, j, k);
+                if (i == 1) rl = shear_avg(G, sr, fx, kFluxComp, 0, j, k);
+                if (i == nx) rr = shear_avg(G, sr, fx, kFluxComp, 1, j, k);
             }
             const double ds = (d == 0) ? G.dy * G.dz : (d == 1 ? G.dx * G.dz : G.dx * G.dy);
-            pre[d] = -(ld(F + 5 * fs + FR[d]) * ds - ld(F + 5 * fs + f0) * ds) * dt;
+            pre[d] = -(R[5] * ds - L[5] * ds) * dt;
             ur = ur + (rl - rr) * dvloc;
-            uw = uw + (ld(F + 4 * fs + f0) * one - ld(F + 4 * fs + FR[d]) * one) * dvloc / one;
-            up = up + (ld(F + 1 * fs + f0) - ld(F + 1 * fs + FR[d])) * dvloc;
+            uw = uw + (L[4] * one - R[4] * one) * dvloc / one;
+            up = up + (L[1] - R[1]) * dvloc;
             if (Omega0 > 0.0) {
-                double dfn2 = (ld(F + 2 * fs + f0) - ld(F + 2 * fs + FR[d])) * dvloc;
+                double dfn2 = (L[2] - R[2]) * dvloc;
                 if (d == 0) dfn2 = dfn2 + pre[0] * dvloc;
-                double dfn3 = (ld(F + 3 * fs + f0) - ld(F + 3 * fs + FR[d])) * dvloc;
+                double dfn3 = (L[3] - R[3]) * dvloc;
                 if (d == 1) dfn3 = dfn3 + pre[1] * dvloc;
                 uu = uu + dfn2 / (one + lambda) + Omega0 * dt / (one + lambda) * dfn3;
                 uv = uv + dfn3 / (one + lambda) - 2.5e-1 * Omega0 * dt / (one + lambda) * dfn2;
             } else {
-                uu = uu + (ld(F + 2 * fs + f0) * one - ld(F + 2 * fs + FR[d]) * one) * dvloc / one;
-                uv = uv + (ld(F + 3 * fs + f0) * one - ld(F + 3 * fs + FR[d]) * one) * dvloc / one;
+                uu = uu + (L[2] * one - R[2] * one) * dvloc / one;
+                uv = uv + (L[3] * one - R[3] * one) * dvloc / one;
             }
         }
         if (Omega0 == 0.0) {
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(kThreads) k_update3d(Geo G, const double *__re
     // constrained transport of the left faces, scheme.f90:1957-1993 (ranges 1..n+1)
     auto EYc = [&](int ii, int jj, int kk) -> double {
         if (shear && (ii == 1 || ii == nx + 1) && jj <= ny && kk <= nz + 1)
-            return shear_avg(G, sr, ey, 0, ii == 1 ? 0 : 1, jj, kk);
+            return shear_avg(G, sr, ey, 1, ii == 1 ? 0 : 1, jj, kk);
         return ld(ey + G.fidx(ii, jj, kk));
     };
     const double dx = G.dx, dy = G.dy, dz = G.dz;
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) k_update2d(Geo G, const double *__re
     const int nx = G.nx, ny = G.ny;
     const double dt = S->dt;
     const double one = 1.0, two = 2.0, half = 0.5;
-    const long long sv = G.sv, fs = G.fsz;
+    const long long sv = G.sv;
     const long long c = G.idx(i, j, k);
     if (i <= nx && j <= ny) {
         const double Omega0 = G.omega0;
@@ -149,23 +151,25 @@ __global__ void __launch_bounds__(kThreads) k_update2d(Geo G, const double *__re
         const double *FA[2] = {fx, fy};
         double pre[2];
         for (int d = 0; d < 2; d++) {
-            const double *F = FA[d];
+            double L[8], R[8];
+            load8(FA[d] + t * kFluxComp, L);
+            load8(FA[d] + FR[d] * kFluxComp, R);
             const double ds = (d == 0) ? G.dy * G.dz : G.dx * G.dz;
-            pre[d] = -(ld(F + 5 * fs + FR[d]) * ds - ld(F + 5 * fs + t) * ds) * dt;
-            ur = ur + (ld(F + t) - ld(F + FR[d])) * dvloc;
-            uw = uw + (ld(F + 4 * fs + t) * one - ld(F + 4 * fs + FR[d]) * one) * dvloc / one;
-            up = up + (ld(F + 1 * fs + t) - ld(F + 1 * fs + FR[d])) * dvloc;
-            uc = uc + (ld(F + 6 * fs + t) - ld(F + 6 * fs + FR[d])) * dvloc;
+            pre[d] = -(R[5] * ds - L[5] * ds) * dt;
+            ur = ur + (L[0] - R[0]) * dvloc;
+            uw = uw + (L[4] * one - R[4] * one) * dvloc / one;
+            up = up + (L[1] - R[1]) * dvloc;
+            uc = uc + (L[6] - R[6]) * dvloc;
             if (Omega0 > 0.0) {
-                double dfn2 = (ld(F + 2 * fs + t) - ld(F + 2 * fs + FR[d])) * dvloc;
+                double dfn2 = (L[2] - R[2]) * dvloc;
                 if (d == 0) dfn2 = dfn2 + pre[0] * dvloc;
-                double dfn3 = (ld(F + 3 * fs + t) - ld(F + 3 * fs + FR[d])) * dvloc;
+                double dfn3 = (L[3] - R[3]) * dvloc;
                 if (d == 1) dfn3 = dfn3 + pre[1] * dvloc;
                 uu = uu + dfn2 / (one + lambda) + Omega0 * dt / (one + lambda) * dfn3;
                 uv = uv + dfn3 / (one + lambda) - 2.5e-1 * Omega0 * dt / (one + lambda) * dfn2;
             } else {
-                uu = uu + (ld(F + 2 * fs + t) * one - ld(F + 2 * fs + FR[d]) * one) * dvloc / one;
-                uv = uv + (ld(F + 3 * fs + t) * one - ld(F + 3 * fs + FR[d]) * one) * dvloc / one;
+                uu = uu + (L[2] * one - R[2] * one) * dvloc / one;
+                uv = uv + (L[3] * one - R[3] * one) * dvloc / one;
             }
         }
         if (Omega0 == 0.0) {
@@ -229,6 +233,7 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     double *ex = (double *)B.emf[0], *ey = (double *)B.emf[1], *ez = (double *)B.emf[2];
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
     TIMED(KS_PRIM, s, (k_prim<double, StoreD><<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
         TIMED(KS_TRACE, s, (k_trace3d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
@@ -240,7 +245,7 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         TIMED(KS_RIEMANN, s, (k_riemann2d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S)));
         TIMED(KS_UPDATE, s, (k_update2d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, ez, B.S)));
     }
-    return 5;
+    return 5 + (G.shearing ? 1 : 0);
 }
 
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
@@ -250,9 +255,13 @@ int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
 }
 
 int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
-    const long long n = (long long)G.NX * G.NY * G.NZ;
-    TIMED(KS_BOUNDARY, s, (k_boundary<StoreD><<<nblocks(n, kThreads), kThreads, 0, s>>>(G, st(B, cur), B.nv, B.S)));
-    return 1;
+    int n = 1;
+    if (G.shearing) {
+        TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 1.0)));
+        n++;
+    }
+    TIMED(KS_BOUNDARY, s, (k_boundary<StoreD><<<nblocks(ghost_cells(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), B.nv, B.S)));
+    return n;
 }
 
 int launch_right_faces(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t s) {

@@ -41,6 +41,27 @@ constexpr int kThreads = 128;
 
 template <typename X> __device__ __forceinline__ X ld(const X *p) { return __ldg(p); }
 
+// 8 contiguous values (one face record) with 16-byte vector accesses
+__device__ __forceinline__ void load8(const float *p, float v[8]) {
+    const float4 a = __ldg((const float4 *)p), b = __ldg((const float4 *)p + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void load8(const double *p, double v[8]) {
+#pragma unroll
+    for (int n = 0; n < 4; n++) {
+        const double2 a = __ldg((const double2 *)p + n);
+        v[2 * n] = a.x; v[2 * n + 1] = a.y;
+    }
+}
+__device__ __forceinline__ void store8(float *p, const float v[8]) {
+    ((float4 *)p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    ((float4 *)p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+__device__ __forceinline__ void store8(double *p, const double v[8]) {
+#pragma unroll
+    for (int n = 0; n < 4; n++) ((double2 *)p)[n] = make_double2(v[2 * n], v[2 * n + 1]);
+}
+
 inline unsigned nblocks(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 // ---------------------------------------------------------------------------
@@ -664,7 +685,7 @@ DG_FACE_SOLVER_HOOK
 // writes the compflux-scaled fluxes in uin order plus p*_T (solver.f90:116-262, scheme.f90:1740-1753)
 template <typename T>
 __device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d, int i, double dtd,
-                          T *__restrict__ out, long long fo, long long fsz) {
+                          T *__restrict__ out, long long fo) {
     const T half = T(0.5), one = T(1);
     const T gamma = (T)G.gamma;
     const T smallp = (T)(kSmallr * (kSmallc * kSmallc) / G.gamma);
@@ -709,14 +730,16 @@ __device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, lon
     double dsd;
     if (d == 0) dsd = G.dy * G.dz; else if (d == 1) dsd = G.dx * G.dz; else dsd = G.dx * G.dy;
     const T ds = (T)dsd, dt = (T)dtd;
-    T *o = out + fo;
-    o[0 * fsz] = f[0] * ds * dt;                 // rho
-    o[1 * fsz] = f[1] * ds * dt;                 // E
-    o[(2 + ln - IU) * fsz] = f[2] * ds * dt;      // normal momentum
-    o[(2 + lt1 - IU) * fsz] = f[4] * ds * dt;     // first tangential momentum
-    o[(2 + lt2 - IU) * fsz] = f[6] * ds * dt;     // second tangential momentum
-    o[5 * fsz] = pg;                             // p*_T (zero unless HLLD)
-    if (G.ndim == 2) o[6 * fsz] = f[7] * ds * dt;  // B_t2 = B_z
+    T o[8];
+    o[0] = f[0] * ds * dt;                       // rho
+    o[1] = f[1] * ds * dt;                       // E
+    o[2 + ln - IU] = f[2] * ds * dt;             // normal momentum
+    o[2 + lt1 - IU] = f[4] * ds * dt;            // first tangential momentum
+    o[2 + lt2 - IU] = f[6] * ds * dt;            // second tangential momentum
+    o[5] = pg;                                   // p*_T (zero unless HLLD)
+    o[6] = (G.ndim == 2) ? f[7] * ds * dt : T(0);  // B_t2 = B_z
+    o[7] = T(0);
+    store8(out + fo * kFluxComp, o);
 }
 
 // one edge EMF (riemann_solver_magnetic, solver_magnetic.f90:79-230); e = edge direction
@@ -818,9 +841,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__res
     const CoreView<T> cv{core, G.csz};
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const long long c = G.cidx(i, j, k);
-    if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t, G.fsz);
-    if (i <= nx && k <= nz) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t, G.fsz);
-    if (i <= nx && j <= ny) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t, G.fsz);
+    if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
+    if (i <= nx && k <= nz) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
+    if (i <= nx && j <= ny) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
     if (k <= nz) ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
     if (j <= ny) ey[t] = edge_emf(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
     if (i <= nx) ex[t] = edge_emf(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
@@ -836,8 +859,8 @@ __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restri
     const double dt = S->dt;
     const CoreView<T> cv{core, G.csz};
     const long long c = G.cidx(i, j, 1);
-    if (j <= G.ny) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t, G.fsz);
-    if (i <= G.nx) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t, G.fsz);
+    if (j <= G.ny) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t);
+    if (i <= G.nx) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t);
     ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, 1), G.cidx(i, j - 1, 1), G.cidx(i - 1, j, 1), c, 2, i, dt);
 }
 
@@ -868,11 +891,19 @@ __device__ __forceinline__ int wrap1(int j, int n) {
     return (m < 0 ? m + n : m) + 1;
 }
 
+// shear offset at time + frac*dt, computed once per step phase instead of per thread
+__global__ void k_shear_offset(Geo G, Scalars *S, double frac) {
+    const ShearRemap r = shear_offset(G, S->time + frac * S->dt);
+    S->sh_jp = r.jp;
+    S->sh_epsi = r.epsi;
+}
+
 // shearing_flux / shearing_emf average of a face quantity on the inner (side 0)
 // or outer (side 1) x boundary (shearingbox.f90:250-280, 339-380)
 template <typename T>
-__device__ __forceinline__ T shear_avg(const Geo &G, const ShearRemap &sr, const T *a, long long comp_off, int side,
-                                       int j, int k) {
+__device__ __forceinline__ T shear_avg(const Geo &G, const ShearRemap &sr, const T *a, int stride, int side, int j,
+                                       int k) {
+    auto at = [&](int ii, int jj) { return ld(a + G.fidx(ii, jj, k) * stride); };
     const int ny = G.ny;
     const T one = T(1), half = T(0.5);
     if (side == 0) {
@@ -882,8 +913,7 @@ __device__ __forceinline__ T shear_avg(const Geo &G, const ShearRemap &sr, const
         jremap = wrap1(jremap, ny);
         jremapp = wrap1(jremapp, ny);
         const T eps = (T)(1.0 - sr.epsi / G.dy);
-        T v = ld(a + comp_off + G.fidx(1, j, k)) + (one - eps) * ld(a + comp_off + G.fidx(G.nx + 1, jremap, k))
-            + eps * ld(a + comp_off + G.fidx(G.nx + 1, jremapp, k));
+        T v = at(1, j) + (one - eps) * at(G.nx + 1, jremap) + eps * at(G.nx + 1, jremapp);
         return half * v;
     } else {
         int jremap = j + sr.jp, jremapp = jremap + 1;
@@ -892,8 +922,7 @@ __device__ __forceinline__ T shear_avg(const Geo &G, const ShearRemap &sr, const
         jremap = wrap1(jremap, ny);
         jremapp = wrap1(jremapp, ny);
         const T eps = (T)(sr.epsi / G.dy);
-        T v = ld(a + comp_off + G.fidx(G.nx + 1, j, k)) + (one - eps) * ld(a + comp_off + G.fidx(1, jremap, k))
-            + eps * ld(a + comp_off + G.fidx(1, jremapp, k));
+        T v = at(G.nx + 1, j) + (one - eps) * at(1, jremap) + eps * at(1, jremapp);
         return half * v;
     }
 }
@@ -946,28 +975,53 @@ __device__ double shear_ghost(const Geo &G, const Store &U, const ShearRemap &sr
          + lambda * (sslope(G, U, v, src, jremapp, k) - sslope(G, U, v, src, jremap, k));
 }
 
+// number of ghost cells: the z-ghost planes, the y-ghost rows of the active planes and
+// the x-ghost cells of the active rows
+__host__ __device__ __forceinline__ long long ghost_cells(const Geo &G) {
+    const long long nA = (G.ndim == 3) ? 6LL * G.NX * G.NY : 0;
+    const long long nB = 6LL * G.NX * (G.ndim == 3 ? G.nz : 1);
+    const long long nC = 6LL * G.ny * (G.ndim == 3 ? G.nz : 1);
+    return nA + nB + nC;
+}
+
 template <class Store>
 __global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, const Scalars *S) {
-    const long long n = (long long)G.NX * G.NY * G.NZ;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int i = (int)(t % G.NX) - 2;
-    const long long r = t / G.NX;
-    const int j = (G.ndim > 1) ? (int)(r % G.NY) - 2 : 1;
-    const int k = (G.ndim == 3) ? (int)(r / G.NY) - 2 : 1;
-    const bool gx = (i < 1 || i > G.nx), gy = (G.ndim > 1) && (j < 1 || j > G.ny), gz = (G.ndim == 3) && (k < 1 || k > G.nz);
-    if (!gx && !gy && !gz) return;
+    if (t >= ghost_cells(G)) return;
+    const long long nA = (G.ndim == 3) ? 6LL * G.NX * G.NY : 0;
+    const long long nB = 6LL * G.NX * (G.ndim == 3 ? G.nz : 1);
+    auto ghost = [](int g, int n) { return g < 3 ? g - 2 : n + g - 2; };  // 0..5 -> -2,-1,0,n+1,n+2,n+3
+    int i, j, k;
+    if (t < nA) {
+        i = (int)(t % G.NX) - 2;
+        const long long r = t / G.NX;
+        j = (int)(r % G.NY) - 2;
+        k = ghost((int)(r / G.NY), G.nz);
+    } else if (t - nA < nB) {
+        const long long u = t - nA;
+        i = (int)(u % G.NX) - 2;
+        const long long r = u / G.NX;
+        j = ghost((int)(r % 6), G.ny);
+        k = (G.ndim == 3) ? (int)(r / 6) + 1 : 1;
+    } else {
+        const long long u = t - nA - nB;
+        i = ghost((int)(u % 6), G.nx);
+        const long long r = u / 6;
+        j = (int)(r % G.ny) + 1;
+        k = (G.ndim == 3) ? (int)(r / G.ny) + 1 : 1;
+    }
+    const bool gx = (i < 1 || i > G.nx);
     const int jj = (G.ndim > 1) ? map_bc(G.bc[1], j, G.ny) : 1;
     const int kk = (G.ndim == 3) ? map_bc(G.bc[2], k, G.nz) : 1;
-    const long long c = t;
+    const long long c = G.idx(i, j, k);
     if (!gx || G.bc[0] != DG_BC_SHEARINGBOX) {
         const int ii = map_bc(G.bc[0], i, G.nx);
         const long long src = G.idx(ii, jj, kk);
         for (int v = 0; v < nv; v++) U.set(G, v, c, U.get(G, v, src));
         return;
     }
-    // shear-periodic x ghost (only with ndim = 3)
-    const ShearRemap sr = shear_offset(G, S->time + S->dt);
+    // shear-periodic x ghost (only with ndim = 3); offset for time+dt from k_shear_offset
+    const ShearRemap sr{S->sh_epsi, S->sh_jp};
     for (int v = 0; v < nv; v++) {
         if (v == IA && i == G.nx + 1) {
             // the outer face keeps its own (CT-updated) value; ghost j/k copy it
@@ -1012,7 +1066,7 @@ __global__ void k_f64_to_state(Geo G, const double *__restrict__ in, int nv, Sto
 }
 
 // ---------------------------------------------------------------------------
-// FARGO, fargo.f90:17-288 (FP64 arithmetic on the state in both paths)
+// FARGO, fargo.f90:17-288, FP64 (the FP32 path remaps with FP32 increments instead)
 // ---------------------------------------------------------------------------
 struct FargoShift {
     double vK, eps;
