@@ -300,7 +300,7 @@ int dg_init(const dg_params *p, dg_ctx **out) {
     if (p->precision == DG_PREC_FP32 && (rc = alloc(c, &c->B.stage, nt * c->nv))) return bail(rc);
     if ((rc = alloc_w(c, &c->B.Q, nt * 8))) return bail(rc);
     const int ncore = p->ndim == 3 ? dg::kCore3 : dg::kCore2;
-    if ((rc = alloc_w(c, &c->B.core, (size_t)G.csz * ncore))) return bail(rc);
+    if ((rc = alloc_w(c, &c->B.core, (size_t)dg::core_elems(G.csz, ncore)))) return bail(rc);
     for (int d = 0; d < p->ndim; d++)
         if ((rc = alloc_w(c, &c->B.flx[d], (size_t)G.fsz * dg::kFluxComp))) return bail(rc);
     for (int d = 0; d < 3; d++) {

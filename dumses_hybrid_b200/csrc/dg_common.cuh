@@ -80,6 +80,14 @@ struct Scalars {
 // number of trace-core fields per cell
 constexpr int kCore3 = 47;
 constexpr int kCore2 = 30;
+// the core is stored in blocks of kCoreLane cells, each block field-major
+constexpr int kCoreLane = 32;
+__host__ __device__ __forceinline__ long long core_base(long long c, int nf) {
+    return (c >> 5) * (long long)(nf * kCoreLane) + (c & (kCoreLane - 1));
+}
+__host__ __device__ __forceinline__ long long core_elems(long long csz, int nf) {
+    return (csz + kCoreLane - 1) / kCoreLane * kCoreLane * nf;
+}
 
 // face flux components, stored face-major (8 contiguous values per face): rho, E,
 // rho u, rho v, rho w (scaled by area*dt as compflux does), p*_tot, Bz (2D only), pad

@@ -85,6 +85,12 @@ __device__ void hll1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int iso) 
     T ul = ql[2], ur = qr[2];
     T sl = mn(mn(ul, ur) - mx(vleft, vright), T(0));
     T sr = mx(mx(ul, ur) + mx(vleft, vright), T(0));
+    if constexpr (sizeof(T) == 4) {
+        const T is = T(1) / (sr - sl);
+#pragma unroll
+        for (int n = 0; n < 8; n++) f[n] = (sr * fl[n] - sl * fr[n] + sr * sl * (cr[n] - cl[n])) * is;
+        return;
+    }
 #pragma unroll
     for (int n = 0; n < 8; n++) f[n] = (sr * fl[n] - sl * fr[n] + sr * sl * (cr[n] - cl[n])) / (sr - sl);
 }
@@ -99,9 +105,124 @@ __device__ void upwind1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int is
     for (int n = 0; n < 8; n++) f[n] = half * (fl[n] + fr[n]) - fab(vleft) * half * (cr[n] - cl[n]);
 }
 
+// ---------------------------------------------------------------------------
+// FP32 forms of the same solvers for the mixed path: identical formulas, with each
+// repeated divisor turned into one reciprocal (or reciprocal square root) and the
+// fast-speed discriminant clamped at zero against FP32 rounding.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float cfast_r(float gamma, float p, float irho, float a, float b, float c) {
+    const float c2 = gamma * p * irho;
+    const float d2 = 0.5f * (c2 + (a * a + b * b + c * c) * irho);
+    return sqrtf(d2 + sqrtf(fmaxf(d2 * d2 - c2 * a * a * irho, 0.0f)));
+}
+
+__device__ __forceinline__ void hlld1d_f(const float *ql, const float *qr, float *f, float &pg, float gamma,
+                                         float ciso, int iso) {
+    const float half = 0.5f, zero = 0.0f;
+    const float rl = ql[0], ul = ql[2], vl = ql[4], bl = ql[5], wl = ql[6], cl = ql[7];
+    const float rr = qr[0], ur = qr[2], vr = qr[4], br = qr[5], wr = qr[6], cr = qr[7];
+    const float entho = 1.0f / (gamma - 1.0f);
+    const float a = half * (ql[3] + qr[3]);
+    const float sgnm = copysignf(1.0f, a);
+    float ploc, proc;
+    if (iso) { ploc = rl * (ciso * ciso); proc = rr * (ciso * ciso); }
+    else { ploc = ql[1]; proc = qr[1]; }
+    const float emagl = half * (a * a + bl * bl + cl * cl);
+    const float etotl = ploc * entho + half * (ul * ul + vl * vl + wl * wl) * rl + emagl;
+    const float ptotl = ploc + emagl;
+    const float vdotbl = ul * a + vl * bl + wl * cl;
+    const float emagr = half * (a * a + br * br + cr * cr);
+    const float etotr = proc * entho + half * (ur * ur + vr * vr + wr * wr) * rr + emagr;
+    const float ptotr = proc + emagr;
+    const float vdotbr = ur * a + vr * br + wr * cr;
+    const float cf = fmaxf(cfast_r(gamma, ploc, 1.0f / rl, a, bl, cl), cfast_r(gamma, proc, 1.0f / rr, a, br, cr));
+    const float sl = fminf(ul, ur) - cf;
+    const float sr = fmaxf(ul, ur) + cf;
+    const float rcl = rl * (ul - sl);
+    const float rcr = rr * (sr - ur);
+    const float irc = 1.0f / (rcr + rcl);
+    const float ustar = (rcr * ur + rcl * ul + (ptotl - ptotr)) * irc;
+    const float ptotstar = (rcr * ptotl + rcl * ptotr + rcl * rcr * (ul - ur)) * irc;
+    // left star region
+    const float isl = 1.0f / (sl - ustar);
+    const float rstarl = rl * (sl - ul) * isl;
+    float estar = rl * (sl - ul) * (sl - ustar) - a * a;
+    const float el = rl * (sl - ul) * (sl - ul) - a * a;
+    float vstarl = vl, bstarl = bl, wstarl = wl, cstarl = cl;
+    if (estar != zero) {
+        const float ie = 1.0f / estar;
+        vstarl = vl - a * bl * (ustar - ul) * ie;
+        bstarl = bl * el * ie;
+        wstarl = wl - a * cl * (ustar - ul) * ie;
+        cstarl = cl * el * ie;
+    }
+    const float vdotbstarl = ustar * a + vstarl * bstarl + wstarl * cstarl;
+    const float etotstarl = ((sl - ul) * etotl - ptotl * ul + ptotstar * ustar + a * (vdotbl - vdotbstarl)) * isl;
+    const float rsl = rsqrtf(rstarl);
+    const float sqrrstarl = rstarl * rsl;
+    const float sal = ustar - fabsf(a) * rsl;
+    // right star region
+    const float isr = 1.0f / (sr - ustar);
+    const float rstarr = rr * (sr - ur) * isr;
+    estar = rr * (sr - ur) * (sr - ustar) - a * a;
+    const float er = rr * (sr - ur) * (sr - ur) - a * a;
+    float vstarr = vr, bstarr = br, wstarr = wr, cstarr = cr;
+    if (estar != zero) {
+        const float ie = 1.0f / estar;
+        vstarr = vr - a * br * (ustar - ur) * ie;
+        bstarr = br * er * ie;
+        wstarr = wr - a * cr * (ustar - ur) * ie;
+        cstarr = cr * er * ie;
+    }
+    const float vdotbstarr = ustar * a + vstarr * bstarr + wstarr * cstarr;
+    const float etotstarr = ((sr - ur) * etotr - ptotr * ur + ptotstar * ustar + a * (vdotbr - vdotbstarr)) * isr;
+    const float rsr = rsqrtf(rstarr);
+    const float sqrrstarr = rstarr * rsr;
+    const float sar = ustar + fabsf(a) * rsr;
+    // double star region
+    const float isum = 1.0f / (sqrrstarl + sqrrstarr);
+    const float vstarstar = (sqrrstarl * vstarl + sqrrstarr * vstarr + sgnm * (bstarr - bstarl)) * isum;
+    const float wstarstar = (sqrrstarl * wstarl + sqrrstarr * wstarr + sgnm * (cstarr - cstarl)) * isum;
+    const float bstarstar = (sqrrstarl * bstarr + sqrrstarr * bstarl + sgnm * sqrrstarl * sqrrstarr * (vstarr - vstarl)) * isum;
+    const float cstarstar = (sqrrstarl * cstarr + sqrrstarr * cstarl + sgnm * sqrrstarl * sqrrstarr * (wstarr - wstarl)) * isum;
+    const float vdotbstarstar = ustar * a + vstarstar * bstarstar + wstarstar * cstarstar;
+    // sample at x/t = 0
+    float ro, uo, vo, wo, bo, co, ptoto, etoto, vdotbo;
+    if (sl > zero) {
+        ro = rl; uo = ul; vo = vl; wo = wl; bo = bl; co = cl; ptoto = ptotl; etoto = etotl; vdotbo = vdotbl;
+    } else if (sal > zero) {
+        ro = rstarl; uo = ustar; vo = vstarl; wo = wstarl; bo = bstarl; co = cstarl;
+        ptoto = ptotstar; etoto = etotstarl; vdotbo = vdotbstarl;
+    } else if (ustar > zero) {
+        ro = rstarl; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
+        ptoto = ptotstar; etoto = etotstarl - sgnm * sqrrstarl * (vdotbstarl - vdotbstarstar); vdotbo = vdotbstarstar;
+    } else if (sar > zero) {
+        ro = rstarr; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
+        ptoto = ptotstar; etoto = etotstarr + sgnm * sqrrstarr * (vdotbstarr - vdotbstarstar); vdotbo = vdotbstarstar;
+    } else if (sr > zero) {
+        ro = rstarr; uo = ustar; vo = vstarr; wo = wstarr; bo = bstarr; co = cstarr;
+        ptoto = ptotstar; etoto = etotstarr; vdotbo = vdotbstarr;
+    } else {
+        ro = rr; uo = ur; vo = vr; wo = wr; bo = br; co = cr; ptoto = ptotr; etoto = etotr; vdotbo = vdotbr;
+    }
+    f[0] = ro * uo;
+    f[1] = (etoto + ptoto) * uo - a * vdotbo;
+    f[2] = ro * uo * uo - a * a;
+    f[3] = zero;
+    f[4] = ro * uo * vo - a * bo;
+    f[5] = bo * uo - a * vo;
+    f[6] = ro * uo * wo - a * co;
+    f[7] = co * uo - a * wo;
+    pg = ptoto;
+}
+
 // HLLD; returns p*_T in pg
 template <typename T>
 __device__ void hlld1d(const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso, int iso) {
+    if constexpr (sizeof(T) == 4) {
+        hlld1d_f(ql, qr, f, pg, gamma, ciso, iso);
+        return;
+    }
     const T one = T(1), half = T(0.5), zero = T(0);
     const T rl = ql[0], ul = ql[2], vl = ql[4], bl = ql[5], wl = ql[6], cl = ql[7];
     const T rr = qr[0], ur = qr[2], vr = qr[4], br = qr[5], wr = qr[6], cr = qr[7];
@@ -243,8 +364,89 @@ __device__ T llf2d(const Corners<T> &c, T dt, T gamma, T ciso, int iso) {
     return emf * dt;
 }
 
+// FP32 form of hlld2d: per corner one reciprocal density shared by the x and y fast
+// speeds, reciprocal square roots of the star densities
+__device__ __forceinline__ float hlld2d_f(const Corners<float> &c, float dt, float gamma) {
+    const float half = 0.5f, zero = 0.0f, smallc = (float)kSmallc;
+    const float iLL = 1.0f / c.rLL, iLR = 1.0f / c.rLR, iRL = 1.0f / c.rRL, iRR = 1.0f / c.rRR;
+    const float cfx = mx4(cfast_r(gamma, c.pLL, iLL, c.ALL, c.BLL, c.CLL), cfast_r(gamma, c.pLR, iLR, c.ALR, c.BLR, c.CLR),
+                          cfast_r(gamma, c.pRL, iRL, c.ARL, c.BRL, c.CRL), cfast_r(gamma, c.pRR, iRR, c.ARR, c.BRR, c.CRR));
+    const float cfy = mx4(cfast_r(gamma, c.pLL, iLL, c.BLL, c.ALL, c.CLL), cfast_r(gamma, c.pLR, iLR, c.BLR, c.ALR, c.CLR),
+                          cfast_r(gamma, c.pRL, iRL, c.BRL, c.ARL, c.CRL), cfast_r(gamma, c.pRR, iRR, c.BRR, c.ARR, c.CRR));
+    const float SL = mn4(c.uLL, c.uLR, c.uRL, c.uRR) - cfx;
+    const float SR = mx4(c.uLL, c.uLR, c.uRL, c.uRR) + cfx;
+    const float SB = mn4(c.vLL, c.vLR, c.vRL, c.vRR) - cfy;
+    const float ST = mx4(c.vLL, c.vLR, c.vRL, c.vRR) + cfy;
+    const float PtotLL = c.pLL + half * (c.ALL * c.ALL + c.BLL * c.BLL + c.CLL * c.CLL);
+    const float PtotLR = c.pLR + half * (c.ALR * c.ALR + c.BLR * c.BLR + c.CLR * c.CLR);
+    const float PtotRL = c.pRL + half * (c.ARL * c.ARL + c.BRL * c.BRL + c.CRL * c.CRL);
+    const float PtotRR = c.pRR + half * (c.ARR * c.ARR + c.BRR * c.BRR + c.CRR * c.CRR);
+    const float rcLLx = c.rLL * (c.uLL - SL), rcRLx = c.rRL * (SR - c.uRL);
+    const float rcLRx = c.rLR * (c.uLR - SL), rcRRx = c.rRR * (SR - c.uRR);
+    const float rcLLy = c.rLL * (c.vLL - SB), rcLRy = c.rLR * (ST - c.vLR);
+    const float rcRLy = c.rRL * (c.vRL - SB), rcRRy = c.rRR * (ST - c.vRR);
+    const float ustar = (rcLLx * c.uLL + rcLRx * c.uLR + rcRLx * c.uRL + rcRRx * c.uRR + (PtotLL - PtotRL + PtotLR - PtotRR))
+                      / (rcLLx + rcLRx + rcRLx + rcRRx);
+    const float vstar = (rcLLy * c.vLL + rcLRy * c.vLR + rcRLy * c.vRL + rcRRy * c.vRR + (PtotLL - PtotLR + PtotRL - PtotRR))
+                      / (rcLLy + rcLRy + rcRLy + rcRRy);
+    const float SLustar = 1.0f / (SL - ustar), SRustar = 1.0f / (SR - ustar);
+    const float SBvstar = 1.0f / (SB - vstar), STvstar = 1.0f / (ST - vstar);
+    const float fLLx = (SL - c.uLL) * SLustar, fLLy = (SB - c.vLL) * SBvstar;
+    const float fLRx = (SL - c.uLR) * SLustar, fLRy = (ST - c.vLR) * STvstar;
+    const float fRLx = (SR - c.uRL) * SRustar, fRLy = (SB - c.vRL) * SBvstar;
+    const float fRRx = (SR - c.uRR) * SRustar, fRRy = (ST - c.vRR) * STvstar;
+    const float BstarLL = c.BLL * fLLx, AstarLL = c.ALL * fLLy;
+    const float BstarLR = c.BLR * fLRx, AstarLR = c.ALR * fLRy;
+    const float BstarRL = c.BRL * fRLx, AstarRL = c.ARL * fRLy;
+    const float BstarRR = c.BRR * fRRx, AstarRR = c.ARR * fRRy;
+    const float EstarLLx = ustar * BstarLL - c.vLL * c.ALL, EstarLLy = c.uLL * c.BLL - vstar * AstarLL;
+    const float EstarLRx = ustar * BstarLR - c.vLR * c.ALR, EstarLRy = c.uLR * c.BLR - vstar * AstarLR;
+    const float EstarRLx = ustar * BstarRL - c.vRL * c.ARL, EstarRLy = c.uRL * c.BRL - vstar * AstarRL;
+    const float EstarRRx = ustar * BstarRR - c.vRR * c.ARR, EstarRRy = c.uRR * c.BRR - vstar * AstarRR;
+    const float EstarLL = ustar * BstarLL - vstar * AstarLL, EstarLR = ustar * BstarLR - vstar * AstarLR;
+    const float EstarRL = ustar * BstarRL - vstar * AstarRL, EstarRR = ustar * BstarRR - vstar * AstarRR;
+    // 1/sqrt of rstar, rstarx, rstary per corner (rstar = rho fx fy)
+    const float qLL = rsqrtf(c.rLL * fLLx * fLLy), qLR = rsqrtf(c.rLR * fLRx * fLRy);
+    const float qRL = rsqrtf(c.rRL * fRLx * fRLy), qRR = rsqrtf(c.rRR * fRRx * fRRy);
+    const float calfvenL = fmaxf(fmaxf(fmaxf(fmaxf(fabsf(c.ALR) * rsqrtf(c.rLR * fLRx), fabsf(AstarLR) * qLR),
+                                             fabsf(c.ALL) * rsqrtf(c.rLL * fLLx)), fabsf(AstarLL) * qLL), smallc);
+    const float calfvenR = fmaxf(fmaxf(fmaxf(fmaxf(fabsf(c.ARR) * rsqrtf(c.rRR * fRRx), fabsf(AstarRR) * qRR),
+                                             fabsf(c.ARL) * rsqrtf(c.rRL * fRLx)), fabsf(AstarRL) * qRL), smallc);
+    const float calfvenB = fmaxf(fmaxf(fmaxf(fmaxf(fabsf(c.BLL) * rsqrtf(c.rLL * fLLy), fabsf(BstarLL) * qLL),
+                                             fabsf(c.BRL) * rsqrtf(c.rRL * fRLy)), fabsf(BstarRL) * qRL), smallc);
+    const float calfvenT = fmaxf(fmaxf(fmaxf(fmaxf(fabsf(c.BLR) * rsqrtf(c.rLR * fLRy), fabsf(BstarLR) * qLR),
+                                             fabsf(c.BRR) * rsqrtf(c.rRR * fRRy)), fabsf(BstarRR) * qRR), smallc);
+    const float SAL = fminf(ustar - calfvenL, zero), SAR = fmaxf(ustar + calfvenR, zero);
+    const float SAB = fminf(vstar - calfvenB, zero), SAT = fmaxf(vstar + calfvenT, zero);
+    const float SARSAL = 1.0f / (SAR - SAL);
+    const float SATSAB = 1.0f / (SAT - SAB);
+    float E;
+    if (SB > zero) {
+        if (SL > zero) E = c.ELL;
+        else if (SR < zero) E = c.ERL;
+        else E = (SAR * EstarLLx - SAL * EstarRLx + SAR * SAL * (c.BRL - c.BLL)) * SARSAL;
+    } else if (ST < zero) {
+        if (SL > zero) E = c.ELR;
+        else if (SR < zero) E = c.ERR;
+        else E = (SAR * EstarLRx - SAL * EstarRRx + SAR * SAL * (c.BRR - c.BLR)) * SARSAL;
+    } else if (SL > zero) {
+        E = (SAT * EstarLLy - SAB * EstarLRy - SAT * SAB * (c.ALR - c.ALL)) * SATSAB;
+    } else if (SR < zero) {
+        E = (SAT * EstarRLy - SAB * EstarRRy - SAT * SAB * (c.ARR - c.ARL)) * SATSAB;
+    } else {
+        const float AstarT = (SAR * AstarRR - SAL * AstarLR) * SARSAL;
+        const float AstarB = (SAR * AstarRL - SAL * AstarLL) * SARSAL;
+        const float BstarR = (SAT * BstarRR - SAB * BstarRL) * SATSAB;
+        const float BstarL = (SAT * BstarLR - SAB * BstarLL) * SATSAB;
+        E = (SAL * SAB * EstarRR - SAL * SAT * EstarRL - SAR * SAB * EstarLR + SAR * SAT * EstarLL) * SARSAL * SATSAB
+          - SAT * SAB * SATSAB * (AstarT - AstarB) + SAR * SAL * SARSAL * (BstarR - BstarL);
+    }
+    return E * dt;
+}
+
 template <typename T>
 __device__ T hlld2d(const Corners<T> &c, T dt, T gamma) {
+    if constexpr (sizeof(T) == 4) return hlld2d_f(c, dt, gamma);
     const T one = T(1), half = T(0.5), zero = T(0), smallc = T(kSmallc);
     const T cfastLLx = cfast(gamma, c.pLL, c.rLL, c.ALL, c.BLL, c.CLL);
     const T cfastLRx = cfast(gamma, c.pLR, c.rLR, c.ALR, c.BLR, c.CLR);

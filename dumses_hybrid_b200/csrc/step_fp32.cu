@@ -2,9 +2,9 @@
 // compensated FP32 (hi, lo) state, compiled with fast FP32 math.
 //
 // FP64 is used only where it carries accuracy: the gas pressure from the total
-// energy (which cancels in low-beta zones), the CFL
-// reduction, the orbital-advection shift of each x column and the history sums.
-// Trace, Riemann solvers, fluxes, EMFs, FARGO's remap and the constrained-transport
+// energy (which cancels in low-beta zones), the minimum of the CFL time steps, the
+// orbital-advection shift of each x column and the history sums.  Signal speeds,
+// trace, Riemann solvers, fluxes, EMFs, FARGO's remap and the constrained-transport
 // increments are FP32; every update adds an FP32 increment to a (hi, lo) pair with
 // an error-free two-sum, so the state carries about 48 significant bits across steps.
 #define DG_NS f32
@@ -203,9 +203,33 @@ __global__ void __launch_bounds__(kThreads) k_update2d_hl(Geo G, StoreHL U, Stor
     }
 }
 
-// primitive variables (scheme.f90:44-86) from the compensated state: velocities and
-// cell-centred B in FP32, the pressure in FP64 as (gamma-1) (E - emag - rho eken), which
-// is (gamma-1) rho eint of the reference without its division when rho >= smallr
+// primitive variables (scheme.f90:44-86) of one cell from the compensated state,
+// without the rotation half-kick: velocities and cell-centred B in FP32, the pressure
+// in FP64 as (gamma-1) (E - emag - rho eken), which is (gamma-1) rho eint of the
+// reference without its division when rho >= smallr
+__device__ __forceinline__ void prim_hl(const Geo &G, const StoreHL &U, long long c, float q[8]) {
+    auto f = [&](int v, long long cc) { return ld(U.hi + G.sv * v + cc) + ld(U.lo + G.sv * v + cc); };
+    const double d = (double)ld(U.hi + G.sv * IR + c) + (double)ld(U.lo + G.sv * IR + c);
+    const float ri = 1.0f / (float)d;
+    q[IR] = (float)mx(d, kSmallr);
+    q[IU] = f(IU, c) * ri;
+    q[IV] = f(IV, c) * ri;
+    q[IW] = f(IW, c) * ri;
+    q[IA] = 0.5f * (f(IA, c) + f(IA, c + 1));
+    q[IB] = 0.5f * (f(IB, c) + f(IB, c + G.sy));
+    q[IC] = 0.5f * (f(IC, c) + ((G.ndim == 3) ? f(IC, c + G.sz) : f(8, c)));
+    if (G.iso) {
+        q[IP] = (float)(d * (G.ciso * G.ciso));
+    } else {
+        const double E = (double)ld(U.hi + G.sv * IP + c) + (double)ld(U.lo + G.sv * IP + c);
+        const double emag = 0.5 * ((double)q[IA] * q[IA] + (double)q[IB] * q[IB] + (double)q[IC] * q[IC]);
+        const double eken = 0.5 * ((double)q[IU] * q[IU] + (double)q[IV] * q[IV] + (double)q[IW] * q[IW]);
+        double pe = (G.gamma - 1.0) * (E - emag - d * eken);
+        if (d < kSmallr) pe = pe * (kSmallr / d);
+        q[IP] = (float)mx(pe, kSmallr * (kSmallc * kSmallc) / G.gamma);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) k_prim_hl(Geo G, StoreHL U, float *__restrict__ Q, const Scalars *S) {
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
     const long long n = (long long)ni * nj * nk;
@@ -216,35 +240,57 @@ __global__ void __launch_bounds__(kThreads) k_prim_hl(Geo G, StoreHL U, float *_
     const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
     const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
     const long long c = G.idx(i, j, k);
-    auto f = [&](int v, long long cc) { return ld(U.hi + G.sv * v + cc) + ld(U.lo + G.sv * v + cc); };
-    const double d = (double)ld(U.hi + G.sv * IR + c) + (double)ld(U.lo + G.sv * IR + c);
-    const float rho = (float)mx(d, kSmallr);
-    const float ri = 1.0f / (float)d;
-    float u = f(IU, c) * ri, v = f(IV, c) * ri, w = f(IW, c) * ri;
-    const float bx = 0.5f * (f(IA, c) + f(IA, c + 1));
-    const float by = 0.5f * (f(IB, c) + f(IB, c + G.sy));
-    const float bz = 0.5f * (f(IC, c) + ((G.ndim == 3) ? f(IC, c + G.sz) : f(8, c)));
-    float p;
-    if (G.iso) {
-        p = (float)(d * (G.ciso * G.ciso));
-    } else {
-        const double E = (double)ld(U.hi + G.sv * IP + c) + (double)ld(U.lo + G.sv * IP + c);
-        const double emag = 0.5 * ((double)bx * bx + (double)by * by + (double)bz * bz);
-        const double eken = 0.5 * ((double)u * u + (double)v * v + (double)w * w);
-        double pe = (G.gamma - 1.0) * (E - emag - d * eken);
-        if (d < kSmallr) pe = pe * (kSmallr / d);
-        const double smallp = kSmallr * (kSmallc * kSmallc) / G.gamma;
-        p = (float)mx(pe, smallp);
-    }
-    if (G.omega0 > 0.0) {
+    float q[8];
+    prim_hl(G, U, c, q);
+    if (G.omega0 > 0.0) {  // rotation half-kick, scheme.f90:78-85
         const float om = (float)G.omega0, hdt = 0.5f * (float)S->dt;
-        const float dvx = 2.0f * om * v, dvy = -(0.5f * om * u);
-        u = u + dvx * hdt;
-        v = v + dvy * hdt;
+        const float dvx = 2.0f * om * q[IV], dvy = -(0.5f * om * q[IU]);
+        q[IU] = q[IU] + dvx * hdt;
+        q[IV] = q[IV] + dvy * hdt;
     }
-    float *q = Q + c;
-    q[G.sv * IR] = rho; q[G.sv * IU] = u; q[G.sv * IV] = v; q[G.sv * IW] = w;
-    q[G.sv * IP] = p; q[G.sv * IA] = bx; q[G.sv * IB] = by; q[G.sv * IC] = bz;
+#pragma unroll
+    for (int v = 0; v < 8; v++) Q[G.sv * v + c] = q[v];
+}
+
+// compute_dt (physics.f90:42-121): FP32 signal speeds from prim_hl, the minimum of
+// the per-cell time steps taken in FP64 on their bit patterns
+__global__ void __launch_bounds__(kThreads) k_dt_hl(Geo G, StoreHL U, Scalars *S) {
+    const long long n = (long long)G.nx * G.ny * G.nz;
+    const float gamma = (float)G.gamma;
+    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
+    const float vsh = ((G.omega0 > 0.0) && !G.fargo) ? (float)(1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5) : 0.0f;
+    float best = __int_as_float(0x7f800000);  // +inf
+    int bad = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % G.nx) + 1;
+        const long long r = t / G.nx;
+        const int j = (int)(r % G.ny) + 1;
+        const int k = (int)(r / G.ny) + 1;
+        float q[8];
+        prim_hl(G, U, G.idx(i, j, k), q);
+        const float ir = 1.0f / q[IR];
+        float sum = 0.0f;
+        if (G.nx != 1) sum += (cfast_r(gamma, q[IP], ir, q[IA], q[IB], q[IC]) + fabsf(q[IU])) * rdx;
+        if (G.ny != 1) sum += (cfast_r(gamma, q[IP], ir, q[IB], q[IC], q[IA]) + fabsf(q[IV]) + vsh) * rdy;
+        if (G.ndim == 3 && G.nz != 1) sum += (cfast_r(gamma, q[IP], ir, q[IC], q[IA], q[IB]) + fabsf(q[IW])) * rdz;
+        const float cdt = 1.0f / sum;
+        if (!(cdt > 0.0f)) bad = 1;  // NaN or non-positive
+        else best = fminf(best, cdt);
+    }
+    unsigned long long b = (unsigned long long)__double_as_longlong((double)best);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+        b = ob < b ? ob : b;
+    }
+    __shared__ unsigned long long sb[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = b;
+    if (bad) S->err = DG_ERR_STATE;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = sb[0];
+        for (int w = 1; w < kThreads / 32; w++) m = sb[w] < m ? sb[w] : m;
+        atomicMin(&S->red, m);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -409,7 +455,7 @@ int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     const long long n = (long long)G.nx * G.ny * G.nz;
     long long nb = (n + kThreads - 1) / kThreads;
     if (nb > 148 * 16) nb = 148 * 16;
-    TIMED(KS_DT, s, (k_dt<StoreHL><<<(unsigned)nb, kThreads, 0, s>>>(G, st(B, cur), B.S)));
+    TIMED(KS_DT, s, (k_dt_hl<<<(unsigned)nb, kThreads, 0, s>>>(G, st(B, cur), B.S)));
     TIMED(KS_DT, s, (k_dt_final<<<1, 1, 0, s>>>(G, B.S)));
     return 3;
 }

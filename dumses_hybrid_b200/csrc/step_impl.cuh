@@ -474,8 +474,8 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
     const T sCL0 = +(FRL - FLL) * dtdx * half - (ERL - ELL) * dtdy * half;
     const T sCR0 = +(FRR - FLR) * dtdx * half - (ERR - ELR) * dtdy * half;
 
-    T *o = core + t;
-    const long long cs = G.csz;
+    T *o = core + core_base(t, kCore3);
+    const int cs = kCoreLane;
     o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
     o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
     o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
@@ -540,8 +540,8 @@ __global__ void __launch_bounds__(kThreads) k_trace2d(Geo G, const T *__restrict
     const T sBL0 = -(ERL - ELL) * half * dtdx;
     const T sBR0 = -(ERR - ELR) * half * dtdx;
 
-    T *o = core + t;
-    const long long cs = G.csz;
+    T *o = core + core_base(t, kCore2);
+    const int cs = kCoreLane;
     o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
     o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
     o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
@@ -570,11 +570,16 @@ enum {
     D_AL = 22, D_AR, D_BL, D_BR, D_DALY, D_DARY, D_DBLX, D_DBRX
 };
 
+// the core in blocks of kCoreLane cells: field f of cell c at core_base(c, nf) + f * kCoreLane,
+// so one warp reads one field of 32 consecutive cells as one 128-byte line and all fields of
+// a cell sit at small constant offsets from one address
 template <typename T>
 struct CoreView {
     const T *core;
-    long long cs;
-    __device__ __forceinline__ T f(int field, long long c) const { return ld(core + cs * field + c); }
+    int nf;  // fields per cell (kCore3 or kCore2)
+    __device__ __forceinline__ T f(int field, long long c) const {
+        return ld(core + core_base(c, nf) + field * kCoreLane);
+    }
 };
 
 // face state (uin order r,u,v,w,p,A,B,C) of a cell on its minus (sgn=-1, "qp")
@@ -838,7 +843,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__res
     const int j = (int)(r % G.FY) + 1;
     const int k = (int)(r / G.FY) + 1;
     const double dt = S->dt;
-    const CoreView<T> cv{core, G.csz};
+    const CoreView<T> cv{core, kCore3};
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const long long c = G.cidx(i, j, k);
     if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
@@ -857,7 +862,7 @@ __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restri
     const int i = (int)(t % G.FX) + 1;
     const int j = (int)(t / G.FX) + 1;
     const double dt = S->dt;
-    const CoreView<T> cv{core, G.csz};
+    const CoreView<T> cv{core, kCore2};
     const long long c = G.cidx(i, j, 1);
     if (j <= G.ny) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t);
     if (i <= G.nx) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t);
