@@ -74,6 +74,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
     lib = ctypes.CDLL(str(p))
     c_p = ctypes.POINTER(DgParams)
     vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+    fp = ctypes.POINTER(ctypes.c_float)
     sig = {
         "dg_default_params": (None, [c_p]),
         "dg_uin_size": (ctypes.c_longlong, [c_p]),
@@ -98,6 +99,23 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_profile_slot_name": (ctypes.c_char_p, [ctypes.c_int]),
         "dg_debug_copy": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
         "dg_condinit": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong, dp]),
+        "dg_nn_param_count": (ctypes.c_longlong, []),
+        "dg_nn_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(vp)]),
+        "dg_nn_destroy": (ctypes.c_int, [vp]),
+        "dg_nn_set_samples": (ctypes.c_int, [vp, fp, fp, ctypes.c_longlong]),
+        "dg_nn_reserve_samples": (ctypes.c_int, [vp, ctypes.c_longlong]),
+        "dg_nn_sample_count": (ctypes.c_longlong, [vp]),
+        "dg_nn_samples_copy": (ctypes.c_int, [vp, ctypes.c_longlong, ctypes.c_longlong, fp, fp]),
+        "dg_nn_harvest": (ctypes.c_int, [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+        "dg_nn_train": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, fp]),
+        "dg_nn_gradients": (ctypes.c_int, [vp, fp, fp, ctypes.c_int, fp, fp]),
+        "dg_nn_forward": (ctypes.c_int, [vp, fp, ctypes.c_longlong, fp]),
+        "dg_nn_get_params": (ctypes.c_int, [vp, fp, ctypes.c_longlong]),
+        "dg_nn_set_params": (ctypes.c_int, [vp, fp, ctypes.c_longlong]),
+        "dg_nn_fit_envelope": (ctypes.c_int, [vp, ctypes.c_float]),
+        "dg_nn_set_gates": (ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
+        "dg_attach_surrogate": (ctypes.c_int, [vp, vp]),
+        "dg_surrogate_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -285,7 +303,7 @@ class Context:
 
     def profile_read(self) -> dict[str, tuple[float, int]]:
         """{kernel slot: (total ms, launches)} since the last read."""
-        n = 12
+        n = 13
         ms = np.zeros(n)
         cnt = (ctypes.c_longlong * n)()
         _check(self.lib.dg_profile_read(self.h, self._ptr(ms), cnt, n))
@@ -298,3 +316,109 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.dg_kernel_launches(self.h))
+
+    def attach_surrogate(self, net: "FluxNet | None") -> None:
+        """Use `net` for the faces of this FP32 context (made with surrogate=True); None detaches."""
+        _check(self.lib.dg_attach_surrogate(self.h, net.h if net is not None else None))
+
+    def surrogate_stats(self) -> tuple[int, int]:
+        """(faces seen by the network, faces that fell back to HLLD) since the last call."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self.lib.dg_surrogate_stats(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+
+N_IN, N_OUT = 17, 8
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class FluxNet:
+    """The learned face-flux network (a dg_nn of the C-ABI): 17 -> 128 -> 128 -> 128 -> 8,
+    GELU, BF16 weights with FP32 accumulation, trained on the device.  Parameters are a
+    flat float32 vector in the order W1[17][128], b1, W2[128][128], b2, W3, b3, W4[128][8], b4."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        _check(self.lib.dg_nn_create(device, seed, ctypes.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.dg_nn_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def param_count(self) -> int:
+        return int(self.lib.dg_nn_param_count())
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.param_count, dtype=np.float32)
+        _check(self.lib.dg_nn_get_params(self.h, _fptr(p), p.size))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self.lib.dg_nn_set_params(self.h, _fptr(p), p.size))
+
+    def set_samples(self, x: np.ndarray, t: np.ndarray) -> None:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        _check(self.lib.dg_nn_set_samples(self.h, _fptr(x), _fptr(t), x.shape[0]))
+
+    @property
+    def sample_count(self) -> int:
+        return int(self.lib.dg_nn_sample_count(self.h))
+
+    def samples(self, first: int = 0, count: int | None = None) -> tuple[np.ndarray, np.ndarray]:
+        n = self.sample_count - first if count is None else count
+        x = np.zeros((n, N_IN), dtype=np.float32)
+        t = np.zeros((n, N_OUT), dtype=np.float32)
+        _check(self.lib.dg_nn_samples_copy(self.h, first, n, _fptr(x), _fptr(t)))
+        return x, t
+
+    def harvest(self, ctx: Context, stride: int = 1) -> int:
+        """Append the interfaces of an FP32 context's current state, with HLLD labels."""
+        n = ctypes.c_longlong()
+        _check(self.lib.dg_nn_harvest(ctx.h, self.h, stride, ctypes.byref(n)))
+        return n.value
+
+    def train(self, steps: int, batch: int = 65536, lr: float = 1e-3) -> float:
+        loss = ctypes.c_float()
+        _check(self.lib.dg_nn_train(self.h, steps, batch, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def gradients(self, x: np.ndarray, t: np.ndarray) -> tuple[float, np.ndarray]:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(self.param_count, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(self.lib.dg_nn_gradients(self.h, _fptr(x), _fptr(t), x.shape[0], ctypes.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], N_OUT), dtype=np.float32)
+        _check(self.lib.dg_nn_forward(self.h, _fptr(x), x.shape[0], _fptr(y)))
+        return y
+
+    def fit_envelope(self, margin: float = 0.0) -> None:
+        _check(self.lib.dg_nn_fit_envelope(self.h, margin))
+
+    def set_gates(self, jump: float = 0.1, compress: float = 0.1) -> None:
+        _check(self.lib.dg_nn_set_gates(self.h, jump, compress))

@@ -31,7 +31,8 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
 # FP32 mixed path: fast FP32 math (contraction, approximate division and sqrt, FTZ)
 EXACT = ["--fmad=false"]
 FAST = ["--use_fast_math"]
-CU_SOURCES = {"step_fp64.cu": EXACT, "step_fp32.cu": FAST, "dg_api.cu": EXACT, "dg_noalloc.cu": EXACT}
+CU_SOURCES = {"step_fp64.cu": EXACT, "step_fp32.cu": FAST, "dg_api.cu": EXACT, "dg_noalloc.cu": EXACT,
+              "nn_flux.cu": FAST}
 CXX_SOURCES = ["condinit.cpp"]
 
 

@@ -16,6 +16,7 @@
 
 #include "dumses_gpu.h"
 #include "mhd_kernels.cuh"
+#include "nn_host.h"
 
 namespace {
 // CUDA-event timing of every kernel the context enqueues, on the context's stream
@@ -43,7 +44,8 @@ struct EventTimer : dg::KernelTimer {
     }
 };
 const char *kSlotNames[dg::KS_COUNT] = {"scalars", "cfl_dt", "primitive", "trace", "riemann_flux_emf", "update_ct",
-                                       "fargo_emf", "fargo_update", "boundary", "history", "right_faces", "edge_efield"};
+                                       "fargo_emf", "fargo_update", "boundary", "history", "right_faces", "edge_efield",
+                                       "nn_faces"};
 }  // namespace
 
 namespace {
@@ -87,6 +89,8 @@ struct dg_ctx {
     double *h_hist = nullptr;       // pinned read-back of history sums
     size_t bytes = 0;
     EventTimer *timer = nullptr;    // non-null while per-kernel profiling is on
+    dg_nn *nn = nullptr;            // attached flux network (surrogate = 1)
+    dg::nn::NetView view{};         // its device view, as of dg_attach_surrogate
 };
 
 namespace {
@@ -170,7 +174,9 @@ int validate(const dg_params *p) {
     if (p->fargo && (p->ndim != 3 || p->bc[1] != DG_BC_PERIODIC))
         return fail(DG_ERR_UNSUPPORTED, "FARGO needs ndim = 3 and a periodic y direction");
     if (p->precision != DG_PREC_FP64 && p->precision != DG_PREC_FP32) return fail(DG_ERR_ARG, "unknown precision");
-    if (p->surrogate) return fail(DG_ERR_UNSUPPORTED, "the flux surrogate needs the FP32 path");
+    if (p->surrogate && p->precision != DG_PREC_FP32) return fail(DG_ERR_UNSUPPORTED, "the flux surrogate needs the FP32 path");
+    if (p->surrogate && p->iriemann != DG_RIEMANN_HLLD)
+        return fail(DG_ERR_UNSUPPORTED, "the flux surrogate stands in for HLLD (iriemann = hlld)");
     return DG_OK;
 }
 
@@ -314,6 +320,12 @@ int dg_init(const dg_params *p, dg_ctx **out) {
     if (p->fargo)
         for (int d = 0; d < 2; d++)
             if ((rc = alloc(c, &c->B.femf[d], (size_t)G.fsz))) return bail(rc);
+    if (p->surrogate) {
+        for (int d = 0; d < p->ndim; d++)
+            if ((rc = alloc_bytes(c, (void **)&c->B.skip[d], (size_t)G.fsz))) return bail(rc);
+        if ((rc = alloc_bytes(c, (void **)&c->B.nn_count, 4 * sizeof(unsigned long long)))) return bail(rc);
+        c->B.nn_err = (int *)(c->B.nn_count + 2);
+    }
     if ((rc = alloc(c, &c->B.part, (size_t)(2 * p->nx + 8 * 296 + 64)))) return bail(rc);
     if ((rc = alloc(c, &c->B.hist, 16))) return bail(rc);
     {
@@ -334,7 +346,8 @@ int dg_finalize(dg_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *bufs[] = {c->B.U[0], c->B.U[1], c->B.Q, c->B.core, c->B.flx[0], c->B.flx[1], c->B.flx[2], c->B.emf[0],
                     c->B.emf[1], c->B.emf[2], c->B.femf[0], c->B.femf[1], c->B.part, c->B.hist,
-                    c->B.E[0], c->B.E[1], c->B.E[2], c->B.stage};
+                    c->B.E[0], c->B.E[1], c->B.E[2], c->B.stage, c->B.skip[0], c->B.skip[1], c->B.skip[2],
+                    c->B.nn_count};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (c->B.S) cudaFree(c->B.S);
@@ -477,6 +490,70 @@ int dg_history(dg_ctx *c, double out[9]) {
 int dg_sync(dg_ctx *c) {
     if (!c) return fail(DG_ERR_ARG, "null context");
     return bounded_sync(c->stream);
+}
+
+int dg_attach_surrogate(dg_ctx *c, dg_nn *nn) {
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    if (!c->p.surrogate) return fail(DG_ERR_ARG, "the context was made with surrogate = 0");
+    if (nn && dg_nn_device(nn) != c->p.device) return fail(DG_ERR_ARG, "network and context are on different devices");
+    DG_CUDA(cudaSetDevice(c->p.device));
+    DG_CUDA(cudaStreamSynchronize(c->stream));
+    c->nn = nn;
+    if (nn) {
+        dg_nn_view(nn, &c->view);
+        c->B.net = &c->view;
+        DG_CUDA(cudaFuncSetAttribute(dg::f32::nn_faces_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     dg::f32::nn_faces_smem()));
+    } else {
+        c->B.net = nullptr;
+    }
+    return DG_OK;
+}
+
+int dg_surrogate_stats(dg_ctx *c, long long *faces, long long *fallback) {
+    if (!c || !faces || !fallback) return fail(DG_ERR_ARG, "null argument");
+    *faces = 0;
+    *fallback = 0;
+    if (!c->p.surrogate) return DG_OK;
+    DG_CUDA(cudaSetDevice(c->p.device));
+    unsigned long long h[4] = {0, 0, 0, 0};
+    DG_CUDA(cudaMemcpyAsync(h, c->B.nn_count, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    int rc = bounded_sync(c->stream);
+    if (rc) return rc;
+    DG_CUDA(cudaMemsetAsync(c->B.nn_count, 0, 2 * sizeof(unsigned long long), c->stream));
+    *faces = (long long)h[0];
+    *fallback = (long long)h[1];
+    if ((int)h[2]) return fail(DG_ERR_TIMEOUT, "a face-network kernel gave up waiting on a tensor-core transfer");
+    return DG_OK;
+}
+
+int dg_nn_harvest(dg_ctx *c, dg_nn *nn, int stride, long long *added) {
+    if (!c || !nn || stride < 1) return fail(DG_ERR_ARG, "bad harvest arguments");
+    if (c->p.precision != DG_PREC_FP32) return fail(DG_ERR_UNSUPPORTED, "harvesting reads the FP32 trace");
+    if (dg_nn_device(nn) != c->p.device) return fail(DG_ERR_ARG, "network and context are on different devices");
+    DG_CUDA(cudaSetDevice(c->p.device));
+    TimerScope ts(c);
+    const dg::Geo &G = c->G;
+    long long cnt[3] = {0, 0, 0}, total = 0;
+    for (int d = 0; d < G.ndim; d++) {
+        cnt[d] = (dg::f32::harvest_faces(G, d) + stride - 1) / stride;
+        total += cnt[d];
+    }
+    const long long first = dg_nn_sample_count(nn);
+    int rc = dg_nn_reserve_samples(nn, first + total);
+    if (rc) return rc;
+    c->launches += dg::f32::launch_trace_only(G, c->B, c->cur, c->stream);
+    long long at = first;
+    for (int d = 0; d < G.ndim; d++) {
+        c->launches += dg::f32::launch_harvest(G, c->B, d, stride, dg_nn_sample_x(nn), dg_nn_sample_t(nn), at, cnt[d],
+                                               c->stream);
+        at += cnt[d];
+    }
+    DG_CUDA(cudaGetLastError());
+    if ((rc = bounded_sync(c->stream))) return rc;
+    dg_nn_set_count(nn, first + total);
+    if (added) *added = total;
+    return DG_OK;
 }
 
 int dg_debug_copy(dg_ctx *c, int which, double *host, long long count, long long *copied) {

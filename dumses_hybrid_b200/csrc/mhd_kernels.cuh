@@ -5,6 +5,10 @@
 
 namespace dg {
 
+namespace nn {
+struct NetView;
+}
+
 // device buffers of one context; element type of the work arrays is the compute
 // type of the path (double for FP64, float for FP32)
 struct Bufs {
@@ -21,13 +25,18 @@ struct Bufs {
     Scalars *S;        // device scalars
     int nv;            // state variables: 8, or 9 with ndim = 2 (frozen right z-face)
     long long sv;      // cells per plane
+    // learned face flux (FP32 path with surrogate = 1)
+    const nn::NetView *net;         // attached network (host copy of its device view), null: HLLD everywhere
+    unsigned char *skip[3];         // per face: 1 when the network's flux was used
+    unsigned long long *nn_count;   // device counters: faces seen, faces sent back to HLLD
+    int *nn_err;                    // device error word of the network kernels
 };
 
 int nstate_vars(const Geo &G);
 
 // per-kernel timing slots (CUDA events around each launch when a timer is attached)
 enum KernelSlot { KS_SCALARS = 0, KS_DT, KS_PRIM, KS_TRACE, KS_RIEMANN, KS_UPDATE, KS_FARGO_EMF, KS_FARGO_UPDATE,
-                  KS_BOUNDARY, KS_HISTORY, KS_RIGHT_FACES, KS_EFIELD, KS_COUNT };
+                  KS_BOUNDARY, KS_HISTORY, KS_RIGHT_FACES, KS_EFIELD, KS_NN_FACES, KS_COUNT };
 struct KernelTimer {
     virtual void begin(int slot, cudaStream_t st) = 0;
     virtual void end(int slot, cudaStream_t st) = 0;
@@ -58,6 +67,17 @@ long long history_scratch_doubles(const Geo &G);
 
 namespace f32 {
 DG_DECLARE_LAUNCHES
+// primitive variables, edge fields and trace of U[cur] (the first half of godunov)
+int launch_trace_only(const Geo &G, const Bufs &B, int cur, cudaStream_t st);
+// every stride-th interface of direction d from the trace core: scaled inputs into xs and
+// scaled HLLD-minus-LLF targets into ts, samples [first, first + count)
+int launch_harvest(const Geo &G, const Bufs &B, int d, int stride, float *xs, float *ts, long long first,
+                   long long count, cudaStream_t st);
+// faces of direction d (0..ndim-1) enumerated as harvested: (nx+1) ny nz for x, ...
+long long harvest_faces(const Geo &G, int d);
+// the face-network kernel and its dynamic shared memory (for the attribute call)
+const void *nn_faces_kernel();
+int nn_faces_smem();
 }  // namespace f32
 
 // shared host helpers (dg_api.cu)

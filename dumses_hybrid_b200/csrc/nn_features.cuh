@@ -1,0 +1,145 @@
+// Inputs, targets and gates of the learned face-flux surrogate.
+//
+// The network stands in for the HLLD face solver (src/modules/solvers/solver.f90:618-836)
+// on smooth interfaces.  It does not predict the flux itself but the difference between
+// the HLLD flux and the local Lax-Friedrichs flux of the same interface states
+// (solver.f90:393-498).  States are first put in units of the interface: density
+// rho0 = (rhoL + rhoR) / 2, a speed a0 >= both fast magnetosonic speeds, and the field
+// unit sqrt(rho0) a0.  On a smooth interface the HLLD-LLF difference is a dissipation
+// correction proportional to the jump between the two states, so the inputs are the
+// mean state, the direction of the jump and its size J, and the target is the
+// correction divided by J: both stay of order one however small the jump, and the
+// network's error enters the flux multiplied by J.  (BF16 inputs could not resolve a
+// small jump given as two nearly equal states.)
+//
+// Interface state order (as passed to the 1D solvers): 0 rho, 1 P, 2 u_n, 3 B_n (the face
+// mean), 4 v_t1, 5 B_t1, 6 v_t2, 7 B_t2.
+// 17 inputs, from the left/right rho, u_n, v_t1, v_t2, P, B_t1, B_t2 and the face B_n:
+//   0..6   mean of u_n, v_t1, v_t2, P, B_n, B_t1, B_t2 (the mean density is 1 by construction)
+//   7..13  (right - left) / J of rho, u_n, v_t1, v_t2, P, B_t1, B_t2, J = the norm of that jump
+//   14     J,  15  ln(J) / 10,  16  gamma - 1
+// 8 outputs, each divided by J and by its unit: corrections of the mass, energy, full
+// normal-momentum (HLLD's flux plus its p*_T), t1-momentum, B_t1, t2-momentum and B_t2
+// fluxes, and of p*_T against the mean total pressure.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "solvers.cuh"
+
+namespace dg {
+namespace nn {
+
+constexpr int kIn = 17, kInPad = 32, kHid = 128, kOut = 8, kOutPad = 16;
+
+struct FaceUnits {
+    float rho0, a0, b0, jump;  // interface units and the jump size J
+};
+
+constexpr float kTinyJump = 1e-20f;
+
+// per-output scale factor in units of the interface (without J)
+__device__ __forceinline__ float out_scale(const FaceUnits &u, int c) {
+    const float m = u.rho0 * u.a0;
+    switch (c) {
+        case 0: return m;                         // mass
+        case 1: return m * u.a0 * u.a0;           // energy
+        case 4: case 6: return u.b0 * u.a0;       // induction
+        default: return m * u.a0;                 // momenta and p*_T
+    }
+}
+
+// network inputs of one interface; iso states use P = rho ciso^2 as the solvers do
+__device__ __forceinline__ FaceUnits face_inputs(const float *ql, const float *qr, float gamma, float ciso, int iso,
+                                                 float x[kIn]) {
+    const float pl = iso ? ql[0] * (ciso * ciso) : ql[1];
+    const float pr = iso ? qr[0] * (ciso * ciso) : qr[1];
+    const float bn = ql[3];
+    const float b2l = bn * bn + ql[5] * ql[5] + ql[7] * ql[7];
+    const float b2r = bn * bn + qr[5] * qr[5] + qr[7] * qr[7];
+    FaceUnits u;
+    u.rho0 = 0.5f * (ql[0] + qr[0]);
+    u.a0 = sqrtf(fmaxf((gamma * pl + b2l) / ql[0], (gamma * pr + b2r) / qr[0]));
+    u.b0 = sqrtf(u.rho0) * u.a0;
+    const float ir = 1.0f / u.rho0, ia = 1.0f / u.a0, ip = ir * ia * ia, ib = 1.0f / u.b0;
+    // scaled left and right: rho, u_n, v_t1, v_t2, P, B_t1, B_t2
+    const float L[7] = {ql[0] * ir, ql[2] * ia, ql[4] * ia, ql[6] * ia, pl * ip, ql[5] * ib, ql[7] * ib};
+    const float R[7] = {qr[0] * ir, qr[2] * ia, qr[4] * ia, qr[6] * ia, pr * ip, qr[5] * ib, qr[7] * ib};
+    float j2 = 0.0f;
+#pragma unroll
+    for (int n = 0; n < 7; n++) j2 += (R[n] - L[n]) * (R[n] - L[n]);
+    u.jump = sqrtf(j2);
+    const float ij = (u.jump > kTinyJump) ? 1.0f / u.jump : 0.0f;
+    x[0] = 0.5f * (L[1] + R[1]); x[1] = 0.5f * (L[2] + R[2]); x[2] = 0.5f * (L[3] + R[3]);
+    x[3] = 0.5f * (L[4] + R[4]); x[4] = bn * ib;             x[5] = 0.5f * (L[5] + R[5]);
+    x[6] = 0.5f * (L[6] + R[6]);
+#pragma unroll
+    for (int n = 0; n < 7; n++) x[7 + n] = (R[n] - L[n]) * ij;
+    x[14] = u.jump;
+    x[15] = 0.1f * logf(fmaxf(u.jump, kTinyJump));
+    x[16] = gamma - 1.0f;
+    return u;
+}
+
+// the base of the correction: LLF fluxes in output order and the mean total pressure
+template <typename T>
+__device__ __forceinline__ void base_fluxes(const T *ql, const T *qr, T gamma, T ciso, int iso, T b[kOut]) {
+    T f[8];
+    llf1d<T>(ql, qr, f, gamma, ciso, iso);
+    const T half = T(0.5);
+    const T pl = iso ? ql[0] * (ciso * ciso) : ql[1], pr = iso ? qr[0] * (ciso * ciso) : qr[1];
+    const T bn = ql[3];
+    const T ptl = pl + half * (bn * bn + ql[5] * ql[5] + ql[7] * ql[7]);
+    const T ptr = pr + half * (bn * bn + qr[5] * qr[5] + qr[7] * qr[7]);
+    b[0] = f[0]; b[1] = f[1]; b[2] = f[2]; b[3] = f[4]; b[4] = f[5]; b[5] = f[6]; b[6] = f[7];
+    b[7] = half * (ptl + ptr);
+}
+
+// HLLD fluxes in output order (normal momentum including p*_T), FP64 labels
+__device__ __forceinline__ void hlld_targets(const double *ql, const double *qr, double gamma, double ciso, int iso,
+                                             double t[kOut]) {
+    double f[8], pg;
+    hlld1d<double>(ql, qr, f, pg, gamma, ciso, iso);
+    t[0] = f[0]; t[1] = f[1]; t[2] = f[2] + pg; t[3] = f[4]; t[4] = f[5]; t[5] = f[6]; t[6] = f[7]; t[7] = pg;
+}
+
+// gates and the envelope of the training inputs/outputs, set when training ends
+struct Gates {
+    float xmin[kIn], xmax[kIn];  // input envelope seen in training
+    float ymax;                  // largest |output| seen in training (scaled)
+    float jump;                  // relative pressure / density jump above which HLLD is used
+    float compress;              // u_nR - u_nL below -compress * a0 marks a shock: HLLD
+    float margin;                // envelope margin (fraction of its width)
+};
+
+// true when the interface is smooth and inside the network's training envelope
+__device__ __forceinline__ bool gate_inputs(const Gates &g, const float *ql, const float *qr, float ciso, int iso,
+                                            const FaceUnits &u, const float x[kIn]) {
+    const float rl = ql[0], rr = qr[0];
+    const float pl = iso ? rl * (ciso * ciso) : ql[1], pr = iso ? rr * (ciso * ciso) : qr[1];
+    if (!(rl > 0.0f && rr > 0.0f && pl > 0.0f && pr > 0.0f)) return false;           // positivity
+    if (fabsf(pl - pr) > g.jump * fminf(pl, pr)) return false;                         // pressure jump
+    if (fabsf(rl - rr) > g.jump * fminf(rl, rr)) return false;                         // density jump
+    if (qr[2] - ql[2] < -g.compress * u.a0) return false;                              // compression
+#pragma unroll
+    for (int n = 0; n < kIn; n++) {
+        const float w = g.margin * (g.xmax[n] - g.xmin[n]);
+        if (!(x[n] >= g.xmin[n] - w && x[n] <= g.xmax[n] + w)) return false;          // confidence: envelope
+    }
+    return true;
+}
+
+// GELU, 0.5 z (1 + erf(z / sqrt 2)), and its derivative
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+}
+
+// device view of the trained network for inference inside the step
+struct NetView {
+    const __nv_bfloat16 *wt[4];  // forward B operands, blocked K-major [N_l][K_l]
+    const float *b[4];           // biases
+    Gates gates;
+};
+
+}  // namespace nn
+}  // namespace dg

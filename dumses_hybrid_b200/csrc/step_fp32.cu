@@ -9,6 +9,8 @@
 // an error-free two-sum, so the state carries about 48 significant bits across steps.
 #define DG_NS f32
 #include "step_impl.cuh"
+#include "nn_features.cuh"
+#include "nn_umma.cuh"
 
 namespace dg {
 namespace f32 {
@@ -426,6 +428,221 @@ __global__ void __launch_bounds__(kThreads) k_fargo_update_hl(Geo G, StoreHL U, 
     if (i <= nx && j <= ny) apply(U, Un, G, IC, c, -(EX(i, j + 1, k) - EX(i, j, k)) * rdy);
 }
 
+// ---------------------------------------------------------------------------
+// learned face flux
+// ---------------------------------------------------------------------------
+// cells on either side of face (i, j, k) of direction d
+__device__ __forceinline__ void face_cells(const Geo &G, int d, int i, int j, int k, long long &cl, long long &cr) {
+    cr = G.cidx(i, j, k);
+    cl = (d == 0) ? G.cidx(i - 1, j, k) : (d == 1 ? G.cidx(i, j - 1, k) : G.cidx(i, j, k - 1));
+}
+
+// interfaces of direction d in harvest order: x fastest over the faces of that direction
+__host__ __device__ __forceinline__ void harvest_extent(const Geo &G, int d, int &ex, int &ey, int &ez) {
+    ex = G.nx + (d == 0);
+    ey = G.ny + (d == 1);
+    ez = (G.ndim == 3) ? G.nz + (d == 2) : 1;
+}
+
+__global__ void __launch_bounds__(kThreads) k_nn_harvest(Geo G, const float *__restrict__ core, int d, int stride,
+                                                         float *__restrict__ xs, float *__restrict__ ts,
+                                                         long long first, long long count) {
+    const long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    int ex, ey, ez;
+    harvest_extent(G, d, ex, ey, ez);
+    const long long idx = s * stride;
+    const int i = (int)(idx % ex) + 1;
+    const long long r = idx / ex;
+    const int j = (int)(r % ey) + 1, k = (int)(r / ey) + 1;
+    const CoreView<float> cv{core, G.ndim == 3 ? kCore3 : kCore2};
+    long long cl, cr;
+    face_cells(G, d, i, j, k, cl, cr);
+    float ql[8], qr[8], x[nn::kIn];
+    face_io(G, cv, cl, cr, d, ql, qr);
+    const float gamma = (float)G.gamma, ciso = (float)G.ciso;
+    const nn::FaceUnits u = nn::face_inputs(ql, qr, gamma, ciso, G.iso, x);
+    double qld[8], qrd[8], t[nn::kOut], b[nn::kOut];
+#pragma unroll
+    for (int n = 0; n < 8; n++) { qld[n] = ql[n]; qrd[n] = qr[n]; }
+    nn::hlld_targets(qld, qrd, G.gamma, G.ciso, G.iso, t);
+    nn::base_fluxes<double>(qld, qrd, G.gamma, G.ciso, G.iso, b);
+    float *xo = xs + (first + s) * nn::kIn;
+    float *to = ts + (first + s) * nn::kOut;
+#pragma unroll
+    for (int n = 0; n < nn::kIn; n++) xo[n] = x[n];
+#pragma unroll
+    for (int n = 0; n < nn::kOut; n++)
+        to[n] = (u.jump > nn::kTinyJump) ? (float)((t[n] - b[n]) / ((double)nn::out_scale(u, n) * (double)u.jump)) : 0.0f;
+}
+
+// shared-memory plan of the face-network kernel (bytes)
+constexpr int kNW1 = 0, kNW2 = 8192, kNW3 = 40960, kNW4 = 73728, kNX = 77824, kNH = 86016, kNBias = 118784,
+              kNBar = 120448, kNSmem = 120576;
+
+// One 128-face tile at a time per CTA: the faces' interface states, inputs and gates, the
+// four layers as tcgen05 MMAs (weights resident in shared memory, activations through
+// TMEM -> GELU -> shared memory), then the gated flux or a mark for HLLD.
+__global__ void __launch_bounds__(128, 1) k_nn_faces(Geo G, const float *__restrict__ core, float *__restrict__ flux,
+                                                     unsigned char *__restrict__ skip, int d, nn::NetView nv,
+                                                     const Scalars *S, unsigned long long *cnt, int *err) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    using bf16 = __nv_bfloat16;
+    bf16 *W[4] = {(bf16 *)(sm + kNW1), (bf16 *)(sm + kNW2), (bf16 *)(sm + kNW3), (bf16 *)(sm + kNW4)};
+    bf16 *Xs = (bf16 *)(sm + kNX), *Hs = (bf16 *)(sm + kNH);
+    float *bias = (float *)(sm + kNBias);  // 3 x 128 + 8
+    uint64_t *bar = (uint64_t *)(sm + kNBar);
+    uint32_t *tslot = (uint32_t *)(sm + kNBar + 16);
+    int *sflag = (int *)(sm + kNBar + 20);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        nn::mbar_init(&bar[0], 1);
+        nn::mbar_init(&bar[1], 1);
+        nn::mbar_fence_init();
+        *sflag = 1;
+    }
+    for (int q = tid; q < 3 * nn::kHid + nn::kOut; q += 128) {
+        const int l = q / nn::kHid;
+        bias[q] = (l < 3) ? nv.b[l][q % nn::kHid] : nv.b[3][q - 3 * nn::kHid];
+    }
+    if (warp == 0) nn::tmem_alloc(tslot, 128);
+    nn::tc_fence_before();
+    __syncthreads();
+    nn::tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+    if (tid == 0) {
+        const unsigned wb[4] = {128 * nn::kInPad * 2, 128 * 128 * 2, 128 * 128 * 2, nn::kOutPad * 128 * 2};
+        nn::mbar_expect_tx(&bar[0], wb[0] + wb[1] + wb[2] + wb[3]);
+        for (int l = 0; l < 4; l++) nn::bulk_g2s(W[l], nv.wt[l], wb[l], &bar[0]);
+        if (!nn::mbar_wait(&bar[0], 0)) {
+            nn::mbar_wait(&bar[0], 0);
+            *sflag = 0;
+        }
+    }
+    __syncthreads();
+    const CoreView<float> cv{core, G.ndim == 3 ? kCore3 : kCore2};
+    const float gamma = (float)G.gamma, ciso = (float)G.ciso;
+    const double dt = S->dt;
+    unsigned ph = 0;
+    unsigned long long nface = 0, nfall = 0;
+    for (long long tile = blockIdx.x; tile * 128 < G.fsz && *sflag; tile += gridDim.x) {
+        const long long t = tile * 128 + tid;
+        int i = 0, j = 0, k = 1;
+        bool valid = t < G.fsz;
+        if (valid) {
+            i = (int)(t % G.FX) + 1;
+            const long long r = t / G.FX;
+            j = (int)(r % G.FY) + 1;
+            k = (int)(r / G.FY) + 1;
+            valid = (d == 0) ? (j <= G.ny && (G.ndim == 2 || k <= G.nz))
+                  : (d == 1) ? (i <= G.nx && (G.ndim == 2 || k <= G.nz)) : (i <= G.nx && j <= G.ny);
+        }
+        float ql[8], qr[8], x[nn::kInPad], base[nn::kOut];
+        nn::FaceUnits u{1.0f, 1.0f, 1.0f, 0.0f};
+        bool use = false;
+#pragma unroll
+        for (int n = 0; n < nn::kInPad; n++) x[n] = 0.0f;
+        if (valid) {
+            long long cl, cr;
+            face_cells(G, d, i, j, k, cl, cr);
+            face_io(G, cv, cl, cr, d, ql, qr);
+            u = nn::face_inputs(ql, qr, gamma, ciso, G.iso, x);
+            use = nn::gate_inputs(nv.gates, ql, qr, ciso, G.iso, u, x);
+            nn::base_fluxes<float>(ql, qr, gamma, ciso, G.iso, base);
+            if (!use) {
+#pragma unroll
+                for (int n = 0; n < nn::kIn; n++) x[n] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int cg = 0; cg < nn::kInPad / 8; cg++) {
+            __align__(16) bf16 h[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) h[q] = __float2bfloat16_rn(x[cg * 8 + q]);
+            *(uint4 *)(Xs + (cg * 128 + tid) * 8) = *(const uint4 *)h;
+        }
+        nn::fence_async_smem();
+        nn::tc_fence_before();  // this thread's TMEM reads of the previous tile come before the next MMA
+        __syncthreads();
+        float y[nn::kOut];
+        for (int l = 0; l < 4; l++) {
+            if (tid == 0) {
+                nn::tc_fence_after();
+                nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W[l], l == 3 ? nn::kOutPad : nn::kHid, l == 0 ? 2 : 8, 0);
+                nn::mma_commit(&bar[1]);
+                if (!nn::mbar_wait(&bar[1], ph & 1)) {
+                    nn::mbar_wait(&bar[1], ph & 1);
+                    *sflag = 0;
+                }
+            }
+            ph++;
+            nn::tc_fence_before();
+            __syncthreads();
+            nn::tc_fence_after();
+            if (!*sflag) break;
+            if (l < 3) {
+                for (int cc = 0; cc < nn::kHid / 16; cc++) {
+                    float v[16];
+                    nn::tmem_ld16(taddr + cc * 16, v);
+#pragma unroll
+                    for (int hh = 0; hh < 2; hh++) {
+                        __align__(16) bf16 h[8];
+#pragma unroll
+                        for (int q = 0; q < 8; q++)
+                            h[q] = __float2bfloat16_rn(nn::gelu(v[hh * 8 + q] + bias[l * nn::kHid + cc * 16 + hh * 8 + q]));
+                        *(uint4 *)(Hs + ((cc * 2 + hh) * 128 + tid) * 8) = *(const uint4 *)h;
+                    }
+                }
+                nn::fence_async_smem();
+                nn::tc_fence_before();
+                __syncthreads();
+                nn::tc_fence_after();
+            } else {
+                float v[16];
+                nn::tmem_ld16(taddr, v);
+#pragma unroll
+                for (int q = 0; q < nn::kOut; q++) y[q] = v[q] + bias[3 * nn::kHid + q];
+            }
+        }
+        if (!*sflag) break;
+        if (valid) {
+            bool acc = use;
+            float F[nn::kOut];
+#pragma unroll
+            for (int c = 0; c < nn::kOut; c++) {
+                acc = acc && fabsf(y[c]) <= 1.5f * nv.gates.ymax;  // confidence: inside the training range
+                F[c] = base[c] + nn::out_scale(u, c) * u.jump * y[c];
+                acc = acc && isfinite(F[c]);
+            }
+            acc = acc && F[7] > 0.0f;  // positive star pressure
+            if (acc) {
+                float f[8] = {F[0], F[1], F[2] - F[7], 0.0f, F[3], F[4], F[5], F[6]};
+                flux_store(G, ql, qr, f, F[7], d, i, dt, flux, t);
+            }
+            skip[t] = acc ? 1 : 0;
+            nface++;
+            nfall += acc ? 0 : 1;
+        }
+    }
+    if (!*sflag && tid == 0) atomicOr(err, nn::NN_ERR_WAIT);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nface += __shfl_xor_sync(0xffffffffu, nface, o);
+        nfall += __shfl_xor_sync(0xffffffffu, nfall, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&cnt[0], nface);
+        atomicAdd(&cnt[1], nfall);
+    }
+    nn::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        nn::tc_fence_after();
+        nn::tmem_dealloc(tmem, 128);
+    }
+}
+
 StoreHL st(const Bufs &B, int b) {
     float *base = (float *)B.U[b];
     return StoreHL{base, base + (size_t)B.nv * (size_t)B.sv};
@@ -469,18 +686,64 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
     TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
+    int n = 1 + (G.shearing ? 1 : 0) + 4;
+    FaceSkip sk{{nullptr, nullptr, nullptr}};
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
         TIMED(KS_TRACE, s, (k_trace3d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
-        TIMED(KS_RIEMANN, s, (k_riemann3d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S)));
-        TIMED(KS_UPDATE, s, (k_update3d_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U, Un, fx, fy, fz, ex, ey, ez, B.S)));
     } else {
         TIMED(KS_EFIELD, s, (k_efield2d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2)));
         TIMED(KS_TRACE, s, (k_trace2d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2, core, B.S)));
-        TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S)));
+    }
+    if (B.net) {
+        float *fl[3] = {fx, fy, fz};
+        const long long tiles = (G.fsz + 127) / 128;
+        const unsigned grid = (unsigned)(tiles < 148 ? tiles : 148);
+        for (int d = 0; d < G.ndim; d++) {
+            TIMED(KS_NN_FACES, s, (k_nn_faces<<<grid, 128, kNSmem, s>>>(G, core, fl[d], B.skip[d], d, *B.net, B.S, B.nn_count, B.nn_err)));
+            sk.f[d] = B.skip[d];
+            n++;
+        }
+    }
+    if (G.ndim == 3) {
+        TIMED(KS_RIEMANN, s, (k_riemann3d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, sk)));
+        TIMED(KS_UPDATE, s, (k_update3d_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U, Un, fx, fy, fz, ex, ey, ez, B.S)));
+    } else {
+        TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, sk)));
         TIMED(KS_UPDATE, s, (k_update2d_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U, Un, fx, fy, ez, B.S)));
     }
-    return 5 + (G.shearing ? 1 : 0);
+    return n;
+}
+
+int launch_trace_only(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    const StoreHL U = st(B, cur);
+    float *Q = (float *)B.Q, *core = (float *)B.core;
+    float *E0 = (float *)B.E[0], *E1 = (float *)B.E[1], *E2 = (float *)B.E[2];
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    if (G.ndim == 3) {
+        TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
+        TIMED(KS_TRACE, s, (k_trace3d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
+    } else {
+        TIMED(KS_EFIELD, s, (k_efield2d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2)));
+        TIMED(KS_TRACE, s, (k_trace2d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2, core, B.S)));
+    }
+    return 3;
+}
+
+const void *nn_faces_kernel() { return (const void *)k_nn_faces; }
+int nn_faces_smem() { return kNSmem; }
+
+long long harvest_faces(const Geo &G, int d) {
+    int ex, ey, ez;
+    harvest_extent(G, d, ex, ey, ez);
+    return (long long)ex * ey * ez;
+}
+
+int launch_harvest(const Geo &G, const Bufs &B, int d, int stride, float *xs, float *ts, long long first,
+                   long long count, cudaStream_t s) {
+    TIMED(KS_NN_FACES, s, (k_nn_harvest<<<nblocks(count, kThreads), kThreads, 0, s>>>(G, (const float *)B.core, d, stride, xs, ts, first, count)));
+    return 1;
 }
 
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {

@@ -681,18 +681,13 @@ __device__ __forceinline__ void solve1d(int iriemann, const T *ql, const T *qr, 
     }
 }
 
-#ifdef DG_FACE_SOLVER_HOOK
-// the mixed path may route selected faces to another solver (learned surrogate)
-DG_FACE_SOLVER_HOOK
-#endif
-
-// one face flux in direction d between cells cl (minus side) and cr (plus side);
-// writes the compflux-scaled fluxes in uin order plus p*_T (solver.f90:116-262, scheme.f90:1740-1753)
+// solver-order interface states of the face in direction d between cells cl (minus side)
+// and cr (plus side): 0 rho, 1 P, 2 u_n, 3 B_n (face mean), 4 v_t1, 5 B_t1, 6 v_t2, 7 B_t2
+// (solver.f90:116-160)
 template <typename T>
-__device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d, int i, double dtd,
-                          T *__restrict__ out, long long fo) {
-    const T half = T(0.5), one = T(1);
-    const T gamma = (T)G.gamma;
+__device__ __forceinline__ void face_io(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d,
+                                        T ql[8], T qr[8]) {
+    const T half = T(0.5);
     const T smallp = (T)(kSmallr * (kSmallc * kSmallc) / G.gamma);
     T sm[8], sp[8];
     face_state(cv, cl, d, +1, G.ndim, smallp, sm);
@@ -702,15 +697,22 @@ __device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, lon
     else if (d == 1) { ln = IV; lt1 = IU; lt2 = IW; bn = IB; bt1 = IA; bt2 = IC; }
     else { ln = IW; lt1 = IU; lt2 = IV; bn = IC; bt1 = IA; bt2 = IB; }
     const T bn_mean = half * (sm[bn] + sp[bn]);
-    T ql[8] = {sm[IR], sm[IP], sm[ln], bn_mean, sm[lt1], sm[bt1], sm[lt2], sm[bt2]};
-    T qr[8] = {sp[IR], sp[IP], sp[ln], bn_mean, sp[lt1], sp[bt1], sp[lt2], sp[bt2]};
-    T f[8], pg = T(0);
-#ifdef DG_FACE_SOLVER_HOOK
-    face_solver_hook<T>(G, ql, qr, f, pg, d);
-#else
-    solve1d<T>(G.iriemann, ql, qr, f, pg, gamma, (T)G.ciso, G.iso);
-#endif
-    // shearing-box upwind terms (solver.f90:199-241)
+    ql[0] = sm[IR]; ql[1] = sm[IP]; ql[2] = sm[ln]; ql[3] = bn_mean; ql[4] = sm[lt1]; ql[5] = sm[bt1]; ql[6] = sm[lt2]; ql[7] = sm[bt2];
+    qr[0] = sp[IR]; qr[1] = sp[IP]; qr[2] = sp[ln]; qr[3] = bn_mean; qr[4] = sp[lt1]; qr[5] = sp[bt1]; qr[6] = sp[lt2]; qr[7] = sp[bt2];
+}
+
+// shearing-box upwind terms (solver.f90:199-241) and compflux scaling of solver fluxes f
+// (order of ql) and p*_T into the face record (scheme.f90:1740-1753)
+template <typename T>
+__device__ __forceinline__ void flux_store(const Geo &G, const T *ql, const T *qr, T *f, T pg, int d, int i,
+                                           double dtd, T *__restrict__ out, long long fo) {
+    const T half = T(0.5), one = T(1);
+    const T gamma = (T)G.gamma;
+    const T bn_mean = ql[3];
+    int ln, lt1, lt2;
+    if (d == 0) { ln = IU; lt1 = IV; lt2 = IW; }
+    else if (d == 1) { ln = IV; lt1 = IU; lt2 = IW; }
+    else { ln = IW; lt1 = IU; lt2 = IV; }
     if (G.ndim == 2) {
         if (G.omega0 > 0.0) {
             double shear = -1.5 * G.omega0 * G.xc(i);
@@ -745,6 +747,18 @@ __device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, lon
     o[6] = (G.ndim == 2) ? f[7] * ds * dt : T(0);  // B_t2 = B_z
     o[7] = T(0);
     store8(out + fo * kFluxComp, o);
+}
+
+// one face flux in direction d between cells cl (minus side) and cr (plus side);
+// writes the compflux-scaled fluxes in uin order plus p*_T (solver.f90:116-262, scheme.f90:1740-1753)
+template <typename T>
+__device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d, int i, double dtd,
+                          T *__restrict__ out, long long fo) {
+    T ql[8], qr[8];
+    face_io(G, cv, cl, cr, d, ql, qr);
+    T f[8], pg = T(0);
+    solve1d<T>(G.iriemann, ql, qr, f, pg, (T)G.gamma, (T)G.ciso, G.iso);
+    flux_store(G, ql, qr, f, pg, d, i, dtd, out, fo);
 }
 
 // one edge EMF (riemann_solver_magnetic, solver_magnetic.f90:79-230); e = edge direction
@@ -832,10 +846,17 @@ __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long l
     return emf;
 }
 
+// faces whose flux another solver already wrote (null: none)
+struct FaceSkip {
+    const unsigned char *f[3];
+    __device__ __forceinline__ bool skip(int d, long long t) const { return f[d] && f[d][t]; }
+};
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                            T *__restrict__ fy, T *__restrict__ fz, T *__restrict__ ex,
-                                                           T *__restrict__ ey, T *__restrict__ ez, const Scalars *S) {
+                                                           T *__restrict__ ey, T *__restrict__ ez, const Scalars *S,
+                                                           FaceSkip sk) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
     const int i = (int)(t % G.FX) + 1;
@@ -846,9 +867,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__res
     const CoreView<T> cv{core, kCore3};
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const long long c = G.cidx(i, j, k);
-    if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
-    if (i <= nx && k <= nz) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
-    if (i <= nx && j <= ny) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
+    if (j <= ny && k <= nz && !sk.skip(0, t)) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
+    if (i <= nx && k <= nz && !sk.skip(1, t)) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
+    if (i <= nx && j <= ny && !sk.skip(2, t)) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
     if (k <= nz) ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
     if (j <= ny) ey[t] = edge_emf(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
     if (i <= nx) ex[t] = edge_emf(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
@@ -856,7 +877,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__res
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
-                                                        T *__restrict__ fy, T *__restrict__ ez, const Scalars *S) {
+                                                        T *__restrict__ fy, T *__restrict__ ez, const Scalars *S,
+                                                        FaceSkip sk) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
     const int i = (int)(t % G.FX) + 1;
@@ -864,8 +886,8 @@ __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restri
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore2};
     const long long c = G.cidx(i, j, 1);
-    if (j <= G.ny) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t);
-    if (i <= G.nx) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t);
+    if (j <= G.ny && !sk.skip(0, t)) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t);
+    if (i <= G.nx && !sk.skip(1, t)) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t);
     ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, 1), G.cidx(i, j - 1, 1), G.cidx(i - 1, j, 1), c, 2, i, dt);
 }
 

@@ -149,7 +149,7 @@ int  dg_sync(dg_ctx *ctx);
  * dg_profile(ctx, 1) starts recording an event pair around every kernel;
  * dg_profile_read fills ms[slot] and count[slot] for the launches since the
  * last read (slots named by dg_profile_slot_name) and resets them. */
-#define DG_PROFILE_SLOTS 12
+#define DG_PROFILE_SLOTS 13
 int  dg_profile(dg_ctx *ctx, int on);
 int  dg_profile_read(dg_ctx *ctx, double *ms, long long *count, int nslots);
 const char *dg_profile_slot_name(int slot);
@@ -173,6 +173,59 @@ int  dg_debug_copy(dg_ctx *ctx, int which, double *host, long long count, long l
 
 /* message of the last failing call on this thread ("" if none) */
 const char *dg_last_error(void);
+
+/* ---- learned face-flux surrogate --------------------------------------------
+ * No counterpart in the reference, whose face solver is always an exact one
+ * (src/modules/solvers/solver.f90:163-187).  A 17 -> 128 -> 128 -> 128 -> 8 GELU
+ * MLP with BF16 weights and FP32 accumulation on the tensor cores, trained on the
+ * device by the library's own forward, backward and Adam kernels.  Per interface
+ * it predicts HLLD minus LLF of the same states.  States are scaled by the
+ * interface's density rho0 = (rhoL+rhoR)/2, a speed a0 >= both fast speeds and the
+ * field unit sqrt(rho0) a0 (rho / rho0, velocities / a0, P / (rho0 a0^2), fields
+ * / (sqrt(rho0) a0)); J is the norm of the scaled right-minus-left jump of rho,
+ * u_n, v_t1, v_t2, P, B_t1, B_t2.
+ *   inputs (17): mean u_n, v_t1, v_t2, P, B_n, B_t1, B_t2; the jump of rho, u_n,
+ *                v_t1, v_t2, P, B_t1, B_t2 divided by J; J; ln(J)/10; gamma - 1
+ *   outputs (8): mass, energy, normal momentum (HLLD flux + p*_T), t1 momentum,
+ *                B_t1, t2 momentum and B_t2 fluxes, and p*_T - (ptotL+ptotR)/2,
+ *                each divided by J and by its unit (rho0 a0, rho0 a0^3, rho0 a0^2,
+ *                sqrt(rho0) a0^2, rho0 a0^2)
+ * Parameters, in dg_nn_get_params order: W1[17][128], b1[128], W2[128][128],
+ * b2[128], W3[128][128], b3[128], W4[128][8], b4[8] (W[k][n]: input k, output n).
+ * Batches are multiples of 128 rows.  On a context with precision FP32 and
+ * surrogate = 1, an attached network replaces HLLD on faces that pass its gates
+ * (positive states, relative pressure and density jumps and compression below
+ * the thresholds, inputs inside the training envelope, outputs inside the
+ * training range); the other faces get exact HLLD. */
+typedef struct dg_nn dg_nn;
+#define DG_NN_INPUTS  17
+#define DG_NN_OUTPUTS 8
+long long dg_nn_param_count(void);
+int  dg_nn_create(int device, unsigned long long seed, dg_nn **out);
+int  dg_nn_destroy(dg_nn *nn);
+/* training samples: x[count][17], t[count][8] (scaled as above) */
+int  dg_nn_set_samples(dg_nn *nn, const float *x, const float *t, long long count);
+int  dg_nn_reserve_samples(dg_nn *nn, long long count);
+long long dg_nn_sample_count(const dg_nn *nn);
+int  dg_nn_samples_copy(dg_nn *nn, long long first, long long count, float *x, float *t);
+/* append the interfaces of the context's current state (every stride-th face of
+ * each direction, in a fixed order) with FP64 HLLD labels; FP32 contexts only */
+int  dg_nn_harvest(dg_ctx *ctx, dg_nn *nn, int stride, long long *added);
+/* `steps` Adam steps on random batches; *loss = mean squared error of the last */
+int  dg_nn_train(dg_nn *nn, int steps, int batch, float lr, float *loss);
+/* loss and parameter gradients of one batch, without an update */
+int  dg_nn_gradients(dg_nn *nn, const float *x, const float *t, int batch, float *loss, float *grad);
+int  dg_nn_forward(dg_nn *nn, const float *x, long long count, float *y);
+int  dg_nn_get_params(dg_nn *nn, float *params, long long count);
+int  dg_nn_set_params(dg_nn *nn, const float *params, long long count);
+/* the envelope of the current samples (widened by margin x its width) becomes
+ * the confidence gate */
+int  dg_nn_fit_envelope(dg_nn *nn, float margin);
+int  dg_nn_set_gates(dg_nn *nn, float jump, float compress);
+/* use `nn` (NULL: none) for the faces of an FP32 context made with surrogate = 1 */
+int  dg_attach_surrogate(dg_ctx *ctx, dg_nn *nn);
+/* faces seen by the surrogate and faces that fell back to HLLD since the last call */
+int  dg_surrogate_stats(dg_ctx *ctx, long long *faces, long long *fallback);
 
 /* Host-side initial conditions written straight into a reference-layout uin
  * (11 variables, ghosts included), followed by the reference's first boundary

@@ -1,0 +1,180 @@
+"""The flux network on the GPU: tcgen05 forward and backward against the FP64 numpy
+oracle (BF16 rounding emulated at the same points), the Adam step, training on
+interfaces harvested from the FP32 path with HLLD labels, and the surrogate inside the
+step with its HLLD fallback.
+
+Tolerances: forward outputs and gradients agree with the oracle to a relative L2 error
+of 2e-3 per layer (FP32 accumulation order, occasional BF16 rounding flips)."""
+import numpy as np
+import pytest
+
+from dumses_hybrid_b200 import Context, FluxNet, Params, condinit
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def random_params(net, seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    p = []
+    for k, n in mo.SHAPES:
+        p.append(rng.normal(0, scale * np.sqrt(2.0 / k), k * n))
+        p.append(rng.normal(0, 0.1, n))
+    p = np.concatenate(p).astype(np.float32)
+    net.set_params(p)
+    return p.astype(np.float64)
+
+
+def layer_slices():
+    out, off = [], 0
+    for k, n in mo.SHAPES:
+        out.append(slice(off, off + k * n))
+        off += k * n
+        out.append(slice(off, off + n))
+        off += n
+    return out
+
+
+def test_param_roundtrip():
+    with FluxNet(seed=7) as net:
+        p = net.params()
+        assert p.size == 36360 and np.isfinite(p).all() and np.abs(p).max() > 0
+        net.set_params(p * 0.5)
+        assert np.array_equal(net.params(), (p * 0.5).astype(np.float32))
+
+
+@pytest.mark.parametrize("rows", [128, 1000])
+def test_forward_matches_oracle(rows):
+    rng = np.random.default_rng(rows)
+    with FluxNet() as net:
+        p = random_params(net, 11)
+        x = rng.normal(0, 1, (rows, 17)).astype(np.float32)
+        y = net.forward(x)
+        yo, _ = mo.forward(p, x.astype(np.float64))
+        assert rel(y, yo) < 2e-3, rel(y, yo)
+
+
+@pytest.mark.parametrize("batch", [256, 1024])
+def test_gradients_match_oracle(batch):
+    rng = np.random.default_rng(batch)
+    with FluxNet() as net:
+        p = random_params(net, 12)
+        x = rng.normal(0, 1, (batch, 17)).astype(np.float32)
+        t = rng.normal(0, 1, (batch, 8)).astype(np.float32)
+        loss, g = net.gradients(x, t)
+        lo, go = mo.loss_and_grad(p, x.astype(np.float64), t.astype(np.float64))
+        assert abs(loss - lo) <= 1e-3 * lo
+        for s in layer_slices():
+            assert rel(g[s], go[s]) < 2e-3, (s, rel(g[s], go[s]))
+
+
+def test_adam_step_matches_oracle():
+    rng = np.random.default_rng(5)
+    with FluxNet() as net:
+        p = random_params(net, 13)
+        x1 = rng.normal(0, 1, (1, 17))
+        t1 = rng.normal(0, 1, (1, 8))
+        x = np.repeat(x1, 256, axis=0).astype(np.float32)  # every drawn batch is the same
+        t = np.repeat(t1, 256, axis=0).astype(np.float32)
+        _, g = net.gradients(x, t)
+        net.set_samples(x, t)
+        net.train(1, batch=256, lr=1e-3)
+        p1 = net.params().astype(np.float64)
+        po, _, _ = mo.adam_step(p, g.astype(np.float64), np.zeros_like(p), np.zeros_like(p), 1)
+        moved = np.abs(g) > 1e-6 * np.abs(g).max()
+        assert np.allclose(p1[moved], po[moved], rtol=0, atol=2e-6)
+
+
+def test_training_fits_a_smooth_map():
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-1, 1, (1 << 16, 17)).astype(np.float32)
+    t = np.stack([np.sin(2 * x[:, 0] + x[:, 1]), x[:, 2] * x[:, 3], np.tanh(x[:, 4] - x[:, 5]), x[:, 6] ** 2,
+                  np.cos(x[:, 7]), x[:, 8] - x[:, 9], 0.5 * x[:, 10] * x[:, 11], x[:, 12] + x[:, 16]], 1).astype(np.float32)
+    with FluxNet(seed=3) as net:
+        net.set_samples(x, t)
+        l0 = net.train(1, batch=8192, lr=1e-3)
+        l1 = net.train(600, batch=8192, lr=1e-3)
+        print("loss", l0, "->", l1)
+        assert l1 < 0.05 * l0
+
+
+def ot_params(n, precision="fp32", surrogate=False):
+    return Params(ndim=3, nx=n, ny=n, nz=n, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, gamma=5 / 3,
+                  courant=0.8, precision=precision, surrogate=surrogate)
+
+
+def train_on_ot(net, n=32, snapshots=4, steps_between=5, train_steps=800):
+    p = ot_params(n)
+    with Context(p) as g:
+        g.upload(condinit(p, "orszag_tang"))
+        g.boundary(0.0, 0.0)
+        t = 0.0
+        for _ in range(snapshots):
+            t, _ = g.run(steps_between, t)
+            net.harvest(g)
+    x, y = net.samples()
+    assert np.isfinite(x).all() and np.isfinite(y).all()
+    net.fit_envelope(0.0)
+    loss = net.train(train_steps, batch=8192, lr=1e-3)
+    return loss
+
+
+def test_harvest_labels_and_network_gain():
+    """Held-out interfaces: LLF + learned correction is much closer to HLLD than LLF alone."""
+    with FluxNet(seed=2) as net:
+        loss = train_on_ot(net)
+        # a fresh, later snapshot as the held-out set
+        p = ot_params(32)
+        with Context(p) as g, FluxNet(seed=9) as probe:
+            g.upload(condinit(p, "orszag_tang"))
+            g.boundary(0.0, 0.0)
+            g.run(37, 0.0)
+            probe.harvest(g, stride=3)
+            xh, th = probe.samples()
+        yh = net.forward(xh)
+        jump = xh[:, 14:15]  # targets are per unit jump: weigh by the jump to compare fluxes
+        err_nn = np.mean(np.abs(yh - th) * jump)
+        err_llf = np.mean(np.abs(th) * jump)   # LLF alone: correction 0
+        print("train loss", loss, "held-out L1 of the correction: network", err_nn, "LLF alone", err_llf)
+        assert err_nn < 0.2 * err_llf
+
+
+def l1_rel(a, b):
+    return float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+
+
+def test_surrogate_step_with_fallback():
+    """The network inside the FP32 step: some faces fall back to HLLD, the state stays
+    close to the plain FP64 run and div B stays at round-off."""
+    with FluxNet(seed=2) as net:
+        train_on_ot(net)
+        net.set_gates(jump=0.1, compress=0.1)
+        res = {}
+        for prec, sur in (("fp64", False), ("fp32", False), ("fp32", True)):
+            p = ot_params(32, prec, sur)
+            with Context(p) as g:
+                if sur:
+                    g.attach_surrogate(net)
+                g.upload(condinit(p, "orszag_tang"))
+                g.boundary(0.0, 0.0)
+                g.run(20, 0.0)
+                res[(prec, sur)] = g.download()
+                if sur:
+                    faces, fallback = g.surrogate_stats()
+                    hist = g.history()
+        print("faces", faces, "fallback", fallback, "fraction", fallback / faces)
+        assert faces == 20 * 3 * 32 * 32 * 33
+        assert 0 < fallback < faces
+        a64 = res[("fp64", False)][3:-3, 3:-3, 3:-3]
+        for key in (("fp32", False), ("fp32", True)):
+            a = res[key][3:-3, 3:-3, 3:-3]
+            errs = [l1_rel(a[..., v], a64[..., v]) for v in (0, 4, 5, 6)]
+            print(key, "L1 rel rho E Bx By", ["%.2e" % e for e in errs])
+        a = res[("fp32", True)][3:-3, 3:-3, 3:-3]
+        for v in (0, 4, 5, 6):
+            assert l1_rel(a[..., v], a64[..., v]) < 2e-2
+        assert abs(hist[8]) < 1e-10
