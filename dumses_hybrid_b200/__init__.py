@@ -113,6 +113,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_nn_get_params": (ctypes.c_int, [vp, fp, ctypes.c_longlong]),
         "dg_nn_set_params": (ctypes.c_int, [vp, fp, ctypes.c_longlong]),
         "dg_nn_fit_envelope": (ctypes.c_int, [vp, ctypes.c_float]),
+        "dg_nn_fit_scaling": (ctypes.c_int, [vp]),
         "dg_nn_set_gates": (ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
         "dg_attach_surrogate": (ctypes.c_int, [vp, vp]),
         "dg_surrogate_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
@@ -419,6 +420,10 @@ class FluxNet:
 
     def fit_envelope(self, margin: float = 0.0) -> None:
         _check(self.lib.dg_nn_fit_envelope(self.h, margin))
+
+    def fit_scaling(self) -> None:
+        """Standardise inputs and outputs by the current samples (call before training)."""
+        _check(self.lib.dg_nn_fit_scaling(self.h))
 
     def set_gates(self, jump: float = 0.1, compress: float = 0.1) -> None:
         _check(self.lib.dg_nn_set_gates(self.h, jump, compress))

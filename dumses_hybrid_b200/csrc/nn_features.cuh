@@ -128,17 +128,48 @@ __device__ __forceinline__ bool gate_inputs(const Gates &g, const float *ql, con
     return true;
 }
 
-// GELU, 0.5 z (1 + erf(z / sqrt 2)), and its derivative
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(c (z + a z^3))), c = sqrt(2/pi), a = 0.044715,
+// and its derivative
+constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + tanhf(kGeluC * (z + kGeluA * z * z * z))); }
 __device__ __forceinline__ float gelu_d(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+    const float t = tanhf(kGeluC * (z + kGeluA * z * z * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * z * z);
 }
+// the same with the hardware tanh approximation (PTX tanh.approx.f32), for inference
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu_fast(float z) {
+    return 0.5f * z * (1.0f + tanh_approx(kGeluC * (z + kGeluA * z * z * z)));
+}
+// two GELUs packed as BF16x2 (low half = a), the tanh evaluated on BF16x2 (PTX
+// tanh.approx.bf16x2): the results are BF16 activations, so BF16 accuracy suffices
+__device__ __forceinline__ uint32_t gelu2_bf16(float a, float b) {
+    const float ua = kGeluC * (a + kGeluA * a * a * a), ub = kGeluC * (b + kGeluA * b * b * b);
+    const __nv_bfloat162 u2 = __floats2bfloat162_rn(ua, ub);
+    uint32_t t2, in = *reinterpret_cast<const uint32_t *>(&u2);
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t2) : "r"(in));
+    const __nv_bfloat162 tt = *reinterpret_cast<const __nv_bfloat162 *>(&t2);
+    const float2 t = __bfloat1622float2(tt);
+    const __nv_bfloat162 r = __floats2bfloat162_rn(0.5f * a * (1.0f + t.x), 0.5f * b * (1.0f + t.y));
+    return *reinterpret_cast<const uint32_t *>(&r);
+}
+
+// standardisation of the network's inputs and outputs, fitted on the training samples:
+// the network sees (x - xmu) / xsd and its output is multiplied by ysd
+struct Scaling {
+    float xmu[kIn], xsd[kIn], ysd[kOut];
+};
 
 // device view of the trained network for inference inside the step
 struct NetView {
     const __nv_bfloat16 *wt[4];  // forward B operands, blocked K-major [N_l][K_l]
     const float *b[4];           // biases
     Gates gates;
+    Scaling sc;
 };
 
 }  // namespace nn

@@ -201,8 +201,8 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {  // 
 // batch assembly: rows drawn at random (with replacement) or in order from `first`;
 // rows past the end of the sample set are zero
 __global__ void k_gather(const float *__restrict__ xs, const float *__restrict__ ts, long long ns, long long rows,
-                         int random, unsigned long long seed, long long first, bf16 *__restrict__ Xn,
-                         bf16 *__restrict__ Xt, float *__restrict__ Tb) {
+                         int random, unsigned long long seed, long long first, const Scaling *__restrict__ sc,
+                         bf16 *__restrict__ Xn, bf16 *__restrict__ Xt, float *__restrict__ Tb) {
     const long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (b >= rows) return;
     long long idx = random ? (long long)(mix64(seed ^ (unsigned long long)b * 0xD1B54A32D192ED03ull) % (unsigned long long)ns)
@@ -214,10 +214,10 @@ __global__ void k_gather(const float *__restrict__ xs, const float *__restrict__
     for (int n = 0; n < kOut; n++) t[n] = 0.0f;
     if (idx < ns) {
 #pragma unroll
-        for (int n = 0; n < kIn; n++) x[n] = xs[idx * kIn + n];
+        for (int n = 0; n < kIn; n++) x[n] = (xs[idx * kIn + n] - sc->xmu[n]) / sc->xsd[n];
         if (ts) {
 #pragma unroll
-            for (int n = 0; n < kOut; n++) t[n] = ts[idx * kOut + n];
+            for (int n = 0; n < kOut; n++) t[n] = ts[idx * kOut + n] / sc->ysd[n];
         }
     }
     const long long tile = b / kTileRows, rl = b % kTileRows;
@@ -362,6 +362,33 @@ __global__ void k_envelope(const float *__restrict__ xs, const float *__restrict
     atomicMax(ymax, ym);
 }
 
+// sums and sums of squares of every input and output over the sample set (FP64)
+__global__ void k_moments(const float *__restrict__ xs, const float *__restrict__ ts, long long ns, double *acc) {
+    double a[2 * (kIn + kOut)];
+#pragma unroll
+    for (int n = 0; n < 2 * (kIn + kOut); n++) a[n] = 0.0;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < ns; s += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int n = 0; n < kIn; n++) {
+            const double v = xs[s * kIn + n];
+            a[n] += v;
+            a[kIn + kOut + n] += v * v;
+        }
+#pragma unroll
+        for (int n = 0; n < kOut; n++) {
+            const double v = ts[s * kOut + n];
+            a[kIn + n] += v;
+            a[2 * kIn + kOut + n] += v * v;
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < 2 * (kIn + kOut); n++) {
+        double v = a[n];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&acc[n], v);
+    }
+}
+
 }  // namespace nn
 }  // namespace dg
 
@@ -386,6 +413,8 @@ struct dg_nn {
     unsigned long long seed = 1;
     float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
     Gates gates{};
+    Scaling sc{};              // host copy of the standardisation
+    Scaling *d_sc = nullptr;   // device copy read by the batch gather
     int trained = 0;
     std::vector<void *> allocs, scratch;
 };
@@ -551,7 +580,7 @@ int adam(dg_nn *n, long long rows, float lr, int apply, float *gout) {
 int gather(dg_nn *n, long long rows, int random, long long first) {
     k_gather<<<(unsigned)((rows + 127) / 128), 128, 0, n->stream>>>(n->xs, n->ts, n->ns, rows, random,
                                                                       n->seed + 0x9E37ull * (unsigned long long)n->step,
-                                                                      first, n->Xn, n->Xt, n->Tb);
+                                                                      first, n->d_sc, n->Xn, n->Xt, n->Tb);
     NN_CUDA(cudaGetLastError());
     return 0;
 }
@@ -617,6 +646,11 @@ int dg_nn_create(int device, unsigned long long seed, dg_nn **out) {
         if (cudaMemcpyAsync(n->W[l], w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, n->stream) != cudaSuccess)
             return bail(nn_fail(DG_ERR_CUDA, "weight upload failed"));
     }
+    for (int q = 0; q < kIn; q++) { n->sc.xmu[q] = 0.0f; n->sc.xsd[q] = 1.0f; }
+    for (int q = 0; q < kOut; q++) n->sc.ysd[q] = 1.0f;
+    if ((rc = nn_alloc_t(n, &n->d_sc, 1))) return bail(rc);
+    if (cudaMemcpyAsync(n->d_sc, &n->sc, sizeof(Scaling), cudaMemcpyHostToDevice, n->stream) != cudaSuccess)
+        return bail(nn_fail(DG_ERR_CUDA, "scaling upload failed"));
     for (int q = 0; q < kIn; q++) { n->gates.xmin[q] = -1e30f; n->gates.xmax[q] = 1e30f; }
     n->gates.ymax = 1e30f;
     n->gates.jump = 0.1f;
@@ -762,6 +796,8 @@ int dg_nn_forward(dg_nn *n, const float *x, long long count, float *y) {
                                    n->stream) != cudaSuccess)
             rc = nn_fail(DG_ERR_CUDA, "output read-back failed");
         if (!rc) rc = nn_sync(n);
+        for (long long r2 = 0; !rc && r2 < m; r2++)
+            for (int c = 0; c < kOut; c++) y[(first + r2) * kOut + c] *= n->sc.ysd[c];
     }
     if (n->xs) cudaFree(n->xs);
     if (n->ts) cudaFree(n->ts);
@@ -827,6 +863,33 @@ int dg_nn_fit_envelope(dg_nn *n, float margin) {
     return DG_OK;
 }
 
+int dg_nn_fit_scaling(dg_nn *n) {
+    if (!n || n->ns <= 0) return nn_fail(DG_ERR_ARG, "no samples");
+    NN_CUDA(cudaSetDevice(n->device));
+    const int na = 2 * (kIn + kOut);
+    double *d = nullptr;
+    NN_CUDA(cudaMalloc(&d, na * sizeof(double)));
+    cudaMemsetAsync(d, 0, na * sizeof(double), n->stream);
+    k_moments<<<296, 128, 0, n->stream>>>(n->xs, n->ts, n->ns, d);
+    std::vector<double> h(na);
+    cudaMemcpyAsync(h.data(), d, na * sizeof(double), cudaMemcpyDeviceToHost, n->stream);
+    const cudaError_t e = cudaStreamSynchronize(n->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return nn_fail(DG_ERR_CUDA, cudaGetErrorString(e));
+    const double N = (double)n->ns;
+    for (int q = 0; q < kIn; q++) {
+        const double mu = h[q] / N, var = std::max(h[kIn + kOut + q] / N - mu * mu, 0.0);
+        n->sc.xmu[q] = (float)mu;
+        n->sc.xsd[q] = var > 1e-12 ? (float)std::sqrt(var) : 1.0f;  // a constant input stays at zero
+    }
+    for (int q = 0; q < kOut; q++) {
+        const double rms = std::sqrt(h[2 * kIn + kOut + q] / N);
+        n->sc.ysd[q] = rms > 1e-30 ? (float)rms : 1.0f;
+    }
+    NN_CUDA(cudaMemcpyAsync(n->d_sc, &n->sc, sizeof(Scaling), cudaMemcpyHostToDevice, n->stream));
+    return nn_sync(n);
+}
+
 int dg_nn_set_gates(dg_nn *n, float jump, float compress) {
     if (!n || !(jump >= 0.0f) || !(compress >= 0.0f)) return nn_fail(DG_ERR_ARG, "bad gate thresholds");
     n->gates.jump = jump;
@@ -841,6 +904,7 @@ int dg_nn_view(const dg_nn *n, dg::nn::NetView *v) {
     if (!n) return DG_ERR_ARG;
     for (int l = 0; l < 4; l++) { v->wt[l] = n->Wt[l]; v->b[l] = n->b[l]; }
     v->gates = n->gates;
+    v->sc = n->sc;
     return DG_OK;
 }
 int dg_nn_device(const dg_nn *n) { return n ? n->device : -1; }

@@ -476,48 +476,59 @@ __global__ void __launch_bounds__(kThreads) k_nn_harvest(Geo G, const float *__r
         to[n] = (u.jump > nn::kTinyJump) ? (float)((t[n] - b[n]) / ((double)nn::out_scale(u, n) * (double)u.jump)) : 0.0f;
 }
 
-// shared-memory plan of the face-network kernel (bytes)
-constexpr int kNW1 = 0, kNW2 = 8192, kNW3 = 40960, kNW4 = 73728, kNX = 77824, kNH = 86016, kNBias = 118784,
-              kNBar = 120448, kNSmem = 120576;
+// shared-memory plan of the face-network kernel (bytes): the four weight tiles, then per
+// warpgroup one activation tile (its first 8 KB hold the input tile of layer 1), the
+// biases and the barriers
+constexpr int kNWG = 4;  // warpgroups per CTA (4 x 128 TMEM columns)
+constexpr int kNW1 = 0, kNW2 = 8192, kNW3 = 40960, kNW4 = 73728, kNH0 = 77824, kNHsz = 32768,
+              kNBias = kNH0 + kNWG * kNHsz, kNBar = kNBias + 1600, kNSmem = kNBar + 128;
 
-// One 128-face tile at a time per CTA: the faces' interface states, inputs and gates, the
-// four layers as tcgen05 MMAs (weights resident in shared memory, activations through
-// TMEM -> GELU -> shared memory), then the gated flux or a mark for HLLD.
-__global__ void __launch_bounds__(128, 1) k_nn_faces(Geo G, const float *__restrict__ core, float *__restrict__ flux,
-                                                     unsigned char *__restrict__ skip, int d, nn::NetView nv,
-                                                     const Scalars *S, unsigned long long *cnt, int *err) {
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory"); }
+
+// Four warpgroups per CTA, each taking 128-face tiles in turn: the faces' interface states,
+// inputs and gates, the four layers as tcgen05 MMAs (weights resident in shared memory,
+// each warpgroup with its own 128 TMEM columns, activations through TMEM -> GELU -> shared
+// memory), then the gated flux or a mark for HLLD.
+__global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *__restrict__ core,
+                                                            float *__restrict__ flux, unsigned char *__restrict__ skip,
+                                                            int d, nn::NetView nv, const Scalars *S,
+                                                            unsigned long long *cnt, int *err) {
     extern __shared__ __align__(1024) unsigned char sm[];
     using bf16 = __nv_bfloat16;
+    const int tid = threadIdx.x, wg = tid >> 7, wt = tid & 127, warp = tid >> 5, lane = tid & 31;
     bf16 *W[4] = {(bf16 *)(sm + kNW1), (bf16 *)(sm + kNW2), (bf16 *)(sm + kNW3), (bf16 *)(sm + kNW4)};
-    bf16 *Xs = (bf16 *)(sm + kNX), *Hs = (bf16 *)(sm + kNH);
+    bf16 *Hs = (bf16 *)(sm + kNH0 + wg * kNHsz), *Xs = Hs;
     float *bias = (float *)(sm + kNBias);  // 3 x 128 + 8
-    uint64_t *bar = (uint64_t *)(sm + kNBar);
-    uint32_t *tslot = (uint32_t *)(sm + kNBar + 16);
-    int *sflag = (int *)(sm + kNBar + 20);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint64_t *wbar = (uint64_t *)(sm + kNBar);
+    uint64_t *mbar = (uint64_t *)(sm + kNBar + 8 + 8 * wg);
+    uint32_t *tslot = (uint32_t *)(sm + kNBar + 8 + 8 * kNWG);
+    int *flags = (int *)(sm + kNBar + 16 + 8 * kNWG);
+    int *flag = flags + wg;
     if (tid == 0) {
-        nn::mbar_init(&bar[0], 1);
-        nn::mbar_init(&bar[1], 1);
+        nn::mbar_init(wbar, 1);
+        for (int g = 0; g < kNWG; g++) {
+            nn::mbar_init((uint64_t *)(sm + kNBar + 8 + 8 * g), 1);
+            flags[g] = 1;
+        }
         nn::mbar_fence_init();
-        *sflag = 1;
     }
-    for (int q = tid; q < 3 * nn::kHid + nn::kOut; q += 128) {
+    for (int q = tid; q < 3 * nn::kHid + nn::kOut; q += 128 * kNWG) {
         const int l = q / nn::kHid;
         bias[q] = (l < 3) ? nv.b[l][q % nn::kHid] : nv.b[3][q - 3 * nn::kHid];
     }
-    if (warp == 0) nn::tmem_alloc(tslot, 128);
+    if (warp == 0) nn::tmem_alloc(tslot, 128 * kNWG);
     nn::tc_fence_before();
     __syncthreads();
     nn::tc_fence_after();
-    const uint32_t tmem = *tslot;
-    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t tmem = *tslot + (uint32_t)(wg * 128);
+    const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     if (tid == 0) {
         const unsigned wb[4] = {128 * nn::kInPad * 2, 128 * 128 * 2, 128 * 128 * 2, nn::kOutPad * 128 * 2};
-        nn::mbar_expect_tx(&bar[0], wb[0] + wb[1] + wb[2] + wb[3]);
-        for (int l = 0; l < 4; l++) nn::bulk_g2s(W[l], nv.wt[l], wb[l], &bar[0]);
-        if (!nn::mbar_wait(&bar[0], 0)) {
-            nn::mbar_wait(&bar[0], 0);
-            *sflag = 0;
+        nn::mbar_expect_tx(wbar, wb[0] + wb[1] + wb[2] + wb[3]);
+        for (int l = 0; l < 4; l++) nn::bulk_g2s(W[l], nv.wt[l], wb[l], wbar);
+        if (!nn::mbar_wait(wbar, 0)) {
+            nn::mbar_wait(wbar, 0);
+            for (int g = 0; g < kNWG; g++) flags[g] = 0;
         }
     }
     __syncthreads();
@@ -526,8 +537,9 @@ __global__ void __launch_bounds__(128, 1) k_nn_faces(Geo G, const float *__restr
     const double dt = S->dt;
     unsigned ph = 0;
     unsigned long long nface = 0, nfall = 0;
-    for (long long tile = blockIdx.x; tile * 128 < G.fsz && *sflag; tile += gridDim.x) {
-        const long long t = tile * 128 + tid;
+    for (long long tile = (long long)kNWG * blockIdx.x + wg; tile * 128 < G.fsz && *flag;
+         tile += (long long)kNWG * gridDim.x) {
+        const long long t = tile * 128 + wt;
         int i = 0, j = 0, k = 1;
         bool valid = t < G.fsz;
         if (valid) {
@@ -550,62 +562,63 @@ __global__ void __launch_bounds__(128, 1) k_nn_faces(Geo G, const float *__restr
             u = nn::face_inputs(ql, qr, gamma, ciso, G.iso, x);
             use = nn::gate_inputs(nv.gates, ql, qr, ciso, G.iso, u, x);
             nn::base_fluxes<float>(ql, qr, gamma, ciso, G.iso, base);
-            if (!use) {
-#pragma unroll
-                for (int n = 0; n < nn::kIn; n++) x[n] = 0.0f;
-            }
         }
+#pragma unroll
+        for (int n = 0; n < nn::kIn; n++) x[n] = use ? (x[n] - nv.sc.xmu[n]) / nv.sc.xsd[n] : 0.0f;
 #pragma unroll
         for (int cg = 0; cg < nn::kInPad / 8; cg++) {
             __align__(16) bf16 h[8];
 #pragma unroll
             for (int q = 0; q < 8; q++) h[q] = __float2bfloat16_rn(x[cg * 8 + q]);
-            *(uint4 *)(Xs + (cg * 128 + tid) * 8) = *(const uint4 *)h;
+            *(uint4 *)(Xs + (cg * 128 + wt) * 8) = *(const uint4 *)h;
         }
         nn::fence_async_smem();
-        nn::tc_fence_before();  // this thread's TMEM reads of the previous tile come before the next MMA
-        __syncthreads();
+        nn::tc_fence_before();  // this warpgroup's TMEM reads of the previous tile come before the next MMA
+        wg_sync(wg);
         float y[nn::kOut];
         for (int l = 0; l < 4; l++) {
-            if (tid == 0) {
+            if (wt == 0) {
                 nn::tc_fence_after();
                 nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W[l], l == 3 ? nn::kOutPad : nn::kHid, l == 0 ? 2 : 8, 0);
-                nn::mma_commit(&bar[1]);
-                if (!nn::mbar_wait(&bar[1], ph & 1)) {
-                    nn::mbar_wait(&bar[1], ph & 1);
-                    *sflag = 0;
+                nn::mma_commit(mbar);
+                if (!nn::mbar_wait(mbar, ph & 1)) {
+                    nn::mbar_wait(mbar, ph & 1);
+                    *flag = 0;
                 }
             }
             ph++;
             nn::tc_fence_before();
-            __syncthreads();
+            wg_sync(wg);
             nn::tc_fence_after();
-            if (!*sflag) break;
+            if (!*flag) break;
             if (l < 3) {
                 for (int cc = 0; cc < nn::kHid / 16; cc++) {
                     float v[16];
                     nn::tmem_ld16(taddr + cc * 16, v);
 #pragma unroll
                     for (int hh = 0; hh < 2; hh++) {
-                        __align__(16) bf16 h[8];
+                        uint32_t h[4];
 #pragma unroll
-                        for (int q = 0; q < 8; q++)
-                            h[q] = __float2bfloat16_rn(nn::gelu(v[hh * 8 + q] + bias[l * nn::kHid + cc * 16 + hh * 8 + q]));
-                        *(uint4 *)(Hs + ((cc * 2 + hh) * 128 + tid) * 8) = *(const uint4 *)h;
+                        for (int q = 0; q < 4; q++) {
+                            const int c0 = cc * 16 + hh * 8 + 2 * q;
+                            h[q] = nn::gelu2_bf16(v[hh * 8 + 2 * q] + bias[l * nn::kHid + c0],
+                                                  v[hh * 8 + 2 * q + 1] + bias[l * nn::kHid + c0 + 1]);
+                        }
+                        *(uint4 *)(Hs + ((cc * 2 + hh) * 128 + wt) * 8) = make_uint4(h[0], h[1], h[2], h[3]);
                     }
                 }
                 nn::fence_async_smem();
                 nn::tc_fence_before();
-                __syncthreads();
+                wg_sync(wg);
                 nn::tc_fence_after();
             } else {
                 float v[16];
                 nn::tmem_ld16(taddr, v);
 #pragma unroll
-                for (int q = 0; q < nn::kOut; q++) y[q] = v[q] + bias[3 * nn::kHid + q];
+                for (int q = 0; q < nn::kOut; q++) y[q] = (v[q] + bias[3 * nn::kHid + q]) * nv.sc.ysd[q];
             }
         }
-        if (!*sflag) break;
+        if (!*flag) break;
         if (valid) {
             bool acc = use;
             float F[nn::kOut];
@@ -625,7 +638,7 @@ __global__ void __launch_bounds__(128, 1) k_nn_faces(Geo G, const float *__restr
             nfall += acc ? 0 : 1;
         }
     }
-    if (!*sflag && tid == 0) atomicOr(err, nn::NN_ERR_WAIT);
+    if (!*flag && wt == 0) atomicOr(err, nn::NN_ERR_WAIT);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         nface += __shfl_xor_sync(0xffffffffu, nface, o);
@@ -639,7 +652,7 @@ __global__ void __launch_bounds__(128, 1) k_nn_faces(Geo G, const float *__restr
     __syncthreads();
     if (warp == 0) {
         nn::tc_fence_after();
-        nn::tmem_dealloc(tmem, 128);
+        nn::tmem_dealloc(*tslot, 128 * kNWG);
     }
 }
 
@@ -697,10 +710,10 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     }
     if (B.net) {
         float *fl[3] = {fx, fy, fz};
-        const long long tiles = (G.fsz + 127) / 128;
-        const unsigned grid = (unsigned)(tiles < 148 ? tiles : 148);
+        const long long groups = (G.fsz + 128 * kNWG - 1) / (128 * kNWG);
+        const unsigned grid = (unsigned)(groups < 148 ? groups : 148);
         for (int d = 0; d < G.ndim; d++) {
-            TIMED(KS_NN_FACES, s, (k_nn_faces<<<grid, 128, kNSmem, s>>>(G, core, fl[d], B.skip[d], d, *B.net, B.S, B.nn_count, B.nn_err)));
+            TIMED(KS_NN_FACES, s, (k_nn_faces<<<grid, 128 * kNWG, kNSmem, s>>>(G, core, fl[d], B.skip[d], d, *B.net, B.S, B.nn_count, B.nn_err)));
             sk.f[d] = B.skip[d];
             n++;
         }

@@ -221,6 +221,9 @@ int  dg_nn_set_params(dg_nn *nn, const float *params, long long count);
 /* the envelope of the current samples (widened by margin x its width) becomes
  * the confidence gate */
 int  dg_nn_fit_envelope(dg_nn *nn, float margin);
+/* standardise inputs (mean, standard deviation) and outputs (root mean square) by
+ * the current samples; call before training (identity until then) */
+int  dg_nn_fit_scaling(dg_nn *nn);
 int  dg_nn_set_gates(dg_nn *nn, float jump, float compress);
 /* use `nn` (NULL: none) for the faces of an FP32 context made with surrogate = 1 */
 int  dg_attach_surrogate(dg_ctx *ctx, dg_nn *nn);

@@ -16,7 +16,6 @@ W3[128][128], b3, W4[128][8], b4 (W[k][n] maps input k to output n).
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 SHAPES = [(17, 128), (128, 128), (128, 128), (128, 8)]
 
@@ -44,12 +43,17 @@ def bf16(a: np.ndarray) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z: np.ndarray) -> np.ndarray:
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """GELU in its tanh form, as the library uses it."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_d(z: np.ndarray) -> np.ndarray:
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def forward(p: np.ndarray, x: np.ndarray, bf16_rounding: bool = True):

@@ -107,7 +107,7 @@ def ot_params(n, precision="fp32", surrogate=False):
                   courant=0.8, precision=precision, surrogate=surrogate)
 
 
-def train_on_ot(net, n=32, snapshots=4, steps_between=5, train_steps=800):
+def train_on_ot(net, n=32, snapshots=4, steps_between=5, train_steps=2400):
     p = ot_params(n)
     with Context(p) as g:
         g.upload(condinit(p, "orszag_tang"))
@@ -119,28 +119,43 @@ def train_on_ot(net, n=32, snapshots=4, steps_between=5, train_steps=800):
     x, y = net.samples()
     assert np.isfinite(x).all() and np.isfinite(y).all()
     net.fit_envelope(0.0)
-    loss = net.train(train_steps, batch=8192, lr=1e-3)
+    net.fit_scaling()
+    for lr in (1e-3, 3e-4, 1e-4):
+        loss = net.train(train_steps // 3, batch=8192, lr=lr)
     return loss
 
 
+def mri_params(n, precision="fp32", surrogate=False):
+    return Params(ndim=3, iso=1, nx=n, ny=n, nz=n, xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5, zmin=-0.5, zmax=0.5,
+                  ciso=1.0, omega0=1.0, courant=0.8, bdtypex="shearingbox", fargo=True, precision=precision,
+                  surrogate=surrogate)
+
+
 def test_harvest_labels_and_network_gain():
-    """Held-out interfaces: LLF + learned correction is much closer to HLLD than LLF alone."""
-    with FluxNet(seed=2) as net:
-        loss = train_on_ot(net)
-        # a fresh, later snapshot as the held-out set
-        p = ot_params(32)
-        with Context(p) as g, FluxNet(seed=9) as probe:
-            g.upload(condinit(p, "orszag_tang"))
-            g.boundary(0.0, 0.0)
-            g.run(37, 0.0)
-            probe.harvest(g, stride=3)
-            xh, th = probe.samples()
+    """Held-out interfaces of a shearing-box MRI run: per flux component, LLF + the learned
+    correction is much closer to HLLD than LLF alone."""
+    p = mri_params(48)
+    with FluxNet(seed=2) as net, FluxNet(seed=9) as probe, Context(p) as g:
+        g.upload(condinit(p, "mri", beta=1000.0, amp=0.1, seed=2024))
+        g.boundary(0.0, 0.0)
+        t = 0.0
+        for _ in range(4):
+            t, _ = g.run(5, t)
+            net.harvest(g)
+        t, _ = g.run(7, t)
+        probe.harvest(g, stride=3)
+        xh, th = probe.samples()
+        net.fit_envelope(0.0)
+        net.fit_scaling()
+        for lr in (1e-3, 3e-4, 1e-4):
+            loss = net.train(800, batch=8192, lr=lr)
         yh = net.forward(xh)
         jump = xh[:, 14:15]  # targets are per unit jump: weigh by the jump to compare fluxes
-        err_nn = np.mean(np.abs(yh - th) * jump)
-        err_llf = np.mean(np.abs(th) * jump)   # LLF alone: correction 0
-        print("train loss", loss, "held-out L1 of the correction: network", err_nn, "LLF alone", err_llf)
-        assert err_nn < 0.2 * err_llf
+        # per output: L1 error of LLF + network against HLLD over that of LLF alone (correction 0)
+        ratio = np.sum(np.abs(yh - th) * jump, 0) / np.sum(np.abs(th) * jump, 0)
+        print("samples", net.sample_count, "train loss", loss, "held-out error ratio per output",
+              np.array2string(ratio, precision=3))
+        assert np.mean(ratio) < 0.2 and np.max(ratio) < 0.6
 
 
 def l1_rel(a, b):
