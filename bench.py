@@ -214,6 +214,7 @@ def main() -> None:
 
     import dumses_hybrid_b200 as dg
     from dumses_hybrid_b200 import build as dgbuild
+    from dumses_hybrid_b200.surrogate import train_flux_net
 
     if rank == 0:
         dgbuild.build()
@@ -245,58 +246,17 @@ def main() -> None:
 
     ncell = args.n ** 3
 
-    def train_network(P) -> tuple[object, dict]:
-        """Harvest interfaces (FP64 HLLD labels) from snapshots of a plain FP32 run of the same
-        workload, train the network on the device, and measure it on a held-out snapshot."""
-        t0 = time.perf_counter()
-        net = dg.FluxNet(device=local_rank, seed=7)
-        Pt = dg.Params(**{**P.__dict__, "surrogate": False})
-        with dg.Context(Pt) as tc:
-            tc.upload(initial_state(Pt, args.workload))
-            tc.boundary(0.0, 0.0)
-            ts = 0.0
-            for _ in range(args.nn_snapshots):
-                ts, _ = tc.run(args.nn_every, ts)
-                net.harvest(tc, stride=args.nn_stride)
-            ts, _ = tc.run(args.nn_every, ts)
-            probe = dg.FluxNet(device=local_rank, seed=8)
-            probe.harvest(tc, stride=max(1, args.nn_stride * 16 + 1))
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        ns = net.sample_count
-        net.fit_scaling()
-        steps = max(3, int(args.nn_epochs * ns / args.nn_batch))
-        for lr in (1e-3, 3e-4, 1e-4):  # step-wise decay over three equal phases
-            loss = net.train(steps // 3, batch=args.nn_batch, lr=lr)
-        steps = 3 * (steps // 3)
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        net.fit_envelope(0.0)
-        xh, th = probe.samples()
-        probe.close()
-        yh = net.forward(xh)
-        jump = xh[:, 14:15]
-        ratio = np.sum(np.abs(yh - th) * jump, 0) / np.maximum(np.sum(np.abs(th) * jump, 0), 1e-300)
-        info = {"samples": int(ns), "batch": args.nn_batch, "adam_steps": steps, "final_loss": loss,
-                "harvest_s": t1 - t0, "train_s": t2 - t1, "train_samples_per_s": steps * args.nn_batch / (t2 - t1),
-                "held_out_faces": int(xh.shape[0]),
-                "held_out_error_ratio": {
-                    "definition": "per output, L1 of (LLF + network - HLLD) over L1 of (LLF - HLLD) on held-out faces",
-                    "outputs": ["mass", "energy", "normal_momentum", "t1_momentum", "B_t1", "t2_momentum", "B_t2",
-                                "p_star"],
-                    "ratio": [float(r) for r in ratio], "mean": float(np.mean(ratio))},
-                "network": "17-128-128-128-8 GELU (tanh form), bf16 weights, fp32 accumulate (tcgen05), Adam, "
-                           "lr 1e-3 / 3e-4 / 1e-4 in three equal phases, standardised inputs and outputs"}
-        return net, info
-
     def measure(precision: str, with_e2e: bool) -> dict:
         surrogate = precision == "fp32nn"
         P = workload_params(args.n, device=local_rank, precision="fp32" if surrogate else precision,
                             kind=args.workload)
+        u0 = initial_state(P, args.workload)
         if surrogate:
             P.surrogate = True
-            net, nn_info = train_network(P)
-        u0 = initial_state(P, args.workload)
+            torch.cuda.synchronize()
+            net, nn_info = train_flux_net(P, u0, snapshots=args.nn_snapshots, every=args.nn_every,
+                                          stride=args.nn_stride, epochs=args.nn_epochs, batch=args.nn_batch)
+            torch.cuda.synchronize()
         ctx = dg.Context(P)
         if surrogate:
             ctx.attach_surrogate(net)
