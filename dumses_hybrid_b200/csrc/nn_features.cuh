@@ -80,18 +80,46 @@ __device__ __forceinline__ FaceUnits face_inputs(const float *ql, const float *q
     return u;
 }
 
-// the base of the correction: LLF fluxes in output order and the mean total pressure
+// the base of the correction: LLF fluxes in output order and the mean total pressure, and
+// the LLF dissipation term dis (central flux minus LLF flux; zero for p*_T)
 template <typename T>
-__device__ __forceinline__ void base_fluxes(const T *ql, const T *qr, T gamma, T ciso, int iso, T b[kOut]) {
-    T f[8];
-    llf1d<T>(ql, qr, f, gamma, ciso, iso);
+__device__ __forceinline__ void base_fluxes(const T *ql, const T *qr, T gamma, T ciso, int iso, T b[kOut],
+                                            T dis[kOut]) {
+    T fl[8], cl[8], fr[8], cr[8], ploc, proc, a;
+    lr_fluxes(ql, qr, gamma, ciso, iso, fl, cl, fr, cr, ploc, proc, a);
     const T half = T(0.5);
-    const T pl = iso ? ql[0] * (ciso * ciso) : ql[1], pr = iso ? qr[0] * (ciso * ciso) : qr[1];
+    const T vel = mx(cfast(gamma, ploc, ql[0], a, ql[5], ql[7]) + fab(ql[2]),
+                     cfast(gamma, proc, qr[0], a, qr[5], qr[7]) + fab(qr[2]));
+    const int src[7] = {0, 1, 2, 4, 5, 6, 7};
+#pragma unroll
+    for (int c = 0; c < 7; c++) {
+        const int n = src[c];
+        dis[c] = vel * half * (cr[n] - cl[n]);
+        b[c] = half * (fl[n] + fr[n]) - dis[c];
+    }
     const T bn = ql[3];
-    const T ptl = pl + half * (bn * bn + ql[5] * ql[5] + ql[7] * ql[7]);
-    const T ptr = pr + half * (bn * bn + qr[5] * qr[5] + qr[7] * qr[7]);
-    b[0] = f[0]; b[1] = f[1]; b[2] = f[2]; b[3] = f[4]; b[4] = f[5]; b[5] = f[6]; b[6] = f[7];
+    const T ptl = ploc + half * (bn * bn + ql[5] * ql[5] + ql[7] * ql[7]);
+    const T ptr = proc + half * (bn * bn + qr[5] * qr[5] + qr[7] * qr[7]);
     b[7] = half * (ptl + ptr);
+    dis[7] = T(0);
+}
+
+// dissipation gate: per flux component, the learned correction k (in units of scale x J)
+// must move the flux from LLF towards the central flux, no further than the whole LLF
+// dissipation dn (same units), up to eps = 5% of the largest |dn|.  A flux outside that
+// band would be anti-diffusive or more diffusive than LLF: HLLD is used instead.
+__device__ __forceinline__ bool gate_dissipation(const float y[kOut], const float dn[kOut]) {
+    float dmax = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 7; c++) dmax = fmaxf(dmax, fabsf(dn[c]));
+    const float eps = 0.05f * dmax;
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < 7; c++) {
+        const float k = (dn[c] >= 0.0f) ? y[c] : -y[c];
+        ok = ok && k >= -eps && k <= fabsf(dn[c]) + eps;
+    }
+    return ok;
 }
 
 // HLLD fluxes in output order (normal momentum including p*_T), FP64 labels

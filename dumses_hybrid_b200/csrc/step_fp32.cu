@@ -466,7 +466,8 @@ __global__ void __launch_bounds__(kThreads) k_nn_harvest(Geo G, const float *__r
 #pragma unroll
     for (int n = 0; n < 8; n++) { qld[n] = ql[n]; qrd[n] = qr[n]; }
     nn::hlld_targets(qld, qrd, G.gamma, G.ciso, G.iso, t);
-    nn::base_fluxes<double>(qld, qrd, G.gamma, G.ciso, G.iso, b);
+    double dis[nn::kOut];
+    nn::base_fluxes<double>(qld, qrd, G.gamma, G.ciso, G.iso, b, dis);
     float *xo = xs + (first + s) * nn::kIn;
     float *to = ts + (first + s) * nn::kOut;
 #pragma unroll
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
             valid = (d == 0) ? (j <= G.ny && (G.ndim == 2 || k <= G.nz))
                   : (d == 1) ? (i <= G.nx && (G.ndim == 2 || k <= G.nz)) : (i <= G.nx && j <= G.ny);
         }
-        float ql[8], qr[8], x[nn::kInPad], base[nn::kOut];
+        float ql[8], qr[8], x[nn::kInPad], base[nn::kOut], dis[nn::kOut];
         nn::FaceUnits u{1.0f, 1.0f, 1.0f, 0.0f};
         bool use = false;
 #pragma unroll
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
             face_io(G, cv, cl, cr, d, ql, qr);
             u = nn::face_inputs(ql, qr, gamma, ciso, G.iso, x);
             use = nn::gate_inputs(nv.gates, ql, qr, ciso, G.iso, u, x);
-            nn::base_fluxes<float>(ql, qr, gamma, ciso, G.iso, base);
+            nn::base_fluxes<float>(ql, qr, gamma, ciso, G.iso, base, dis);
         }
 #pragma unroll
         for (int n = 0; n < nn::kIn; n++) x[n] = use ? (x[n] - nv.sc.xmu[n]) / nv.sc.xsd[n] : 0.0f;
@@ -621,14 +622,17 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         if (!*flag) break;
         if (valid) {
             bool acc = use;
-            float F[nn::kOut];
+            float F[nn::kOut], dn[nn::kOut];
 #pragma unroll
             for (int c = 0; c < nn::kOut; c++) {
                 acc = acc && fabsf(y[c]) <= 1.5f * nv.gates.ymax;  // confidence: inside the training range
-                F[c] = base[c] + nn::out_scale(u, c) * u.jump * y[c];
+                const float sj = nn::out_scale(u, c) * u.jump;
+                F[c] = base[c] + sj * y[c];
+                dn[c] = (sj > 0.0f) ? dis[c] / sj : 0.0f;
                 acc = acc && isfinite(F[c]);
             }
-            acc = acc && F[7] > 0.0f;  // positive star pressure
+            acc = acc && F[7] > 0.0f;                      // positive star pressure
+            acc = acc && nn::gate_dissipation(y, dn);    // no anti-diffusion, no more than LLF's
             if (acc) {
                 float f[8] = {F[0], F[1], F[2] - F[7], 0.0f, F[3], F[4], F[5], F[6]};
                 flux_store(G, ql, qr, f, F[7], d, i, dt, flux, t);
