@@ -304,7 +304,7 @@ class Context:
 
     def profile_read(self) -> dict[str, tuple[float, int]]:
         """{kernel slot: (total ms, launches)} since the last read."""
-        n = 13
+        n = 14
         ms = np.zeros(n)
         cnt = (ctypes.c_longlong * n)()
         _check(self.lib.dg_profile_read(self.h, self._ptr(ms), cnt, n))

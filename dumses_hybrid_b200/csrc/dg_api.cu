@@ -45,7 +45,7 @@ struct EventTimer : dg::KernelTimer {
 };
 const char *kSlotNames[dg::KS_COUNT] = {"scalars", "cfl_dt", "primitive", "trace", "riemann_flux_emf", "update_ct",
                                        "fargo_emf", "fargo_update", "boundary", "history", "right_faces", "edge_efield",
-                                       "nn_faces"};
+                                       "nn_faces", "nn_fallback"};
 }  // namespace
 
 namespace {
@@ -322,8 +322,8 @@ int dg_init(const dg_params *p, dg_ctx **out) {
             if ((rc = alloc(c, &c->B.femf[d], (size_t)G.fsz))) return bail(rc);
     if (p->surrogate) {
         for (int d = 0; d < p->ndim; d++)
-            if ((rc = alloc_bytes(c, (void **)&c->B.skip[d], (size_t)G.fsz))) return bail(rc);
-        if ((rc = alloc_bytes(c, (void **)&c->B.nn_count, 4 * sizeof(unsigned long long)))) return bail(rc);
+            if ((rc = alloc_bytes(c, (void **)&c->B.fb_list[d], (size_t)G.fsz * sizeof(int)))) return bail(rc);
+        if ((rc = alloc_bytes(c, (void **)&c->B.nn_count, 8 * sizeof(unsigned long long)))) return bail(rc);
         c->B.nn_err = (int *)(c->B.nn_count + 2);
     }
     if ((rc = alloc(c, &c->B.part, (size_t)(2 * p->nx + 8 * 296 + 64)))) return bail(rc);
@@ -346,7 +346,7 @@ int dg_finalize(dg_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *bufs[] = {c->B.U[0], c->B.U[1], c->B.Q, c->B.core, c->B.flx[0], c->B.flx[1], c->B.flx[2], c->B.emf[0],
                     c->B.emf[1], c->B.emf[2], c->B.femf[0], c->B.femf[1], c->B.part, c->B.hist,
-                    c->B.E[0], c->B.E[1], c->B.E[2], c->B.stage, c->B.skip[0], c->B.skip[1], c->B.skip[2],
+                    c->B.E[0], c->B.E[1], c->B.E[2], c->B.stage, c->B.fb_list[0], c->B.fb_list[1], c->B.fb_list[2],
                     c->B.nn_count};
     for (void *b : bufs)
         if (b) cudaFree(b);

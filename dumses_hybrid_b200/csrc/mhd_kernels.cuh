@@ -27,8 +27,9 @@ struct Bufs {
     long long sv;      // cells per plane
     // learned face flux (FP32 path with surrogate = 1)
     const nn::NetView *net;         // attached network (host copy of its device view), null: HLLD everywhere
-    unsigned char *skip[3];         // per face: 1 when the network's flux was used
-    unsigned long long *nn_count;   // device counters: faces seen, faces sent back to HLLD
+    int *fb_list[3];                // per direction: faces sent back to HLLD in the current step
+    unsigned long long *nn_count;   // device counters: [0] faces seen, [1] faces sent back to HLLD
+                                    // (both since the last read), [3 + d] length of fb_list[d]
     int *nn_err;                    // device error word of the network kernels
 };
 
@@ -36,7 +37,7 @@ int nstate_vars(const Geo &G);
 
 // per-kernel timing slots (CUDA events around each launch when a timer is attached)
 enum KernelSlot { KS_SCALARS = 0, KS_DT, KS_PRIM, KS_TRACE, KS_RIEMANN, KS_UPDATE, KS_FARGO_EMF, KS_FARGO_UPDATE,
-                  KS_BOUNDARY, KS_HISTORY, KS_RIGHT_FACES, KS_EFIELD, KS_NN_FACES, KS_COUNT };
+                  KS_BOUNDARY, KS_HISTORY, KS_RIGHT_FACES, KS_EFIELD, KS_NN_FACES, KS_NN_FALLBACK, KS_COUNT };
 struct KernelTimer {
     virtual void begin(int slot, cudaStream_t st) = 0;
     virtual void end(int slot, cudaStream_t st) = 0;

@@ -173,17 +173,19 @@ __device__ __forceinline__ float tanh_approx(float x) {
 __device__ __forceinline__ float gelu_fast(float z) {
     return 0.5f * z * (1.0f + tanh_approx(kGeluC * (z + kGeluA * z * z * z)));
 }
-// two GELUs packed as BF16x2 (low half = a), the tanh evaluated on BF16x2 (PTX
-// tanh.approx.bf16x2): the results are BF16 activations, so BF16 accuracy suffices
+// two GELUs packed as BF16x2 (low half = a), evaluated in BF16x2 arithmetic with the
+// PTX tanh.approx.bf16x2: the results are BF16 activations, so BF16 accuracy suffices
 __device__ __forceinline__ uint32_t gelu2_bf16(float a, float b) {
-    const float ua = kGeluC * (a + kGeluA * a * a * a), ub = kGeluC * (b + kGeluA * b * b * b);
-    const __nv_bfloat162 u2 = __floats2bfloat162_rn(ua, ub);
-    uint32_t t2, in = *reinterpret_cast<const uint32_t *>(&u2);
+    const __nv_bfloat162 z = __floats2bfloat162_rn(a, b);
+    const __nv_bfloat162 ca = __float2bfloat162_rn(kGeluC * kGeluA), c = __float2bfloat162_rn(kGeluC);
+    const __nv_bfloat162 half = __float2bfloat162_rn(0.5f);
+    const __nv_bfloat162 u = __hmul2(z, __hfma2(__hmul2(z, z), ca, c));  // c (z + a z^3)
+    uint32_t t2, in = *reinterpret_cast<const uint32_t *>(&u);
     asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t2) : "r"(in));
-    const __nv_bfloat162 tt = *reinterpret_cast<const __nv_bfloat162 *>(&t2);
-    const float2 t = __bfloat1622float2(tt);
-    const __nv_bfloat162 r = __floats2bfloat162_rn(0.5f * a * (1.0f + t.x), 0.5f * b * (1.0f + t.y));
-    return *reinterpret_cast<const uint32_t *>(&r);
+    const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162 *>(&t2);
+    const __nv_bfloat162 hz = __hmul2(z, half);
+    const __nv_bfloat162 g = __hfma2(hz, t, hz);  // 0.5 z (1 + t)
+    return *reinterpret_cast<const uint32_t *>(&g);
 }
 
 // standardisation of the network's inputs and outputs, fitted on the training samples:

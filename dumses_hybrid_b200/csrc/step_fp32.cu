@@ -491,7 +491,7 @@ __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128
 // each warpgroup with its own 128 TMEM columns, activations through TMEM -> GELU -> shared
 // memory), then the gated flux or a mark for HLLD.
 __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *__restrict__ core,
-                                                            float *__restrict__ flux, unsigned char *__restrict__ skip,
+                                                            float *__restrict__ flux, int *__restrict__ fallback,
                                                             int d, nn::NetView nv, const Scalars *S,
                                                             unsigned long long *cnt, int *err) {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
                 float f[8] = {F[0], F[1], F[2] - F[7], 0.0f, F[3], F[4], F[5], F[6]};
                 flux_store(G, ql, qr, f, F[7], d, i, dt, flux, t);
             }
-            skip[t] = acc ? 1 : 0;
+            if (!acc) fallback[atomicAdd(&cnt[3 + d], 1ULL)] = (int)t;  // HLLD for this face
             nface++;
             nfall += acc ? 0 : 1;
         }
@@ -657,6 +657,26 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     if (warp == 0) {
         nn::tc_fence_after();
         nn::tmem_dealloc(*tslot, 128 * kNWG);
+    }
+}
+
+// exact HLLD for the faces of direction d that the network sent back
+__global__ void __launch_bounds__(kThreads) k_nn_fallback(Geo G, const float *__restrict__ core,
+                                                          float *__restrict__ flux, const int *__restrict__ list,
+                                                          const unsigned long long *__restrict__ cnt, int d,
+                                                          const Scalars *S) {
+    const unsigned long long n = cnt[3 + d];
+    const CoreView<float> cv{core, G.ndim == 3 ? kCore3 : kCore2};
+    const double dt = S->dt;
+    for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < n;
+         q += (unsigned long long)gridDim.x * blockDim.x) {
+        const long long t = list[q];
+        const int i = (int)(t % G.FX) + 1;
+        const long long r = t / G.FX;
+        const int j = (int)(r % G.FY) + 1, k = (int)(r / G.FY) + 1;
+        long long cl, cr;
+        face_cells(G, d, i, j, k, cl, cr);
+        face_flux(G, cv, cl, cr, d, i, dt, flux, t);
     }
 }
 
@@ -704,7 +724,7 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     int n = 1 + (G.shearing ? 1 : 0) + 4;
-    FaceSkip sk{{nullptr, nullptr, nullptr}};
+    int faces = 1;
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
         TIMED(KS_TRACE, s, (k_trace3d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
@@ -712,21 +732,32 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         TIMED(KS_EFIELD, s, (k_efield2d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2)));
         TIMED(KS_TRACE, s, (k_trace2d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2, core, B.S)));
     }
+    float *fl[3] = {fx, fy, fz};
     if (B.net) {
-        float *fl[3] = {fx, fy, fz};
+        // the network's faces, with the faces it sends back to HLLD listed per direction
+        cudaMemsetAsync(B.nn_count + 3, 0, 3 * sizeof(unsigned long long), s);
         const long long groups = (G.fsz + 128 * kNWG - 1) / (128 * kNWG);
         const unsigned grid = (unsigned)(groups < 148 ? groups : 148);
         for (int d = 0; d < G.ndim; d++) {
-            TIMED(KS_NN_FACES, s, (k_nn_faces<<<grid, 128 * kNWG, kNSmem, s>>>(G, core, fl[d], B.skip[d], d, *B.net, B.S, B.nn_count, B.nn_err)));
-            sk.f[d] = B.skip[d];
+            TIMED(KS_NN_FACES, s, (k_nn_faces<<<grid, 128 * kNWG, kNSmem, s>>>(G, core, fl[d], B.fb_list[d], d, *B.net, B.S, B.nn_count, B.nn_err)));
+            n++;
+        }
+        faces = 0;
+    }
+    if (G.ndim == 3) {
+        TIMED(KS_RIEMANN, s, (k_riemann3d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
+    } else {
+        TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, faces)));
+    }
+    if (B.net) {
+        for (int d = 0; d < G.ndim; d++) {
+            TIMED(KS_NN_FALLBACK, s, (k_nn_fallback<<<148 * 4, kThreads, 0, s>>>(G, core, fl[d], B.fb_list[d], B.nn_count, d, B.S)));
             n++;
         }
     }
     if (G.ndim == 3) {
-        TIMED(KS_RIEMANN, s, (k_riemann3d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, sk)));
         TIMED(KS_UPDATE, s, (k_update3d_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U, Un, fx, fy, fz, ex, ey, ez, B.S)));
     } else {
-        TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, sk)));
         TIMED(KS_UPDATE, s, (k_update2d_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U, Un, fx, fy, ez, B.S)));
     }
     return n;

@@ -237,12 +237,12 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
         TIMED(KS_TRACE, s, (k_trace3d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
-        TIMED(KS_RIEMANN, s, (k_riemann3d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, FaceSkip{{nullptr, nullptr, nullptr}})));
+        TIMED(KS_RIEMANN, s, (k_riemann3d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, 1)));
         TIMED(KS_UPDATE, s, (k_update3d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, fz, ex, ey, ez, B.S)));
     } else {
         TIMED(KS_EFIELD, s, (k_efield2d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2)));
         TIMED(KS_TRACE, s, (k_trace2d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2, core, B.S)));
-        TIMED(KS_RIEMANN, s, (k_riemann2d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, FaceSkip{{nullptr, nullptr, nullptr}})));
+        TIMED(KS_RIEMANN, s, (k_riemann2d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, 1)));
         TIMED(KS_UPDATE, s, (k_update2d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, ez, B.S)));
     }
     return 5 + (G.shearing ? 1 : 0);

@@ -846,17 +846,11 @@ __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long l
     return emf;
 }
 
-// faces whose flux another solver already wrote (null: none)
-struct FaceSkip {
-    const unsigned char *f[3];
-    __device__ __forceinline__ bool skip(int d, long long t) const { return f[d] && f[d][t]; }
-};
-
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                            T *__restrict__ fy, T *__restrict__ fz, T *__restrict__ ex,
                                                            T *__restrict__ ey, T *__restrict__ ez, const Scalars *S,
-                                                           FaceSkip sk) {
+                                                           int faces) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
     const int i = (int)(t % G.FX) + 1;
@@ -867,9 +861,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__res
     const CoreView<T> cv{core, kCore3};
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const long long c = G.cidx(i, j, k);
-    if (j <= ny && k <= nz && !sk.skip(0, t)) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
-    if (i <= nx && k <= nz && !sk.skip(1, t)) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
-    if (i <= nx && j <= ny && !sk.skip(2, t)) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
+    if (faces) {  // faces = 0: the face fluxes come from the learned flux and its HLLD fallback list
+        if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
+        if (i <= nx && k <= nz) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
+        if (i <= nx && j <= ny) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
+    }
     if (k <= nz) ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
     if (j <= ny) ey[t] = edge_emf(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
     if (i <= nx) ex[t] = edge_emf(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
@@ -878,7 +874,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__res
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                         T *__restrict__ fy, T *__restrict__ ez, const Scalars *S,
-                                                        FaceSkip sk) {
+                                                        int faces) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
     const int i = (int)(t % G.FX) + 1;
@@ -886,8 +882,8 @@ __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restri
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore2};
     const long long c = G.cidx(i, j, 1);
-    if (j <= G.ny && !sk.skip(0, t)) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t);
-    if (i <= G.nx && !sk.skip(1, t)) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t);
+    if (faces && j <= G.ny) face_flux(G, cv, G.cidx(i - 1, j, 1), c, 0, i, dt, fx, t);
+    if (faces && i <= G.nx) face_flux(G, cv, G.cidx(i, j - 1, 1), c, 1, i, dt, fy, t);
     ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, 1), G.cidx(i, j - 1, 1), G.cidx(i - 1, j, 1), c, 2, i, dt);
 }
 

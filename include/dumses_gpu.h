@@ -149,7 +149,7 @@ int  dg_sync(dg_ctx *ctx);
  * dg_profile(ctx, 1) starts recording an event pair around every kernel;
  * dg_profile_read fills ms[slot] and count[slot] for the launches since the
  * last read (slots named by dg_profile_slot_name) and resets them. */
-#define DG_PROFILE_SLOTS 13
+#define DG_PROFILE_SLOTS 14
 int  dg_profile(dg_ctx *ctx, int on);
 int  dg_profile_read(dg_ctx *ctx, double *ms, long long *count, int nslots);
 const char *dg_profile_slot_name(int slot);
