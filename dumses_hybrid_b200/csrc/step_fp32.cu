@@ -374,58 +374,58 @@ __global__ void __launch_bounds__(kThreads) k_fargo_emf_hl(Geo G, StoreHL U, flo
     if (k <= G.nz) fez[t] = -emf(IA, fargo_shift(G, 0.5 * (G.xc(i) + G.xc(i - 1)), dt));  // fargo.f90:204-235
 }
 
-// remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119)
+// remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119), along
+// y lines as the FP64 kernel does (one thread per face column and segment, a sliding window
+// of (hi, lo) source values and slopes)
 __global__ void __launch_bounds__(kThreads) k_fargo_update_hl(Geo G, StoreHL U, StoreHL Un,
                                                               const float *__restrict__ fex,
                                                               const float *__restrict__ fez, const Scalars *S) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    FargoLine L;
+    if (!fargo_line(G, blockIdx.x * (long long)blockDim.x + threadIdx.x, L)) return;
+    const int i = L.i, k = L.k;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
-    const long long c = G.idx(i, j, k);
-    if (i <= nx && j <= ny && k <= nz) {
+    if (i <= nx && k <= nz && L.jb <= ny) {
         const FargoShift f = fargo_shift(G, G.xc(i), S->dt);
-        int js, jsp;
-        if (f.vK > 0.0) {
-            js = j - f.nshft - 1;
-            if (js < 1) js = js + ny;
-        } else {
-            js = j + f.nshft;
-            if (js > ny) js = js - ny;
-        }
-        jsp = js + 1;
-        if (jsp > ny) jsp = jsp - ny;
-        js = wrap1(js, ny);
-        jsp = wrap1(jsp, ny);
         const float eps = (float)f.eps;
         const float w = (f.vK > 0.0) ? 1.0f - eps : eps;  // weight of the upper donor
         const float hme = 0.5f - eps;
         const float q = 0.5f * (0.25f - hme * hme);
         const int ist = mn(G.slope_type, 2);
-        const long long cm = G.idx(i, map_bc(G.bc[1], js - 1, ny), k), c0 = G.idx(i, js, k);
-        const long long c1 = G.idx(i, map_bc(G.bc[1], js + 1, ny), k), d0 = G.idx(i, map_bc(G.bc[1], jsp - 1, ny), k);
-        const long long d1 = G.idx(i, jsp, k), dp = G.idx(i, map_bc(G.bc[1], jsp + 1, ny), k);
+        const int jend = mn(L.je, ny);
         for (int v = IR; v <= IP; v++) {
-            HL a0 = hl_at(G, U, v, c0);
-            const HL a1 = hl_at(G, U, v, d1);
-            const float s0 = slope_hl(ist, hl_at(G, U, v, cm), a0, hl_at(G, U, v, c1));
-            const float s1 = slope_hl(ist, hl_at(G, U, v, d0), a1, hl_at(G, U, v, dp));
-            const float inc = hl_diff(a1, a0) * w + (s0 - s1) * q;
-            add_hl(a0.h, a0.l, inc);
-            Un.hi[G.sv * v + c] = a0.h;
-            Un.lo[G.sv * v + c] = a0.l;
+            auto A = [&](int jj) { return hl_at(G, U, v, G.idx(i, jj, k)); };
+            int js = fargo_src(f, L.jb, ny);
+            int jsp = next_row(js, ny);
+            HL w0 = A(js - 1 < 1 ? js - 1 + ny : js - 1), w1 = A(js), w2 = A(jsp), w3 = A(next_row(jsp, ny));
+            float s0 = slope_hl(ist, w0, w1, w2), s1 = slope_hl(ist, w1, w2, w3);
+            for (int j = L.jb; j <= jend; j++) {
+                if (j > L.jb) {  // slide by one row
+                    js = jsp;
+                    jsp = next_row(js, ny);
+                    w1 = w2;
+                    w2 = w3;
+                    w3 = A(next_row(jsp, ny));
+                    s0 = s1;
+                    s1 = slope_hl(ist, w1, w2, w3);
+                }
+                HL a0 = w1;
+                add_hl(a0.h, a0.l, hl_diff(w2, w1) * w + (s0 - s1) * q);
+                const long long c = G.idx(i, j, k);
+                Un.hi[G.sv * v + c] = a0.h;
+                Un.lo[G.sv * v + c] = a0.l;
+            }
         }
     }
     const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
     auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, jj, kk)); };
     auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, jj, kk)) : 0.0f; };
-    if (j <= ny && k <= nz) apply(U, Un, G, IA, c, (EZ(i, j + 1, k) - EZ(i, j, k)) * rdy);
-    if (i <= nx && k <= nz)
-        apply(U, Un, G, IB, c, -(EZ(i + 1, j, k) - EZ(i, j, k)) * rdx + (EX(i, j, k + 1) - EX(i, j, k)) * rdz);
-    if (i <= nx && j <= ny) apply(U, Un, G, IC, c, -(EX(i, j + 1, k) - EX(i, j, k)) * rdy);
+    for (int j = L.jb; j <= L.je; j++) {
+        const long long c = G.idx(i, j, k);
+        if (j <= ny && k <= nz) apply(U, Un, G, IA, c, (EZ(i, j + 1, k) - EZ(i, j, k)) * rdy);
+        if (i <= nx && k <= nz)
+            apply(U, Un, G, IB, c, -(EZ(i + 1, j, k) - EZ(i, j, k)) * rdx + (EX(i, j, k + 1) - EX(i, j, k)) * rdz);
+        if (i <= nx && j <= ny) apply(U, Un, G, IC, c, -(EX(i, j + 1, k) - EX(i, j, k)) * rdy);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -797,7 +797,7 @@ int launch_harvest(const Geo &G, const Bufs &B, int d, int stride, float *xs, fl
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     float *fex = (float *)B.femf[0], *fez = (float *)B.femf[1];
     TIMED(KS_FARGO_EMF, s, (k_fargo_emf_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), fex, fez, B.S)));
-    TIMED(KS_FARGO_UPDATE, s, (k_fargo_update_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), fex, fez, B.S)));
+    TIMED(KS_FARGO_UPDATE, s, (k_fargo_update_hl<<<nblocks(fargo_line_threads(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), fex, fez, B.S)));
     return 2;
 }
 

@@ -1189,55 +1189,95 @@ __global__ void __launch_bounds__(kThreads) k_fargo_emf(Geo G, Store U, double *
     }
 }
 
-// remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119)
+// FARGO line layout: one thread per (i, k) face column and per segment of kFargoSeg faces
+// along y; consecutive threads take consecutive i (coalesced), and a thread slides a
+// window of source values along its segment so each source value is read once
+constexpr int kFargoSeg = 32;
+__host__ __device__ __forceinline__ long long fargo_line_threads(const Geo &G) {
+    return (long long)G.FX * G.FZ * ((G.FY + kFargoSeg - 1) / kFargoSeg);
+}
+struct FargoLine {
+    int i, k, jb, je;  // face column and the segment [jb, je] of y faces
+};
+__device__ __forceinline__ bool fargo_line(const Geo &G, long long t, FargoLine &L) {
+    const int nseg = (G.FY + kFargoSeg - 1) / kFargoSeg;
+    L.i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    L.k = (int)(r % G.FZ) + 1;
+    const long long sg = r / G.FZ;
+    if (sg >= nseg) return false;
+    L.jb = (int)sg * kFargoSeg + 1;
+    L.je = mn(L.jb + kFargoSeg - 1, G.FY);
+    return true;
+}
+// donor row js of row j for the column's shift, fargo.f90:63-77
+__device__ __forceinline__ int fargo_src(const FargoShift &f, int j, int ny) {
+    int js;
+    if (f.vK > 0.0) {
+        js = j - f.nshft - 1;
+        if (js < 1) js = js + ny;
+    } else {
+        js = j + f.nshft;
+        if (js > ny) js = js - ny;
+    }
+    return wrap1(js, ny);
+}
+__device__ __forceinline__ int next_row(int j, int ny) { return j + 1 > ny ? j + 1 - ny : j + 1; }
+
+// remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119).
+// Per row: val = a(js) eps + a(jsp) (1-eps) (or mirrored) + the two slope terms, with
+// slope(js) = limit(a(js-1), a(js), a(jsp)) and slope(jsp) = limit(a(js), a(jsp), a(jsp+1))
+// (periodic y, the only y boundary FARGO runs with); the row after shares slope(jsp).
 template <class Store>
 __global__ void __launch_bounds__(kThreads) k_fargo_update(Geo G, Store U, Store Un, const double *__restrict__ fex,
                                                            const double *__restrict__ fez, const Scalars *S) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    FargoLine L;
+    if (!fargo_line(G, blockIdx.x * (long long)blockDim.x + threadIdx.x, L)) return;
+    const int i = L.i, k = L.k;
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const double dt = S->dt, half = 0.5, forth = 0.25, one = 1.0;
-    const long long c = G.idx(i, j, k);
-    if (i <= nx && j <= ny && k <= nz) {
+    if (i <= nx && k <= nz && L.jb <= ny) {
         const FargoShift f = fargo_shift(G, G.xc(i), dt);
-        int js, jsp;
-        if (f.vK > 0.0) {
-            js = j - f.nshft - 1;
-            if (js < 1) js = js + ny;
-            jsp = js + 1;
-            if (jsp > ny) jsp = jsp - ny;
-        } else {
-            js = j + f.nshft;
-            if (js > ny) js = js - ny;
-            jsp = js + 1;
-            if (jsp > ny) jsp = jsp - ny;
-        }
-        js = wrap1(js, ny);
-        jsp = wrap1(jsp, ny);
         const double hme = half - f.eps;
+        const int jend = mn(L.je, ny);
+        const int st = mn(G.slope_type, 2);
         for (int v = IR; v <= IP; v++) {
-            const double a0 = U.getr(G, v, G.idx(i, js, k)), a1 = U.getr(G, v, G.idx(i, jsp, k));
-            double val = (f.vK > 0.0) ? a0 * f.eps + a1 * (one - f.eps) : a0 * (one - f.eps) + a1 * f.eps;
-            val = val + half * fslope(G, U, v, i, js, k) * (forth - hme * hme)
-                      + half * fslope(G, U, v, i, jsp, k) * (hme * hme - forth);
-            Un.set(G, v, c, val);
+            auto A = [&](int jj) { return U.getr(G, v, G.idx(i, jj, k)); };
+            auto lim = [&](double m, double c, double p) { return st == 0 ? 0.0 : limit1<double>((double)st, m, c, p); };
+            int js = fargo_src(f, L.jb, ny);
+            int jsp = next_row(js, ny);
+            double w0 = A(js - 1 < 1 ? js - 1 + ny : js - 1), w1 = A(js), w2 = A(jsp), w3 = A(next_row(jsp, ny));
+            double s0 = lim(w0, w1, w2), s1 = lim(w1, w2, w3);
+            for (int j = L.jb; j <= jend; j++) {
+                if (j > L.jb) {  // slide by one row
+                    js = jsp;
+                    jsp = next_row(js, ny);
+                    w1 = w2;
+                    w2 = w3;
+                    w3 = A(next_row(jsp, ny));
+                    s0 = s1;
+                    s1 = lim(w1, w2, w3);
+                }
+                double val = (f.vK > 0.0) ? w1 * f.eps + w2 * (one - f.eps) : w1 * (one - f.eps) + w2 * f.eps;
+                val = val + half * s0 * (forth - hme * hme) + half * s1 * (hme * hme - forth);
+                Un.set(G, v, G.idx(i, j, k), val);
+            }
         }
     }
     const double dx = G.dx, dy = G.dy, dz = G.dz;
     auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, jj, kk)); };
     auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, jj, kk)) : 0.0; };
-    if (j <= ny && k <= nz) {
-        Un.set(G, IA, c, U.getr(G, IA, c) + (EZ(i, j + 1, k) - EZ(i, j, k)) / dy);
-    }
-    if (i <= nx && k <= nz) {
-        Un.set(G, IB, c, U.getr(G, IB, c) - (EZ(i + 1, j, k) - EZ(i, j, k)) / dx + (EX(i, j, k + 1) - EX(i, j, k)) / dz);
-    }
-    if (i <= nx && j <= ny) {
-        Un.set(G, IC, c, U.getr(G, IC, c) - (EX(i, j + 1, k) - EX(i, j, k)) / dy);
+    for (int j = L.jb; j <= L.je; j++) {
+        const long long c = G.idx(i, j, k);
+        if (j <= ny && k <= nz) {
+            Un.set(G, IA, c, U.getr(G, IA, c) + (EZ(i, j + 1, k) - EZ(i, j, k)) / dy);
+        }
+        if (i <= nx && k <= nz) {
+            Un.set(G, IB, c, U.getr(G, IB, c) - (EZ(i + 1, j, k) - EZ(i, j, k)) / dx + (EX(i, j, k + 1) - EX(i, j, k)) / dz);
+        }
+        if (i <= nx && j <= ny) {
+            Un.set(G, IC, c, U.getr(G, IC, c) - (EX(i, j + 1, k) - EX(i, j, k)) / dy);
+        }
     }
 }
 
