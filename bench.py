@@ -329,7 +329,7 @@ def main() -> None:
 
     precisions = ["fp64", "fp32", "fp32nn"] if args.precision == "both" else [args.precision]
     head = precisions[-1]
-    res = {pr: measure(pr, with_e2e=(pr != "fp64")) for pr in precisions}
+    res = {pr: measure(pr, with_e2e=(pr != "fp64" or len(precisions) == 1)) for pr in precisions}
 
     if dist is not None:
         dist.barrier()
