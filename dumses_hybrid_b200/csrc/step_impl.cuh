@@ -395,7 +395,22 @@ __device__ __forceinline__ T face_slope(const QV<T> &a, int c, int dir, int i, i
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? 3 : 4))
+// resident blocks of 128 threads per SM that the trace and Riemann kernels are compiled
+// for (register caps 128/80 for the trace, 128/64 for the Riemann kernel, FP64/FP32),
+// chosen by timing the variants at 256^3
+#ifndef DG_TRACE_MINB64
+#define DG_TRACE_MINB64 4
+#endif
+#ifndef DG_TRACE_MINB32
+#define DG_TRACE_MINB32 6
+#endif
+#ifndef DG_RIEMANN_MINB64
+#define DG_RIEMANN_MINB64 4
+#endif
+#ifndef DG_RIEMANN_MINB32
+#define DG_RIEMANN_MINB32 8
+#endif
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_TRACE_MINB64 : DG_TRACE_MINB32))
 k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
           const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -847,7 +862,7 @@ __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long l
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 4) k_riemann3d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 : DG_RIEMANN_MINB32)) k_riemann3d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                            T *__restrict__ fy, T *__restrict__ fz, T *__restrict__ ex,
                                                            T *__restrict__ ey, T *__restrict__ ez, const Scalars *S,
                                                            int faces) {
