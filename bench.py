@@ -149,6 +149,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def replica_barrier(dist, cuda: bool = True) -> None:
+    """All ranks (independent replicas) meet before and after a timed region."""
+    if dist is not None:
+        dist.barrier()
+    if cuda:
+        import torch
+        torch.cuda.synchronize()
+
+
+def replica_max(x: float, dist, device: str = "cuda") -> float:
+    """The largest value of x over the ranks (a timed region ends when its slowest replica does)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_baseline(steps: int, warmup: int, n: int = 128, kind: str = "ot") -> dict:
     """The CPU restatement (oracle) on all host cores, n^3 sample of the workload."""
     sys.path.insert(0, str(ROOT / "tests"))
@@ -240,16 +259,10 @@ def main() -> None:
         pass
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replica_barrier(dist, cuda=True)
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(x, dist, device="cuda")
 
     ncell = args.n ** 3
 
