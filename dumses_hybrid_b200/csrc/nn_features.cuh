@@ -164,15 +164,6 @@ __device__ __forceinline__ float gelu_d(float z) {
     const float t = tanhf(kGeluC * (z + kGeluA * z * z * z));
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * z * z);
 }
-// the same with the hardware tanh approximation (PTX tanh.approx.f32), for inference
-__device__ __forceinline__ float tanh_approx(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float gelu_fast(float z) {
-    return 0.5f * z * (1.0f + tanh_approx(kGeluC * (z + kGeluA * z * z * z)));
-}
 // two GELUs packed as BF16x2 (low half = a), evaluated in BF16x2 arithmetic with the
 // PTX tanh.approx.bf16x2: the results are BF16 activations, so BF16 accuracy suffices
 __device__ __forceinline__ uint32_t gelu2_bf16(float a, float b) {

@@ -8,9 +8,7 @@
 // reference, whose face solver is always exact (src/modules/solvers/solver.f90:163-187).
 #include <algorithm>
 #include <cmath>
-#include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -420,11 +418,7 @@ struct dg_nn {
 };
 
 namespace {
-thread_local std::string g_nn_err;
-int nn_fail(int code, const std::string &m) {
-    g_nn_err = m;
-    return dg::set_error(code, m.c_str());
-}
+int nn_fail(int code, const std::string &m) { return dg::set_error(code, m.c_str()); }
 #define NN_CUDA(x)                                                                                       \
     do {                                                                                                 \
         cudaError_t e_ = (x);                                                                            \
@@ -911,4 +905,3 @@ int dg_nn_device(const dg_nn *n) { return n ? n->device : -1; }
 float *dg_nn_sample_x(dg_nn *n) { return n->xs; }
 float *dg_nn_sample_t(dg_nn *n) { return n->ts; }
 void dg_nn_set_count(dg_nn *n, long long c) { n->ns = c; }
-long long dg_nn_capacity(const dg_nn *n) { return n->cap; }

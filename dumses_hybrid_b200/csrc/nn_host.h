@@ -8,4 +8,3 @@ int dg_nn_device(const dg_nn *n);
 float *dg_nn_sample_x(dg_nn *n);
 float *dg_nn_sample_t(dg_nn *n);
 void dg_nn_set_count(dg_nn *n, long long c);
-long long dg_nn_capacity(const dg_nn *n);

@@ -21,7 +21,7 @@ constexpr int kTileRows = 128;               // rows per tcgen05 tile (cta_group
 constexpr unsigned kWaitPolls = 1u << 26;    // upper bound on mbarrier polls (about a second or more)
 
 // error bits written to the network's device error word
-enum { NN_ERR_WAIT = 1, NN_ERR_SHAPE = 2 };
+enum { NN_ERR_WAIT = 1 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
