@@ -560,7 +560,7 @@ int dg_debug_copy(dg_ctx *c, int which, double *host, long long count, long long
     if (!c || !host) return fail(DG_ERR_ARG, "null argument");
     const void *src = nullptr;
     long long n = 0;
-    if (which >= 0 && which <= 2) { src = c->B.flx[which]; n = c->G.fsz * dg::kFluxComp; }
+    if (which >= 0 && which <= 2) { src = c->B.flx[which]; n = c->G.fsz * dg::flux_rec(c->G.ndim); }
     else if (which >= 3 && which <= 5) { src = c->B.emf[which - 3]; n = c->G.fsz; }
     else if (which == 6) { src = c->B.Q; n = c->G.sv * 8; }
     if (!src) return fail(DG_ERR_ARG, "no such array for this context");

@@ -89,8 +89,11 @@ __host__ __device__ __forceinline__ long long core_elems(long long csz, int nf) 
     return (csz + kCoreLane - 1) / kCoreLane * kCoreLane * nf;
 }
 
-// face flux components, stored face-major (8 contiguous values per face): rho, E,
-// rho u, rho v, rho w (scaled by area*dt as compflux does), p*_tot, Bz (2D only), pad
-constexpr int kFluxComp = 8;
+// face flux records, face-major: rho, E, rho u, rho v, rho w (scaled by area*dt as
+// compflux does), p*_tot, then in 2D the B_z flux and a pad (6 values per face in 3D,
+// 8 in 2D)
+constexpr int kFluxComp = 8;  // the larger record (allocation)
+constexpr int kFluxRec3 = 6, kFluxRec2 = 8;
+__host__ __device__ __forceinline__ int flux_rec(int ndim) { return ndim == 3 ? kFluxRec3 : kFluxRec2; }
 
 }  // namespace dg

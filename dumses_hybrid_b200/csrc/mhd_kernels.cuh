@@ -15,7 +15,7 @@ struct Bufs {
     void *U[2];        // state: FP64 path nv double planes; FP32 path 2*nv float planes (hi planes, then lo planes)
     void *Q;           // primitive variables (8 planes) on the ghosted grid
     void *core;        // trace core over the core index space
-    void *flx[3];      // face fluxes per direction, face-major: kFluxComp values per face
+    void *flx[3];      // face fluxes per direction, face-major records (flux_rec(ndim) values per face)
     void *emf[3];      // edge EMFs (x, y, z) over the face index space, already multiplied by dt
     void *E[3];        // edge electric fields of the trace over the edge index space
     double *femf[2];   // FARGO EMFs (x, z), FP64

@@ -73,13 +73,13 @@ __global__ void __launch_bounds__(kThreads) k_update3d_hl(Geo G, StoreHL U, Stor
         const float ds[3] = {(float)(G.dy * G.dz), (float)(G.dx * G.dz), (float)(G.dx * G.dy)};
         float pre[3];
         for (int d = 0; d < 3; d++) {
-            float L[8], R[8];
-            load8(FA[d] + t * kFluxComp, L);
-            load8(FA[d] + FR[d] * kFluxComp, R);
+            float L[6], R[6];
+            load6(FA[d] + t * kFluxRec3, L);
+            load6(FA[d] + FR[d] * kFluxRec3, R);
             float rl = L[0], rr = R[0];
             if (d == 0 && shear) {
-                if (i == 1) rl = shear_avg(G, sr, fx, kFluxComp, 0, j, k);
-                if (i == nx) rr = shear_avg(G, sr, fx, kFluxComp, 1, j, k);
+                if (i == 1) rl = shear_avg(G, sr, fx, kFluxRec3, 0, j, k);
+                if (i == nx) rr = shear_avg(G, sr, fx, kFluxRec3, 1, j, k);
             }
             pre[d] = -(R[5] * ds[d] - L[5] * ds[d]) * dt;
             dr += (rl - rr) * dvloc;
@@ -163,8 +163,8 @@ __global__ void __launch_bounds__(kThreads) k_update2d_hl(Geo G, StoreHL U, Stor
         float pre[2];
         for (int d = 0; d < 2; d++) {
             float L[8], R[8];
-            load8(FA[d] + t * kFluxComp, L);
-            load8(FA[d] + FR[d] * kFluxComp, R);
+            load8(FA[d] + t * kFluxRec2, L);
+            load8(FA[d] + FR[d] * kFluxRec2, R);
             pre[d] = -(R[5] * ds[d] - L[5] * ds[d]) * dt;
             dr += (L[0] - R[0]) * dvloc;
             dw += (L[4] - R[4]) * dvloc;

@@ -54,13 +54,13 @@ __global__ void __launch_bounds__(kThreads) k_update3d(Geo G, const double *__re
         const long long FR[3] = {fxr, fyr, fzr};
         double pre[3];
         for (int d = 0; d < 3; d++) {
-            double L[8], R[8];
-            load8(FA[d] + f0 * kFluxComp, L);
-            load8(FA[d] + FR[d] * kFluxComp, R);
+            double L[6], R[6];
+            load6(FA[d] + f0 * kFluxRec3, L);
+            load6(FA[d] + FR[d] * kFluxRec3, R);
             double rl = L[0], rr = R[0];
             if (d == 0 && shear) {
-                if (i == 1) rl = shear_avg(G, sr, fx, kFluxComp, 0, j, k);
-                if (i == nx) rr = shear_avg(G, sr, fx, kFluxComp, 1, j, k);
+                if (i == 1) rl = shear_avg(G, sr, fx, kFluxRec3, 0, j, k);
+                if (i == nx) rr = shear_avg(G, sr, fx, kFluxRec3, 1, j, k);
             }
             const double ds = (d == 0) ? G.dy * G.dz : (d == 1 ? G.dx * G.dz : G.dx * G.dy);
             pre[d] = -(R[5] * ds - L[5] * ds) * dt;
@@ -152,8 +152,8 @@ __global__ void __launch_bounds__(kThreads) k_update2d(Geo G, const double *__re
         double pre[2];
         for (int d = 0; d < 2; d++) {
             double L[8], R[8];
-            load8(FA[d] + t * kFluxComp, L);
-            load8(FA[d] + FR[d] * kFluxComp, R);
+            load8(FA[d] + t * kFluxRec2, L);
+            load8(FA[d] + FR[d] * kFluxRec2, R);
             const double ds = (d == 0) ? G.dy * G.dz : G.dx * G.dz;
             pre[d] = -(R[5] * ds - L[5] * ds) * dt;
             ur = ur + (L[0] - R[0]) * dvloc;

@@ -61,6 +61,29 @@ __device__ __forceinline__ void store8(double *p, const double v[8]) {
 #pragma unroll
     for (int n = 0; n < 4; n++) ((double2 *)p)[n] = make_double2(v[2 * n], v[2 * n + 1]);
 }
+// 6 contiguous values (a 3D face record) with 8-byte (float) / 16-byte (double) vector accesses
+__device__ __forceinline__ void load6(const float *p, float v[6]) {
+#pragma unroll
+    for (int n = 0; n < 3; n++) {
+        const float2 a = __ldg((const float2 *)p + n);
+        v[2 * n] = a.x; v[2 * n + 1] = a.y;
+    }
+}
+__device__ __forceinline__ void load6(const double *p, double v[6]) {
+#pragma unroll
+    for (int n = 0; n < 3; n++) {
+        const double2 a = __ldg((const double2 *)p + n);
+        v[2 * n] = a.x; v[2 * n + 1] = a.y;
+    }
+}
+__device__ __forceinline__ void store6(float *p, const float v[6]) {
+#pragma unroll
+    for (int n = 0; n < 3; n++) ((float2 *)p)[n] = make_float2(v[2 * n], v[2 * n + 1]);
+}
+__device__ __forceinline__ void store6(double *p, const double v[6]) {
+#pragma unroll
+    for (int n = 0; n < 3; n++) ((double2 *)p)[n] = make_double2(v[2 * n], v[2 * n + 1]);
+}
 
 inline unsigned nblocks(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
@@ -759,9 +782,13 @@ __device__ __forceinline__ void flux_store(const Geo &G, const T *ql, const T *q
     o[2 + lt1 - IU] = f[4] * ds * dt;            // first tangential momentum
     o[2 + lt2 - IU] = f[6] * ds * dt;            // second tangential momentum
     o[5] = pg;                                   // p*_T (zero unless HLLD)
-    o[6] = (G.ndim == 2) ? f[7] * ds * dt : T(0);  // B_t2 = B_z
-    o[7] = T(0);
-    store8(out + fo * kFluxComp, o);
+    if (G.ndim == 3) {
+        store6(out + fo * kFluxRec3, o);
+    } else {
+        o[6] = f[7] * ds * dt;  // B_t2 = B_z
+        o[7] = T(0);
+        store8(out + fo * kFluxRec2, o);
+    }
 }
 
 // one face flux in direction d between cells cl (minus side) and cr (plus side);

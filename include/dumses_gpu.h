@@ -162,8 +162,9 @@ void *dg_stream(dg_ctx *ctx);
 
 /* Test hook: copy one device work array of the last step to the host.
  *   which 0..2  face fluxes of direction x/y/z over faces [1,nx+1]x[1,ny+1]x[1,nz+1],
- *               face-major with 8 values per face: rho, E, rho u, rho v, rho w
- *               (scaled by area*dt as compflux does), p*_T, the 2D B_z flux, 0
+ *               face-major: rho, E, rho u, rho v, rho w (scaled by area*dt as compflux
+ *               does), p*_T (6 values per face in 3D), then in 2D the B_z flux and 0
+ *               (8 values per face)
  *   which 3..5  edge EMFs x/y/z (already multiplied by dt) over the same index space
  *   which 6     primitive variables (8) on the ghosted grid
  * count is the number of doubles the host buffer holds; returns the number of

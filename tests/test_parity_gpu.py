@@ -158,7 +158,7 @@ def test_stage_fluxes_and_emfs():
         assert g.compute_dt() == dt
         g.godunov(dt, 0.0)
         for d in range(3):
-            gf = g.debug_array(d, F * 8).reshape((nz + 1, ny + 1, nx + 1, 8)).transpose(3, 0, 1, 2)
+            gf = g.debug_array(d, F * 6).reshape((nz + 1, ny + 1, nx + 1, 6)).transpose(3, 0, 1, 2)
             hi = [nx + 1 if d == 0 else nx, ny + 1 if d == 1 else ny, nz + 1 if d == 2 else nz]
             for comp, var in ((0, 0), (1, 4), (2, 1), (3, 2), (4, 3)):
                 a = gf[comp, : hi[2], : hi[1], : hi[0]].transpose(2, 1, 0)
