@@ -193,3 +193,47 @@ def test_surrogate_step_with_fallback():
         for v in (0, 4, 5, 6):
             assert l1_rel(a[..., v], a64[..., v]) < 2e-2
         assert abs(hist[8]) < 1e-10
+
+
+def test_surrogate_in_2d():
+    """The learned flux on the 2D field loop (NDIM = 2 face records with the B_z flux):
+    trained on its own interfaces, finite, div B at round-off, close to the FP64 run."""
+    def loop(precision, surrogate=False):
+        return Params(ndim=2, nx=64, ny=32, nz=1, xmin=-1, xmax=1, ymin=-0.5, ymax=0.5, courant=0.7,
+                      precision=precision, surrogate=surrogate)
+    with FluxNet(seed=4) as net:
+        p = loop("fp32")
+        u0 = condinit(p, "field_loop")
+        with Context(p) as g:
+            g.upload(u0)
+            g.boundary(0.0, 0.0)
+            t = 0.0
+            for _ in range(3):
+                t, _ = g.run(5, t)
+                net.harvest(g)
+        net.fit_envelope(0.0)
+        net.fit_scaling()
+        for lr in (1e-3, 3e-4, 1e-4):
+            net.train(300, batch=4096, lr=lr)
+        out = {}
+        for prec, sur in (("fp64", False), ("fp32", True)):
+            q = loop(prec, sur)
+            with Context(q) as g:
+                if sur:
+                    g.attach_surrogate(net)
+                g.upload(u0)
+                g.boundary(0.0, 0.0)
+                g.run(20, 0.0)
+                out[prec] = g.download()
+                if sur:
+                    faces, fallback = g.surrogate_stats()
+        a, b = out["fp32"][3:-3, 3:-3, 0], out["fp64"][3:-3, 3:-3, 0]
+        assert faces == 20 * (65 * 32 + 64 * 33) and fallback < faces
+        assert np.isfinite(a[..., :8]).all()
+        errs = [l1_rel(a[..., v], b[..., v]) for v in (0, 4, 5, 6)]
+        print("2D loop, faces", faces, "fallback", fallback, "L1 rel rho E Bx By", ["%.2e" % e for e in errs])
+        assert max(errs) < 2e-2
+        bx, by = out["fp32"][..., 5], out["fp32"][..., 6]
+        divb = (bx[4:-2, 3:-3, 0] - bx[3:-3, 3:-3, 0]) + (by[3:-3, 4:-2, 0] - by[3:-3, 3:-3, 0])
+        # CT keeps div B at the round-off of the FP32 increments (about 1e-8 of |B| per face difference)
+        assert np.max(np.abs(divb)) < 1e-6 * max(np.max(np.abs(bx)), 1e-30)

@@ -192,3 +192,24 @@ def test_history_sums_match_oracle():
     for q in (0, 1, 2, 3, 4, 5, 6, 7):
         assert abs(h_g[q] - h_o[q]) <= 1e-12 * scale[q] + 1e-18, (q, h_g[q], h_o[q])
     assert abs(h_g[8]) < 1e-9 and abs(h_o[8]) < 1e-9
+
+
+def test_field_loop_full_run_to_t2():
+    """The 2D field-loop configuration as specified (128x64 on [-1,1]x[-0.5,0.5], HLLD + CT, MC, CFL 0.7,
+    v = (2, 1), A_z = 1e-3 (0.3 - r)) run to t = 2: every step's dt and the final state bit-identical."""
+    p = Params(ndim=2, nx=128, ny=64, nz=1, xmin=-1, xmax=1, ymin=-0.5, ymax=0.5, courant=0.7)
+    u0 = condinit(p, "field_loop")
+    o = Oracle(p)
+    o.set_state(u0)
+    o.boundary(0.0, 0.0)
+    t_o, n = 0.0, 0
+    while t_o < 2.0:
+        t_o, _ = o.step(t_o)
+        n += 1
+    with Context(p) as g:
+        g.upload(u0)
+        g.boundary(0.0, 0.0)
+        t_g, _ = g.run(n, 0.0)
+        ug = g.download()
+    assert t_g == t_o and n > 100
+    compare_states(ug, o.uin, p)
