@@ -538,7 +538,8 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     const double dt = S->dt;
     unsigned ph = 0;
     unsigned long long nface = 0, nfall = 0;
-    for (long long tile = (long long)kNWG * blockIdx.x + wg; tile * 128 < G.fsz && *flag;
+    const bool weights_ok = *flag != 0;  // set before the block-wide barrier above
+    for (long long tile = (long long)kNWG * blockIdx.x + wg; weights_ok && tile * 128 < G.fsz;
          tile += (long long)kNWG * gridDim.x) {
         const long long t = tile * 128 + wt;
         int i = 0, j = 0, k = 1;
@@ -576,50 +577,56 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         nn::fence_async_smem();
         nn::tc_fence_before();  // this warpgroup's TMEM reads of the previous tile come before the next MMA
         wg_sync(wg);
+        if (!*flag) break;  // read right after a barrier, so the whole warpgroup agrees
         float y[nn::kOut];
+        bool tile_ok = true;
         for (int l = 0; l < 4; l++) {
             if (wt == 0) {
                 nn::tc_fence_after();
                 nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W[l], l == 3 ? nn::kOutPad : nn::kHid, l == 0 ? 2 : 8, 0);
                 nn::mma_commit(mbar);
-                if (!nn::mbar_wait(mbar, ph & 1)) {
-                    nn::mbar_wait(mbar, ph & 1);
-                    *flag = 0;
-                }
             }
+            // every thread observes the MMA's completion itself; the warp agrees on the outcome
+            bool ok = nn::mbar_wait(mbar, ph & 1);
+            if (!ok) {
+                nn::mbar_wait(mbar, ph & 1);  // let the MMA finish before this warp moves on
+                *flag = 0;
+            }
+            ok = __all_sync(0xffffffffu, ok);
+            tile_ok = tile_ok && ok;
             ph++;
-            nn::tc_fence_before();
-            wg_sync(wg);
             nn::tc_fence_after();
-            if (!*flag) break;
             if (l < 3) {
-                for (int cc = 0; cc < nn::kHid / 16; cc++) {
-                    float v[16];
-                    nn::tmem_ld16(taddr + cc * 16, v);
+                if (ok) {
+                    for (int cc = 0; cc < nn::kHid / 32; cc++) {
+                        float v[32];
+                        nn::tmem_ld32(taddr + cc * 32, v);
 #pragma unroll
-                    for (int hh = 0; hh < 2; hh++) {
-                        uint32_t h[4];
+                        for (int hh = 0; hh < 4; hh++) {
+                            uint32_t h[4];
 #pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            const int c0 = cc * 16 + hh * 8 + 2 * q;
-                            h[q] = nn::gelu2_bf16(v[hh * 8 + 2 * q] + bias[l * nn::kHid + c0],
-                                                  v[hh * 8 + 2 * q + 1] + bias[l * nn::kHid + c0 + 1]);
+                            for (int q = 0; q < 4; q++) {
+                                const int c0 = cc * 32 + hh * 8 + 2 * q;
+                                h[q] = nn::gelu2_bf16(v[hh * 8 + 2 * q] + bias[l * nn::kHid + c0],
+                                                      v[hh * 8 + 2 * q + 1] + bias[l * nn::kHid + c0 + 1]);
+                            }
+                            *(uint4 *)(Hs + ((cc * 4 + hh) * 128 + wt) * 8) = make_uint4(h[0], h[1], h[2], h[3]);
                         }
-                        *(uint4 *)(Hs + ((cc * 2 + hh) * 128 + wt) * 8) = make_uint4(h[0], h[1], h[2], h[3]);
                     }
                 }
                 nn::fence_async_smem();
                 nn::tc_fence_before();
-                wg_sync(wg);
+                wg_sync(wg);  // the next layer's MMA reads every warp's activations
                 nn::tc_fence_after();
-            } else {
+                if (!*flag) break;
+            } else if (ok) {
                 float v[16];
                 nn::tmem_ld16(taddr, v);
 #pragma unroll
                 for (int q = 0; q < nn::kOut; q++) y[q] = (v[q] + bias[3 * nn::kHid + q]) * nv.sc.ysd[q];
             }
         }
-        if (!*flag) break;
+        if (!tile_ok || !*flag) valid = false;  // a failed tile writes nothing (the error word reports it)
         if (valid) {
             bool acc = use;
             float F[nn::kOut], dn[nn::kOut];
