@@ -89,6 +89,8 @@ struct dg_ctx {
     double *h_hist = nullptr;       // pinned read-back of history sums
     size_t bytes = 0;
     EventTimer *timer = nullptr;    // non-null while per-kernel profiling is on
+    long long version = 0;          // bumped by every call that changes the device state
+    long long q_version = -1;       // state version whose primitive variables the FP32 CFL pass left in Q
     dg_nn *nn = nullptr;            // attached flux network (surrogate = 1)
     dg::nn::NetView view{};         // its device view, as of dg_attach_surrogate
 };
@@ -384,6 +386,7 @@ int dg_upload(dg_ctx *c, const double *uin) {
         int rc = check_launch();
         if (rc) return rc;
     }
+    c->version++;
     return bounded_sync(c->stream);
 }
 
@@ -413,6 +416,7 @@ int dg_compute_dt(dg_ctx *c, double *dt) {
     TimerScope ts_(c);
     if (!c || !dt) return fail(DG_ERR_ARG, "null argument");
     c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
+    if (c->p.precision == DG_PREC_FP32) c->q_version = c->version;
     int rc = check_launch();
     if (rc) return rc;
     if ((rc = read_scalars(c))) return rc;
@@ -425,8 +429,10 @@ int dg_godunov(dg_ctx *c, double dt, double time) {
     if (!c) return fail(DG_ERR_ARG, "null context");
     if (!(dt > 0) || !std::isfinite(dt)) return fail(DG_ERR_DT, "dt must be positive and finite");
     c->launches += c->L->set_scalars(c->B, dt, time, 1, 1, c->stream);
+    c->B.q_fresh = (c->q_version == c->version);
     c->launches += c->L->godunov(c->G, c->B, c->cur, c->stream);
     c->cur ^= 1;
+    c->version++;
     return check_launch();
 }
 
@@ -437,6 +443,7 @@ int dg_fargo_update(dg_ctx *c, double dt) {
     c->launches += c->L->set_scalars(c->B, dt, 0.0, 1, 0, c->stream);
     c->launches += c->L->fargo(c->G, c->B, c->cur, c->stream);
     c->cur ^= 1;
+    c->version++;
     return check_launch();
 }
 
@@ -445,6 +452,7 @@ int dg_boundary(dg_ctx *c, double time, double dt) {
     if (!c) return fail(DG_ERR_ARG, "null context");
     c->launches += c->L->set_scalars(c->B, dt, time, 1, 1, c->stream);
     c->launches += c->L->boundary(c->G, c->B, c->cur, c->stream);
+    c->version++;
     return check_launch();
 }
 
@@ -455,6 +463,7 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
     c->launches += c->L->set_scalars(c->B, 0.0, *time, 0, 1, c->stream);
     for (int n = 0; n < nsteps; n++) {
         c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
+        c->B.q_fresh = (c->p.precision == DG_PREC_FP32);
         c->launches += c->L->godunov(c->G, c->B, c->cur, c->stream);
         c->cur ^= 1;
         if (c->p.fargo) {
@@ -462,6 +471,7 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
             c->cur ^= 1;
         }
         c->launches += c->L->boundary(c->G, c->B, c->cur, c->stream);
+        c->version++;
         c->launches += c->L->advance_time(c->B, c->stream);
     }
     int rc = check_launch();
@@ -543,6 +553,7 @@ int dg_nn_harvest(dg_ctx *c, dg_nn *nn, int stride, long long *added) {
     int rc = dg_nn_reserve_samples(nn, first + total);
     if (rc) return rc;
     c->launches += dg::f32::launch_trace_only(G, c->B, c->cur, c->stream);
+    c->q_version = -1;  // Q now holds the kicked primitive variables
     long long at = first;
     for (int d = 0; d < G.ndim; d++) {
         c->launches += dg::f32::launch_harvest(G, c->B, d, stride, dg_nn_sample_x(nn), dg_nn_sample_t(nn), at, cnt[d],

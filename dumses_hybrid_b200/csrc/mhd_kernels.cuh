@@ -25,6 +25,8 @@ struct Bufs {
     Scalars *S;        // device scalars
     int nv;            // state variables: 8, or 9 with ndim = 2 (frozen right z-face)
     long long sv;      // cells per plane
+    int q_fresh;       // FP32 path: Q holds the primitive variables (without the rotation half-kick)
+                       // of U[cur], written by the last launch_dt with no state change since
     // learned face flux (FP32 path with surrogate = 1)
     const nn::NetView *net;         // attached network (host copy of its device view), null: HLLD everywhere
     int *fb_list[3];                // per direction: faces sent back to HLLD in the current step

@@ -295,6 +295,74 @@ __global__ void __launch_bounds__(kThreads) k_dt_hl(Geo G, StoreHL U, Scalars *S
     }
 }
 
+// compute_dt fused with the primitive variables of the next godunov: one pass over the
+// ghosted grid writes Q without the rotation half-kick (prim_hl) and reduces the CFL time
+// step over the active cells as k_dt_hl does; k_kick adds the half-kick once dt is known
+__global__ void __launch_bounds__(kThreads) k_prim_dt_hl(Geo G, StoreHL U, float *__restrict__ Q, Scalars *S) {
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    const long long n = (long long)ni * nj * nk;
+    const float gamma = (float)G.gamma;
+    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
+    const float vsh = ((G.omega0 > 0.0) && !G.fargo) ? (float)(1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5) : 0.0f;
+    float best = __int_as_float(0x7f800000);  // +inf
+    int bad = 0;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < n) {
+        const int i = (int)(t % ni) - 2;
+        const long long r = t / ni;
+        const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
+        const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+        const long long c = G.idx(i, j, k);
+        float q[8];
+        prim_hl(G, U, c, q);
+#pragma unroll
+        for (int v = 0; v < 8; v++) Q[G.sv * v + c] = q[v];
+        if (i >= 1 && i <= G.nx && j >= 1 && j <= G.ny && k >= 1 && k <= G.nz) {
+            const float ir = 1.0f / q[IR];
+            float sum = 0.0f;
+            if (G.nx != 1) sum += (cfast_r(gamma, q[IP], ir, q[IA], q[IB], q[IC]) + fabsf(q[IU])) * rdx;
+            if (G.ny != 1) sum += (cfast_r(gamma, q[IP], ir, q[IB], q[IC], q[IA]) + fabsf(q[IV]) + vsh) * rdy;
+            if (G.ndim == 3 && G.nz != 1) sum += (cfast_r(gamma, q[IP], ir, q[IC], q[IA], q[IB]) + fabsf(q[IW])) * rdz;
+            const float cdt = 1.0f / sum;
+            if (!(cdt > 0.0f)) bad = 1;  // NaN or non-positive
+            else best = fminf(best, cdt);
+        }
+    }
+    unsigned long long b = (unsigned long long)__double_as_longlong((double)best);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+        b = ob < b ? ob : b;
+    }
+    __shared__ unsigned long long sb[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = b;
+    if (bad) S->err = DG_ERR_STATE;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long m = sb[0];
+        for (int w = 1; w < kThreads / 32; w++) m = sb[w] < m ? sb[w] : m;
+        // one block per 128 cells: skip the atomic when the running minimum is already smaller
+        if (m < *(volatile unsigned long long *)&S->red) atomicMin(&S->red, m);
+    }
+}
+
+// rotation half-kick (scheme.f90:78-85) on the primitive velocities of the ghosted grid
+__global__ void __launch_bounds__(kThreads) k_kick(Geo G, float *__restrict__ Q, const Scalars *S) {
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    const long long n = (long long)ni * nj * nk;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int i = (int)(t % ni) - 2;
+    const long long r = t / ni;
+    const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
+    const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+    const long long c = G.idx(i, j, k);
+    const float om = (float)G.omega0, hdt = 0.5f * (float)S->dt;
+    const float u = Q[G.sv * IU + c], v = Q[G.sv * IV + c];
+    const float dvx = 2.0f * om * v, dvy = -(0.5f * om * u);
+    Q[G.sv * IU + c] = u + dvx * hdt;
+    Q[G.sv * IV + c] = v + dvy * hdt;
+}
+
 // ---------------------------------------------------------------------------
 // FARGO (fargo.f90:17-288) on the compensated state: the shift of each x column is
 // computed in FP64 exactly as in the FP64 path; the remapped value is written as the
@@ -713,10 +781,9 @@ int launch_advance_time(const Bufs &B, cudaStream_t s) {
 
 int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     TIMED(KS_DT, s, (k_dt_reset<<<1, 1, 0, s>>>(G, B.S)));
-    const long long n = (long long)G.nx * G.ny * G.nz;
-    long long nb = (n + kThreads - 1) / kThreads;
-    if (nb > 148 * 16) nb = 148 * 16;
-    TIMED(KS_DT, s, (k_dt_hl<<<(unsigned)nb, kThreads, 0, s>>>(G, st(B, cur), B.S)));
+    // the primitive variables of godunov come out of the same pass (Q without the half-kick)
+    const long long ng = (long long)(G.nx + 5) * ((G.ndim > 1) ? G.ny + 5 : 1) * ((G.ndim == 3) ? G.nz + 5 : 1);
+    TIMED(KS_DT, s, (k_prim_dt_hl<<<nblocks(ng, kThreads), kThreads, 0, s>>>(G, st(B, cur), (float *)B.Q, B.S)));
     TIMED(KS_DT, s, (k_dt_final<<<1, 1, 0, s>>>(G, B.S)));
     return 3;
 }
@@ -728,9 +795,15 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     float *fx = (float *)B.flx[0], *fy = (float *)B.flx[1], *fz = (float *)B.flx[2];
     float *ex = (float *)B.emf[0], *ey = (float *)B.emf[1], *ez = (float *)B.emf[2];
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
-    TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    int n = (G.shearing ? 1 : 0) + 4;
+    if (!B.q_fresh) {
+        TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+        n++;
+    } else if (G.omega0 > 0.0) {  // Q of this state from launch_dt: add the rotation half-kick
+        TIMED(KS_PRIM, s, (k_kick<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, Q, B.S)));
+        n++;
+    }
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
-    int n = 1 + (G.shearing ? 1 : 0) + 4;
     int faces = 1;
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));

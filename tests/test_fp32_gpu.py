@@ -85,3 +85,32 @@ def test_fp32_divergence_free():
            + (bz[3:-3, 3:-3, 4:-2] - bz[3:-3, 3:-3, 3:-3])) / dx
     bmax = np.max(np.abs(u[..., 5:8]))
     assert np.max(np.abs(div)) * dx / bmax < 1e-6
+
+
+def test_fp32_fused_primitives_match_separate_pass():
+    """The FP32 CFL pass leaves the primitive variables in place for godunov (the rotation
+    half-kick added once dt is known); a godunov whose state changed since (here by an extra
+    boundary call) recomputes them in one pass.  Both give the same bits as the device loop."""
+    p = Params(ndim=3, iso=1, nx=16, ny=32, nz=16, xmin=-0.25, xmax=0.25, ymin=-0.5, ymax=0.5, zmin=-0.25,
+               zmax=0.25, ciso=1.0, omega0=1.0, courant=0.8, bdtypex="shearingbox", fargo=True, precision="fp32")
+    u0 = condinit(p, "mri", beta=1000.0, amp=0.1, seed=5)
+    out = []
+    for mode in ("run", "calls", "calls_recompute"):
+        with Context(p) as g:
+            g.upload(u0)
+            g.boundary(0.0, 0.0)
+            t = 0.0
+            if mode == "run":
+                t, _ = g.run(6, t)
+            else:
+                for _ in range(6):
+                    dt = g.compute_dt()
+                    if mode == "calls_recompute":
+                        g.boundary(t, dt)  # a state change after compute_dt: godunov recomputes Q
+                    g.godunov(dt, t)
+                    g.fargo_update(dt)
+                    g.boundary(t, dt)
+                    t = t + dt
+            out.append(g.download())
+    assert np.array_equal(out[0][..., :8], out[1][..., :8])
+    assert np.array_equal(out[0][..., :8], out[2][..., :8])
