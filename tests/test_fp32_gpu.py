@@ -99,17 +99,18 @@ def test_fp32_fused_primitives_match_separate_pass():
         with Context(p) as g:
             g.upload(u0)
             g.boundary(0.0, 0.0)
-            t = 0.0
+            t, last = 0.0, (0.0, 0.0)
             if mode == "run":
                 t, _ = g.run(6, t)
             else:
                 for _ in range(6):
                     dt = g.compute_dt()
                     if mode == "calls_recompute":
-                        g.boundary(t, dt)  # a state change after compute_dt: godunov recomputes Q
+                        g.boundary(*last)  # the same ghost fill again: a state change, so godunov recomputes Q
                     g.godunov(dt, t)
                     g.fargo_update(dt)
                     g.boundary(t, dt)
+                    last = (t, dt)
                     t = t + dt
             out.append(g.download())
     assert np.array_equal(out[0][..., :8], out[1][..., :8])
