@@ -386,60 +386,55 @@ __device__ __forceinline__ float slope_hl(int ist, HL m, HL c, HL p) {
     const float dlim = (dlft * drgt <= 0.0f) ? 0.0f : fminf(fabsf(dlft), fabsf(drgt));
     return copysignf(fminf(dlim, fabsf(dcen)), dcen);
 }
-// uin_slope of variable v at (i, j, k) with y wrap
-__device__ __forceinline__ float fslope_hl(const Geo &G, const StoreHL &U, int v, int i, int j, int k) {
-    auto at = [&](int jj) { return hl_at(G, U, v, G.idx(i, map_bc(G.bc[1], jj, G.ny), k)); };
-    return slope_hl(mn(G.slope_type, 2), at(j - 1), at(j), at(j + 1));
-}
-
-// emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1
+// emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1,
+// along y lines as the FP64 kernel does (shift once per column, sliding donor window)
 __global__ void __launch_bounds__(kThreads) k_fargo_emf_hl(Geo G, StoreHL U, float *__restrict__ fex,
                                                            float *__restrict__ fez, const Scalars *S) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    FargoLine L;
+    if (!fargo_line(G, blockIdx.x * (long long)blockDim.x + threadIdx.x, L)) return;
+    const int i = L.i, k = L.k;
     const double dt = S->dt;
     const float dy = (float)G.dy;
-    const int ny = G.ny;
+    const int ny = G.ny, ist = mn(G.slope_type, 2);
     const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
-    auto B = [&](int v, int jj) {
-        const HL b = hl_at(G, U, v, G.idx(i, jj, kw));
-        return b.h + b.l;
-    };
-    // sum over the shifted-through cells and the fractional donor (get_emfx / get_emfz)
-    auto emf = [&](int v, const FargoShift &f) {
+    // the sum over the shifted-through cells and the fractional donor (get_emfx / get_emfz)
+    auto line = [&](int v, float sgn, const FargoShift &f, float *out) {
+        auto A = [&](int jj) { return hl_at(G, U, v, G.idx(i, jj, kw)); };
         const float eps = (float)f.eps;
-        float e = 0.0f;
-        if (f.vK > 0.0) {
-            const float lambda = 0.5f * eps * (1.0f - eps);
-            for (int jj = 1; jj <= f.nshft; jj++) {
-                int js = j - jj;
-                if (js < 1) js = js + ny;
-                e += B(v, wrap1(js, ny)) * dy;
+        int js = fargo_src(f, L.jb, ny);
+        HL w0 = A(js - 1 < 1 ? js - 1 + ny : js - 1), w1 = A(js), w2 = A(next_row(js, ny));
+        for (int j = L.jb; j <= L.je; j++) {
+            if (j > L.jb) {  // slide by one row
+                js = next_row(js, ny);
+                w0 = w1;
+                w1 = w2;
+                w2 = A(next_row(js, ny));
             }
-            int js = j - f.nshft - 1;
-            if (js < 1) js = js + ny;
-            js = wrap1(js, ny);
-            e += (eps * B(v, js) + lambda * fslope_hl(G, U, v, i, js, kw)) * dy;
-        } else {
-            const float lambda = 0.5f * eps * (eps - 1.0f);
-            for (int jj = 0; jj <= f.nshft - 1; jj++) {
-                int js = j + jj;
-                if (js > ny) js = js - ny;
-                e -= B(v, wrap1(js, ny)) * dy;
+            float e = 0.0f;
+            if (f.vK > 0.0) {
+                const float lambda = 0.5f * eps * (1.0f - eps);
+                for (int jj = 1; jj <= f.nshft; jj++) {
+                    int jr = j - jj;
+                    if (jr < 1) jr = jr + ny;
+                    const HL b = A(wrap1(jr, ny));
+                    e += (b.h + b.l) * dy;
+                }
+                e += (eps * (w1.h + w1.l) + lambda * slope_hl(ist, w0, w1, w2)) * dy;
+            } else {
+                const float lambda = 0.5f * eps * (eps - 1.0f);
+                for (int jj = 0; jj <= f.nshft - 1; jj++) {
+                    int jr = j + jj;
+                    if (jr > ny) jr = jr - ny;
+                    const HL b = A(wrap1(jr, ny));
+                    e -= (b.h + b.l) * dy;
+                }
+                e += (-eps * (w1.h + w1.l) - lambda * slope_hl(ist, w0, w1, w2)) * dy;
             }
-            int js = j + f.nshft;
-            if (js > ny) js = js - ny;
-            js = wrap1(js, ny);
-            e += (-eps * B(v, js) - lambda * fslope_hl(G, U, v, i, js, kw)) * dy;
+            out[G.fidx(i, j, k)] = sgn * e;
         }
-        return e;
     };
-    if (i <= G.nx) fex[t] = emf(IC, fargo_shift(G, G.xc(i), dt));                        // fargo.f90:146-177
-    if (k <= G.nz) fez[t] = -emf(IA, fargo_shift(G, 0.5 * (G.xc(i) + G.xc(i - 1)), dt));  // fargo.f90:204-235
+    if (i <= G.nx) line(IC, 1.0f, fargo_shift(G, G.xc(i), dt), fex);                         // fargo.f90:146-177
+    if (k <= G.nz) line(IA, -1.0f, fargo_shift(G, 0.5 * (G.xc(i) + G.xc(i - 1)), dt), fez);  // fargo.f90:204-235
 }
 
 // remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119), along
@@ -876,7 +871,7 @@ int launch_harvest(const Geo &G, const Bufs &B, int d, int stride, float *xs, fl
 
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     float *fex = (float *)B.femf[0], *fez = (float *)B.femf[1];
-    TIMED(KS_FARGO_EMF, s, (k_fargo_emf_hl<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), fex, fez, B.S)));
+    TIMED(KS_FARGO_EMF, s, (k_fargo_emf_hl<<<nblocks(fargo_line_threads(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), fex, fez, B.S)));
     TIMED(KS_FARGO_UPDATE, s, (k_fargo_update_hl<<<nblocks(fargo_line_threads(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), fex, fez, B.S)));
     return 2;
 }

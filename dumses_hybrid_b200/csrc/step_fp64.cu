@@ -249,7 +249,7 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
 }
 
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
-    TIMED(KS_FARGO_EMF, s, (k_fargo_emf<StoreD><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, st(B, cur), B.femf[0], B.femf[1], B.S)));
+    TIMED(KS_FARGO_EMF, s, (k_fargo_emf<StoreD><<<nblocks(fargo_line_threads(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), B.femf[0], B.femf[1], B.S)));
     TIMED(KS_FARGO_UPDATE, s, (k_fargo_update<StoreD><<<nblocks(fargo_line_threads(G), kThreads), kThreads, 0, s>>>(G, st(B, cur), st(B, cur ^ 1), B.femf[0], B.femf[1], B.S)));
     return 2;
 }

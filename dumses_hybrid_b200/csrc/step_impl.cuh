@@ -1155,82 +1155,6 @@ __device__ __forceinline__ double fslope(const Geo &G, const Store &U, int v, in
     return limit1<double>((double)st, val(j - 1), val(j), val(j + 1));
 }
 
-// emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1
-template <class Store>
-__global__ void __launch_bounds__(kThreads) k_fargo_emf(Geo G, Store U, double *__restrict__ fex,
-                                                        double *__restrict__ fez, const Scalars *S) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
-    const double dt = S->dt, dy = G.dy, half = 0.5, one = 1.0;
-    const int ny = G.ny;
-    const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
-    auto B = [&](int v, int ii, int jj) { return U.getr(G, v, G.idx(ii, jj, kw)); };
-    if (i <= G.nx) {  // get_emfx, fargo.f90:146-177
-        const FargoShift f = fargo_shift(G, G.xc(i), dt);
-        double e = 0.0;
-        if (f.vK > 0.0) {
-            const double lambda = half * f.eps * (one - f.eps);
-            for (int jj = 1; jj <= f.nshft; jj++) {
-                int js = j - jj;
-                if (js < 1) js = js + ny;
-                e = e + B(IC, i, wrap1(js, ny)) * dy;
-            }
-            int js = j - f.nshft - 1;
-            if (js < 1) js = js + ny;
-            js = wrap1(js, ny);
-            const double demf = f.eps * B(IC, i, js) + lambda * fslope(G, U, IC, i, js, kw);
-            e = e + demf * dy;
-        } else {
-            const double lambda = half * f.eps * (f.eps - one);
-            for (int jj = 0; jj <= f.nshft - 1; jj++) {
-                int js = j + jj;
-                if (js > ny) js = js - ny;
-                e = e - B(IC, i, wrap1(js, ny)) * dy;
-            }
-            int js = j + f.nshft;
-            if (js > ny) js = js - ny;
-            js = wrap1(js, ny);
-            const double demf = -f.eps * B(IC, i, js) - lambda * fslope(G, U, IC, i, js, kw);
-            e = e + demf * dy;
-        }
-        fex[t] = e;
-    }
-    if (k <= G.nz) {  // get_emfz, fargo.f90:204-235
-        const FargoShift f = fargo_shift(G, half * (G.xc(i) + G.xc(i - 1)), dt);
-        double e = 0.0;
-        if (f.vK > 0.0) {
-            const double lambda = half * f.eps * (one - f.eps);
-            for (int jj = 1; jj <= f.nshft; jj++) {
-                int js = j - jj;
-                if (js < 1) js = js + ny;
-                e = e - B(IA, i, wrap1(js, ny)) * dy;
-            }
-            int js = j - f.nshft - 1;
-            if (js < 1) js = js + ny;
-            js = wrap1(js, ny);
-            const double demf = f.eps * B(IA, i, js) + lambda * fslope(G, U, IA, i, js, kw);
-            e = e - demf * dy;
-        } else {
-            const double lambda = half * f.eps * (f.eps - one);
-            for (int jj = 0; jj <= f.nshft - 1; jj++) {
-                int js = j + jj;
-                if (js > ny) js = js - ny;
-                e = e + B(IA, i, wrap1(js, ny)) * dy;
-            }
-            int js = j + f.nshft;
-            if (js > ny) js = js - ny;
-            js = wrap1(js, ny);
-            const double demf = -f.eps * B(IA, i, js) - lambda * fslope(G, U, IA, i, js, kw);
-            e = e - demf * dy;
-        }
-        fez[t] = e;
-    }
-}
-
 // FARGO line layout: one thread per (i, k) face column and per segment of kFargoSeg faces
 // along y; consecutive threads take consecutive i (coalesced), and a thread slides a
 // window of source values along its segment so each source value is read once
@@ -1265,6 +1189,58 @@ __device__ __forceinline__ int fargo_src(const FargoShift &f, int j, int ny) {
     return wrap1(js, ny);
 }
 __device__ __forceinline__ int next_row(int j, int ny) { return j + 1 > ny ? j + 1 - ny : j + 1; }
+
+// emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1,
+// along y lines (fargo_line): per column the shift is computed once and the donor field and
+// its two neighbours (for uin_slope) slide along the segment
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_fargo_emf(Geo G, Store U, double *__restrict__ fex,
+                                                        double *__restrict__ fez, const Scalars *S) {
+    FargoLine L;
+    if (!fargo_line(G, blockIdx.x * (long long)blockDim.x + threadIdx.x, L)) return;
+    const int i = L.i, k = L.k;
+    const double dt = S->dt, dy = G.dy, half = 0.5, one = 1.0;
+    const int ny = G.ny, st = mn(G.slope_type, 2);
+    const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
+    auto lim = [&](double m, double c, double p) { return st == 0 ? 0.0 : limit1<double>((double)st, m, c, p); };
+    // one component: get_emfx (v = IC, sign +1, fargo.f90:146-177) or get_emfz (v = IA, sign -1, :204-235)
+    auto line = [&](int v, double sgn, const FargoShift &f, double *out) {
+        auto B = [&](int jj) { return U.getr(G, v, G.idx(i, jj, kw)); };
+        int js = fargo_src(f, L.jb, ny);
+        double w0 = B(js - 1 < 1 ? js - 1 + ny : js - 1), w1 = B(js), w2 = B(next_row(js, ny));
+        for (int j = L.jb; j <= L.je; j++) {
+            if (j > L.jb) {  // slide by one row
+                js = next_row(js, ny);
+                w0 = w1;
+                w1 = w2;
+                w2 = B(next_row(js, ny));
+            }
+            double e = 0.0;
+            if (f.vK > 0.0) {
+                const double lambda = half * f.eps * (one - f.eps);
+                for (int jj = 1; jj <= f.nshft; jj++) {
+                    int jr = j - jj;
+                    if (jr < 1) jr = jr + ny;
+                    e = sgn > 0.0 ? e + B(wrap1(jr, ny)) * dy : e - B(wrap1(jr, ny)) * dy;
+                }
+                const double demf = f.eps * w1 + lambda * lim(w0, w1, w2);
+                e = sgn > 0.0 ? e + demf * dy : e - demf * dy;
+            } else {
+                const double lambda = half * f.eps * (f.eps - one);
+                for (int jj = 0; jj <= f.nshft - 1; jj++) {
+                    int jr = j + jj;
+                    if (jr > ny) jr = jr - ny;
+                    e = sgn > 0.0 ? e - B(wrap1(jr, ny)) * dy : e + B(wrap1(jr, ny)) * dy;
+                }
+                const double demf = -f.eps * w1 - lambda * lim(w0, w1, w2);
+                e = sgn > 0.0 ? e + demf * dy : e - demf * dy;
+            }
+            out[G.fidx(i, j, k)] = e;
+        }
+    };
+    if (i <= G.nx) line(IC, 1.0, fargo_shift(G, G.xc(i), dt), fex);
+    if (k <= G.nz) line(IA, -1.0, fargo_shift(G, half * (G.xc(i) + G.xc(i - 1)), dt), fez);
+}
 
 // remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119).
 // Per row: val = a(js) eps + a(jsp) (1-eps) (or mirrored) + the two slope terms, with
