@@ -10,7 +10,16 @@ namespace {
 
 // update + constrained_transport of the FP64 state (scheme.f90:1764-1993), in the
 // reference's statement order
-__global__ void __launch_bounds__(kThreads) k_update3d(Geo G, const double *__restrict__ U, double *__restrict__ Un,
+// 8 resident blocks (64 registers), chosen by timing at 256^3
+#ifndef DG_UPDATE_MINB64
+#define DG_UPDATE_MINB64 8
+#endif
+#if DG_UPDATE_MINB64 > 0
+__global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB64) k_update3d(
+#else
+__global__ void __launch_bounds__(kThreads) k_update3d(
+#endif
+    Geo G, const double *__restrict__ U, double *__restrict__ Un,
                                                        const double *__restrict__ fx, const double *__restrict__ fy,
                                                        const double *__restrict__ fz, const double *__restrict__ ex,
                                                        const double *__restrict__ ey, const double *__restrict__ ez,

@@ -1158,7 +1158,10 @@ __device__ __forceinline__ double fslope(const Geo &G, const Store &U, int v, in
 // FARGO line layout: one thread per (i, k) face column and per segment of kFargoSeg faces
 // along y; consecutive threads take consecutive i (coalesced), and a thread slides a
 // window of source values along its segment so each source value is read once
-constexpr int kFargoSeg = 32;
+#ifndef DG_FARGO_SEG
+#define DG_FARGO_SEG 16
+#endif
+constexpr int kFargoSeg = DG_FARGO_SEG;
 __host__ __device__ __forceinline__ long long fargo_line_threads(const Geo &G) {
     return (long long)G.FX * G.FZ * ((G.FY + kFargoSeg - 1) / kFargoSeg);
 }
