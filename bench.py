@@ -371,10 +371,21 @@ def main() -> None:
             src = "measured (sustained)" if tpeak else "fallback"
             tpeak = tpeak or 1400.0
             achieved = flops / per_launch_s / 1e12
-            return {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": tpeak, "unit": "TFLOP/s",
-                    "frac": achieved / tpeak, "traffic": None, "peak_source": src,
-                    "algorithmic_flops_per_launch": flops,
-                    "note": "one launch per face direction; 2 x 35968 flops per face (17-128-128-128-8 MLP)"}
+            out = {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": tpeak, "unit": "TFLOP/s",
+                   "frac": achieved / tpeak, "traffic": None, "peak_source": src,
+                   "algorithmic_flops_per_launch": flops,
+                   "note": "one launch per face direction; 2 x 35968 flops per face (17-128-128-128-8 MLP)"}
+            upath = ROOT / "profiles" / "pipe_util_mri128.json"
+            if upath.exists():
+                try:
+                    util = json.loads(upath.read_text()).get("fp32nn", {}).get(dom)
+                    if util:
+                        out["binding"] = {"pipe": "xu", "pipe_frac": util["xu"], "tensor_frac": util["tensor"],
+                                          "issue_frac": util["issue"],
+                                          "source": "profiles/pipe_util_mri128.json (ncu, 128^3)"}
+                except Exception:
+                    pass
+            return out
         achieved = ALGO_BYTES_PER_ZONE * ncell / per_launch_s / 1e9
         traffic = None
         tpath = ROOT / "profiles" / f"ncu_traffic_{args.workload}{args.n}_{precision}.json"
@@ -384,10 +395,22 @@ def main() -> None:
             except Exception:
                 traffic = None
         step = ALGO_BYTES_PER_ZONE * ncell * args.steps / (r["ms"] / 1e3) / 1e9 / world
-        return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_ZONE * ncell, "step_achieved": step,
-                "step_frac": step / hbm_peak}
+        out = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+               "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
+               "algorithmic_bytes_per_launch": ALGO_BYTES_PER_ZONE * ncell, "step_achieved": step,
+               "step_frac": step / hbm_peak}
+        # the pipe that binds the dominant kernel, from the committed ncu summary of the same kernel
+        upath = ROOT / "profiles" / "pipe_util_mri128.json"
+        if upath.exists():
+            try:
+                util = json.loads(upath.read_text()).get(precision, {}).get(dom)
+                if util:
+                    pipe = max(("fp64", "fma", "alu", "xu", "tensor"), key=lambda p: util[p])
+                    out["binding"] = {"pipe": pipe, "pipe_frac": util[pipe], "issue_frac": util["issue"],
+                                      "dram_frac": util["dram"], "source": "profiles/pipe_util_mri128.json (ncu, 128^3)"}
+            except Exception:
+                pass
+        return out
 
     arith = {"fp64": "fp64 (bit-exact)",
              "fp32": "fp32 trace/Riemann/CT, compensated fp32 hi/lo state, fp64 gas pressure/dt minimum/diagnostics",
