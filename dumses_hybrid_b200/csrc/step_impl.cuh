@@ -254,7 +254,9 @@ __device__ __forceinline__ T limit1(T st, T qm1, T q0, T qp1) {
     const T half = T(0.5);
     T dlft = st * (q0 - qm1);
     T drgt = st * (qp1 - q0);
-    T dcen = half * (dlft + drgt) / st;
+    T dcen;
+    if constexpr (sizeof(T) == 4) dcen = (dlft + drgt) * (half / st);  // FP32: one shared reciprocal
+    else dcen = half * (dlft + drgt) / st;
     T dsgn = sgn1(dcen);
     T slop = mn(fab(dlft), fab(drgt));
     T dlim = slop;
