@@ -34,6 +34,13 @@ __device__ __forceinline__ void apply(const StoreHL &U, const StoreHL &Un, const
     Un.hi[G.sv * v + c] = h;
     Un.lo[G.sv * v + c] = l;
 }
+// the same on a pair loaded beforehand: a kernel loads every pair it updates before its
+// first store, since the compiler cannot move a load of U across a store to Un
+__device__ __forceinline__ void put(const StoreHL &Un, const Geo &G, int v, long long c, float h, float l, float inc) {
+    add_hl(h, l, inc);
+    Un.hi[G.sv * v + c] = h;
+    Un.lo[G.sv * v + c] = l;
+}
 
 // update + constrained_transport (scheme.f90:1764-1993) as FP32 increments on the compensated state
 // 12 resident blocks (40 registers): faster than the uncapped allocation at 256^3 despite a few spills
@@ -57,6 +64,13 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
     const bool shear = G.shearing != 0;
     ShearRemap sr{0.0, 0};
     if (shear) sr = ShearRemap{S->sh_epsi, S->sh_jp};  // time + dt/2, from k_shear_offset
+    // the 8 pairs of the cell (c lies inside the ghosted grid for every face cell)
+    float uh[8], ul[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        uh[v] = U.hi[G.sv * v + c];
+        ul[v] = U.lo[G.sv * v + c];
+    }
 
     if (i <= nx && j <= ny && k <= nz) {
         const float dvloc = (float)(1.0 / (G.dx * G.dy * G.dz));
@@ -68,7 +82,7 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
             const double lam = 0.25 * (G.omega0 * dtd) * (G.omega0 * dtd);
             opl = (float)(1.0 + lam);
             const float rm1 = (float)(-2.0 * lam / (1.0 + lam));
-            const float uu = U.hi[G.sv * IU + c], uv = U.hi[G.sv * IV + c];
+            const float uu = uh[IU], uv = uh[IV];
             du += uu * rm1 + 2.f * Om * dt * uv / opl;
             dv += uv * rm1 - 0.5f * Om * dt * uu / opl;
         }
@@ -106,11 +120,11 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
             dv += pre[1] * dvloc;
         }
         dw += pre[2] * dvloc;
-        apply(U, Un, G, IR, c, dr);
-        apply(U, Un, G, IU, c, du);
-        apply(U, Un, G, IV, c, dv);
-        apply(U, Un, G, IW, c, dw);
-        apply(U, Un, G, IP, c, dp);
+        put(Un, G, IR, c, uh[IR], ul[IR], dr);
+        put(Un, G, IU, c, uh[IU], ul[IU], du);
+        put(Un, G, IV, c, uh[IV], ul[IV], dv);
+        put(Un, G, IW, c, uh[IW], ul[IW], dw);
+        put(Un, G, IP, c, uh[IP], ul[IP], dp);
     }
     auto EYc = [&](int ii, int jj, int kk) -> float {
         if (shear && (ii == 1 || ii == nx + 1) && jj <= ny && kk <= nz + 1)
@@ -122,17 +136,17 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
     if (j <= ny && k <= nz) {
         float inc = 0.f;
         if (ct) inc = (ld(ez + G.fidx(i, j + 1, k)) - ld(ez + t)) * rdy - (EYc(i, j, k + 1) - EYc(i, j, k)) * rdz;
-        apply(U, Un, G, IA, c, inc);
+        put(Un, G, IA, c, uh[IA], ul[IA], inc);
     }
     if (i <= nx && k <= nz) {
         float inc = 0.f;
         if (ct) inc = -(ld(ez + G.fidx(i + 1, j, k)) - ld(ez + t)) * rdx + (ld(ex + G.fidx(i, j, k + 1)) - ld(ex + t)) * rdz;
-        apply(U, Un, G, IB, c, inc);
+        put(Un, G, IB, c, uh[IB], ul[IB], inc);
     }
     if (i <= nx && j <= ny) {
         float inc = 0.f;
         if (ct) inc = (EYc(i + 1, j, k) - EYc(i, j, k)) * rdx - (ld(ex + G.fidx(i, j + 1, k)) - ld(ex + t)) * rdy;
-        apply(U, Un, G, IC, c, inc);
+        put(Un, G, IC, c, uh[IC], ul[IC], inc);
     }
 }
 
@@ -349,17 +363,12 @@ __global__ void __launch_bounds__(kThreads) k_prim_dt_hl(Geo G, StoreHL U, float
     }
 }
 
-// rotation half-kick (scheme.f90:78-85) on the primitive velocities of the ghosted grid
+// rotation half-kick (scheme.f90:78-85) on the primitive velocities of the ghosted grid:
+// one thread per element of the velocity planes, the never-read outer ghost layer included,
+// so no cell index is decomposed
 __global__ void __launch_bounds__(kThreads) k_kick(Geo G, float *__restrict__ Q, const Scalars *S) {
-    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
-    const long long n = (long long)ni * nj * nk;
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int i = (int)(t % ni) - 2;
-    const long long r = t / ni;
-    const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
-    const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
-    const long long c = G.idx(i, j, k);
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= G.sv) return;
     const float om = (float)G.omega0, hdt = 0.5f * (float)S->dt;
     const float u = Q[G.sv * IU + c], v = Q[G.sv * IV + c];
     const float dvx = 2.0f * om * v, dvy = -(0.5f * om * u);
@@ -442,9 +451,14 @@ __global__ void __launch_bounds__(kThreads) k_fargo_emf_hl(Geo G, StoreHL U, flo
 }
 
 // remap of rho, rho v, E (fargo.f90:59-93) and CT of the face B (fargo.f90:100-119), along
-// y lines as the FP64 kernel does (one thread per face column and segment, a sliding window
-// of (hi, lo) source values and slopes)
-__global__ void __launch_bounds__(kThreads) k_fargo_update_hl(Geo G, StoreHL U, StoreHL Un,
+// y lines as the FP64 kernel does (one thread per face column and segment). Every value a
+// row needs is loaded before the row's stores: the donor window of a whole segment per
+// variable, and the face B and EMFs of kFargoChunk rows at a time for the CT part.
+// 3 resident blocks (168 registers): the window stays in registers; timed best at 256^3
+#ifndef DG_FARGO_MINB32
+#define DG_FARGO_MINB32 3
+#endif
+__global__ void __launch_bounds__(kThreads, DG_FARGO_MINB32) k_fargo_update_hl(Geo G, StoreHL U, StoreHL Un,
                                                               const float *__restrict__ fex,
                                                               const float *__restrict__ fez, const Scalars *S) {
     FargoLine L;
@@ -458,40 +472,63 @@ __global__ void __launch_bounds__(kThreads) k_fargo_update_hl(Geo G, StoreHL U, 
         const float hme = 0.5f - eps;
         const float q = 0.5f * (0.25f - hme * hme);
         const int ist = mn(G.slope_type, 2);
-        const int jend = mn(L.je, ny);
+        const int js = fargo_src(f, L.jb, ny);
+        const int j0 = js - 1 < 1 ? js - 1 + ny : js - 1;  // the window starts one row below the first donor
         for (int v = IR; v <= IP; v++) {
-            auto A = [&](int jj) { return hl_at(G, U, v, G.idx(i, jj, k)); };
-            int js = fargo_src(f, L.jb, ny);
-            int jsp = next_row(js, ny);
-            HL w0 = A(js - 1 < 1 ? js - 1 + ny : js - 1), w1 = A(js), w2 = A(jsp), w3 = A(next_row(jsp, ny));
-            float s0 = slope_hl(ist, w0, w1, w2), s1 = slope_hl(ist, w1, w2, w3);
-            for (int j = L.jb; j <= jend; j++) {
-                if (j > L.jb) {  // slide by one row
-                    js = jsp;
-                    jsp = next_row(js, ny);
-                    w1 = w2;
-                    w2 = w3;
-                    w3 = A(next_row(jsp, ny));
-                    s0 = s1;
-                    s1 = slope_hl(ist, w1, w2, w3);
-                }
-                HL a0 = w1;
-                add_hl(a0.h, a0.l, hl_diff(w2, w1) * w + (s0 - s1) * q);
+            // rows js-1 .. js+kFargoSeg+1 (periodic y); rows past the segment's end are loaded but unused
+            HL wn[kFargoSeg + 3];
+            int row = j0;
+#pragma unroll
+            for (int m = 0; m < kFargoSeg + 3; m++) {
+                wn[m] = hl_at(G, U, v, G.idx(i, row, k));
+                row = next_row(row, ny);
+            }
+            float s0 = slope_hl(ist, wn[0], wn[1], wn[2]);
+#pragma unroll
+            for (int m = 0; m < kFargoSeg; m++) {
+                const int j = L.jb + m;
+                if (j > L.je || j > ny) break;
+                const float s1 = slope_hl(ist, wn[m + 1], wn[m + 2], wn[m + 3]);
+                HL a0 = wn[m + 1];
+                add_hl(a0.h, a0.l, hl_diff(wn[m + 2], wn[m + 1]) * w + (s0 - s1) * q);
                 const long long c = G.idx(i, j, k);
                 Un.hi[G.sv * v + c] = a0.h;
                 Un.lo[G.sv * v + c] = a0.l;
+                s0 = s1;
             }
         }
     }
     const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
-    auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, jj, kk)); };
-    auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, jj, kk)) : 0.0f; };
-    for (int j = L.jb; j <= L.je; j++) {
-        const long long c = G.idx(i, j, k);
-        if (j <= ny && k <= nz) apply(U, Un, G, IA, c, (EZ(i, j + 1, k) - EZ(i, j, k)) * rdy);
-        if (i <= nx && k <= nz)
-            apply(U, Un, G, IB, c, -(EZ(i + 1, j, k) - EZ(i, j, k)) * rdx + (EX(i, j, k + 1) - EX(i, j, k)) * rdz);
-        if (i <= nx && j <= ny) apply(U, Un, G, IC, c, -(EX(i, j + 1, k) - EX(i, j, k)) * rdy);
+    // face indices clamped into the EMF arrays; a clamped value is never used
+    auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, mn(jj, G.FY), mn(kk, G.FZ))); };
+    auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, mn(jj, G.FY), kk)) : 0.0f; };
+    for (int jb = L.jb; jb <= L.je; jb += kFargoChunk) {
+        HL a[kFargoChunk], b[kFargoChunk], cz[kFargoChunk];
+        float ezj[kFargoChunk + 1], exj[kFargoChunk + 1], ezr[kFargoChunk], exu[kFargoChunk];
+#pragma unroll
+        for (int m = 0; m <= kFargoChunk; m++) {
+            ezj[m] = EZ(i, jb + m, k);
+            exj[m] = EX(i, jb + m, k);
+            if (m < kFargoChunk) {
+                const int j = mn(jb + m, L.je);
+                const long long c = G.idx(i, j, k);
+                a[m] = hl_at(G, U, IA, c);
+                b[m] = hl_at(G, U, IB, c);
+                cz[m] = hl_at(G, U, IC, c);
+                ezr[m] = EZ(i + 1, j, k);
+                exu[m] = EX(i, j, k + 1);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < kFargoChunk; m++) {
+            const int j = jb + m;
+            if (j > L.je) break;
+            const long long c = G.idx(i, j, k);
+            if (j <= ny && k <= nz) put(Un, G, IA, c, a[m].h, a[m].l, (ezj[m + 1] - ezj[m]) * rdy);
+            if (i <= nx && k <= nz)
+                put(Un, G, IB, c, b[m].h, b[m].l, -(ezr[m] - ezj[m]) * rdx + (exu[m] - exj[m]) * rdz);
+            if (i <= nx && j <= ny) put(Un, G, IC, c, cz[m].h, cz[m].l, -(exj[m + 1] - exj[m]) * rdy);
+        }
     }
 }
 
@@ -799,7 +836,7 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         TIMED(KS_PRIM, s, (k_prim_hl<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
         n++;
     } else if (G.omega0 > 0.0) {  // Q of this state from launch_dt: add the rotation half-kick
-        TIMED(KS_PRIM, s, (k_kick<<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, Q, B.S)));
+        TIMED(KS_PRIM, s, (k_kick<<<nblocks(G.sv, kThreads), kThreads, 0, s>>>(G, Q, B.S)));
         n++;
     }
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));

@@ -256,7 +256,9 @@ __device__ __forceinline__ T limit1(T st, T qm1, T q0, T qp1) {
     T drgt = st * (qp1 - q0);
     T dcen;
     if constexpr (sizeof(T) == 4) dcen = (dlft + drgt) * (half / st);  // FP32: one shared reciprocal
-    else dcen = half * (dlft + drgt) / st;
+    // FP64: every caller passes st = 1 or 2, whose reciprocal is exact, so the product rounds
+    // the same real number as the reference's division by st (no FP64 division)
+    else dcen = half * (dlft + drgt) * (st == T(1) ? T(1) : T(0.5));
     T dsgn = sgn1(dcen);
     T slop = mn(fab(dlft), fab(drgt));
     T dlim = slop;
@@ -1004,44 +1006,6 @@ __device__ __forceinline__ int map_bc(int type, int i, int n) {
     return i < 1 ? i + n : i - n;
 }
 
-// the limiter of shearing_slope (shearingbox.f90:415-430), at y index j, FP64
-template <class Store>
-__device__ __forceinline__ double sslope(const Geo &G, const Store &U, int v, int i, int j, int k) {
-    const int st = mn(G.slope_type, 2);
-    if (st == 0) return 0.0;
-    auto val = [&](int jj) { return U.get(G, v, G.idx(i, map_bc(G.bc[1], jj, G.ny), k)); };
-    if (v == IB) return val(j + 1) - val(j);  // By: one-sided difference (shearingbox.f90:493-499)
-    return limit1<double>((double)st, val(j - 1), val(j), val(j + 1));
-}
-
-// shear-periodic x ghost value of variable v at ghost cell i, active (j,k) (shearingbox.f90:62-147)
-template <class Store>
-__device__ double shear_ghost(const Geo &G, const Store &U, const ShearRemap &sr, int v, int i, int j, int k) {
-    const int nx = G.nx, ny = G.ny;
-    const double one = 1.0, half = 0.5;
-    auto val = [&](int ii, int jj) { return U.get(G, v, G.idx(ii, map_bc(G.bc[1], jj, ny), k)); };
-    if (i < 1) {
-        const int src = nx + i;  // outer(1:3) = uin(nx-2:nx) feeds ghosts iu1..iu1+2
-        int jremap = j - sr.jp - 1, jremapp = jremap + 1;
-        if (jremap <= 0) jremap = jremap + ny;
-        if (jremapp <= 0) jremapp = jremapp + ny;
-        const double eps = one - sr.epsi / G.dy;
-        const double lambda = half * eps * (eps - one);
-        if (v == IB) return val(src, jremap) + eps * sslope(G, U, v, src, jremap, k);
-        return (one - eps) * val(src, jremap) + eps * val(src, jremapp)
-             + lambda * (sslope(G, U, v, src, jremap, k) - sslope(G, U, v, src, jremapp, k));
-    }
-    const int src = i - nx;  // inner(1:3) = uin(1:3) feeds ghosts iu2-2..iu2
-    int jremap = j + sr.jp, jremapp = jremap + 1;
-    if (jremap > ny) jremap = jremap - ny;
-    if (jremapp > ny) jremapp = jremapp - ny;
-    const double eps = sr.epsi / G.dy;
-    const double lambda = half * eps * (eps - one);
-    if (v == IB) return val(src, jremap) + eps * sslope(G, U, v, src, jremap, k);
-    return (one - eps) * val(src, jremap) + eps * val(src, jremapp)
-         + lambda * (sslope(G, U, v, src, jremapp, k) - sslope(G, U, v, src, jremap, k));
-}
-
 // number of ghost cells: the z-ghost planes, the y-ghost rows of the active planes and
 // the x-ghost cells of the active rows
 __host__ __device__ __forceinline__ long long ghost_cells(const Geo &G) {
@@ -1051,52 +1015,104 @@ __host__ __device__ __forceinline__ long long ghost_cells(const Geo &G) {
     return nA + nB + nC;
 }
 
+constexpr int kMaxVars = 9;  // stored state variables: 8, plus the frozen right z-face B in 2D
 template <class Store>
 __global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= ghost_cells(G)) return;
-    const long long nA = (G.ndim == 3) ? 6LL * G.NX * G.NY : 0;
-    const long long nB = 6LL * G.NX * (G.ndim == 3 ? G.nz : 1);
+    // the ghost counts of any grid that fits a GPU are far below 2^32: 32-bit index arithmetic
+    const unsigned NX = G.NX, NY = G.NY;
+    const unsigned nA = (G.ndim == 3) ? 6u * NX * NY : 0u;
+    const unsigned nB = 6u * NX * (G.ndim == 3 ? (unsigned)G.nz : 1u);
     auto ghost = [](int g, int n) { return g < 3 ? g - 2 : n + g - 2; };  // 0..5 -> -2,-1,0,n+1,n+2,n+3
     int i, j, k;
-    if (t < nA) {
-        i = (int)(t % G.NX) - 2;
-        const long long r = t / G.NX;
-        j = (int)(r % G.NY) - 2;
-        k = ghost((int)(r / G.NY), G.nz);
-    } else if (t - nA < nB) {
-        const long long u = t - nA;
-        i = (int)(u % G.NX) - 2;
-        const long long r = u / G.NX;
-        j = ghost((int)(r % 6), G.ny);
-        k = (G.ndim == 3) ? (int)(r / 6) + 1 : 1;
+    const unsigned u0 = (unsigned)t;
+    if (u0 < nA) {
+        i = (int)(u0 % NX) - 2;
+        const unsigned r = u0 / NX;
+        j = (int)(r % NY) - 2;
+        k = ghost((int)(r / NY), G.nz);
+    } else if (u0 - nA < nB) {
+        const unsigned u = u0 - nA;
+        i = (int)(u % NX) - 2;
+        const unsigned r = u / NX;
+        j = ghost((int)(r % 6u), G.ny);
+        k = (G.ndim == 3) ? (int)(r / 6u) + 1 : 1;
     } else {
-        const long long u = t - nA - nB;
-        i = ghost((int)(u % 6), G.nx);
-        const long long r = u / 6;
-        j = (int)(r % G.ny) + 1;
-        k = (G.ndim == 3) ? (int)(r / G.ny) + 1 : 1;
+        const unsigned u = u0 - nA - nB;
+        i = ghost((int)(u % 6u), G.nx);
+        const unsigned r = u / 6u;
+        j = (int)(r % (unsigned)G.ny) + 1;
+        k = (G.ndim == 3) ? (int)(r / (unsigned)G.ny) + 1 : 1;
     }
     const bool gx = (i < 1 || i > G.nx);
     const int jj = (G.ndim > 1) ? map_bc(G.bc[1], j, G.ny) : 1;
     const int kk = (G.ndim == 3) ? map_bc(G.bc[2], k, G.nz) : 1;
     const long long c = G.idx(i, j, k);
+    // every value is read (from active cells, or the outer x face that no thread writes)
+    // before the first store, so the loads of all variables are in flight together
+    double out[kMaxVars];
     if (!gx || G.bc[0] != DG_BC_SHEARINGBOX) {
-        const int ii = map_bc(G.bc[0], i, G.nx);
-        const long long src = G.idx(ii, jj, kk);
-        for (int v = 0; v < nv; v++) U.set(G, v, c, U.get(G, v, src));
+        const long long src = G.idx(map_bc(G.bc[0], i, G.nx), jj, kk);
+#pragma unroll
+        for (int v = 0; v < kMaxVars; v++)
+            if (v < nv) out[v] = U.get(G, v, src);
+#pragma unroll
+        for (int v = 0; v < kMaxVars; v++)
+            if (v < nv) U.set(G, v, c, out[v]);
         return;
     }
-    // shear-periodic x ghost (only with ndim = 3); offset for time+dt from k_shear_offset
+    // shear-periodic x ghost (only with ndim = 3; shearingbox.f90:62-147): the remapped rows,
+    // eps and lambda are the same for every variable; offset for time+dt from k_shear_offset
     const ShearRemap sr{S->sh_epsi, S->sh_jp};
-    for (int v = 0; v < nv; v++) {
-        if (v == IA && i == G.nx + 1) {
-            // the outer face keeps its own (CT-updated) value; ghost j/k copy it
-            if (jj != j || kk != k) U.set(G, v, c, U.get(G, v, G.idx(i, jj, kk)));
-            continue;
-        }
-        U.set(G, v, c, shear_ghost(G, U, sr, v, i, jj, kk));
+    const int nx = G.nx, ny = G.ny;
+    const double one = 1.0, half = 0.5;
+    const bool lower = i < 1;
+    const int src = lower ? nx + i : i - nx;  // outer(1:3) = uin(nx-2:nx) / inner(1:3) = uin(1:3)
+    int jr, jrp;
+    double eps;
+    if (lower) {
+        jr = jj - sr.jp - 1;
+        jrp = jr + 1;
+        if (jr <= 0) jr = jr + ny;
+        if (jrp <= 0) jrp = jrp + ny;
+        eps = one - sr.epsi / G.dy;
+    } else {
+        jr = jj + sr.jp;
+        jrp = jr + 1;
+        if (jr > ny) jr = jr - ny;
+        if (jrp > ny) jrp = jrp - ny;
+        eps = sr.epsi / G.dy;
     }
+    const double lambda = half * eps * (eps - one);
+    const int st = mn(G.slope_type, 2);
+    auto row = [&](int r) { return G.idx(src, map_bc(G.bc[1], r, ny), kk); };
+    // rows of the two values and of shearing_slope at each (shearingbox.f90:415-430, 493-499)
+    const long long cm = row(jr - 1), c0 = row(jr), cp = row(jr + 1);
+    const long long dm = row(jrp - 1), d0 = row(jrp), dp = row(jrp + 1);
+    // the outer face keeps its own (CT-updated) value; ghost j/k copy it
+    const bool outer = (i == nx + 1);
+    const bool keep_a = outer && jj == j && kk == k;
+    const long long ca = G.idx(i, jj, kk);
+#pragma unroll
+    for (int v = 0; v < kMaxVars; v++) {
+        if (v >= nv) continue;
+        if (v == IA && outer) {
+            out[v] = U.get(G, v, ca);
+        } else if (v == IB) {  // By: one-sided slope
+            const double a0 = U.get(G, v, c0), a1 = U.get(G, v, cp);
+            out[v] = a0 + eps * (st == 0 ? 0.0 : a1 - a0);
+        } else {
+            const double am = U.get(G, v, cm), a0 = U.get(G, v, c0), ap = U.get(G, v, cp);
+            const double bm = U.get(G, v, dm), b0 = U.get(G, v, d0), bp = U.get(G, v, dp);
+            const double sa = st == 0 ? 0.0 : limit1<double>((double)st, am, a0, ap);
+            const double sb = st == 0 ? 0.0 : limit1<double>((double)st, bm, b0, bp);
+            out[v] = (one - eps) * a0 + eps * b0 + lambda * (lower ? sa - sb : sb - sa);
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < kMaxVars; v++)
+        if (v < nv && !(v == IA && keep_a)) U.set(G, v, c, out[v]);
 }
 
 // right-face B (uin vars 9-11) of the reference layout, from the stored left faces
@@ -1164,6 +1180,7 @@ __device__ __forceinline__ double fslope(const Geo &G, const Store &U, int v, in
 #define DG_FARGO_SEG 16
 #endif
 constexpr int kFargoSeg = DG_FARGO_SEG;
+constexpr int kFargoChunk = 4;  // rows of the CT part whose loads are issued together
 __host__ __device__ __forceinline__ long long fargo_line_threads(const Geo &G) {
     return (long long)G.FX * G.FZ * ((G.FY + kFargoSeg - 1) / kFargoSeg);
 }
@@ -1251,8 +1268,15 @@ __global__ void __launch_bounds__(kThreads) k_fargo_emf(Geo G, Store U, double *
 // Per row: val = a(js) eps + a(jsp) (1-eps) (or mirrored) + the two slope terms, with
 // slope(js) = limit(a(js-1), a(js), a(jsp)) and slope(jsp) = limit(a(js), a(jsp), a(jsp+1))
 // (periodic y, the only y boundary FARGO runs with); the row after shares slope(jsp).
+// Every value a row needs is loaded before the row's stores (the compiler cannot move a
+// load of U across a store to Un): the donor window of the whole segment per variable, and
+// the face B and EMFs of kFargoChunk rows at a time for the CT part.
+// 3 resident blocks (168 registers): the window stays in registers; timed best at 256^3
+#ifndef DG_FARGO_MINB64
+#define DG_FARGO_MINB64 3
+#endif
 template <class Store>
-__global__ void __launch_bounds__(kThreads) k_fargo_update(Geo G, Store U, Store Un, const double *__restrict__ fex,
+__global__ void __launch_bounds__(kThreads, DG_FARGO_MINB64) k_fargo_update(Geo G, Store U, Store Un, const double *__restrict__ fex,
                                                            const double *__restrict__ fez, const Scalars *S) {
     FargoLine L;
     if (!fargo_line(G, blockIdx.x * (long long)blockDim.x + threadIdx.x, L)) return;
@@ -1262,44 +1286,62 @@ __global__ void __launch_bounds__(kThreads) k_fargo_update(Geo G, Store U, Store
     if (i <= nx && k <= nz && L.jb <= ny) {
         const FargoShift f = fargo_shift(G, G.xc(i), dt);
         const double hme = half - f.eps;
-        const int jend = mn(L.je, ny);
         const int st = mn(G.slope_type, 2);
+        auto lim = [&](double m, double c, double p) { return st == 0 ? 0.0 : limit1<double>((double)st, m, c, p); };
+        const int js = fargo_src(f, L.jb, ny);
+        const int j0 = js - 1 < 1 ? js - 1 + ny : js - 1;  // the window starts one row below the first donor
         for (int v = IR; v <= IP; v++) {
-            auto A = [&](int jj) { return U.getr(G, v, G.idx(i, jj, k)); };
-            auto lim = [&](double m, double c, double p) { return st == 0 ? 0.0 : limit1<double>((double)st, m, c, p); };
-            int js = fargo_src(f, L.jb, ny);
-            int jsp = next_row(js, ny);
-            double w0 = A(js - 1 < 1 ? js - 1 + ny : js - 1), w1 = A(js), w2 = A(jsp), w3 = A(next_row(jsp, ny));
-            double s0 = lim(w0, w1, w2), s1 = lim(w1, w2, w3);
-            for (int j = L.jb; j <= jend; j++) {
-                if (j > L.jb) {  // slide by one row
-                    js = jsp;
-                    jsp = next_row(js, ny);
-                    w1 = w2;
-                    w2 = w3;
-                    w3 = A(next_row(jsp, ny));
-                    s0 = s1;
-                    s1 = lim(w1, w2, w3);
-                }
+            // rows js-1 .. js+kFargoSeg+1 (periodic y); rows past the segment's end are loaded but unused
+            double wn[kFargoSeg + 3];
+            int row = j0;
+#pragma unroll
+            for (int m = 0; m < kFargoSeg + 3; m++) {
+                wn[m] = U.getr(G, v, G.idx(i, row, k));
+                row = next_row(row, ny);
+            }
+            double s0 = lim(wn[0], wn[1], wn[2]);
+#pragma unroll
+            for (int m = 0; m < kFargoSeg; m++) {
+                const int j = L.jb + m;
+                if (j > L.je || j > ny) break;
+                const double s1 = lim(wn[m + 1], wn[m + 2], wn[m + 3]);
+                const double w1 = wn[m + 1], w2 = wn[m + 2];
                 double val = (f.vK > 0.0) ? w1 * f.eps + w2 * (one - f.eps) : w1 * (one - f.eps) + w2 * f.eps;
                 val = val + half * s0 * (forth - hme * hme) + half * s1 * (hme * hme - forth);
                 Un.set(G, v, G.idx(i, j, k), val);
+                s0 = s1;
             }
         }
     }
     const double dx = G.dx, dy = G.dy, dz = G.dz;
-    auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, jj, kk)); };
-    auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, jj, kk)) : 0.0; };
-    for (int j = L.jb; j <= L.je; j++) {
-        const long long c = G.idx(i, j, k);
-        if (j <= ny && k <= nz) {
-            Un.set(G, IA, c, U.getr(G, IA, c) + (EZ(i, j + 1, k) - EZ(i, j, k)) / dy);
+    // face indices clamped into the EMF arrays; a clamped value is never used
+    auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, mn(jj, G.FY), mn(kk, G.FZ))); };
+    auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, mn(jj, G.FY), kk)) : 0.0; };
+    for (int jb = L.jb; jb <= L.je; jb += kFargoChunk) {
+        double a[kFargoChunk], b[kFargoChunk], cz[kFargoChunk];
+        double ezj[kFargoChunk + 1], exj[kFargoChunk + 1], ezr[kFargoChunk], exu[kFargoChunk];
+#pragma unroll
+        for (int m = 0; m <= kFargoChunk; m++) {
+            ezj[m] = EZ(i, jb + m, k);
+            exj[m] = EX(i, jb + m, k);
+            if (m < kFargoChunk) {
+                const int j = mn(jb + m, L.je);
+                const long long c = G.idx(i, j, k);
+                a[m] = U.getr(G, IA, c);
+                b[m] = U.getr(G, IB, c);
+                cz[m] = U.getr(G, IC, c);
+                ezr[m] = EZ(i + 1, j, k);
+                exu[m] = EX(i, j, k + 1);
+            }
         }
-        if (i <= nx && k <= nz) {
-            Un.set(G, IB, c, U.getr(G, IB, c) - (EZ(i + 1, j, k) - EZ(i, j, k)) / dx + (EX(i, j, k + 1) - EX(i, j, k)) / dz);
-        }
-        if (i <= nx && j <= ny) {
-            Un.set(G, IC, c, U.getr(G, IC, c) - (EX(i, j + 1, k) - EX(i, j, k)) / dy);
+#pragma unroll
+        for (int m = 0; m < kFargoChunk; m++) {
+            const int j = jb + m;
+            if (j > L.je) break;
+            const long long c = G.idx(i, j, k);
+            if (j <= ny && k <= nz) Un.set(G, IA, c, a[m] + (ezj[m + 1] - ezj[m]) / dy);
+            if (i <= nx && k <= nz) Un.set(G, IB, c, b[m] - (ezr[m] - ezj[m]) / dx + (exu[m] - exj[m]) / dz);
+            if (i <= nx && j <= ny) Un.set(G, IC, c, cz[m] - (exj[m + 1] - exj[m]) / dy);
         }
     }
 }
