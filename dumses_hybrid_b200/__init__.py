@@ -54,6 +54,16 @@ class DgParams(ctypes.Structure):
                 ("device", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
+class DgDumpInfo(ctypes.Structure):
+    """ctypes mirror of ``dg_dump_info`` (include/dumses_gpu.h)."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("nxslice", ctypes.c_int),
+                ("nyslice", ctypes.c_int), ("nzslice", ctypes.c_int), ("time", ctypes.c_double),
+                ("dt", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+                ("xmin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymin", ctypes.c_double),
+                ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("ciso", ctypes.c_double), ("uin_bytes", ctypes.c_longlong)]
+
+
 class DumsesError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
@@ -89,6 +99,11 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_run": (ctypes.c_int, [vp, ctypes.c_int, dp, dp]),
         "dg_step": (ctypes.c_int, [vp, dp, dp]),
         "dg_history": (ctypes.c_int, [vp, dp]),
+        "dg_dump_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(DgDumpInfo)]),
+        "dg_dump_write": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_double]),
+        "dg_dump_read": (ctypes.c_int, [vp, ctypes.c_char_p, dp, dp]),
+        "dg_dump_write_host": (ctypes.c_int, [ctypes.c_char_p, c_p, ctypes.c_double, ctypes.c_double, dp]),
+        "dg_dump_read_host": (ctypes.c_int, [ctypes.c_char_p, c_p, dp, dp, dp]),
         "dg_sync": (ctypes.c_int, [vp]),
         "dg_kernel_launches": (ctypes.c_longlong, [vp]),
         "dg_stream": (vp, [vp]),
@@ -216,6 +231,81 @@ def condinit(params: Params, ic: str, beta: float = 1000.0, amp: float = 0.0, se
     return u
 
 
+def dump_filename(ndump: int, mype: int = 0, base: str | pathlib.Path = ".", make_dir: bool = True) -> pathlib.Path:
+    """Path of dump `ndump` of rank `mype` as the reference names it: get_filename
+    (src/modules/file.f90) gives output_NNNNNN/data.RRRRRR, output.f90:225 adds .bin."""
+    d = pathlib.Path(base) / f"output_{ndump % 1000000:06d}"
+    if make_dir:
+        d.mkdir(parents=True, exist_ok=True)
+    return d / f"data.{mype % 1000000:06d}.bin"
+
+
+def dump_header(path: str | pathlib.Path) -> dict:
+    """Header records of a 'binary' dump (output.f90:228-231) and the byte length of its uin record."""
+    info = DgDumpInfo()
+    _check(load_library().dg_dump_header(str(path).encode(), ctypes.byref(info)))
+    return {name: getattr(info, name) for name, _ in DgDumpInfo._fields_}
+
+
+def write_dump(path: str | pathlib.Path, params: Params, uin: np.ndarray, time: float, dt: float) -> None:
+    """Write a host uin array as a 'binary' dump (output.f90:224-235)."""
+    if uin.shape != params.shape or uin.dtype != np.float64 or not uin.flags.f_contiguous:
+        raise ValueError(f"uin must be a Fortran-ordered float64 array of shape {params.shape}")
+    cp = params.to_c()
+    _check(load_library().dg_dump_write_host(str(path).encode(), ctypes.byref(cp), time, dt,
+                                             uin.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+
+def read_dump(path: str | pathlib.Path, params: Params) -> tuple[np.ndarray, float, float]:
+    """Read a 'binary' dump of the grid of `params` (restart.f90:212-221): (uin, time, dt)."""
+    cp = params.to_c()
+    u = np.zeros(params.shape, dtype=np.float64, order="F")
+    t, dt = ctypes.c_double(), ctypes.c_double()
+    _check(load_library().dg_dump_read_host(str(path).encode(), ctypes.byref(cp), ctypes.byref(t), ctypes.byref(dt),
+                                            u.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return u, t.value, dt.value
+
+
+HISTORY_KEYS = ("time", "dt", "mass", "maxwell", "reynolds", "max+rey", "magp", "meanBx", "meanBy", "meanBz", "divB")
+
+
+def _fortran_1pe(x: float, w: int) -> str:
+    """Fortran edit 1PEw.5: one digit before the point, five after; a three-digit
+    exponent drops the E (d.ddddd+ddd), as the Fortran standard prescribes."""
+    s = f"{x:.5E}"
+    mant, exp = s.split("E")
+    if len(exp) > 3:  # sign + three digits
+        s = mant + exp
+    return s.rjust(w)
+
+
+def history_header() -> str:
+    """Header line of the MRI history file, format ('# ', A11, 1X, A12, 1X, 9(A14,1X))
+    (src/problem/mri/history.f90:152-154)."""
+    k = HISTORY_KEYS
+    return "# " + k[0].rjust(11) + " " + k[1].rjust(12) + " " + "".join(n.rjust(14) + " " for n in k[2:])
+
+
+def history_line(time: float, dt: float, sums: np.ndarray) -> str:
+    """One line of the MRI history file for the sums of :meth:`Context.history`, format
+    (1X, 1PE12.5, 1X, 1PE12.5, 1X, 9(E14.5,1X)) (history.f90:166-168); the scale factor
+    1P carries over to the E14.5 fields."""
+    vals = [float(v) for v in sums]
+    return " " + _fortran_1pe(time, 12) + " " + _fortran_1pe(dt, 12) + " " + "".join(
+        _fortran_1pe(v, 14) + " " for v in vals)
+
+
+def write_history(path: str | pathlib.Path, time: float, dt: float, sums: np.ndarray) -> None:
+    """Append one line to history.txt as the MRI history routine does: a new file (or
+    time = 0) starts with the header line (history.f90:150-164)."""
+    path = pathlib.Path(path)
+    fresh = time == 0.0 or not path.exists()
+    with open(path, "w" if fresh else "a") as f:
+        if fresh:
+            f.write(history_header() + "\n")
+        f.write(history_line(time, dt, sums) + "\n")
+
+
 class Context:
     """One device state of the MHD step (a dg_ctx of the C-ABI)."""
 
@@ -290,6 +380,16 @@ class Context:
 
     def sync(self) -> None:
         _check(self.lib.dg_sync(self.h))
+
+    def dump(self, path: str | pathlib.Path, time: float, dt: float) -> None:
+        """Write the state as a 'binary' dump (output.f90:224-235), streamed from the device."""
+        _check(self.lib.dg_dump_write(self.h, str(path).encode(), time, dt))
+
+    def restart(self, path: str | pathlib.Path) -> tuple[float, float]:
+        """Load a 'binary' dump of this grid (restart.f90:212-221); returns (time, dt)."""
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.dg_dump_read(self.h, str(path).encode(), ctypes.byref(t), ctypes.byref(dt)))
+        return t.value, dt.value
 
     def debug_array(self, which: int, size: int) -> np.ndarray:
         """Copy a device work array of the last step (see dg_debug_copy)."""

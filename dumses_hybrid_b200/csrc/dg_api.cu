@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "dumses_gpu.h"
+#include "dump_io.h"
 #include "mhd_kernels.cuh"
 #include "nn_host.h"
 
@@ -136,6 +137,20 @@ int bounded_sync(cudaStream_t s) {
         cudaError_t e = cudaStreamQuery(s);
         if (e == cudaSuccess) return DG_OK;
         if (e != cudaErrorNotReady) return fail(DG_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) return fail(DG_ERR_TIMEOUT, "device work did not finish within DG_SYNC_TIMEOUT_S");
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
+    }
+}
+
+// wait for an event with the same wall-clock bound
+int bounded_event(cudaEvent_t ev) {
+    const double limit = sync_timeout_s();
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return DG_OK;
+        if (e != cudaErrorNotReady) return fail(DG_ERR_CUDA, std::string("event: ") + cudaGetErrorString(e));
         double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el > limit) return fail(DG_ERR_TIMEOUT, "device work did not finish within DG_SYNC_TIMEOUT_S");
         std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
@@ -402,7 +417,7 @@ int dg_download(dg_ctx *c, double *uin) {
     } else {
         c->launches += c->L->to_f64(c->G, c->B, c->cur, c->B.stage, c->stream);
         DG_CUDA(cudaMemcpyAsync(uin, c->B.stage, nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        DG_CUDA(cudaStreamSynchronize(c->stream));
+        if (int rc = bounded_sync(c->stream)) return rc;
         scratch = c->B.stage;
     }
     c->launches += c->L->right_faces(c->G, c->B, c->cur, scratch, c->stream);
@@ -410,6 +425,222 @@ int dg_download(dg_ctx *c, double *uin) {
     if (rc) return rc;
     DG_CUDA(cudaMemcpyAsync(uin + nt * 8, scratch, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return bounded_sync(c->stream);
+}
+
+// ---------------------------------------------------------------------------
+// Fortran 'binary' dumps (output.f90:224-235, restart.f90:212-221), record layout in dump_io.h
+// ---------------------------------------------------------------------------
+namespace {
+dg::dump::Header make_header(const dg_params &p, double time, double dt) {
+    const dg::Geo G = dg::make_geo(p);
+    dg::dump::Header h{};
+    h.nx = p.nx; h.ny = p.ny; h.nz = p.nz;
+    h.nxslice = h.nyslice = h.nzslice = 1;  // one rank
+    h.time = time; h.dt = dt; h.dx = G.dx; h.dy = G.dy; h.dz = G.dz;
+    h.xmin = p.xmin; h.xmax = p.xmax; h.ymin = p.ymin; h.ymax = p.ymax; h.zmin = p.zmin; h.zmax = p.zmax;
+    h.gamma = p.gamma; h.ciso = p.ciso;
+    return h;
+}
+
+// a dump read into a context (or a host array of its grid) must hold the same grid and constants
+int check_header(const dg::dump::Header &h, const dg_params &p, const char *path) {
+    if (h.nxslice != 1 || h.nyslice != 1 || h.nzslice != 1)
+        return fail(DG_ERR_UNSUPPORTED, std::string(path) + ": a dump of one rank of a decomposed run");
+    if (h.nx != p.nx || h.ny != p.ny || h.nz != p.nz)
+        return fail(DG_ERR_ARG, std::string(path) + ": grid " + std::to_string(h.nx) + "x" + std::to_string(h.ny) +
+                                    "x" + std::to_string(h.nz) + " differs from the context's");
+    const dg::dump::Header e = make_header(p, 0.0, 0.0);
+    const double got[] = {h.dx, h.dy, h.dz, h.xmin, h.xmax, h.ymin, h.ymax, h.zmin, h.zmax, h.gamma, h.ciso};
+    const double want[] = {e.dx, e.dy, e.dz, e.xmin, e.xmax, e.ymin, e.ymax, e.zmin, e.zmax, e.gamma, e.ciso};
+    for (int q = 0; q < 11; q++)
+        if (!(got[q] == want[q]))
+            return fail(DG_ERR_ARG, std::string(path) + ": domain, gamma or ciso differ from the context's");
+    return DG_OK;
+}
+
+struct FileCloser {
+    FILE *f = nullptr;
+    ~FileCloser() { if (f) std::fclose(f); }
+    int close_checked(const char *path) {
+        const int e = std::fclose(f);
+        f = nullptr;
+        return e == 0 ? DG_OK : fail(DG_ERR_ARG, std::string(path) + ": write failed");
+    }
+};
+
+// two pinned host planes and their copy events, for streaming the uin record
+struct PlaneBuffers {
+    double *b[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int init(size_t n) {
+        for (int q = 0; q < 2; q++) {
+            if (cudaMallocHost(&b[q], n * sizeof(double)) != cudaSuccess)
+                return fail(DG_ERR_NOMEM, "cudaMallocHost of a dump plane failed");
+            if (cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming) != cudaSuccess)
+                return fail(DG_ERR_CUDA, "cudaEventCreate failed");
+        }
+        return DG_OK;
+    }
+    ~PlaneBuffers() {
+        for (int q = 0; q < 2; q++) {
+            if (ev[q]) cudaEventDestroy(ev[q]);
+            if (b[q]) cudaFreeHost(b[q]);
+        }
+    }
+};
+}  // namespace
+
+int dg_dump_header(const char *path, dg_dump_info *out) {
+    if (!path || !out) return fail(DG_ERR_ARG, "null argument");
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return fail(DG_ERR_ARG, std::string("cannot open ") + path);
+    dg::dump::Header h;
+    if (!dg::dump::read_header(fc.f, h)) return fail(DG_ERR_ARG, std::string(path) + ": not a dump header");
+    // length of the uin record: walk its subrecord markers
+    long long bytes = 0;
+    for (;;) {
+        int32_t lead, trail;
+        if (std::fread(&lead, 4, 1, fc.f) != 1) return fail(DG_ERR_ARG, std::string(path) + ": no uin record");
+        const long long len = lead < 0 ? -(long long)lead : (long long)lead;
+        if (std::fseek(fc.f, (long)len, SEEK_CUR) != 0 || std::fread(&trail, 4, 1, fc.f) != 1)
+            return fail(DG_ERR_ARG, std::string(path) + ": truncated uin record");
+        bytes += len;
+        if (lead >= 0) break;
+    }
+    out->nx = h.nx; out->ny = h.ny; out->nz = h.nz;
+    out->nxslice = h.nxslice; out->nyslice = h.nyslice; out->nzslice = h.nzslice;
+    out->time = h.time; out->dt = h.dt; out->dx = h.dx; out->dy = h.dy; out->dz = h.dz;
+    out->xmin = h.xmin; out->xmax = h.xmax; out->ymin = h.ymin; out->ymax = h.ymax; out->zmin = h.zmin; out->zmax = h.zmax;
+    out->gamma = h.gamma; out->ciso = h.ciso;
+    out->uin_bytes = bytes;
+    return DG_OK;
+}
+
+int dg_dump_write_host(const char *path, const dg_params *p, double time, double dt, const double *uin) {
+    if (!path || !uin) return fail(DG_ERR_ARG, "null argument");
+    if (int rc = validate(p)) return rc;
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return fail(DG_ERR_ARG, std::string("cannot open ") + path + " for writing");
+    const long long bytes = dg_uin_size(p) * (long long)sizeof(double);
+    if (!dg::dump::write_header(fc.f, make_header(*p, time, dt))) return fail(DG_ERR_ARG, std::string(path) + ": write failed");
+    dg::dump::RecordWriter w(fc.f, bytes);
+    if (!w.write(uin, bytes) || !w.close()) return fail(DG_ERR_ARG, std::string(path) + ": write failed");
+    return fc.close_checked(path);
+}
+
+int dg_dump_read_host(const char *path, const dg_params *p, double *time, double *dt, double *uin) {
+    if (!path || !uin || !time || !dt) return fail(DG_ERR_ARG, "null argument");
+    if (int rc = validate(p)) return rc;
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return fail(DG_ERR_ARG, std::string("cannot open ") + path);
+    dg::dump::Header h;
+    if (!dg::dump::read_header(fc.f, h)) return fail(DG_ERR_ARG, std::string(path) + ": not a dump header");
+    if (int rc = check_header(h, *p, path)) return rc;
+    dg::dump::RecordReader r(fc.f);
+    if (!r.read(uin, dg_uin_size(p) * (long long)sizeof(double)) || !r.close())
+        return fail(DG_ERR_ARG, std::string(path) + ": the uin record does not hold this grid");
+    *time = h.time;
+    *dt = h.dt;
+    return DG_OK;
+}
+
+int dg_dump_write(dg_ctx *c, const char *path, double time, double dt) {
+    if (!c || !path) return fail(DG_ERR_ARG, "null argument");
+    TimerScope ts_(c);
+    DG_CUDA(cudaSetDevice(c->p.device));
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return fail(DG_ERR_ARG, std::string("cannot open ") + path + " for writing");
+    const size_t nt = (size_t)c->G.sv;
+    PlaneBuffers pb;
+    if (int rc = pb.init(nt)) return rc;
+    // device planes of uin vars 1-8: the FP64 state, or its FP64 values in the staging buffer;
+    // vars 9-11 from the right-face kernel into a scratch buffer that is free at this point
+    const double *left;
+    double *scratch;
+    if (c->p.precision == DG_PREC_FP64) {
+        left = (const double *)c->B.U[c->cur];
+        scratch = (double *)c->B.Q;
+    } else {
+        // the staging buffer: its planes 0-2 take vars 9-11 once vars 1-8 are copied out
+        c->launches += c->L->to_f64(c->G, c->B, c->cur, c->B.stage, c->stream);
+        left = c->B.stage;
+        scratch = c->B.stage;
+    }
+    if (int rc = check_launch()) return rc;
+    if (!dg::dump::write_header(fc.f, make_header(c->p, time, dt)))
+        return fail(DG_ERR_ARG, std::string(path) + ": write failed");
+    dg::dump::RecordWriter w(fc.f, (long long)nt * 11 * (long long)sizeof(double));
+    // plane v is copied while plane v-1 is written to the file
+    for (int v = 0; v <= 11; v++) {
+        if (v < 11) {
+            if (v == 8) {
+                // vars 9-11, after the copies of vars 1-8 in stream order
+                c->launches += c->L->right_faces(c->G, c->B, c->cur, scratch, c->stream);
+                if (int rc = check_launch()) return rc;
+            }
+            const double *src = v < 8 ? left + (size_t)v * nt : scratch + (size_t)(v - 8) * nt;
+            DG_CUDA(cudaMemcpyAsync(pb.b[v & 1], src, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            DG_CUDA(cudaEventRecord(pb.ev[v & 1], c->stream));
+        }
+        if (v > 0) {
+            if (int rc = bounded_event(pb.ev[(v - 1) & 1])) return rc;
+            if (!w.write(pb.b[(v - 1) & 1], (long long)(nt * sizeof(double))))
+                return fail(DG_ERR_ARG, std::string(path) + ": write failed");
+        }
+    }
+    if (!w.close()) return fail(DG_ERR_ARG, std::string(path) + ": write failed");
+    if (int rc = bounded_sync(c->stream)) return rc;
+    return fc.close_checked(path);
+}
+
+int dg_dump_read(dg_ctx *c, const char *path, double *time, double *dt) {
+    if (!c || !path || !time || !dt) return fail(DG_ERR_ARG, "null argument");
+    TimerScope ts_(c);
+    DG_CUDA(cudaSetDevice(c->p.device));
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return fail(DG_ERR_ARG, std::string("cannot open ") + path);
+    dg::dump::Header h;
+    if (!dg::dump::read_header(fc.f, h)) return fail(DG_ERR_ARG, std::string(path) + ": not a dump header");
+    if (int rc = check_header(h, c->p, path)) return rc;
+    const size_t nt = (size_t)c->G.sv;
+    PlaneBuffers pb;
+    if (int rc = pb.init(nt)) return rc;
+    if (int rc = bounded_sync(c->stream)) return rc;  // no step may still read the state
+    const bool f64 = c->p.precision == DG_PREC_FP64;
+    dg::dump::RecordReader r(fc.f);
+    // plane v is read from the file while plane v-1 is copied; vars 9-10 (right faces) are
+    // derived from the left faces and skipped; var 11 is stored only in 2D (frozen, both buffers)
+    for (int v = 0; v < 11; v++) {
+        if (v >= 2)
+            if (int rc = bounded_event(pb.ev[v & 1])) return rc;  // the copy of plane v-2 is done
+        if (!r.read(pb.b[v & 1], (long long)(nt * sizeof(double))))
+            return fail(DG_ERR_ARG, std::string(path) + ": the uin record does not hold this grid");
+        double *dst[2] = {nullptr, nullptr};
+        if (v < 8) {
+            dst[0] = f64 ? (double *)c->B.U[c->cur] + (size_t)v * nt : c->B.stage + (size_t)v * nt;
+        } else if (v == 10 && c->nv == 9) {
+            if (f64) {
+                dst[0] = (double *)c->B.U[0] + nt * 8;
+                dst[1] = (double *)c->B.U[1] + nt * 8;
+            } else {
+                dst[0] = c->B.stage + nt * 8;
+            }
+        }
+        for (double *d : dst)
+            if (d) DG_CUDA(cudaMemcpyAsync(d, pb.b[v & 1], nt * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        DG_CUDA(cudaEventRecord(pb.ev[v & 1], c->stream));
+    }
+    if (!r.close()) return fail(DG_ERR_ARG, std::string(path) + ": the uin record does not hold this grid");
+    if (!f64) {
+        c->launches += c->L->from_f64(c->G, c->B, c->cur, c->B.stage, c->nv, c->stream);
+        if (c->nv == 9) c->launches += c->L->from_f64(c->G, c->B, c->cur ^ 1, c->B.stage, c->nv, c->stream);
+        if (int rc = check_launch()) return rc;
+    }
+    c->version++;
+    if (int rc = bounded_sync(c->stream)) return rc;
+    *time = h.time;
+    *dt = h.dt;
+    return DG_OK;
 }
 
 int dg_compute_dt(dg_ctx *c, double *dt) {

@@ -117,6 +117,41 @@ int  dg_run(dg_ctx *ctx, int nsteps, double *time, double *dt);
 /* one step, as dg_run(ctx, 1, ...) */
 int  dg_step(dg_ctx *ctx, double *time, double *dt);
 
+/* Fortran 'binary' dumps: output (src/subroutines/output.f90:224-235, io_type =
+ * 'binary') and restart (src/subroutines/restart.f90:212-221).  The file is an
+ * unformatted sequential file as gfortran writes it (4-byte record markers; a
+ * record over 2147483639 bytes split into subrecords with signed markers):
+ *   record 1  int32  nx, ny, nz, nxslice, nyslice, nzslice   (slices = 1 here)
+ *   record 2  double time, dt, dx, dy, dz
+ *   record 3  double xmin, xmax, ymin, ymax, zmin, zmax
+ *   record 4  double gamma, ciso
+ *   record 5  double uin(iu1:iu2, ju1:ju2, ku1:ku2, 1:11) in the host layout above
+ * The reference names the file output_NNNNNN/data.RRRRRR.bin (get_filename,
+ * src/modules/file.f90); dumpy reads it (utils/dumpy/data/rd_dumses.py). */
+typedef struct dg_dump_info {
+    int       nx, ny, nz, nxslice, nyslice, nzslice;
+    double    time, dt, dx, dy, dz;
+    double    xmin, xmax, ymin, ymax, zmin, zmax;
+    double    gamma, ciso;
+    long long uin_bytes;     /* length of the uin record                               */
+} dg_dump_info;
+
+/* header of a dump, and the length of its uin record (no device needed) */
+int  dg_dump_header(const char *path, dg_dump_info *info);
+/* dump of the context's state, streamed from the device plane by plane through two
+ * pinned buffers (the copy of one plane overlaps the file write of the previous
+ * one); FP32 contexts write hi + lo.  time and dt go to record 2. */
+int  dg_dump_write(dg_ctx *ctx, const char *path, double time, double dt);
+/* restart: the dump must hold the context's grid, domain, gamma and ciso (else
+ * DG_ERR_ARG) and one rank (else DG_ERR_UNSUPPORTED).  Loads the state (the
+ * right-face B of vars 9-10 is derived, as dg_upload does) and returns time and
+ * dt of record 2.  The ghost cells come from the file, as in the reference's
+ * restart (init.f90:114-120 calls no boundary after restart_run). */
+int  dg_dump_read(dg_ctx *ctx, const char *path, double *time, double *dt);
+/* the same two operations on a host uin array of grid p (no device needed) */
+int  dg_dump_write_host(const char *path, const dg_params *p, double time, double dt, const double *uin);
+int  dg_dump_read_host(const char *path, const dg_params *p, double *time, double *dt, double *uin);
+
 /* MRI history sums (src/problem/mri/history.f90:60-125) of the current state:
  * out[0] mass, out[1] maxwell, out[2] reynolds, out[3] maxwell+reynolds,
  * out[4] magp, out[5..7] <B>, out[8] divB.  FP64 sums in a fixed tree order. */
