@@ -12,6 +12,7 @@ driver loop (src/dumses.f90:82-120); the same calls exist here as methods of
     call godunov                       ctx.godunov(dt, time)
     if (fargo) call fargo_update       ctx.fargo_update(dt)
     call boundary                      ctx.boundary(time, dt)
+    call dissipation (nu or eta > 0)   ctx.dissipation(time, dt)
     call history (MRI problem)         ctx.history()
     !$acc update host(uin)             uin = ctx.download()
 
@@ -51,7 +52,8 @@ class DgParams(ctypes.Structure):
                 ("omega0", ctypes.c_double), ("courant", ctypes.c_double), ("slope_type", ctypes.c_int),
                 ("iriemann", ctypes.c_int), ("iriemann2d", ctypes.c_int), ("bc", ctypes.c_int * 3),
                 ("fargo", ctypes.c_int), ("precision", ctypes.c_int), ("surrogate", ctypes.c_int),
-                ("device", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("device", ctypes.c_int), ("nu", ctypes.c_double), ("eta", ctypes.c_double),
+                ("reserved", ctypes.c_int * 6)]
 
 
 class DgDumpInfo(ctypes.Structure):
@@ -97,6 +99,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_fargo_update": (ctypes.c_int, [vp, ctypes.c_double]),
         "dg_boundary": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double]),
         "dg_run": (ctypes.c_int, [vp, ctypes.c_int, dp, dp]),
+        "dg_dissipation": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double]),
         "dg_step": (ctypes.c_int, [vp, dp, dp]),
         "dg_history": (ctypes.c_int, [vp, dp]),
         "dg_dump_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(DgDumpInfo)]),
@@ -174,6 +177,8 @@ class Params:
     precision: str = "fp64"
     surrogate: bool = False
     device: int = 0
+    nu: float = 0.0
+    eta: float = 0.0
 
     def to_c(self) -> DgParams:
         p = DgParams()
@@ -184,6 +189,7 @@ class Params:
         p.iriemann, p.iriemann2d = RIEMANN[self.riemann], RIEMANN[self.riemann2d]
         p.bc[0], p.bc[1], p.bc[2] = BC[self.bdtypex], BC[self.bdtypey], BC[self.bdtypez]
         p.fargo, p.precision, p.surrogate, p.device = int(self.fargo), PREC[self.precision], int(self.surrogate), self.device
+        p.nu, p.eta = self.nu, self.eta
         return p
 
     @property
@@ -207,7 +213,7 @@ def read_namelist(path: str | pathlib.Path, ndim: int = 3, iso: int = 0) -> Para
     for key in ("nx", "ny", "nz", "slope_type"):
         if key in kv:
             setattr(p, key, int(kv[key]))
-    for key in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "gamma", "ciso", "courant"):
+    for key in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "gamma", "ciso", "courant", "nu", "eta"):
         if key in kv:
             setattr(p, key, num(kv[key]))
     if "omega0" in kv:
@@ -368,6 +374,10 @@ class Context:
     def boundary(self, time: float, dt: float) -> None:
         _check(self.lib.dg_boundary(self.h, time, dt))
 
+    def dissipation(self, time: float, dt: float) -> None:
+        """Viscosity and resistivity after boundary (physics.f90:272-664); a no-op when nu = eta = 0."""
+        _check(self.lib.dg_dissipation(self.h, time, dt))
+
     def run(self, nsteps: int, time: float) -> tuple[float, float]:
         t, dt = ctypes.c_double(time), ctypes.c_double(0.0)
         _check(self.lib.dg_run(self.h, nsteps, ctypes.byref(t), ctypes.byref(dt)))
@@ -404,7 +414,7 @@ class Context:
 
     def profile_read(self) -> dict[str, tuple[float, int]]:
         """{kernel slot: (total ms, launches)} since the last read."""
-        n = 14
+        n = 15
         ms = np.zeros(n)
         cnt = (ctypes.c_longlong * n)()
         _check(self.lib.dg_profile_read(self.h, self._ptr(ms), cnt, n))

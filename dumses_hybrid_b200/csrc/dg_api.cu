@@ -46,7 +46,7 @@ struct EventTimer : dg::KernelTimer {
 };
 const char *kSlotNames[dg::KS_COUNT] = {"scalars", "cfl_dt", "primitive", "trace", "riemann_flux_emf", "update_ct",
                                        "fargo_emf", "fargo_update", "boundary", "history", "right_faces", "edge_efield",
-                                       "nn_faces", "nn_fallback"};
+                                       "nn_faces", "nn_fallback", "dissipation"};
 }  // namespace
 
 namespace {
@@ -59,14 +59,15 @@ struct Launches {
     int (*fargo)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*boundary)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*history)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*dissipation)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*right_faces)(const dg::Geo &, const dg::Bufs &, int, double *, cudaStream_t);
     int (*to_f64)(const dg::Geo &, const dg::Bufs &, int, double *, cudaStream_t);
     int (*from_f64)(const dg::Geo &, const dg::Bufs &, int, const double *, int, cudaStream_t);
 };
 #define DG_LAUNCH_TABLE(ns)                                                                                  \
     Launches{ns::launch_set_scalars, ns::launch_advance_time, ns::launch_dt, ns::launch_godunov, ns::launch_fargo, \
-             ns::launch_boundary, ns::launch_history, ns::launch_right_faces, ns::launch_state_to_f64,        \
-             ns::launch_f64_to_state}
+             ns::launch_boundary, ns::launch_history, ns::launch_dissipation, ns::launch_right_faces,        \
+             ns::launch_state_to_f64, ns::launch_f64_to_state}
 const Launches kLaunchF64 = DG_LAUNCH_TABLE(dg::f64);
 const Launches kLaunchF32 = DG_LAUNCH_TABLE(dg::f32);
 }  // namespace
@@ -192,6 +193,7 @@ int validate(const dg_params *p) {
         return fail(DG_ERR_UNSUPPORTED, "FARGO needs ndim = 3 and a periodic y direction");
     if (p->precision != DG_PREC_FP64 && p->precision != DG_PREC_FP32) return fail(DG_ERR_ARG, "unknown precision");
     if (p->surrogate && p->precision != DG_PREC_FP32) return fail(DG_ERR_UNSUPPORTED, "the flux surrogate needs the FP32 path");
+    if (!(p->nu >= 0.0) || !(p->eta >= 0.0)) return fail(DG_ERR_ARG, "nu and eta must be >= 0");
     if (p->surrogate && p->iriemann != DG_RIEMANN_HLLD)
         return fail(DG_ERR_UNSUPPORTED, "the flux surrogate stands in for HLLD (iriemann = hlld)");
     return DG_OK;
@@ -227,6 +229,7 @@ dg::Geo dg::make_geo(const dg_params &p) {
     G.dz = (p.zmax - p.zmin) / p.nz;
     G.xmin = p.xmin; G.xmax = p.xmax; G.ymin = p.ymin; G.ymax = p.ymax; G.zmin = p.zmin; G.zmax = p.zmax;
     G.gamma = p.gamma; G.ciso = p.ciso; G.omega0 = p.omega0; G.courant = p.courant;
+    G.nu = p.nu; G.eta = p.eta;
     G.iso = p.iso; G.slope_type = p.slope_type; G.iriemann = p.iriemann; G.iriemann2d = p.iriemann2d;
     G.fargo = p.fargo;
     G.shearing = (p.bc[0] == DG_BC_SHEARINGBOX);
@@ -687,6 +690,16 @@ int dg_boundary(dg_ctx *c, double time, double dt) {
     return check_launch();
 }
 
+int dg_dissipation(dg_ctx *c, double time, double dt) {
+    TimerScope ts_(c);
+    if (!c) return fail(DG_ERR_ARG, "null context");
+    if (!(c->G.nu > 0.0) && !(c->G.eta > 0.0)) return DG_OK;  // dumses.f90:104 calls it only then
+    c->launches += c->L->set_scalars(c->B, dt, time, 1, 1, c->stream);
+    c->launches += c->L->dissipation(c->G, c->B, c->cur, c->stream);
+    c->version++;
+    return check_launch();
+}
+
 int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
     TimerScope ts_(c);
     if (!c || !time) return fail(DG_ERR_ARG, "null argument");
@@ -702,6 +715,7 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
             c->cur ^= 1;
         }
         c->launches += c->L->boundary(c->G, c->B, c->cur, c->stream);
+        if (c->G.nu > 0.0 || c->G.eta > 0.0) c->launches += c->L->dissipation(c->G, c->B, c->cur, c->stream);
         c->version++;
         c->launches += c->L->advance_time(c->B, c->stream);
     }

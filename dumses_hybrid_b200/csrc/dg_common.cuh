@@ -47,6 +47,7 @@ struct Geo {
     double dx, dy, dz;
     double xmin, xmax, ymin, ymax, zmin, zmax;
     double gamma, ciso, omega0, courant;
+    double nu, eta;           // viscosity and resistivity of dissipation (0 = off)
     int iso, slope_type, iriemann, iriemann2d, fargo, shearing;
     int bc[3];
     int ndim_act;

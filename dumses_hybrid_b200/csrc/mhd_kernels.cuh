@@ -39,7 +39,8 @@ int nstate_vars(const Geo &G);
 
 // per-kernel timing slots (CUDA events around each launch when a timer is attached)
 enum KernelSlot { KS_SCALARS = 0, KS_DT, KS_PRIM, KS_TRACE, KS_RIEMANN, KS_UPDATE, KS_FARGO_EMF, KS_FARGO_UPDATE,
-                  KS_BOUNDARY, KS_HISTORY, KS_RIGHT_FACES, KS_EFIELD, KS_NN_FACES, KS_NN_FALLBACK, KS_COUNT };
+                  KS_BOUNDARY, KS_HISTORY, KS_RIGHT_FACES, KS_EFIELD, KS_NN_FACES, KS_NN_FALLBACK, KS_DISSIPATION,
+                  KS_COUNT };
 struct KernelTimer {
     virtual void begin(int slot, cudaStream_t st) = 0;
     virtual void end(int slot, cudaStream_t st) = 0;
@@ -56,6 +57,7 @@ extern thread_local KernelTimer *g_timer;  // set by the context that enqueues (
     int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t st);     /* U[cur] -> U[cur^1] */ \
     int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t st);  /* in place on U[cur] */ \
     int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st);                       \
+    int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t st); /* in place, then boundary */ \
     int launch_right_faces(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t st);      \
     int launch_state_to_f64(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t st);     \
     int launch_f64_to_state(const Geo &G, const Bufs &B, int b, const double *in, int nv, cudaStream_t st);

@@ -16,18 +16,6 @@ namespace dg {
 namespace f32 {
 namespace {
 
-// compensated add of an FP32 increment to a normalised (hi, lo) pair: Knuth's
-// two-sum of hi and inc, the rounding error folded into lo, then renormalised
-__device__ __forceinline__ void add_hl(float &hi, float &lo, float inc) {
-    const float s = hi + inc;
-    const float bp = s - hi;
-    const float e = (hi - (s - bp)) + (inc - bp);
-    const float l = lo + e;
-    const float h = s + l;
-    lo = l - (h - s);
-    hi = h;
-}
-
 __device__ __forceinline__ void apply(const StoreHL &U, const StoreHL &Un, const Geo &G, int v, long long c, float inc) {
     float h = U.hi[G.sv * v + c], l = U.lo[G.sv * v + c];
     add_hl(h, l, inc);
@@ -941,6 +929,28 @@ int launch_state_to_f64(const Geo &G, const Bufs &B, int cur, double *out, cudaS
 int launch_f64_to_state(const Geo &G, const Bufs &B, int b, const double *in, int nv, cudaStream_t s) {
     TIMED(KS_RIGHT_FACES, s, (k_f64_to_state<StoreHL><<<nblocks(G.sv * nv, 256), 256, 0, s>>>(G, in, nv, st(B, b))));
     return 1;
+}
+
+// dissipation (physics.f90:272-291): resistive EMFs + CT, viscous fluxes + update, in
+// place on U[cur], then boundary; the step's EMF and flux arrays are free at this point
+int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    const StoreHL U = st(B, cur);
+    float *e0 = (float *)B.emf[0], *e1 = (float *)B.emf[1], *e2 = (float *)B.emf[2];
+    float *f0 = (float *)B.flx[0], *f1 = (float *)B.flx[1], *f2 = G.ndim == 3 ? (float *)B.flx[2] : f0;
+    if (G.ndim == 2) e0 = e1 = e2;  // 2D: only emfz is allocated and used
+    const unsigned nb = nblocks(G.fsz, kThreads);
+    int n = 0;
+    if (G.eta > 0.0) {
+        TIMED(KS_DISSIPATION, s, (k_resist_emf<StoreHL><<<nb, kThreads, 0, s>>>(G, U, e0, e1, e2, B.S)));
+        TIMED(KS_DISSIPATION, s, (k_ct<StoreHL><<<nb, kThreads, 0, s>>>(G, U, e0, e1, e2)));
+        n += 2;
+    }
+    if (G.nu > 0.0) {
+        TIMED(KS_DISSIPATION, s, (k_visc_flux<StoreHL><<<nb, kThreads, 0, s>>>(G, U, f0, f1, f2, B.S)));
+        TIMED(KS_DISSIPATION, s, (k_visc_update<StoreHL><<<nb, kThreads, 0, s>>>(G, U, f0, f1, f2)));
+        n += 2;
+    }
+    return n + launch_boundary(G, B, cur, s);
 }
 
 int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {

@@ -302,6 +302,28 @@ int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *
     return 3;
 }
 
+// dissipation (physics.f90:272-291): resistive EMFs + CT, viscous fluxes + update, in
+// place on U[cur], then boundary; the step's EMF and flux arrays are free at this point
+int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    const StoreD U = st(B, cur);
+    double *e0 = (double *)B.emf[0], *e1 = (double *)B.emf[1], *e2 = (double *)B.emf[2];
+    double *f0 = (double *)B.flx[0], *f1 = (double *)B.flx[1], *f2 = G.ndim == 3 ? (double *)B.flx[2] : f0;
+    if (G.ndim == 2) e0 = e1 = e2;  // 2D: only emfz is allocated and used
+    const unsigned nb = nblocks(G.fsz, kThreads);
+    int n = 0;
+    if (G.eta > 0.0) {
+        TIMED(KS_DISSIPATION, s, (k_resist_emf<StoreD><<<nb, kThreads, 0, s>>>(G, U, e0, e1, e2, B.S)));
+        TIMED(KS_DISSIPATION, s, (k_ct<StoreD><<<nb, kThreads, 0, s>>>(G, U, e0, e1, e2)));
+        n += 2;
+    }
+    if (G.nu > 0.0) {
+        TIMED(KS_DISSIPATION, s, (k_visc_flux<StoreD><<<nb, kThreads, 0, s>>>(G, U, f0, f1, f2, B.S)));
+        TIMED(KS_DISSIPATION, s, (k_visc_update<StoreD><<<nb, kThreads, 0, s>>>(G, U, f0, f1, f2)));
+        n += 2;
+    }
+    return n + launch_boundary(G, B, cur, s);
+}
+
 int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     return launch_history_ptrs(G, (const double *)B.U[cur], B.part, B.hist, s);
 }

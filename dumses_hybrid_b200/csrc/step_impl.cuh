@@ -92,16 +92,34 @@ inline unsigned nblocks(long long n, int threads) { return (unsigned)((n + threa
 // ---------------------------------------------------------------------------
 // FP64 state: nv planes of doubles, plane v at p + v*sv
 struct StoreD {
+    using T = double;  // arithmetic of the kernels on this state
     double *p;
     __device__ __forceinline__ double get(const Geo &G, int v, long long c) const { return p[G.sv * v + c]; }
     __device__ __forceinline__ double getr(const Geo &G, int v, long long c) const { return ld(p + G.sv * v + c); }
     __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const { p[G.sv * v + c] = x; }
+    // u = u + inc, the reference's in-place update
+    __device__ __forceinline__ void add(const Geo &G, int v, long long c, double inc) const {
+        p[G.sv * v + c] = p[G.sv * v + c] + inc;
+    }
     __device__ __forceinline__ const double *faces() const { return p; }
 };
+
+// compensated add of an FP32 increment to a normalised (hi, lo) pair: Knuth's
+// two-sum of hi and inc, the rounding error folded into lo, then renormalised
+__device__ __forceinline__ void add_hl(float &hi, float &lo, float inc) {
+    const float s = hi + inc;
+    const float bp = s - hi;
+    const float e = (hi - (s - bp)) + (inc - bp);
+    const float l = lo + e;
+    const float h = s + l;
+    lo = l - (h - s);
+    hi = h;
+}
 
 // Compensated FP32 state: value = hi + lo with |lo| <= ulp(hi)/2 (renormalised on
 // every write), hi planes at hi + v*sv and lo planes at lo + v*sv.
 struct StoreHL {
+    using T = float;
     float *hi, *lo;
     __device__ __forceinline__ double get(const Geo &G, int v, long long c) const {
         return (double)hi[G.sv * v + c] + (double)lo[G.sv * v + c];
@@ -113,6 +131,12 @@ struct StoreHL {
         const float h = (float)x;
         hi[G.sv * v + c] = h;
         lo[G.sv * v + c] = (float)(x - (double)h);
+    }
+    __device__ __forceinline__ void add(const Geo &G, int v, long long c, float inc) const {
+        float h = hi[G.sv * v + c], l = lo[G.sv * v + c];
+        add_hl(h, l, inc);
+        hi[G.sv * v + c] = h;
+        lo[G.sv * v + c] = l;
     }
     __device__ __forceinline__ const float *faces() const { return hi; }
 };
@@ -1344,6 +1368,189 @@ __global__ void __launch_bounds__(kThreads, DG_FARGO_MINB64) k_fargo_update(Geo 
             if (i <= nx && j <= ny) Un.set(G, IC, c, cz[m] - (exj[m + 1] - exj[m]) / dy);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// dissipation (physics.f90:272-664): after boundary when nu > 0 or eta > 0
+// (dumses.f90:104); resistivity, then viscosity, then boundary again
+// ---------------------------------------------------------------------------
+// one thread per point of the face index space [1, nx+1] x [1, ny+1] x [1, nz+1]
+__device__ __forceinline__ bool face_point(const Geo &G, long long t, int &i, int &j, int &k) {
+    if (t >= G.fsz) return false;
+    i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    j = (int)(r % G.FY) + 1;
+    k = (int)(r / G.FY) + 1;
+    return true;
+}
+
+// resistivity edge EMFs -eta J dt (physics.f90:310-345), J from the face B of the
+// state (in 2D only emfz, the one the CT reads).  The resistive energy flux of :350-451 never
+// reaches the state in the reference (dissipation zeroes the flux array before
+// viscosity and godunov overwrites it), so it is not computed.
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_resist_emf(Geo G, Store U, typename Store::T *__restrict__ ex,
+                                                         typename Store::T *__restrict__ ey,
+                                                         typename Store::T *__restrict__ ez, const Scalars *S) {
+    using T = typename Store::T;
+    int i, j, k;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (!face_point(G, t, i, j, k)) return;
+    const T dx = (T)G.dx, dy = (T)G.dy, dz = (T)G.dz, eta = (T)G.eta, dt = (T)S->dt, zero = T(0);
+    auto B = [&](int v, int ii, int jj, int kk) { return (T)U.getr(G, v, G.idx(ii, jj, kk)); };
+    T dBxdy = zero, dBxdz = zero, dBydz = zero, dBzdy = zero, jx = zero;
+    const T dBydx = (B(IB, i, j, k) - B(IB, i - 1, j, k)) / dx;
+    const T dBzdx = (B(IC, i, j, k) - B(IC, i - 1, j, k)) / dx;
+    if (G.ndim > 1) {
+        dBxdy = (B(IA, i, j, k) - B(IA, i, j - 1, k)) / dy;
+        dBzdy = (B(IC, i, j, k) - B(IC, i, j - 1, k)) / dy;
+    }
+    if (G.ndim == 3) {
+        dBxdz = (B(IA, i, j, k) - B(IA, i, j, k - 1)) / dz;
+        dBydz = (B(IB, i, j, k) - B(IB, i, j, k - 1)) / dz;
+    }
+    if (G.ndim > 1) jx = dBzdy - dBydz;
+    const T jy = dBxdz - dBzdx, jz = dBydx - dBxdy;
+    if (G.ndim == 3) {  // emfx and emfy enter only the ndim = 3 terms of the CT
+        ex[t] = -eta * jx * dt;
+        ey[t] = -eta * jy * dt;
+    }
+    ez[t] = -eta * jz * dt;
+}
+
+// constrained_transport (scheme.f90:1940-1993) of the resistive EMFs, in place, on the
+// faces that the following boundary keeps: B_x on i = 1..nx+1 (the outer x face is the
+// shearing box's own), B_y and B_z of the active cells.  The two loop nests of the
+// reference (the ndim >= 2 terms, then the ndim = 3 terms) become two increments.
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_ct(Geo G, Store U, const typename Store::T *__restrict__ ex,
+                                                 const typename Store::T *__restrict__ ey,
+                                                 const typename Store::T *__restrict__ ez) {
+    using T = typename Store::T;
+    int i, j, k;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (!face_point(G, t, i, j, k)) return;
+    const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const T dx = (T)G.dx, dy = (T)G.dy, dz = (T)G.dz;
+    auto E = [&](const T *e, int ii, int jj, int kk) { return ld(e + G.fidx(ii, jj, kk)); };
+    const long long c = G.idx(i, j, k);
+    if (j <= ny && k <= nz) {
+        U.add(G, IA, c, (E(ez, i, j + 1, k) - E(ez, i, j, k)) / dy);
+        if (G.ndim == 3) U.add(G, IA, c, -((E(ey, i, j, k + 1) - E(ey, i, j, k)) / dz));
+    }
+    if (i <= nx && k <= nz) {
+        U.add(G, IB, c, -((E(ez, i + 1, j, k) - E(ez, i, j, k)) / dx));
+        if (G.ndim == 3) U.add(G, IB, c, (E(ex, i, j, k + 1) - E(ex, i, j, k)) / dz);
+    }
+    if (G.ndim == 3 && i <= nx && j <= ny) {
+        U.add(G, IC, c, (E(ey, i + 1, j, k) - E(ey, i, j, k)) / dx);
+        U.add(G, IC, c, -((E(ex, i, j + 1, k) - E(ex, i, j, k)) / dy));
+    }
+}
+
+// viscous fluxes of momentum and energy (physics.f90:481-643) on the faces the update
+// reads: four values per face (rho v_x, rho v_y, rho v_z, E), already x dt/dx_d.
+// As in the reference, dudx of the first direction divides the momentum of cell i-1
+// by the density of cell i (:494-496).
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_visc_flux(Geo G, Store U, typename Store::T *__restrict__ f0,
+                                                        typename Store::T *__restrict__ f1,
+                                                        typename Store::T *__restrict__ f2, const Scalars *S) {
+    using T = typename Store::T;
+    int i, j, k;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (!face_point(G, t, i, j, k)) return;
+    const int nx = G.nx, ny = G.ny, nz = G.nz, nd = G.ndim;
+    const T dx = (T)G.dx, dy = (T)G.dy, dz = (T)G.dz, nu = (T)G.nu, dt = (T)S->dt;
+    const T zero = T(0), half = T(0.5), forth = T(0.25), two = T(2), two3rd = T(0.66666666666666667);
+    auto R = [&](int ii, int jj, int kk) { return (T)U.getr(G, IR, G.idx(ii, jj, kk)); };
+    auto M = [&](int m, int ii, int jj, int kk) { return (T)U.getr(G, IR + m, G.idx(ii, jj, kk)); };
+    auto V = [&](int m, int ii, int jj, int kk) { return M(m, ii, jj, kk) / R(ii, jj, kk); };
+    // (d_a u_m) centred on the face: forth ((u(+a) + u(+a,-n)) - (u(-a) + u(-a,-n))) / h_a
+    auto cross = [&](int m, int ai, int aj, int ak, int ni, int nj, int nk, T h) {
+        const T uR = V(m, i + ai, j + aj, k + ak) + V(m, i + ai - ni, j + aj - nj, k + ak - nk);
+        const T uL = V(m, i - ai, j - aj, k - ak) + V(m, i - ai - ni, j - aj - nj, k - ak - nk);
+        return forth * (uR - uL) / h;
+    };
+    T dudx[4], dudy[4], dudz[4];
+    if (j <= ny && k <= nz) {  // first direction
+        const T rho = half * (R(i, j, k) + R(i - 1, j, k));
+        for (int m = 1; m <= 3; m++) dudx[m] = (V(m, i, j, k) - M(m, i - 1, j, k) / R(i, j, k)) / dx;
+        if (nd > 1) { dudy[1] = cross(1, 0, 1, 0, 1, 0, 0, dy); dudy[2] = cross(2, 0, 1, 0, 1, 0, 0, dy); }
+        if (nd == 3) { dudz[1] = cross(1, 0, 0, 1, 1, 0, 0, dz); dudz[3] = cross(3, 0, 0, 1, 1, 0, 0, dz); }
+        else dudz[1] = dudz[3] = zero;
+        const T txx = -two3rd * nu * rho * (two * dudx[1] - dudy[2] - dudz[3]);
+        const T txy = -nu * rho * (dudy[1] + dudx[2]);
+        const T txz = -nu * rho * (dudz[1] + dudx[3]);
+        T *f = f0 + t * 4;
+        f[0] = txx * dt / dx;
+        f[1] = txy * dt / dx;
+        f[2] = txz * dt / dx;
+        f[3] = zero;
+        if (!G.iso) {
+            const T u = half * (V(1, i, j, k) + V(1, i - 1, j, k)), v = half * (V(2, i, j, k) + V(2, i - 1, j, k));
+            const T w = half * (V(3, i, j, k) + V(3, i - 1, j, k));
+            f[3] = (u * txx + v * txy + w * txz) * dt / dx;
+        }
+    }
+    if (nd > 1 && i <= nx && k <= nz) {  // second direction
+        const T rho = half * (R(i, j, k) + R(i, j - 1, k));
+        for (int m = 1; m <= 3; m++) dudy[m] = (V(m, i, j, k) - V(m, i, j - 1, k)) / dy;
+        dudx[1] = cross(1, 1, 0, 0, 0, 1, 0, dx);
+        dudx[2] = cross(2, 1, 0, 0, 0, 1, 0, dx);
+        if (nd == 3) { dudz[2] = cross(2, 0, 0, 1, 0, 1, 0, dz); dudz[3] = cross(3, 0, 0, 1, 0, 1, 0, dz); }
+        else dudz[2] = dudz[3] = zero;
+        const T tyy = -two3rd * nu * rho * (two * dudy[2] - dudx[1] - dudz[3]);
+        const T txy = -nu * rho * (dudy[1] + dudx[2]);
+        const T tyz = -nu * rho * (dudz[2] + dudy[3]);
+        T *f = f1 + t * 4;
+        f[0] = txy * dt / dy;
+        f[1] = tyy * dt / dy;
+        f[2] = tyz * dt / dy;
+        f[3] = zero;
+        if (!G.iso) {
+            const T u = half * (V(1, i, j, k) + V(1, i, j - 1, k)), v = half * (V(2, i, j, k) + V(2, i, j - 1, k));
+            const T w = half * (V(3, i, j, k) + V(3, i, j - 1, k));
+            f[3] = (u * txy + v * tyy + w * tyz) * dt / dy;
+        }
+    }
+    if (nd == 3 && i <= nx && j <= ny) {  // third direction
+        const T rho = half * (R(i, j, k) + R(i, j, k - 1));
+        for (int m = 1; m <= 3; m++) dudz[m] = (V(m, i, j, k) - V(m, i, j, k - 1)) / dz;
+        dudx[1] = cross(1, 1, 0, 0, 0, 0, 1, dx);
+        dudx[3] = cross(3, 1, 0, 0, 0, 0, 1, dx);
+        dudy[2] = cross(2, 0, 1, 0, 0, 0, 1, dy);
+        dudy[3] = cross(3, 0, 1, 0, 0, 0, 1, dy);
+        const T tzz = -two3rd * nu * rho * (two * dudz[3] - dudx[1] - dudy[2]);
+        const T txz = -nu * rho * (dudz[1] + dudx[3]);
+        const T tyz = -nu * rho * (dudz[2] + dudy[3]);
+        T *f = f2 + t * 4;
+        f[0] = txz * dt / dz;
+        f[1] = tyz * dt / dz;
+        f[2] = tzz * dt / dz;
+        f[3] = zero;
+        if (!G.iso) {
+            const T u = half * (V(1, i, j, k) + V(1, i, j, k - 1)), v = half * (V(2, i, j, k) + V(2, i, j, k - 1));
+            const T w = half * (V(3, i, j, k) + V(3, i, j, k - 1));
+            f[3] = (u * txz + v * tyz + w * tzz) * dt / dz;
+        }
+    }
+}
+
+// conservative update of momentum and energy with the viscous fluxes (physics.f90:647-663),
+// directions in the order 1, 2, 3
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_visc_update(Geo G, Store U, const typename Store::T *__restrict__ f0,
+                                                          const typename Store::T *__restrict__ f1,
+                                                          const typename Store::T *__restrict__ f2) {
+    int i, j, k;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (!face_point(G, t, i, j, k) || i > G.nx || j > G.ny || k > G.nz) return;
+    const long long c = G.idx(i, j, k);
+    const typename Store::T *F[3] = {f0, f1, f2};
+    const long long R[3] = {G.fidx(i + 1, j, k), G.fidx(i, j + 1, k), G.fidx(i, j, k + 1)};
+    for (int d = 0; d < G.ndim; d++)
+        for (int m = 0; m < 4; m++) U.add(G, IU + m, c, ld(F[d] + t * 4 + m) - ld(F[d] + R[d] * 4 + m));
 }
 
 // ---------------------------------------------------------------------------

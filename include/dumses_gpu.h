@@ -14,6 +14,7 @@
  *   dg_godunov       <- godunov                         src/subroutines/scheme.f90:104-189
  *   dg_fargo_update  <- fargo_update                    src/subroutines/fargo.f90:17-124
  *   dg_boundary      <- boundary                        src/subroutines/boundary.f90:18-92
+ *   dg_dissipation   <- dissipation                     src/subroutines/physics.f90:272-664
  *   dg_history       <- history (MRI problem variant)   src/problem/mri/history.f90:19-174
  *   dg_step          <- one pass of the loop body       src/dumses.f90:82-120
  *   dg_finalize      <- deallocate_workspace            src/subroutines/finalize.f90
@@ -84,6 +85,8 @@ typedef struct dg_params {
     int    precision;        /* DG_PREC_*                                              */
     int    surrogate;        /* 1: learned flux surrogate with HLLD fallback (FP32)    */
     int    device;           /* CUDA device ordinal                                    */
+    double nu;               /* kinematic viscosity (physics.f90:459-664); 0 = off     */
+    double eta;              /* Ohmic resistivity (physics.f90:295-455); 0 = off       */
     int    reserved[6];
 } dg_params;
 
@@ -109,8 +112,15 @@ int  dg_fargo_update(dg_ctx *ctx, double dt);
 /* ghost fill, shear-periodic remap at time+dt (boundary.f90:18-92) */
 int  dg_boundary(dg_ctx *ctx, double time, double dt);
 
+/* dissipation (src/subroutines/physics.f90:272-664), called by the reference after
+ * boundary when nu > 0 or eta > 0 (dumses.f90:104): Ohmic resistivity (edge EMFs
+ * -eta J dt and constrained transport), Navier-Stokes viscosity (face fluxes of
+ * momentum and, adiabatic, energy; conservative update), then boundary at
+ * time + dt.  A no-op when nu = eta = 0. */
+int  dg_dissipation(dg_ctx *ctx, double time, double dt);
+
 /* Loop body of dumses.f90:82-120: compute_dt, godunov, fargo (if on), boundary,
- * time += dt.  dt and time stay on the device; nsteps steps are enqueued without
+ * dissipation (if nu > 0 or eta > 0), time += dt.  dt and time stay on the device; nsteps steps are enqueued without
  * any host synchronisation.  On return *time and *dt hold the values after the
  * last step (this waits for the stream). */
 int  dg_run(dg_ctx *ctx, int nsteps, double *time, double *dt);
@@ -184,7 +194,7 @@ int  dg_sync(dg_ctx *ctx);
  * dg_profile(ctx, 1) starts recording an event pair around every kernel;
  * dg_profile_read fills ms[slot] and count[slot] for the launches since the
  * last read (slots named by dg_profile_slot_name) and resets them. */
-#define DG_PROFILE_SLOTS 14
+#define DG_PROFILE_SLOTS 15
 int  dg_profile(dg_ctx *ctx, int on);
 int  dg_profile_read(dg_ctx *ctx, double *ms, long long *count, int nslots);
 const char *dg_profile_slot_name(int slot);

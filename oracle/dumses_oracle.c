@@ -1866,6 +1866,219 @@ void or_history_mri(or_state *s, double out[9])
 }
 
 /* ------------------------------------------------------------------------- */
+/* dissipation, src/subroutines/physics.f90:272-664                           */
+/* ------------------------------------------------------------------------- */
+static const double two3rd = 0.66666666666666667; /* commons.f90:45 */
+
+/* resistivity, physics.f90:295-455: edge EMFs -eta J dt, then constrained_transport.
+ * The ISO = 0 loop of :350-451 adds a resistive energy flux to flux(:,:,:,ip,:); that
+ * array is zeroed by dissipation before viscosity (:284-285) and overwritten by the next
+ * godunov's compflux, so the flux never reaches uin and is not restated here. */
+static void resistivity(or_state *s, double dt)
+{
+    const double eta = s->p.eta, dx = s->dx, dy = s->dy, dz = s->dz;
+    memset(s->emfx.d, 0, sizeof(double) * s->emfx.size);
+    memset(s->emfy.d, 0, sizeof(double) * s->emfy.size);
+    memset(s->emfz.d, 0, sizeof(double) * s->emfz.size);
+#pragma omp parallel for schedule(static)
+    for (int k = s->kf1; k <= s->kf2; k++)
+        for (int j = s->jf1; j <= s->jf2; j++)
+            for (int i = s->if1; i <= s->if2; i++) {
+                double dBxdy = zero, dBxdz = zero, dBydz = zero, dBzdy = zero, jx = zero;
+                const double dBydx = (A4(s->uin, i, j, k, iB) - A4(s->uin, i - 1, j, k, iB)) / dx;
+                const double dBzdx = (A4(s->uin, i, j, k, iC) - A4(s->uin, i - 1, j, k, iC)) / dx;
+                if (s->ndim > 1) {
+                    dBxdy = (A4(s->uin, i, j, k, iA) - A4(s->uin, i, j - 1, k, iA)) / dy;
+                    dBzdy = (A4(s->uin, i, j, k, iC) - A4(s->uin, i, j - 1, k, iC)) / dy;
+                }
+                if (s->ndim == 3) {
+                    dBxdz = (A4(s->uin, i, j, k, iA) - A4(s->uin, i, j, k - 1, iA)) / dz;
+                    dBydz = (A4(s->uin, i, j, k, iB) - A4(s->uin, i, j, k - 1, iB)) / dz;
+                }
+                if (s->ndim > 1) jx = dBzdy - dBydz;
+                const double jy = dBxdz - dBzdx, jz = dBydx - dBxdy;
+                if (s->ndim > 1) A3(s->emfx, i, j, k) = -eta * jx * dt;
+                A3(s->emfy, i, j, k) = -eta * jy * dt;
+                A3(s->emfz, i, j, k) = -eta * jz * dt;
+            }
+    constrained_transport(s);
+}
+
+/* velocity component m (1..3) of cell (i,j,k) over the density of cell (ii,jj,kk) */
+#define VEL(m, i, j, k, ii, jj, kk) (A4(s->uin, i, j, k, (m) + 1) / A4(s->uin, ii, jj, kk, ir))
+
+/* viscosity, physics.f90:459-664: viscous fluxes of momentum (and energy when ISO = 0)
+ * on the faces, then the conservative update.  The reference runs the update's idim
+ * loop as an OpenMP/OpenACC parallel loop although every idim updates the same cells;
+ * the restatement takes the serial order idim = 1, 2, 3. */
+static void viscosity(or_state *s, double dt)
+{
+    const double nu = s->p.nu, dx = s->dx, dy = s->dy, dz = s->dz;
+    const int iso = s->p.iso, nd = s->ndim;
+#pragma omp parallel for schedule(static)
+    for (int k = s->kf1; k <= s->kf2; k++)
+        for (int j = s->jf1; j <= s->jf2; j++)
+            for (int i = s->if1; i <= s->if2; i++) {
+                double dudx[4] = {0, 0, 0, 0}, dudy[4] = {0, 0, 0, 0}, dudz[4] = {0, 0, 0, 0};
+                double rho, u = zero, v = zero, w = zero, uR, uL, uRR, uRL, uLR, uLL, txx, tyy, tzz, txy, txz, tyz;
+                /* first direction, :482-541 */
+                rho = half * (A4(s->uin, i, j, k, ir) + A4(s->uin, i - 1, j, k, ir));
+                if (!iso) {
+                    u = half * (VEL(1, i, j, k, i, j, k) + VEL(1, i - 1, j, k, i - 1, j, k));
+                    v = half * (VEL(2, i, j, k, i, j, k) + VEL(2, i - 1, j, k, i - 1, j, k));
+                    w = half * (VEL(3, i, j, k, i, j, k) + VEL(3, i - 1, j, k, i - 1, j, k));
+                }
+                for (int m = 1; m <= 3; m++) {
+                    uR = VEL(m, i, j, k, i, j, k);
+                    uL = VEL(m, i - 1, j, k, i, j, k); /* :495, over the density of cell i */
+                    dudx[m] = (uR - uL) / dx;
+                }
+                if (nd > 1) {
+                    for (int m = 1; m <= 2; m++) {
+                        uRR = VEL(m, i, j + 1, k, i, j + 1, k);
+                        uRL = VEL(m, i - 1, j + 1, k, i - 1, j + 1, k);
+                        uLR = VEL(m, i, j - 1, k, i, j - 1, k);
+                        uLL = VEL(m, i - 1, j - 1, k, i - 1, j - 1, k);
+                        uR = uRR + uRL; uL = uLR + uLL;
+                        dudy[m] = forth * (uR - uL) / dy;
+                    }
+                } else {
+                    dudy[1] = dudy[2] = dudy[3] = zero;
+                }
+                if (nd == 3) {
+                    for (int m = 1; m <= 3; m += 2) {
+                        uRR = VEL(m, i, j, k + 1, i, j, k + 1);
+                        uRL = VEL(m, i - 1, j, k + 1, i - 1, j, k + 1);
+                        uLR = VEL(m, i, j, k - 1, i, j, k - 1);
+                        uLL = VEL(m, i - 1, j, k - 1, i - 1, j, k - 1);
+                        uR = uRR + uRL; uL = uLR + uLL;
+                        dudz[m] = forth * (uR - uL) / dz;
+                    }
+                } else {
+                    dudz[1] = dudz[2] = dudz[3] = zero;
+                }
+                txx = -two3rd * nu * rho * (two * dudx[1] - dudy[2] - dudz[3]);
+                txy = -nu * rho * (dudy[1] + dudx[2]);
+                txz = -nu * rho * (dudz[1] + dudx[3]);
+                A5(s->flux, i, j, k, iu, 1) = txx * dt / dx;
+                A5(s->flux, i, j, k, iv, 1) = txy * dt / dx;
+                A5(s->flux, i, j, k, iw, 1) = txz * dt / dx;
+                if (!iso) {
+                    A5(s->flux, i, j, k, ip, 1) = u * txx + v * txy + w * txz;
+                    A5(s->flux, i, j, k, ip, 1) = A5(s->flux, i, j, k, ip, 1) * dt / dx;
+                }
+                /* second direction, :544-593 */
+                if (nd > 1) {
+                    rho = half * (A4(s->uin, i, j, k, ir) + A4(s->uin, i, j - 1, k, ir));
+                    if (!iso) {
+                        u = half * (VEL(1, i, j, k, i, j, k) + VEL(1, i, j - 1, k, i, j - 1, k));
+                        v = half * (VEL(2, i, j, k, i, j, k) + VEL(2, i, j - 1, k, i, j - 1, k));
+                        w = half * (VEL(3, i, j, k, i, j, k) + VEL(3, i, j - 1, k, i, j - 1, k));
+                    }
+                    for (int m = 1; m <= 3; m++) {
+                        uR = VEL(m, i, j, k, i, j, k);
+                        uL = VEL(m, i, j - 1, k, i, j - 1, k);
+                        dudy[m] = (uR - uL) / dy;
+                    }
+                    for (int m = 1; m <= 2; m++) {
+                        uRR = VEL(m, i + 1, j, k, i + 1, j, k);
+                        uRL = VEL(m, i + 1, j - 1, k, i + 1, j - 1, k);
+                        uLR = VEL(m, i - 1, j, k, i - 1, j, k);
+                        uLL = VEL(m, i - 1, j - 1, k, i - 1, j - 1, k);
+                        uR = uRR + uRL; uL = uLR + uLL;
+                        dudx[m] = forth * (uR - uL) / dx;
+                    }
+                    if (nd == 3) {
+                        for (int m = 2; m <= 3; m++) {
+                            uRR = VEL(m, i, j, k + 1, i, j, k + 1);
+                            uRL = VEL(m, i, j - 1, k + 1, i, j - 1, k + 1);
+                            uLR = VEL(m, i, j, k - 1, i, j, k - 1);
+                            uLL = VEL(m, i, j - 1, k - 1, i, j - 1, k - 1);
+                            uR = uRR + uRL; uL = uLR + uLL;
+                            dudz[m] = forth * (uR - uL) / dz;
+                        }
+                    } else {
+                        dudz[1] = dudz[2] = dudz[3] = zero;
+                    }
+                    tyy = -two3rd * nu * rho * (two * dudy[2] - dudx[1] - dudz[3]);
+                    txy = -nu * rho * (dudy[1] + dudx[2]);
+                    tyz = -nu * rho * (dudz[2] + dudy[3]);
+                    A5(s->flux, i, j, k, iu, 2) = txy * dt / dy;
+                    A5(s->flux, i, j, k, iv, 2) = tyy * dt / dy;
+                    A5(s->flux, i, j, k, iw, 2) = tyz * dt / dy;
+                    if (!iso) {
+                        A5(s->flux, i, j, k, ip, 2) = u * txy + v * tyy + w * tyz;
+                        A5(s->flux, i, j, k, ip, 2) = A5(s->flux, i, j, k, ip, 2) * dt / dy;
+                    }
+                }
+                /* third direction, :596-643 */
+                if (nd == 3) {
+                    rho = half * (A4(s->uin, i, j, k, ir) + A4(s->uin, i, j, k - 1, ir));
+                    if (!iso) {
+                        u = half * (VEL(1, i, j, k, i, j, k) + VEL(1, i, j, k - 1, i, j, k - 1));
+                        v = half * (VEL(2, i, j, k, i, j, k) + VEL(2, i, j, k - 1, i, j, k - 1));
+                        w = half * (VEL(3, i, j, k, i, j, k) + VEL(3, i, j, k - 1, i, j, k - 1));
+                    }
+                    for (int m = 1; m <= 3; m++) {
+                        uR = VEL(m, i, j, k, i, j, k);
+                        uL = VEL(m, i, j, k - 1, i, j, k - 1);
+                        dudz[m] = (uR - uL) / dz;
+                    }
+                    for (int m = 1; m <= 3; m += 2) {
+                        uRR = VEL(m, i + 1, j, k, i + 1, j, k);
+                        uRL = VEL(m, i + 1, j, k - 1, i + 1, j, k - 1);
+                        uLR = VEL(m, i - 1, j, k, i - 1, j, k);
+                        uLL = VEL(m, i - 1, j, k - 1, i - 1, j, k - 1);
+                        uR = uRR + uRL; uL = uLR + uLL;
+                        dudx[m] = forth * (uR - uL) / dx;
+                    }
+                    for (int m = 2; m <= 3; m++) {
+                        uRR = VEL(m, i, j + 1, k, i, j + 1, k);
+                        uRL = VEL(m, i, j + 1, k - 1, i, j + 1, k - 1);
+                        uLR = VEL(m, i, j - 1, k, i, j - 1, k);
+                        uLL = VEL(m, i, j - 1, k - 1, i, j - 1, k - 1);
+                        uR = uRR + uRL; uL = uLR + uLL;
+                        dudy[m] = forth * (uR - uL) / dy;
+                    }
+                    tzz = -two3rd * nu * rho * (two * dudz[3] - dudx[1] - dudy[2]);
+                    txz = -nu * rho * (dudz[1] + dudx[3]);
+                    tyz = -nu * rho * (dudz[2] + dudy[3]);
+                    A5(s->flux, i, j, k, iu, 3) = txz * dt / dz;
+                    A5(s->flux, i, j, k, iv, 3) = tyz * dt / dz;
+                    A5(s->flux, i, j, k, iw, 3) = tzz * dt / dz;
+                    if (!iso) {
+                        A5(s->flux, i, j, k, ip, 3) = u * txz + v * tyz + w * tzz;
+                        A5(s->flux, i, j, k, ip, 3) = A5(s->flux, i, j, k, ip, 3) * dt / dz;
+                    }
+                }
+            }
+    /* conservative update, :647-663 */
+    for (int idim = 1; idim <= nd; idim++) {
+        const int i0 = idim == 1, j0 = idim == 2, k0 = idim == 3;
+#pragma omp parallel for schedule(static)
+        for (int k = 1; k <= s->nz; k++)
+            for (int j = 1; j <= s->ny; j++)
+                for (int i = 1; i <= s->nx; i++)
+                    for (int v = iu; v <= ip; v++)
+                        A4(s->uin, i, j, k, v) = A4(s->uin, i, j, k, v)
+                            + (A5(s->flux, i, j, k, v, idim) - A5(s->flux, i + i0, j + j0, k + k0, v, idim));
+    }
+}
+#undef VEL
+
+/* dissipation, physics.f90:272-291, called after boundary when nu > 0 or eta > 0
+ * (dumses.f90:104) */
+void or_dissipation(or_state *s, double time, double dt)
+{
+    if (s->p.eta > zero) resistivity(s, dt);
+    if (s->p.nu > zero) {
+        memset(s->flux.d, 0, sizeof(double) * s->flux.size);
+        viscosity(s, dt);
+    }
+    or_boundary(s, time, dt);
+}
+
+/* ------------------------------------------------------------------------- */
 /* driver loop, src/dumses.f90:75-160                                         */
 /* ------------------------------------------------------------------------- */
 double or_step(or_state *s, double *time)
@@ -1874,6 +2087,7 @@ double or_step(or_state *s, double *time)
     or_godunov(s, dt, *time);
     if (s->p.fargo) or_fargo_update(s, dt);
     or_boundary(s, *time, dt);
+    if (s->p.nu > zero || s->p.eta > zero) or_dissipation(s, *time, dt);
     *time = *time + dt;
     return dt;
 }

@@ -41,6 +41,7 @@ def lib() -> ctypes.CDLL:
         L.or_boundary.restype, L.or_boundary.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
         L.or_history_mri.restype, L.or_history_mri.argtypes = None, [vp, dp]
         L.or_step.restype, L.or_step.argtypes = ctypes.c_double, [vp, dp]
+        L.or_dissipation.restype, L.or_dissipation.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
         L.or_run_history.restype = ctypes.c_int
         L.or_run_history.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, ctypes.c_int]
         L.or_array.restype, L.or_array.argtypes = dp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
@@ -82,6 +83,9 @@ class Oracle:
 
     def boundary(self, time: float, dt: float) -> None:
         self.L.or_boundary(self.h, time, dt)
+
+    def dissipation(self, time: float, dt: float) -> None:
+        self.L.or_dissipation(self.h, time, dt)
 
     def step(self, time: float) -> tuple[float, float]:
         t = ctypes.c_double(time)
