@@ -56,18 +56,21 @@ NN_MACS_PER_FACE = 17 * 128 + 128 * 128 + 128 * 128 + 128 * 8  # the face networ
 WORKLOADS = {"ot": "orszag_tang_3d", "mri": "shearing_box_mri_fargo"}
 
 
-def workload_params(n: int, device: int = 0, precision: str = "fp64", kind: str = "ot"):
+def workload_params(n: int, device: int = 0, precision: str = "fp64", kind: str = "ot", nu: float = 0.0,
+                    eta: float = 0.0):
     """ot: the 3D Orszag-Tang-type vortex on the periodic unit cube (adiabatic).
     mri: the unstratified isothermal shearing box of the MRI set-up at n^3 with cubic cells on
-    [-0.5,0.5]^3 H, Omega = 1, q = 1.5, c_s = 1, shear-periodic x, FARGO on."""
+    [-0.5,0.5]^3 H, Omega = 1, q = 1.5, c_s = 1, shear-periodic x, FARGO on.
+    nu, eta > 0 add the dissipation step (viscosity, resistivity) after boundary."""
     from dumses_hybrid_b200 import Params
     if kind == "mri":
         return Params(ndim=3, iso=1, nx=n, ny=n, nz=n, xmin=-0.5, xmax=0.5, ymin=-0.5, ymax=0.5, zmin=-0.5,
                       zmax=0.5, gamma=5.0 / 3.0, ciso=1.0, omega0=1.0, courant=0.8, slope_type=2, riemann="hlld",
-                      riemann2d="hlld", bdtypex="shearingbox", fargo=True, device=device, precision=precision)
+                      riemann2d="hlld", bdtypex="shearingbox", fargo=True, device=device, precision=precision,
+                      nu=nu, eta=eta)
     return Params(ndim=3, nx=n, ny=n, nz=n, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
                   gamma=5.0 / 3.0, courant=0.8, slope_type=2, riemann="hlld", riemann2d="hlld", device=device,
-                  precision=precision)
+                  precision=precision, nu=nu, eta=eta)
 
 
 def initial_state(P, kind: str):
@@ -168,14 +171,14 @@ def replica_max(x: float, dist, device: str = "cuda") -> float:
     return float(t.item())
 
 
-def cpu_baseline(steps: int, warmup: int, n: int = 128, kind: str = "ot") -> dict:
+def cpu_baseline(steps: int, warmup: int, n: int = 128, kind: str = "ot", nu: float = 0.0, eta: float = 0.0) -> dict:
     """The CPU restatement (oracle) on all host cores, n^3 sample of the workload."""
     sys.path.insert(0, str(ROOT / "tests"))
     from _oracle import Oracle, lib as oracle_lib
     from dumses_hybrid_b200 import condinit
     cores = os.cpu_count() or 1
     oracle_lib().or_set_threads(cores)
-    P = workload_params(n, kind=kind)
+    P = workload_params(n, kind=kind, nu=nu, eta=eta)
     o = Oracle(P)
     o.set_state(initial_state(P, kind))
     o.boundary(0.0, 0.0)
@@ -196,7 +199,7 @@ def cpu_baseline(steps: int, warmup: int, n: int = 128, kind: str = "ot") -> dic
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
-    cb = cpu_baseline(max(args.steps, 1), max(args.warmup, 0), n=128, kind=args.workload)
+    cb = cpu_baseline(max(args.steps, 1), max(args.warmup, 0), n=128, kind=args.workload, nu=args.nu, eta=args.eta)
     line = {"metric": METRIC, "value": cb["value"], "unit": "zone-cycles/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds"] / max(args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -224,6 +227,8 @@ def main() -> None:
     ap.add_argument("--nn-epochs", type=float, default=3.0, help="passes over the harvested samples")
     ap.add_argument("--nn-batch", type=int, default=65536)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mri")
+    ap.add_argument("--nu", type=float, default=0.0, help="viscosity: adds the dissipation step (default off)")
+    ap.add_argument("--eta", type=float, default=0.0, help="resistivity: adds the dissipation step (default off)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -269,7 +274,7 @@ def main() -> None:
     def measure(precision: str, with_e2e: bool) -> dict:
         surrogate = precision == "fp32nn"
         P = workload_params(args.n, device=local_rank, precision="fp32" if surrogate else precision,
-                            kind=args.workload)
+                            kind=args.workload, nu=args.nu, eta=args.eta)
         u0 = initial_state(P, args.workload)
         if surrogate:
             P.surrogate = True
@@ -422,7 +427,8 @@ def main() -> None:
             "config": {"workload": f"{WORKLOADS[args.workload]}_{args.n}^3", "grid": [args.n] * 3,
                        "arithmetic": arith[head], "solver": "hlld/hlld", "slope": "mc", "courant": 0.8,
                        "parallelism": f"replicas x{world}",
-                       "l2": "working set 8-13 GB per step >> 126 MB L2, no flush needed"},
+                       "l2": "working set 8-13 GB per step >> 126 MB L2, no flush needed",
+                       **({"nu": args.nu, "eta": args.eta} if args.nu > 0 or args.eta > 0 else {})},
             "e2e": h["e2e"], "gpu_launches": h["launches"], "roofline": roofline(h, head if head != "fp32nn" else "fp32"),
             "kernels": kernel_table(h), "clocks": h["clocks"], "sim_time": h["sim_time"]}
     if "nn" in h:
@@ -455,7 +461,7 @@ def main() -> None:
                                        "l1_rel_vs_fp64": l1_vs(a64, g["state"][3:-3, 3:-3, 3:-3]),
                                        "kernels": kernel_table(g), "clocks": g["clocks"], "e2e": g.get("e2e")}
     if world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(2, 1, n=128, kind=args.workload)
+        cb = cpu_baseline(2, 1, n=128, kind=args.workload, nu=args.nu, eta=args.eta)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
 

@@ -946,9 +946,12 @@ int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         n += 2;
     }
     if (G.nu > 0.0) {
-        TIMED(KS_DISSIPATION, s, (k_visc_flux<StoreHL><<<nb, kThreads, 0, s>>>(G, U, f0, f1, f2, B.S)));
+        // the velocities go to the primitive-variable buffer, which the next step recomputes
+        float *vel = (float *)B.Q;
+        TIMED(KS_DISSIPATION, s, (k_visc_vel<StoreHL><<<nblocks(G.sv, kThreads), kThreads, 0, s>>>(G, U, vel)));
+        TIMED(KS_DISSIPATION, s, (k_visc_flux<StoreHL><<<nb, kThreads, 0, s>>>(G, U, vel, f0, f1, f2, B.S)));
         TIMED(KS_DISSIPATION, s, (k_visc_update<StoreHL><<<nb, kThreads, 0, s>>>(G, U, f0, f1, f2)));
-        n += 2;
+        n += 3;
     }
     return n + launch_boundary(G, B, cur, s);
 }

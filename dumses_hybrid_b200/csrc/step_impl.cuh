@@ -97,10 +97,15 @@ struct StoreD {
     __device__ __forceinline__ double get(const Geo &G, int v, long long c) const { return p[G.sv * v + c]; }
     __device__ __forceinline__ double getr(const Geo &G, int v, long long c) const { return ld(p + G.sv * v + c); }
     __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const { p[G.sv * v + c] = x; }
-    // u = u + inc, the reference's in-place update
+    // u = u + inc, the reference's in-place update; Val holds a value between a load and
+    // a store so that a sequence of increments runs in registers
+    using Val = double;
     __device__ __forceinline__ void add(const Geo &G, int v, long long c, double inc) const {
         p[G.sv * v + c] = p[G.sv * v + c] + inc;
     }
+    __device__ __forceinline__ Val load(const Geo &G, int v, long long c) const { return p[G.sv * v + c]; }
+    __device__ __forceinline__ static void inc(Val &x, double d) { x = x + d; }
+    __device__ __forceinline__ void store(const Geo &G, int v, long long c, Val x) const { p[G.sv * v + c] = x; }
     __device__ __forceinline__ const double *faces() const { return p; }
 };
 
@@ -137,6 +142,17 @@ struct StoreHL {
         add_hl(h, l, inc);
         hi[G.sv * v + c] = h;
         lo[G.sv * v + c] = l;
+    }
+    struct Val {
+        float h, l;
+    };
+    __device__ __forceinline__ Val load(const Geo &G, int v, long long c) const {
+        return Val{hi[G.sv * v + c], lo[G.sv * v + c]};
+    }
+    __device__ __forceinline__ static void inc(Val &x, float d) { add_hl(x.h, x.l, d); }
+    __device__ __forceinline__ void store(const Geo &G, int v, long long c, Val x) const {
+        hi[G.sv * v + c] = x.h;
+        lo[G.sv * v + c] = x.l;
     }
     __device__ __forceinline__ const float *faces() const { return hi; }
 };
@@ -1435,17 +1451,35 @@ __global__ void __launch_bounds__(kThreads) k_ct(Geo G, Store U, const typename 
     auto E = [&](const T *e, int ii, int jj, int kk) { return ld(e + G.fidx(ii, jj, kk)); };
     const long long c = G.idx(i, j, k);
     if (j <= ny && k <= nz) {
-        U.add(G, IA, c, (E(ez, i, j + 1, k) - E(ez, i, j, k)) / dy);
-        if (G.ndim == 3) U.add(G, IA, c, -((E(ey, i, j, k + 1) - E(ey, i, j, k)) / dz));
+        auto a = U.load(G, IA, c);
+        Store::inc(a, (E(ez, i, j + 1, k) - E(ez, i, j, k)) / dy);
+        if (G.ndim == 3) Store::inc(a, -((E(ey, i, j, k + 1) - E(ey, i, j, k)) / dz));
+        U.store(G, IA, c, a);
     }
     if (i <= nx && k <= nz) {
-        U.add(G, IB, c, -((E(ez, i + 1, j, k) - E(ez, i, j, k)) / dx));
-        if (G.ndim == 3) U.add(G, IB, c, (E(ex, i, j, k + 1) - E(ex, i, j, k)) / dz);
+        auto b = U.load(G, IB, c);
+        Store::inc(b, -((E(ez, i + 1, j, k) - E(ez, i, j, k)) / dx));
+        if (G.ndim == 3) Store::inc(b, (E(ex, i, j, k + 1) - E(ex, i, j, k)) / dz);
+        U.store(G, IB, c, b);
     }
     if (G.ndim == 3 && i <= nx && j <= ny) {
-        U.add(G, IC, c, (E(ey, i + 1, j, k) - E(ey, i, j, k)) / dx);
-        U.add(G, IC, c, -((E(ex, i, j + 1, k) - E(ex, i, j, k)) / dy));
+        auto z = U.load(G, IC, c);
+        Store::inc(z, (E(ey, i + 1, j, k) - E(ey, i, j, k)) / dx);
+        Store::inc(z, -((E(ex, i, j + 1, k) - E(ex, i, j, k)) / dy));
+        U.store(G, IC, c, z);
     }
+}
+
+// the velocities m / rho of every cell of the ghosted grid, once: each is the quotient the
+// reference forms again at every use, so the flux kernel reads them instead
+template <class Store>
+__global__ void __launch_bounds__(kThreads) k_visc_vel(Geo G, Store U, typename Store::T *__restrict__ vel) {
+    using T = typename Store::T;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= G.sv) return;
+    const T r = (T)U.getr(G, IR, c);
+#pragma unroll
+    for (int m = 0; m < 3; m++) vel[G.sv * m + c] = (T)U.getr(G, IU + m, c) / r;
 }
 
 // viscous fluxes of momentum and energy (physics.f90:481-643) on the faces the update
@@ -1453,7 +1487,8 @@ __global__ void __launch_bounds__(kThreads) k_ct(Geo G, Store U, const typename 
 // As in the reference, dudx of the first direction divides the momentum of cell i-1
 // by the density of cell i (:494-496).
 template <class Store>
-__global__ void __launch_bounds__(kThreads) k_visc_flux(Geo G, Store U, typename Store::T *__restrict__ f0,
+__global__ void __launch_bounds__(kThreads) k_visc_flux(Geo G, Store U, const typename Store::T *__restrict__ vel,
+                                                        typename Store::T *__restrict__ f0,
                                                         typename Store::T *__restrict__ f1,
                                                         typename Store::T *__restrict__ f2, const Scalars *S) {
     using T = typename Store::T;
@@ -1465,7 +1500,7 @@ __global__ void __launch_bounds__(kThreads) k_visc_flux(Geo G, Store U, typename
     const T zero = T(0), half = T(0.5), forth = T(0.25), two = T(2), two3rd = T(0.66666666666666667);
     auto R = [&](int ii, int jj, int kk) { return (T)U.getr(G, IR, G.idx(ii, jj, kk)); };
     auto M = [&](int m, int ii, int jj, int kk) { return (T)U.getr(G, IR + m, G.idx(ii, jj, kk)); };
-    auto V = [&](int m, int ii, int jj, int kk) { return M(m, ii, jj, kk) / R(ii, jj, kk); };
+    auto V = [&](int m, int ii, int jj, int kk) { return ld(vel + G.sv * (m - 1) + G.idx(ii, jj, kk)); };
     // (d_a u_m) centred on the face: forth ((u(+a) + u(+a,-n)) - (u(-a) + u(-a,-n))) / h_a
     auto cross = [&](int m, int ai, int aj, int ak, int ni, int nj, int nk, T h) {
         const T uR = V(m, i + ai, j + aj, k + ak) + V(m, i + ai - ni, j + aj - nj, k + ak - nk);
@@ -1549,8 +1584,12 @@ __global__ void __launch_bounds__(kThreads) k_visc_update(Geo G, Store U, const 
     const long long c = G.idx(i, j, k);
     const typename Store::T *F[3] = {f0, f1, f2};
     const long long R[3] = {G.fidx(i + 1, j, k), G.fidx(i, j + 1, k), G.fidx(i, j, k + 1)};
-    for (int d = 0; d < G.ndim; d++)
-        for (int m = 0; m < 4; m++) U.add(G, IU + m, c, ld(F[d] + t * 4 + m) - ld(F[d] + R[d] * 4 + m));
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        auto u = U.load(G, IU + m, c);
+        for (int d = 0; d < G.ndim; d++) Store::inc(u, ld(F[d] + t * 4 + m) - ld(F[d] + R[d] * 4 + m));
+        U.store(G, IU + m, c, u);
+    }
 }
 
 // ---------------------------------------------------------------------------
