@@ -385,8 +385,9 @@ def main() -> None:
                 try:
                     util = json.loads(upath.read_text()).get("fp32nn", {}).get(dom)
                     if util:
-                        out["binding"] = {"pipe": "xu", "pipe_frac": util["xu"], "tensor_frac": util["tensor"],
-                                          "issue_frac": util["issue"],
+                        pipe = max(("fma", "alu", "xu", "tensor"), key=lambda p: util[p])
+                        out["binding"] = {"pipe": pipe, "pipe_frac": util[pipe], "tensor_frac": util["tensor"],
+                                          "issue_frac": util["issue"], "warps_frac": util["warps"],
                                           "source": "profiles/pipe_util_mri128.json (ncu, 128^3)"}
                 except Exception:
                     pass

@@ -448,7 +448,7 @@ def _fptr(a: np.ndarray):
 
 class FluxNet:
     """The learned face-flux network (a dg_nn of the C-ABI): 17 -> 128 -> 128 -> 128 -> 8,
-    GELU, BF16 weights with FP32 accumulation, trained on the device.  Parameters are a
+    SmeLU, BF16 weights with FP32 accumulation, trained on the device.  Parameters are a
     flat float32 vector in the order W1[17][128], b1, W2[128][128], b2, W3, b3, W4[128][8], b4."""
 
     def __init__(self, device: int = 0, seed: int = 1):

@@ -156,33 +156,38 @@ __device__ __forceinline__ bool gate_inputs(const Gates &g, const float *ql, con
     return true;
 }
 
-// GELU in its tanh form, 0.5 z (1 + tanh(c (z + a z^3))), c = sqrt(2/pi), a = 0.044715,
-// and its derivative
-constexpr float kGeluC = 0.7978845608028654f, kGeluA = 0.044715f;
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + tanhf(kGeluC * (z + kGeluA * z * z * z))); }
-__device__ __forceinline__ float gelu_d(float z) {
-    const float t = tanhf(kGeluC * (z + kGeluA * z * z * z));
-    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * kGeluA * z * z);
+// SmeLU, the smooth ReLU of Shamir, Lin, Coviello and Chen ("Smooth activations and
+// reproducibility in deep networks", 2020) with half-width 1:
+//   f(z) = 0 (z <= -1),  (z + 1)^2 / 4 (|z| < 1),  z (z >= 1);   f'(z) = clamp((z + 1) / 2, 0, 1).
+// With h = (clamp(z, -1, 1) + 1) / 2, f = max(z, h^2) ((z + 1)^2 / 4 - z = (z - 1)^2 / 4 >= 0) and f' = h:
+// min/max and multiply-adds only, no transcendental (the tanh of a GELU runs on the XU pipe, at 1/8 of
+// the FMA pipe's rate on this chip, and bound the face kernel with it).
+__device__ __forceinline__ float smelu_h(float z) { return 0.5f * fminf(fmaxf(z, -1.0f), 1.0f) + 0.5f; }
+__device__ __forceinline__ float smelu(float z) {
+    const float h = smelu_h(z);
+    return fmaxf(z, h * h);
 }
-// two GELUs packed as BF16x2 (low half = a), evaluated in BF16x2 arithmetic with the
-// PTX tanh.approx.bf16x2: the results are BF16 activations, so BF16 accuracy suffices
-__device__ __forceinline__ uint32_t gelu2_bf16(float a, float b) {
-    const __nv_bfloat162 z = __floats2bfloat162_rn(a, b);
-    const __nv_bfloat162 ca = __float2bfloat162_rn(kGeluC * kGeluA), c = __float2bfloat162_rn(kGeluC);
-    const __nv_bfloat162 half = __float2bfloat162_rn(0.5f);
-    const __nv_bfloat162 u = __hmul2(z, __hfma2(__hmul2(z, z), ca, c));  // c (z + a z^3)
-    uint32_t t2, in = *reinterpret_cast<const uint32_t *>(&u);
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t2) : "r"(in));
-    const __nv_bfloat162 t = *reinterpret_cast<const __nv_bfloat162 *>(&t2);
-    const __nv_bfloat162 hz = __hmul2(z, half);
-    const __nv_bfloat162 g = __hfma2(hz, t, hz);  // 0.5 z (1 + t)
-    return *reinterpret_cast<const uint32_t *>(&g);
+__device__ __forceinline__ float smelu_d(float z) { return smelu_h(z); }
+// two SmeLUs of accumulator + bias packed as BF16x2 (low half = a): the sums as one packed FP32
+// add, then BF16x2 arithmetic (h = min(relu(z/2 + 1/2), 1) in two instructions); the results
+// are BF16 activations, so BF16 accuracy suffices
+__device__ __forceinline__ uint32_t bias_smelu2_bf16(float a, float b, float ba, float bb) {
+    unsigned long long zab;
+    asm("add.rn.f32x2 %0, %1, %2;"
+        : "=l"(zab)
+        : "l"(((unsigned long long)__float_as_uint(b) << 32) | __float_as_uint(a)),
+          "l"(((unsigned long long)__float_as_uint(bb) << 32) | __float_as_uint(ba)));
+    const __nv_bfloat162 z = __floats2bfloat162_rn(__uint_as_float((unsigned)zab), __uint_as_float((unsigned)(zab >> 32)));
+    const __nv_bfloat162 one = __float2bfloat162_rn(1.0f), half = __float2bfloat162_rn(0.5f);
+    const __nv_bfloat162 h = __hmin2(__hfma2_relu(z, half, half), one);
+    const __nv_bfloat162 f = __hmax2(z, __hmul2(h, h));
+    return *reinterpret_cast<const uint32_t *>(&f);
 }
 
 // standardisation of the network's inputs and outputs, fitted on the training samples:
-// the network sees (x - xmu) / xsd and its output is multiplied by ysd
+// the network sees (x - xmu) * xisd (xisd = 1 / xsd) and its output is multiplied by ysd
 struct Scaling {
-    float xmu[kIn], xsd[kIn], ysd[kOut];
+    float xmu[kIn], xsd[kIn], ysd[kOut], xisd[kIn];
 };
 
 // device view of the trained network for inference inside the step

@@ -1,8 +1,8 @@
-// Learned face-flux surrogate: a 17 -> 128 -> 128 -> 128 -> 8 GELU MLP trained and run
+// Learned face-flux surrogate: a 17 -> 128 -> 128 -> 128 -> 8 SmeLU MLP trained and run
 // on sm_100a.  Every matrix product is a BF16 tcgen05 MMA with an FP32 accumulator in
 // tensor memory; operands are staged into shared memory by bulk copies from the blocked
 // K-major layout of nn_umma.cuh.  The forward products write the next layer's operands
-// (normal and transposed) and the GELU derivative from their epilogues; the backward
+// (normal and transposed) and the activation derivative from their epilogues; the backward
 // products fold that derivative and the bias-gradient sums into theirs; weight gradients
 // are batch-split products reduced by the Adam kernel.  No counterpart exists in the
 // reference, whose face solver is always exact (src/modules/solvers/solver.f90:163-187).
@@ -37,7 +37,7 @@ struct GemmArgs {
     int C;             // reduction columns per CTA
     const float *bias; // forward
     bf16 *Hn, *Ht;     // outputs: blocked normal [rows][128] and transposed [128][rows]
-    float *G;          // GELU derivative [rows][128]: written forward, read backward
+    float *G;          // activation derivative [rows][128]: written forward, read backward
     float *Y;          // network output [rows][8]
     float *part;       // weight-gradient partials [split][128][N] or bias partials [tile][128]
     long long rows;    // batch rows (row tiles x 128)
@@ -82,8 +82,8 @@ __device__ __forceinline__ void epilogue(const GemmArgs &g, uint32_t tmem, long 
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const float z = v[q] + g.bias[cc * 16 + q];
-                    v[q] = gelu(z);
-                    gd[q] = gelu_d(z);
+                    v[q] = smelu(z);
+                    gd[q] = smelu_d(z);
                 }
 #pragma unroll
                 for (int q = 0; q < 4; q++) ((float4 *)gp)[q] = make_float4(gd[4 * q], gd[4 * q + 1], gd[4 * q + 2], gd[4 * q + 3]);
@@ -212,7 +212,7 @@ __global__ void k_gather(const float *__restrict__ xs, const float *__restrict__
     for (int n = 0; n < kOut; n++) t[n] = 0.0f;
     if (idx < ns) {
 #pragma unroll
-        for (int n = 0; n < kIn; n++) x[n] = (xs[idx * kIn + n] - sc->xmu[n]) / sc->xsd[n];
+        for (int n = 0; n < kIn; n++) x[n] = (xs[idx * kIn + n] - sc->xmu[n]) * sc->xisd[n];
         if (ts) {
 #pragma unroll
             for (int n = 0; n < kOut; n++) t[n] = ts[idx * kOut + n] / sc->ysd[n];
@@ -531,7 +531,7 @@ int backward(dg_nn *n, long long rows, long long valid) {
     int cdn = kOutPad;
     for (int l = 2; l >= 0; l--) {
         bf16 *on = n->Dn[l & 1], *ot = n->Dt[l & 1];
-        {   // dZ_l = (dZ_{l+1} W_{l+1}^T) * gelu'(Z_l), bias partials of layer l
+        {   // dZ_l = (dZ_{l+1} W_{l+1}^T) * f'(Z_l), bias partials of layer l
             GemmArgs g{};
             g.A = dn; g.B = n->Wn[l + 1]; g.C = cdn; g.G = n->G[l]; g.Hn = on; g.Ht = ot; g.part = n->db[l];
             g.rows = rows; g.err = n->d_err;
@@ -640,7 +640,7 @@ int dg_nn_create(int device, unsigned long long seed, dg_nn **out) {
         if (cudaMemcpyAsync(n->W[l], w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, n->stream) != cudaSuccess)
             return bail(nn_fail(DG_ERR_CUDA, "weight upload failed"));
     }
-    for (int q = 0; q < kIn; q++) { n->sc.xmu[q] = 0.0f; n->sc.xsd[q] = 1.0f; }
+    for (int q = 0; q < kIn; q++) { n->sc.xmu[q] = 0.0f; n->sc.xsd[q] = 1.0f; n->sc.xisd[q] = 1.0f; }
     for (int q = 0; q < kOut; q++) n->sc.ysd[q] = 1.0f;
     if ((rc = nn_alloc_t(n, &n->d_sc, 1))) return bail(rc);
     if (cudaMemcpyAsync(n->d_sc, &n->sc, sizeof(Scaling), cudaMemcpyHostToDevice, n->stream) != cudaSuccess)
@@ -875,6 +875,7 @@ int dg_nn_fit_scaling(dg_nn *n) {
         const double mu = h[q] / N, var = std::max(h[kIn + kOut + q] / N - mu * mu, 0.0);
         n->sc.xmu[q] = (float)mu;
         n->sc.xsd[q] = var > 1e-12 ? (float)std::sqrt(var) : 1.0f;  // a constant input stays at zero
+        n->sc.xisd[q] = 1.0f / n->sc.xsd[q];
     }
     for (int q = 0; q < kOut; q++) {
         const double rms = std::sqrt(h[2 * kIn + kOut + q] / N);

@@ -580,7 +580,7 @@ __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128
 
 // Four warpgroups per CTA, each taking 128-face tiles in turn: the faces' interface states,
 // inputs and gates, the four layers as tcgen05 MMAs (weights resident in shared memory,
-// each warpgroup with its own 128 TMEM columns, activations through TMEM -> GELU -> shared
+// each warpgroup with its own 128 TMEM columns, activations through TMEM -> SmeLU -> shared
 // memory), then the gated flux or a mark for HLLD.
 __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *__restrict__ core,
                                                             float *__restrict__ flux, int *__restrict__ fallback,
@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
             nn::base_fluxes<float>(ql, qr, gamma, ciso, G.iso, base, dis);
         }
 #pragma unroll
-        for (int n = 0; n < nn::kIn; n++) x[n] = use ? (x[n] - nv.sc.xmu[n]) / nv.sc.xsd[n] : 0.0f;
+        for (int n = 0; n < nn::kIn; n++) x[n] = use ? (x[n] - nv.sc.xmu[n]) * nv.sc.xisd[n] : 0.0f;
 #pragma unroll
         for (int cg = 0; cg < nn::kInPad / 8; cg++) {
             __align__(16) bf16 h[8];
@@ -693,16 +693,16 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
                     for (int cc = 0; cc < nn::kHid / 32; cc++) {
                         float v[32];
                         nn::tmem_ld32(taddr + cc * 32, v);
+                        const float4 *bq = (const float4 *)(bias + l * nn::kHid + cc * 32);
 #pragma unroll
                         for (int hh = 0; hh < 4; hh++) {
-                            uint32_t h[4];
-#pragma unroll
-                            for (int q = 0; q < 4; q++) {
-                                const int c0 = cc * 32 + hh * 8 + 2 * q;
-                                h[q] = nn::gelu2_bf16(v[hh * 8 + 2 * q] + bias[l * nn::kHid + c0],
-                                                      v[hh * 8 + 2 * q + 1] + bias[l * nn::kHid + c0 + 1]);
-                            }
-                            *(uint4 *)(Hs + ((cc * 4 + hh) * 128 + wt) * 8) = make_uint4(h[0], h[1], h[2], h[3]);
+                            const float4 b0 = bq[2 * hh], b1 = bq[2 * hh + 1];
+                            const float *w = v + hh * 8;
+                            const uint32_t h0 = nn::bias_smelu2_bf16(w[0], w[1], b0.x, b0.y);
+                            const uint32_t h1 = nn::bias_smelu2_bf16(w[2], w[3], b0.z, b0.w);
+                            const uint32_t h2 = nn::bias_smelu2_bf16(w[4], w[5], b1.x, b1.y);
+                            const uint32_t h3 = nn::bias_smelu2_bf16(w[6], w[7], b1.z, b1.w);
+                            *(uint4 *)(Hs + ((cc * 4 + hh) * 128 + wt) * 8) = make_uint4(h0, h1, h2, h3);
                         }
                     }
                 }

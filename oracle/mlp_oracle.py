@@ -1,6 +1,6 @@
 """CPU oracle of the learned face-flux network (test infrastructure only).
 
-FP64 numpy forward and backward passes of the 17 -> 128 -> 128 -> 128 -> 8 GELU MLP
+FP64 numpy forward and backward passes of the 17 -> 128 -> 128 -> 128 -> 8 SmeLU MLP
 that the library trains on the GPU, with the mean-squared-error loss and the Adam
 update.  The GPU stores weights, activations and back-propagated errors in BF16 between
 its tensor-core products; with ``bf16=True`` this oracle rounds the same quantities at
@@ -43,17 +43,14 @@ def bf16(a: np.ndarray) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+def smelu(z: np.ndarray) -> np.ndarray:
+    """SmeLU with half-width 1 (Shamir et al. 2020), as the library uses it:
+    0 for z <= -1, (z + 1)^2 / 4 for |z| < 1, z for z >= 1."""
+    return np.where(z >= 1.0, z, np.where(z <= -1.0, 0.0, 0.25 * (z + 1.0) ** 2))
 
 
-def gelu(z: np.ndarray) -> np.ndarray:
-    """GELU in its tanh form, as the library uses it."""
-    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
-
-
-def gelu_d(z: np.ndarray) -> np.ndarray:
-    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
-    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
+def smelu_d(z: np.ndarray) -> np.ndarray:
+    return np.clip(0.5 * (z + 1.0), 0.0, 1.0)
 
 
 def forward(p: np.ndarray, x: np.ndarray, bf16_rounding: bool = True):
@@ -67,8 +64,8 @@ def forward(p: np.ndarray, x: np.ndarray, bf16_rounding: bool = True):
         cache["w"].append(wb)
         z = h @ wb + b
         if l < 3:
-            cache["gd"].append(gelu_d(z))
-            h = r(gelu(z))
+            cache["gd"].append(smelu_d(z))
+            h = r(smelu(z))
             cache["h"].append(h)
         else:
             y = z
