@@ -15,13 +15,20 @@
 
 namespace dg {
 
+// the square of the fast magnetosonic speed; the solvers that only need the largest of several
+// speeds take one square root of the largest square: sqrt is monotone and correctly rounded, so
+// sqrt(max(x)) is max(sqrt(x)) bit for bit (and the ternary max picks the same element either way)
 template <typename T>
-__device__ __forceinline__ T cfast(T gamma, T ploc, T rho, T a, T b, T c) {
+__device__ __forceinline__ T cfast2(T gamma, T ploc, T rho, T a, T b, T c) {
     const T half = T(0.5);
     T c2 = gamma * ploc / rho;
     T b2 = a * a + b * b + c * c;
     T d2 = half * (c2 + b2 / rho);
-    return sqr(d2 + sqr(d2 * d2 - c2 * a * a / rho));
+    return d2 + sqr(d2 * d2 - c2 * a * a / rho);
+}
+template <typename T>
+__device__ __forceinline__ T cfast(T gamma, T ploc, T rho, T a, T b, T c) {
+    return sqr(cfast2(gamma, ploc, rho, a, b, c));
 }
 
 // left/right physical fluxes and conserved states shared by llf, hll, upwind
@@ -80,11 +87,10 @@ template <typename T>
 __device__ void hll1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int iso) {
     T fl[8], cl[8], fr[8], cr[8], ploc, proc, a;
     lr_fluxes(ql, qr, gamma, ciso, iso, fl, cl, fr, cr, ploc, proc, a);
-    T vleft = cfast(gamma, ploc, ql[0], a, ql[5], ql[7]);
-    T vright = cfast(gamma, proc, qr[0], a, qr[5], qr[7]);
+    const T cfmax = sqr(mx(cfast2(gamma, ploc, ql[0], a, ql[5], ql[7]), cfast2(gamma, proc, qr[0], a, qr[5], qr[7])));
     T ul = ql[2], ur = qr[2];
-    T sl = mn(mn(ul, ur) - mx(vleft, vright), T(0));
-    T sr = mx(mx(ul, ur) + mx(vleft, vright), T(0));
+    T sl = mn(mn(ul, ur) - cfmax, T(0));
+    T sr = mx(mx(ul, ur) + cfmax, T(0));
     if constexpr (sizeof(T) == 4) {
         const T is = T(1) / (sr - sl);
 #pragma unroll
@@ -110,10 +116,13 @@ __device__ void upwind1d(const T *ql, const T *qr, T *f, T gamma, T ciso, int is
 // repeated divisor turned into one reciprocal (or reciprocal square root) and the
 // fast-speed discriminant clamped at zero against FP32 rounding.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float cfast_r(float gamma, float p, float irho, float a, float b, float c) {
+__device__ __forceinline__ float cfast2_r(float gamma, float p, float irho, float a, float b, float c) {
     const float c2 = gamma * p * irho;
     const float d2 = 0.5f * (c2 + (a * a + b * b + c * c) * irho);
-    return sqrtf(d2 + sqrtf(fmaxf(d2 * d2 - c2 * a * a * irho, 0.0f)));
+    return d2 + sqrtf(fmaxf(d2 * d2 - c2 * a * a * irho, 0.0f));
+}
+__device__ __forceinline__ float cfast_r(float gamma, float p, float irho, float a, float b, float c) {
+    return sqrtf(cfast2_r(gamma, p, irho, a, b, c));
 }
 
 __device__ __forceinline__ void hlld1d_f(const float *ql, const float *qr, float *f, float &pg, float gamma,
@@ -135,7 +144,7 @@ __device__ __forceinline__ void hlld1d_f(const float *ql, const float *qr, float
     const float etotr = proc * entho + half * (ur * ur + vr * vr + wr * wr) * rr + emagr;
     const float ptotr = proc + emagr;
     const float vdotbr = ur * a + vr * br + wr * cr;
-    const float cf = fmaxf(cfast_r(gamma, ploc, 1.0f / rl, a, bl, cl), cfast_r(gamma, proc, 1.0f / rr, a, br, cr));
+    const float cf = sqrtf(fmaxf(cfast2_r(gamma, ploc, 1.0f / rl, a, bl, cl), cfast2_r(gamma, proc, 1.0f / rr, a, br, cr)));
     const float sl = fminf(ul, ur) - cf;
     const float sr = fmaxf(ul, ur) + cf;
     const float rcl = rl * (ul - sl);
@@ -242,10 +251,9 @@ __device__ void hlld1d(const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso, i
     const T etotr = proc * entho + ecinr + emagr;
     const T ptotr = proc + emagr;
     const T vdotbr = ur * a + vr * br + wr * cr;
-    const T cfastl = cfast(gamma, ploc, rl, a, bl, cl);
-    const T cfastr = cfast(gamma, proc, rr, a, br, cr);
-    const T sl = mn(ul, ur) - mx(cfastl, cfastr);
-    const T sr = mx(ul, ur) + mx(cfastl, cfastr);
+    const T cfmax = sqr(mx(cfast2(gamma, ploc, rl, a, bl, cl), cfast2(gamma, proc, rr, a, br, cr)));
+    const T sl = mn(ul, ur) - cfmax;
+    const T sr = mx(ul, ur) + cfmax;
     const T rcl = rl * (ul - sl);
     const T rcr = rr * (sr - ur);
     const T ustar = (rcr * ur + rcl * ul + (ptotl - ptotr)) / (rcr + rcl);
@@ -369,10 +377,10 @@ __device__ T llf2d(const Corners<T> &c, T dt, T gamma, T ciso, int iso) {
 __device__ __forceinline__ float hlld2d_f(const Corners<float> &c, float dt, float gamma) {
     const float half = 0.5f, zero = 0.0f, smallc = (float)kSmallc;
     const float iLL = 1.0f / c.rLL, iLR = 1.0f / c.rLR, iRL = 1.0f / c.rRL, iRR = 1.0f / c.rRR;
-    const float cfx = mx4(cfast_r(gamma, c.pLL, iLL, c.ALL, c.BLL, c.CLL), cfast_r(gamma, c.pLR, iLR, c.ALR, c.BLR, c.CLR),
-                          cfast_r(gamma, c.pRL, iRL, c.ARL, c.BRL, c.CRL), cfast_r(gamma, c.pRR, iRR, c.ARR, c.BRR, c.CRR));
-    const float cfy = mx4(cfast_r(gamma, c.pLL, iLL, c.BLL, c.ALL, c.CLL), cfast_r(gamma, c.pLR, iLR, c.BLR, c.ALR, c.CLR),
-                          cfast_r(gamma, c.pRL, iRL, c.BRL, c.ARL, c.CRL), cfast_r(gamma, c.pRR, iRR, c.BRR, c.ARR, c.CRR));
+    const float cfx = sqrtf(mx4(cfast2_r(gamma, c.pLL, iLL, c.ALL, c.BLL, c.CLL), cfast2_r(gamma, c.pLR, iLR, c.ALR, c.BLR, c.CLR),
+                                cfast2_r(gamma, c.pRL, iRL, c.ARL, c.BRL, c.CRL), cfast2_r(gamma, c.pRR, iRR, c.ARR, c.BRR, c.CRR)));
+    const float cfy = sqrtf(mx4(cfast2_r(gamma, c.pLL, iLL, c.BLL, c.ALL, c.CLL), cfast2_r(gamma, c.pLR, iLR, c.BLR, c.ALR, c.CLR),
+                                cfast2_r(gamma, c.pRL, iRL, c.BRL, c.ARL, c.CRL), cfast2_r(gamma, c.pRR, iRR, c.BRR, c.ARR, c.CRR)));
     const float SL = mn4(c.uLL, c.uLR, c.uRL, c.uRR) - cfx;
     const float SR = mx4(c.uLL, c.uLR, c.uRL, c.uRR) + cfx;
     const float SB = mn4(c.vLL, c.vLR, c.vRL, c.vRR) - cfy;
@@ -448,18 +456,14 @@ template <typename T>
 __device__ T hlld2d(const Corners<T> &c, T dt, T gamma) {
     if constexpr (sizeof(T) == 4) return hlld2d_f(c, dt, gamma);
     const T one = T(1), half = T(0.5), zero = T(0), smallc = T(kSmallc);
-    const T cfastLLx = cfast(gamma, c.pLL, c.rLL, c.ALL, c.BLL, c.CLL);
-    const T cfastLRx = cfast(gamma, c.pLR, c.rLR, c.ALR, c.BLR, c.CLR);
-    const T cfastRLx = cfast(gamma, c.pRL, c.rRL, c.ARL, c.BRL, c.CRL);
-    const T cfastRRx = cfast(gamma, c.pRR, c.rRR, c.ARR, c.BRR, c.CRR);
-    const T cfastLLy = cfast(gamma, c.pLL, c.rLL, c.BLL, c.ALL, c.CLL);
-    const T cfastLRy = cfast(gamma, c.pLR, c.rLR, c.BLR, c.ALR, c.CLR);
-    const T cfastRLy = cfast(gamma, c.pRL, c.rRL, c.BRL, c.ARL, c.CRL);
-    const T cfastRRy = cfast(gamma, c.pRR, c.rRR, c.BRR, c.ARR, c.CRR);
-    const T SL = mn4(c.uLL, c.uLR, c.uRL, c.uRR) - mx4(cfastLLx, cfastLRx, cfastRLx, cfastRRx);
-    const T SR = mx4(c.uLL, c.uLR, c.uRL, c.uRR) + mx4(cfastLLx, cfastLRx, cfastRLx, cfastRRx);
-    const T SB = mn4(c.vLL, c.vLR, c.vRL, c.vRR) - mx4(cfastLLy, cfastLRy, cfastRLy, cfastRRy);
-    const T ST = mx4(c.vLL, c.vLR, c.vRL, c.vRR) + mx4(cfastLLy, cfastLRy, cfastRLy, cfastRRy);
+    const T cfx = sqr(mx4(cfast2(gamma, c.pLL, c.rLL, c.ALL, c.BLL, c.CLL), cfast2(gamma, c.pLR, c.rLR, c.ALR, c.BLR, c.CLR),
+                          cfast2(gamma, c.pRL, c.rRL, c.ARL, c.BRL, c.CRL), cfast2(gamma, c.pRR, c.rRR, c.ARR, c.BRR, c.CRR)));
+    const T cfy = sqr(mx4(cfast2(gamma, c.pLL, c.rLL, c.BLL, c.ALL, c.CLL), cfast2(gamma, c.pLR, c.rLR, c.BLR, c.ALR, c.CLR),
+                          cfast2(gamma, c.pRL, c.rRL, c.BRL, c.ARL, c.CRL), cfast2(gamma, c.pRR, c.rRR, c.BRR, c.ARR, c.CRR)));
+    const T SL = mn4(c.uLL, c.uLR, c.uRL, c.uRR) - cfx;
+    const T SR = mx4(c.uLL, c.uLR, c.uRL, c.uRR) + cfx;
+    const T SB = mn4(c.vLL, c.vLR, c.vRL, c.vRR) - cfy;
+    const T ST = mx4(c.vLL, c.vLR, c.vRL, c.vRR) + cfy;
     const T PtotLL = c.pLL + half * (c.ALL * c.ALL + c.BLL * c.BLL + c.CLL * c.CLL);
     const T PtotLR = c.pLR + half * (c.ALR * c.ALR + c.BLR * c.BLR + c.CLR * c.CLR);
     const T PtotRL = c.pRL + half * (c.ARL * c.ARL + c.BRL * c.BRL + c.CRL * c.CRL);
