@@ -30,6 +30,16 @@ template <typename T>
 __device__ __forceinline__ T cfast(T gamma, T ploc, T rho, T a, T b, T c) {
     return sqr(cfast2(gamma, ploc, rho, a, b, c));
 }
+// the same from b2 = a^2 + b^2 + c^2 computed by the caller: the x and y speeds of an edge
+// corner sum the same three squares in two orders, (A^2 + B^2) + C^2 and (B^2 + A^2) + C^2,
+// which are equal (IEEE addition commutes), so one b2 / rho serves both
+template <typename T>
+__device__ __forceinline__ T cfast2_b2(T gamma, T ploc, T rho, T a, T b2) {
+    const T half = T(0.5);
+    T c2 = gamma * ploc / rho;
+    T d2 = half * (c2 + b2 / rho);
+    return d2 + sqr(d2 * d2 - c2 * a * a / rho);
+}
 
 // left/right physical fluxes and conserved states shared by llf, hll, upwind
 template <typename T>
@@ -456,10 +466,12 @@ template <typename T>
 __device__ T hlld2d(const Corners<T> &c, T dt, T gamma) {
     if constexpr (sizeof(T) == 4) return hlld2d_f(c, dt, gamma);
     const T one = T(1), half = T(0.5), zero = T(0), smallc = T(kSmallc);
-    const T cfx = sqr(mx4(cfast2(gamma, c.pLL, c.rLL, c.ALL, c.BLL, c.CLL), cfast2(gamma, c.pLR, c.rLR, c.ALR, c.BLR, c.CLR),
-                          cfast2(gamma, c.pRL, c.rRL, c.ARL, c.BRL, c.CRL), cfast2(gamma, c.pRR, c.rRR, c.ARR, c.BRR, c.CRR)));
-    const T cfy = sqr(mx4(cfast2(gamma, c.pLL, c.rLL, c.BLL, c.ALL, c.CLL), cfast2(gamma, c.pLR, c.rLR, c.BLR, c.ALR, c.CLR),
-                          cfast2(gamma, c.pRL, c.rRL, c.BRL, c.ARL, c.CRL), cfast2(gamma, c.pRR, c.rRR, c.BRR, c.ARR, c.CRR)));
+    const T b2LL = c.ALL * c.ALL + c.BLL * c.BLL + c.CLL * c.CLL, b2LR = c.ALR * c.ALR + c.BLR * c.BLR + c.CLR * c.CLR;
+    const T b2RL = c.ARL * c.ARL + c.BRL * c.BRL + c.CRL * c.CRL, b2RR = c.ARR * c.ARR + c.BRR * c.BRR + c.CRR * c.CRR;
+    const T cfx = sqr(mx4(cfast2_b2(gamma, c.pLL, c.rLL, c.ALL, b2LL), cfast2_b2(gamma, c.pLR, c.rLR, c.ALR, b2LR),
+                          cfast2_b2(gamma, c.pRL, c.rRL, c.ARL, b2RL), cfast2_b2(gamma, c.pRR, c.rRR, c.ARR, b2RR)));
+    const T cfy = sqr(mx4(cfast2_b2(gamma, c.pLL, c.rLL, c.BLL, b2LL), cfast2_b2(gamma, c.pLR, c.rLR, c.BLR, b2LR),
+                          cfast2_b2(gamma, c.pRL, c.rRL, c.BRL, b2RL), cfast2_b2(gamma, c.pRR, c.rRR, c.BRR, b2RR)));
     const T SL = mn4(c.uLL, c.uLR, c.uRL, c.uRR) - cfx;
     const T SR = mx4(c.uLL, c.uLR, c.uRL, c.uRR) + cfx;
     const T SB = mn4(c.vLL, c.vLR, c.vRL, c.vRR) - cfy;
