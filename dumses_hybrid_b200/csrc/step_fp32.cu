@@ -849,7 +849,11 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         faces = 0;
     }
     if (G.ndim == 3) {
-        TIMED(KS_RIEMANN, s, (k_riemann3d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
+        // HLLD/HLLD (the reference's default and every benchmark) runs a kernel without the other solvers
+        if (G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD)
+            TIMED(KS_RIEMANN, s, (k_riemann3d<float, true><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
+        else
+            TIMED(KS_RIEMANN, s, (k_riemann3d<float, false><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
     } else {
         TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, faces)));
     }

@@ -751,10 +751,15 @@ __device__ __forceinline__ void corner_state(const CoreView<T> &cv, long long c,
     }
 }
 
-// the 1D solver for one interface (solver.f90:163-187)
-template <typename T>
+// the 1D solver for one interface (solver.f90:163-187); kHLLD: HLLD fixed at compile time, so
+// a kernel for the HLLD/HLLD configuration carries no code of the other solvers
+template <typename T, bool kHLLD = false>
 __device__ __forceinline__ void solve1d(int iriemann, const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso,
                                         int iso) {
+    if constexpr (kHLLD) {
+        hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso);
+        return;
+    }
     switch (iriemann) {
         case DG_RIEMANN_HLLD: hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso); break;
         case DG_RIEMANN_HLL: hll1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
@@ -837,18 +842,18 @@ __device__ __forceinline__ void flux_store(const Geo &G, const T *ql, const T *q
 
 // one face flux in direction d between cells cl (minus side) and cr (plus side);
 // writes the compflux-scaled fluxes in uin order plus p*_T (solver.f90:116-262, scheme.f90:1740-1753)
-template <typename T>
+template <typename T, bool kHLLD = false>
 __device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d, int i, double dtd,
                           T *__restrict__ out, long long fo) {
     T ql[8], qr[8];
     face_io(G, cv, cl, cr, d, ql, qr);
     T f[8], pg = T(0);
-    solve1d<T>(G.iriemann, ql, qr, f, pg, (T)G.gamma, (T)G.ciso, G.iso);
+    solve1d<T, kHLLD>(G.iriemann, ql, qr, f, pg, (T)G.gamma, (T)G.ciso, G.iso);
     flux_store(G, ql, qr, f, pg, d, i, dtd, out, fo);
 }
 
 // one edge EMF (riemann_solver_magnetic, solver_magnetic.f90:79-230); e = edge direction
-template <typename T>
+template <typename T, bool kHLLD = false>
 __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long long cRL, long long cLR, long long cRR,
                       int e, int i, double dtd) {
     const T half = T(0.5);
@@ -912,7 +917,8 @@ __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long l
     c.pRR = qRR[1]; c.vRR = qRR[3]; c.BRR = qRR[5]; c.ERR = qRR[7];
     const T dt = (T)dtd, gamma = (T)G.gamma;
     T emf;
-    switch (G.iriemann2d) {
+    if constexpr (kHLLD) emf = hlld2d<T>(c, dt, gamma);
+    else switch (G.iriemann2d) {
         case DG_RIEMANN_HLLD: emf = hlld2d<T>(c, dt, gamma); break;
         case DG_RIEMANN_LLF: emf = llf2d<T>(c, dt, gamma, (T)G.ciso, G.iso); break;
         case DG_RIEMANN_HLLA: emf = hlla2d<T>(c, dt); break;
@@ -932,7 +938,7 @@ __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long l
     return emf;
 }
 
-template <typename T>
+template <typename T, bool kHLLD>
 __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 : DG_RIEMANN_MINB32)) k_riemann3d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                            T *__restrict__ fy, T *__restrict__ fz, T *__restrict__ ex,
                                                            T *__restrict__ ey, T *__restrict__ ez, const Scalars *S,
@@ -948,13 +954,16 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const long long c = G.cidx(i, j, k);
     if (faces) {  // faces = 0: the face fluxes come from the learned flux and its HLLD fallback list
-        if (j <= ny && k <= nz) face_flux(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
-        if (i <= nx && k <= nz) face_flux(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
-        if (i <= nx && j <= ny) face_flux(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
+        if (j <= ny && k <= nz) face_flux<T, kHLLD>(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
+        if (i <= nx && k <= nz) face_flux<T, kHLLD>(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
+        if (i <= nx && j <= ny) face_flux<T, kHLLD>(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
     }
-    if (k <= nz) ez[t] = edge_emf(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
-    if (j <= ny) ey[t] = edge_emf(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
-    if (i <= nx) ex[t] = edge_emf(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
+    if (k <= nz)
+        ez[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
+    if (j <= ny)
+        ey[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
+    if (i <= nx)
+        ex[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
 }
 
 template <typename T>
