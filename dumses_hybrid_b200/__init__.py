@@ -134,6 +134,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_nn_fit_scaling": (ctypes.c_int, [vp]),
         "dg_nn_set_gates": (ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
         "dg_attach_surrogate": (ctypes.c_int, [vp, vp]),
+        "dg_wait_selftest": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, dp]),
         "dg_surrogate_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     }
     for name, (res, args) in sig.items():

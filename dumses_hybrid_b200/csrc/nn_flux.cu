@@ -6,6 +6,9 @@
 // products fold that derivative and the bias-gradient sums into theirs; weight gradients
 // are batch-split products reduced by the Adam kernel.  No counterpart exists in the
 // reference, whose face solver is always exact (src/modules/solvers/solver.f90:163-187).
+#include <chrono>
+#include <cstdlib>
+#include <thread>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -433,8 +436,23 @@ int nn_alloc(dg_nn *n, void **p, size_t bytes) {
 }
 template <typename X> int nn_alloc_t(dg_nn *n, X **p, size_t count) { return nn_alloc(n, (void **)p, count * sizeof(X)); }
 
+// wait for a stream with a wall-clock bound (DG_SYNC_TIMEOUT_S, default 300 s)
+int nn_bounded_sync(cudaStream_t st) {
+    const char *e = std::getenv("DG_SYNC_TIMEOUT_S");
+    const double limit = (e && std::atof(e) > 0) ? std::atof(e) : 300.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaStreamQuery(st);
+        if (q == cudaSuccess) return 0;
+        if (q != cudaErrorNotReady) return nn_fail(DG_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(q));
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > limit) return nn_fail(DG_ERR_TIMEOUT, "device work did not finish within DG_SYNC_TIMEOUT_S");
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 5 : 200));
+    }
+}
+
 int nn_sync(dg_nn *n) {
-    NN_CUDA(cudaStreamSynchronize(n->stream));
+    if (int rc = nn_bounded_sync(n->stream)) return rc;
     int err = 0;
     NN_CUDA(cudaMemcpy(&err, n->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return nn_fail(DG_ERR_STATE, "network kernel gave up waiting on a tensor-core transfer (error bits " +
@@ -590,7 +608,50 @@ int check_batch(long long batch) {
 }
 }  // namespace
 
+namespace {
+// one block waiting on an mbarrier with the library's bounded wait; one thread arrives on it
+// (arrive = 1) or nothing does (arrive = 0), so the wait completes or runs out its time
+__global__ void k_wait_selftest(int arrive, int *err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (arrive && threadIdx.x == 0) mbar_arrive(&bar);
+    if (!mbar_wait(&bar, 0)) atomicOr(err, NN_ERR_WAIT);
+}
+}  // namespace
+
 extern "C" {
+
+int dg_wait_selftest(int device, int arrive, double *seconds) {
+    if (cudaSetDevice(device) != cudaSuccess) return nn_fail(DG_ERR_NODEVICE, "no CUDA device");
+    int *d_err = nullptr;
+    NN_CUDA(cudaMalloc(&d_err, sizeof(int)));
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaFree(d_err);
+        return nn_fail(DG_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    int rc = 0, err = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess) rc = nn_fail(DG_ERR_CUDA, "cudaMemsetAsync failed");
+    if (!rc) {
+        k_wait_selftest<<<1, 32, 0, st>>>(arrive, d_err);
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) rc = nn_fail(DG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(le));
+    }
+    if (!rc) rc = nn_bounded_sync(st);
+    if (!rc && cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = nn_fail(DG_ERR_CUDA, "cudaMemcpy failed");
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    cudaStreamDestroy(st);
+    cudaFree(d_err);
+    if (rc) return rc;
+    if (err) return nn_fail(DG_ERR_TIMEOUT, "an mbarrier wait ran out of its time bound");
+    return DG_OK;
+}
 
 long long dg_nn_param_count(void) {
     long long n = 0;

@@ -1,6 +1,6 @@
 // sm_100a building blocks of the flux-surrogate network: BF16 tcgen05 MMAs with FP32
 // accumulators in tensor memory, operands staged in shared memory by bulk copies, and
-// mbarrier waits that give up after a bounded number of polls.
+// mbarrier waits that give up after a bounded time.
 //
 // Operand layout ("blocked K-major"): a matrix X with R rows and C reduction columns
 // (C a multiple of 8) is stored as [R / RT][C / 8][RT][8] BF16, RT = min(R, 128) rows
@@ -18,7 +18,7 @@ namespace dg {
 namespace nn {
 
 constexpr int kTileRows = 128;               // rows per tcgen05 tile (cta_group::1, M = 128)
-constexpr unsigned kWaitPolls = 1u << 26;    // upper bound on mbarrier polls (about a second or more)
+constexpr unsigned long long kWaitNs = 1000000000ull;  // an mbarrier wait gives up after 1 s (%globaltimer)
 
 // error bits written to the network's device error word
 enum { NN_ERR_WAIT = 1 };
@@ -35,10 +35,19 @@ __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
-// poll the phase with the given parity; false when the poll limit ran out
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// poll the phase with the given parity; false when kWaitNs ran out first
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
     const uint32_t a = smem_addr(bar);
-    for (unsigned n = 0; n < kWaitPolls; n++) {
+    const unsigned long long t0 = global_ns();
+    for (unsigned n = 1;; n++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -48,8 +57,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((n & 255) == 0 && global_ns() - t0 > kWaitNs) return false;
     }
-    return false;
 }
 
 // ---- bulk copy global -> shared (contiguous, 16-byte aligned, size % 16 == 0) -----

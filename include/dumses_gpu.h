@@ -199,6 +199,13 @@ int  dg_profile(dg_ctx *ctx, int on);
 int  dg_profile_read(dg_ctx *ctx, double *ms, long long *count, int nslots);
 const char *dg_profile_slot_name(int slot);
 
+/* Self-test of the bounded device-side waits: one block waits on an mbarrier with the
+ * wait every tensor-core kernel of the library uses (1 s bound on %globaltimer).  With
+ * arrive = 1 a thread arrives and the call returns DG_OK; with arrive = 0 nothing
+ * arrives, the wait runs out and the call returns DG_ERR_TIMEOUT after about a second,
+ * the device staying usable.  *seconds (may be NULL) receives the elapsed wall time. */
+int  dg_wait_selftest(int device, int arrive, double *seconds);
+
 /* number of kernels the library launched on this context since dg_init */
 long long dg_kernel_launches(const dg_ctx *ctx);
 
