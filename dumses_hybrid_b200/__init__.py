@@ -25,6 +25,7 @@ calls raise.
 from __future__ import annotations
 
 import ctypes
+import os
 import pathlib
 import re
 from dataclasses import dataclass
@@ -32,7 +33,8 @@ from dataclasses import dataclass
 import numpy as np
 
 PKG = pathlib.Path(__file__).resolve().parent
-LIB_PATH = PKG / "libdumses_gpu.so"
+# DG_LIBRARY selects another build of the library, e.g. the bounds-checked libdumses_gpu_chk.so
+LIB_PATH = pathlib.Path(os.environ["DG_LIBRARY"]) if os.environ.get("DG_LIBRARY") else PKG / "libdumses_gpu.so"
 
 DG_OK = 0
 ERRORS = {-1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -4: "DG_ERR_TIMEOUT", -5: "DG_ERR_STATE",
@@ -135,6 +137,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_nn_set_gates": (ctypes.c_int, [vp, ctypes.c_float, ctypes.c_float]),
         "dg_attach_surrogate": (ctypes.c_int, [vp, vp]),
         "dg_wait_selftest": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, dp]),
+        "dg_debug_oob_count": (ctypes.c_longlong, []),
         "dg_surrogate_stats": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     }
     for name, (res, args) in sig.items():

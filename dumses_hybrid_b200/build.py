@@ -5,8 +5,12 @@ nvcc compiles each CUDA translation unit with
 plus --fmad=false for the FP64 path and the host code (no multiply-add
 contraction: the FP64 path is bit-identical to the CPU reference arithmetic)
 and --use_fast_math for the FP32 mixed path, and links them, with the host-side initial conditions,
-into dumses_hybrid_b200/libdumses_gpu.so against the static CUDA runtime.
-Objects are rebuilt only when a source or header is newer than the library.
+into dumses_hybrid_b200/libdumses_gpu.so against the static CUDA runtime.  A second
+library, libdumses_gpu_chk.so, is the same with the step kernels compiled with
+-DDG_CHECK_BOUNDS: every array access of the step kernels checked against the registered
+device buffers (a debug stand-in for a memory sanitizer, used by the tests).
+Everything is rebuilt, translation units in parallel, when a source or header is newer than
+a library.
 
 Usage: python -m dumses_hybrid_b200.build [--force] [--verbose]
 """
@@ -34,6 +38,8 @@ FAST = ["--use_fast_math"]
 CU_SOURCES = {"step_fp64.cu": EXACT, "step_fp32.cu": FAST, "dg_api.cu": EXACT, "dg_noalloc.cu": EXACT,
               "nn_flux.cu": FAST}
 CXX_SOURCES = ["condinit.cpp"]
+LIB_CHK = PKG / "libdumses_gpu_chk.so"
+CHECKED_SOURCES = ("step_fp64.cu", "step_fp32.cu")  # compiled again with -DDG_CHECK_BOUNDS
 
 
 def _nvcc() -> str:
@@ -67,24 +73,34 @@ def _run(cmd: list[str], verbose: bool) -> None:
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> pathlib.Path:
-    if LIB.exists() and not force and LIB.stat().st_mtime >= _newest_input():
+    newest = _newest_input()
+    if (not force and LIB.exists() and LIB_CHK.exists() and LIB.stat().st_mtime >= newest
+            and LIB_CHK.stat().st_mtime >= newest):
         return LIB
     BUILD.mkdir(exist_ok=True)
     nvcc, cxx = _nvcc(), _cxx()
-    objs = []
+    jobs = {}  # object -> command
     for src, flags in CU_SOURCES.items():
-        obj = BUILD / (src + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_info else []
-        _run([nvcc, *NVCC_FLAGS, *flags, *extra, "-c", str(CSRC / src), "-o", str(obj)], verbose or ptxas_info)
-        objs.append(str(obj))
+        jobs[BUILD / (src + ".o")] = [nvcc, *NVCC_FLAGS, *flags, *extra, "-c", str(CSRC / src), "-o", str(BUILD / (src + ".o"))]
+        if src in CHECKED_SOURCES:
+            obj = BUILD / (src + ".chk.o")
+            jobs[obj] = [nvcc, *NVCC_FLAGS, *flags, "-DDG_CHECK_BOUNDS", "-c", str(CSRC / src), "-o", str(obj)]
     for src in CXX_SOURCES:
         obj = BUILD / (src + ".o")
-        _run([cxx, "-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-I", str(INCLUDE), "-c", str(CSRC / src),
-              "-o", str(obj)], verbose)
-        objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
-    _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", *objs, "-o", str(tmp)], verbose)
-    tmp.replace(LIB)
+        jobs[obj] = [cxx, "-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-I", str(INCLUDE), "-c", str(CSRC / src),
+                     "-o", str(obj)]
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, cmd, verbose or ptxas_info) for cmd in jobs.values()]:
+            f.result()
+    plain = [BUILD / (src + ".o") for src in CU_SOURCES] + [BUILD / (src + ".o") for src in CXX_SOURCES]
+    checked = [BUILD / (src + (".chk.o" if src in CHECKED_SOURCES else ".o")) for src in CU_SOURCES] + \
+              [BUILD / (src + ".o") for src in CXX_SOURCES]
+    for lib, objs in ((LIB, plain), (LIB_CHK, checked)):
+        tmp = lib.with_suffix(".so.tmp")
+        _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)], verbose)
+        tmp.replace(lib)
     return LIB
 
 

@@ -90,6 +90,7 @@ struct dg_ctx {
     dg::Scalars *h_scal = nullptr;  // pinned read-back of the device scalars
     double *h_hist = nullptr;       // pinned read-back of history sums
     size_t bytes = 0;
+    std::vector<std::pair<void *, size_t>> allocations;  // every device buffer, for the checked build
     EventTimer *timer = nullptr;    // non-null while per-kernel profiling is on
     long long version = 0;          // bumped by every call that changes the device state
     long long q_version = -1;       // state version whose primitive variables the FP32 CFL pass left in Q
@@ -253,6 +254,7 @@ int alloc_bytes(dg_ctx *c, void **p, size_t b) {
         return fail(DG_ERR_NOMEM, std::string("cudaMalloc of ") + std::to_string(b) + " bytes: " + cudaGetErrorString(e));
     }
     c->bytes += b;
+    c->allocations.emplace_back(*p, b);
     DG_CUDA(cudaMemsetAsync(*p, 0, b, c->stream));
     return DG_OK;
 }
@@ -357,6 +359,10 @@ int dg_init(const dg_params *p, dg_ctx **out) {
         cudaMallocHost((void **)&c->h_hist, 16 * sizeof(double)) != cudaSuccess)
         return bail(fail(DG_ERR_NOMEM, "cudaMallocHost failed"));
     if ((rc = bounded_sync(c->stream))) return bail(rc);
+    for (auto &a : c->allocations) {  // no-ops unless the library is the bounds-checked build
+        dg::f64::debug_register(a.first, a.second, 1);
+        dg::f32::debug_register(a.first, a.second, 1);
+    }
     *out = c;
     return DG_OK;
 }
@@ -364,6 +370,10 @@ int dg_init(const dg_params *p, dg_ctx **out) {
 int dg_finalize(dg_ctx *c) {
     if (!c) return DG_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &a : c->allocations) {
+        dg::f64::debug_register(a.first, a.second, 0);
+        dg::f32::debug_register(a.first, a.second, 0);
+    }
     void *bufs[] = {c->B.U[0], c->B.U[1], c->B.Q, c->B.core, c->B.flx[0], c->B.flx[1], c->B.flx[2], c->B.emf[0],
                     c->B.emf[1], c->B.emf[2], c->B.femf[0], c->B.femf[1], c->B.part, c->B.hist,
                     c->B.E[0], c->B.E[1], c->B.E[2], c->B.stage, c->B.fb_list[0], c->B.fb_list[1], c->B.fb_list[2],
@@ -740,6 +750,11 @@ int dg_history(dg_ctx *c, double out[9]) {
     if ((rc = bounded_sync(c->stream))) return rc;
     std::memcpy(out, c->h_hist, 9 * sizeof(double));
     return DG_OK;
+}
+
+long long dg_debug_oob_count(void) {
+    const long long a = dg::f64::debug_oob(), b = dg::f32::debug_oob();
+    return (a < 0 || b < 0) ? -1 : a + b;
 }
 
 int dg_sync(dg_ctx *c) {

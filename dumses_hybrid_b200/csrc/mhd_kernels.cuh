@@ -60,7 +60,10 @@ extern thread_local KernelTimer *g_timer;  // set by the context that enqueues (
     int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t st); /* in place, then boundary */ \
     int launch_right_faces(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t st);      \
     int launch_state_to_f64(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t st);     \
-    int launch_f64_to_state(const Geo &G, const Bufs &B, int b, const double *in, int nv, cudaStream_t st);
+    int launch_f64_to_state(const Geo &G, const Bufs &B, int b, const double *in, int nv, cudaStream_t st); \
+    /* bounds-checked build: add (add = 1) or remove a device buffer; accesses outside all of them */ \
+    int debug_register(const void *p, size_t bytes, int add);                                        \
+    long long debug_oob(); /* -1 in a normal build */
 
 namespace f64 {
 DG_DECLARE_LAUNCHES

@@ -25,6 +25,7 @@ __device__ __forceinline__ void apply(const StoreHL &U, const StoreHL &Un, const
 // the same on a pair loaded beforehand: a kernel loads every pair it updates before its
 // first store, since the compiler cannot move a load of U across a store to Un
 __device__ __forceinline__ void put(const StoreHL &Un, const Geo &G, int v, long long c, float h, float l, float inc) {
+    if (!chk(Un.hi + G.sv * v + c, 4) || !chk(Un.lo + G.sv * v + c, 4)) return;
     add_hl(h, l, inc);
     Un.hi[G.sv * v + c] = h;
     Un.lo[G.sv * v + c] = l;
@@ -56,8 +57,8 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
     float uh[8], ul[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) {
-        uh[v] = U.hi[G.sv * v + c];
-        ul[v] = U.lo[G.sv * v + c];
+        uh[v] = ld(U.hi + G.sv * v + c);
+        ul[v] = ld(U.lo + G.sv * v + c);
     }
 
     if (i <= nx && j <= ny && k <= nz) {
@@ -480,6 +481,7 @@ __global__ void __launch_bounds__(kThreads, DG_FARGO_MINB32) k_fargo_update_hl(G
                 HL a0 = wn[m + 1];
                 add_hl(a0.h, a0.l, hl_diff(wn[m + 2], wn[m + 1]) * w + (s0 - s1) * q);
                 const long long c = G.idx(i, j, k);
+                if (!chk(Un.hi + G.sv * v + c, 4) || !chk(Un.lo + G.sv * v + c, 4)) continue;
                 Un.hi[G.sv * v + c] = a0.h;
                 Un.lo[G.sv * v + c] = a0.l;
                 s0 = s1;
@@ -967,6 +969,8 @@ int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     TIMED(KS_HISTORY, s, (k_hist_final<<<1, 32, 0, s>>>(G, B.part + 2 * G.nx, nb, B.hist)));
     return 3;
 }
+
+#include "debug_bounds.cuh"
 
 }  // namespace f32
 }  // namespace dg

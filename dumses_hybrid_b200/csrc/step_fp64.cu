@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
     const double one = 1.0, two = 2.0, half = 0.5;
     const long long sv = G.sv;
     const long long c = G.idx(i, j, k);
+    if (!chk(Un + c, 8) || !chk(Un + sv * IC + c, 8)) return;  // the planes this thread writes
     const bool shear = G.shearing != 0;
     ShearRemap sr{0.0, 0};
     if (shear) sr = ShearRemap{S->sh_epsi, S->sh_jp};  // time + dt/2, from k_shear_offset
@@ -334,6 +335,8 @@ int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
 int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     return launch_history_ptrs(G, (const double *)B.U[cur], B.part, B.hist, s);
 }
+
+#include "debug_bounds.cuh"
 
 }  // namespace f64
 }  // namespace dg

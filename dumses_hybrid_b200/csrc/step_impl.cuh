@@ -26,6 +26,9 @@
 //   k_fargo_*     fargo_update (fargo.f90:17-288)
 //   k_boundary    boundary (boundary.f90:18-92) incl. shearing_boundary (shearingbox.f90:19-203)
 #pragma once
+#include <utility>
+#include <vector>
+
 #include "mhd_kernels.cuh"
 #include "solvers.cuh"
 
@@ -39,14 +42,43 @@ namespace {
 
 constexpr int kThreads = 128;
 
-template <typename X> __device__ __forceinline__ X ld(const X *p) { return __ldg(p); }
+// Checked build (-DDG_CHECK_BOUNDS, a debug stand-in for a memory sanitizer): every array
+// access made through ld(), the record helpers below and the state stores must fall inside
+// a device buffer the host registered (debug_register: all buffers of every live context);
+// an access outside is counted in g_oob and not made (a load returns 0).
+#ifdef DG_CHECK_BOUNDS
+constexpr int kMaxBufs = 256;
+__device__ const char *g_buf_lo[kMaxBufs];
+__device__ const char *g_buf_hi[kMaxBufs];
+__device__ int g_nbuf;
+__device__ unsigned long long g_oob;
+__device__ __forceinline__ bool chk(const void *p, size_t n) {
+    const char *c = (const char *)p;
+    for (int b = 0; b < g_nbuf; b++)
+        if (c >= g_buf_lo[b] && c + n <= g_buf_hi[b]) return true;
+    atomicAdd(&g_oob, 1ull);
+    return false;
+}
+#else
+__device__ __forceinline__ bool chk(const void *, size_t) { return true; }
+#endif
+
+template <typename X> __device__ __forceinline__ X ld(const X *p) { return chk(p, sizeof(X)) ? __ldg(p) : X(0); }
 
 // 8 contiguous values (one face record) with 16-byte vector accesses
 __device__ __forceinline__ void load8(const float *p, float v[8]) {
+    if (!chk(p, 8 * sizeof(float))) {
+        for (int n = 0; n < 8; n++) v[n] = 0.0f;
+        return;
+    }
     const float4 a = __ldg((const float4 *)p), b = __ldg((const float4 *)p + 1);
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
 }
 __device__ __forceinline__ void load8(const double *p, double v[8]) {
+    if (!chk(p, 8 * sizeof(double))) {
+        for (int n = 0; n < 8; n++) v[n] = 0.0;
+        return;
+    }
 #pragma unroll
     for (int n = 0; n < 4; n++) {
         const double2 a = __ldg((const double2 *)p + n);
@@ -54,15 +86,21 @@ __device__ __forceinline__ void load8(const double *p, double v[8]) {
     }
 }
 __device__ __forceinline__ void store8(float *p, const float v[8]) {
+    if (!chk(p, 8 * sizeof(float))) return;
     ((float4 *)p)[0] = make_float4(v[0], v[1], v[2], v[3]);
     ((float4 *)p)[1] = make_float4(v[4], v[5], v[6], v[7]);
 }
 __device__ __forceinline__ void store8(double *p, const double v[8]) {
+    if (!chk(p, 8 * sizeof(double))) return;
 #pragma unroll
     for (int n = 0; n < 4; n++) ((double2 *)p)[n] = make_double2(v[2 * n], v[2 * n + 1]);
 }
 // 6 contiguous values (a 3D face record) with 8-byte (float) / 16-byte (double) vector accesses
 __device__ __forceinline__ void load6(const float *p, float v[6]) {
+    if (!chk(p, 6 * sizeof(float))) {
+        for (int n = 0; n < 6; n++) v[n] = 0.0f;
+        return;
+    }
 #pragma unroll
     for (int n = 0; n < 3; n++) {
         const float2 a = __ldg((const float2 *)p + n);
@@ -70,6 +108,10 @@ __device__ __forceinline__ void load6(const float *p, float v[6]) {
     }
 }
 __device__ __forceinline__ void load6(const double *p, double v[6]) {
+    if (!chk(p, 6 * sizeof(double))) {
+        for (int n = 0; n < 6; n++) v[n] = 0.0;
+        return;
+    }
 #pragma unroll
     for (int n = 0; n < 3; n++) {
         const double2 a = __ldg((const double2 *)p + n);
@@ -77,10 +119,12 @@ __device__ __forceinline__ void load6(const double *p, double v[6]) {
     }
 }
 __device__ __forceinline__ void store6(float *p, const float v[6]) {
+    if (!chk(p, 6 * sizeof(float))) return;
 #pragma unroll
     for (int n = 0; n < 3; n++) ((float2 *)p)[n] = make_float2(v[2 * n], v[2 * n + 1]);
 }
 __device__ __forceinline__ void store6(double *p, const double v[6]) {
+    if (!chk(p, 6 * sizeof(double))) return;
 #pragma unroll
     for (int n = 0; n < 3; n++) ((double2 *)p)[n] = make_double2(v[2 * n], v[2 * n + 1]);
 }
@@ -94,18 +138,22 @@ inline unsigned nblocks(long long n, int threads) { return (unsigned)((n + threa
 struct StoreD {
     using T = double;  // arithmetic of the kernels on this state
     double *p;
-    __device__ __forceinline__ double get(const Geo &G, int v, long long c) const { return p[G.sv * v + c]; }
+    __device__ __forceinline__ double get(const Geo &G, int v, long long c) const {
+        return chk(p + G.sv * v + c, 8) ? p[G.sv * v + c] : 0.0;
+    }
     __device__ __forceinline__ double getr(const Geo &G, int v, long long c) const { return ld(p + G.sv * v + c); }
-    __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const { p[G.sv * v + c] = x; }
+    __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const {
+        if (chk(p + G.sv * v + c, 8)) p[G.sv * v + c] = x;
+    }
     // u = u + inc, the reference's in-place update; Val holds a value between a load and
     // a store so that a sequence of increments runs in registers
     using Val = double;
     __device__ __forceinline__ void add(const Geo &G, int v, long long c, double inc) const {
-        p[G.sv * v + c] = p[G.sv * v + c] + inc;
+        if (chk(p + G.sv * v + c, 8)) p[G.sv * v + c] = p[G.sv * v + c] + inc;
     }
-    __device__ __forceinline__ Val load(const Geo &G, int v, long long c) const { return p[G.sv * v + c]; }
+    __device__ __forceinline__ Val load(const Geo &G, int v, long long c) const { return get(G, v, c); }
     __device__ __forceinline__ static void inc(Val &x, double d) { x = x + d; }
-    __device__ __forceinline__ void store(const Geo &G, int v, long long c, Val x) const { p[G.sv * v + c] = x; }
+    __device__ __forceinline__ void store(const Geo &G, int v, long long c, Val x) const { set(G, v, c, x); }
     __device__ __forceinline__ const double *faces() const { return p; }
 };
 
@@ -127,17 +175,20 @@ struct StoreHL {
     using T = float;
     float *hi, *lo;
     __device__ __forceinline__ double get(const Geo &G, int v, long long c) const {
+        if (!chk(hi + G.sv * v + c, 4) || !chk(lo + G.sv * v + c, 4)) return 0.0;
         return (double)hi[G.sv * v + c] + (double)lo[G.sv * v + c];
     }
     __device__ __forceinline__ double getr(const Geo &G, int v, long long c) const {
         return (double)ld(hi + G.sv * v + c) + (double)ld(lo + G.sv * v + c);
     }
     __device__ __forceinline__ void set(const Geo &G, int v, long long c, double x) const {
+        if (!chk(hi + G.sv * v + c, 4) || !chk(lo + G.sv * v + c, 4)) return;
         const float h = (float)x;
         hi[G.sv * v + c] = h;
         lo[G.sv * v + c] = (float)(x - (double)h);
     }
     __device__ __forceinline__ void add(const Geo &G, int v, long long c, float inc) const {
+        if (!chk(hi + G.sv * v + c, 4) || !chk(lo + G.sv * v + c, 4)) return;
         float h = hi[G.sv * v + c], l = lo[G.sv * v + c];
         add_hl(h, l, inc);
         hi[G.sv * v + c] = h;
@@ -147,10 +198,12 @@ struct StoreHL {
         float h, l;
     };
     __device__ __forceinline__ Val load(const Geo &G, int v, long long c) const {
+        if (!chk(hi + G.sv * v + c, 4) || !chk(lo + G.sv * v + c, 4)) return Val{0.0f, 0.0f};
         return Val{hi[G.sv * v + c], lo[G.sv * v + c]};
     }
     __device__ __forceinline__ static void inc(Val &x, float d) { add_hl(x.h, x.l, d); }
     __device__ __forceinline__ void store(const Geo &G, int v, long long c, Val x) const {
+        if (!chk(hi + G.sv * v + c, 4) || !chk(lo + G.sv * v + c, 4)) return;
         hi[G.sv * v + c] = x.h;
         lo[G.sv * v + c] = x.l;
     }
@@ -558,6 +611,7 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
 
     T *o = core + core_base(t, kCore3);
     const int cs = kCoreLane;
+    if (!chk(o, ((kCore3 - 1) * cs + 1) * sizeof(T))) return;
     o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
     o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
     o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
@@ -624,6 +678,7 @@ __global__ void __launch_bounds__(kThreads) k_trace2d(Geo G, const T *__restrict
 
     T *o = core + core_base(t, kCore2);
     const int cs = kCoreLane;
+    if (!chk(o, ((kCore2 - 1) * cs + 1) * sizeof(T))) return;
     o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
     o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
     o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;

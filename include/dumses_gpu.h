@@ -206,6 +206,11 @@ const char *dg_profile_slot_name(int slot);
  * the device staying usable.  *seconds (may be NULL) receives the elapsed wall time. */
 int  dg_wait_selftest(int device, int arrive, double *seconds);
 
+/* Accesses of the step kernels that fell outside every registered device buffer, since
+ * the library was loaded, in the bounds-checked build (libdumses_gpu_chk.so, compiled with
+ * -DDG_CHECK_BOUNDS, where such an access is counted and not made); -1 in the normal build. */
+long long dg_debug_oob_count(void);
+
 /* number of kernels the library launched on this context since dg_init */
 long long dg_kernel_launches(const dg_ctx *ctx);
 
