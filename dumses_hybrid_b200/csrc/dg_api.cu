@@ -93,7 +93,7 @@ struct dg_ctx {
     std::vector<std::pair<void *, size_t>> allocations;  // every device buffer, for the checked build
     EventTimer *timer = nullptr;    // non-null while per-kernel profiling is on
     long long version = 0;          // bumped by every call that changes the device state
-    long long q_version = -1;       // state version whose primitive variables the FP32 CFL pass left in Q
+    long long q_version = -1;       // state version whose primitive variables the CFL pass left in Q
     dg_nn *nn = nullptr;            // attached flux network (surrogate = 1)
     dg::nn::NetView view{};         // its device view, as of dg_attach_surrogate
 };
@@ -427,6 +427,7 @@ int dg_download(dg_ctx *c, double *uin) {
     if (c->p.precision == DG_PREC_FP64) {
         DG_CUDA(cudaMemcpyAsync(uin, c->B.U[c->cur], nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         scratch = (double *)c->B.Q;  // 8 planes of doubles, recomputed by every step
+        c->q_version = -1;           // no longer the primitive variables of the CFL pass
     } else {
         c->launches += c->L->to_f64(c->G, c->B, c->cur, c->B.stage, c->stream);
         DG_CUDA(cudaMemcpyAsync(uin, c->B.stage, nt * 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -573,6 +574,7 @@ int dg_dump_write(dg_ctx *c, const char *path, double time, double dt) {
     if (c->p.precision == DG_PREC_FP64) {
         left = (const double *)c->B.U[c->cur];
         scratch = (double *)c->B.Q;
+        c->q_version = -1;  // Q is scratch here: a following godunov recomputes the primitives
     } else {
         // the staging buffer: its planes 0-2 take vars 9-11 once vars 1-8 are copied out
         c->launches += c->L->to_f64(c->G, c->B, c->cur, c->B.stage, c->stream);
@@ -660,7 +662,7 @@ int dg_compute_dt(dg_ctx *c, double *dt) {
     TimerScope ts_(c);
     if (!c || !dt) return fail(DG_ERR_ARG, "null argument");
     c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
-    if (c->p.precision == DG_PREC_FP32) c->q_version = c->version;
+    c->q_version = c->version;  // the CFL pass also left primitive(0) of this state in Q
     int rc = check_launch();
     if (rc) return rc;
     if ((rc = read_scalars(c))) return rc;
@@ -717,7 +719,7 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
     c->launches += c->L->set_scalars(c->B, 0.0, *time, 0, 1, c->stream);
     for (int n = 0; n < nsteps; n++) {
         c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
-        c->B.q_fresh = (c->p.precision == DG_PREC_FP32);
+        c->B.q_fresh = 1;  // Q holds primitive(0) of this state from the CFL pass
         c->launches += c->L->godunov(c->G, c->B, c->cur, c->stream);
         c->cur ^= 1;
         if (c->p.fargo) {

@@ -224,14 +224,26 @@ int launch_advance_time(const Bufs &B, cudaStream_t s) {
     return 1;
 }
 
+// compute_dt; the pass also leaves primitive(0) in Q for the godunov that follows (B.q_fresh)
 int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     TIMED(KS_DT, s, (k_dt_reset<<<1, 1, 0, s>>>(G, B.S)));
-    const long long n = (long long)G.nx * G.ny * G.nz;
-    long long nb = (n + kThreads - 1) / kThreads;
-    if (nb > 148 * 16) nb = 148 * 16;
-    TIMED(KS_DT, s, (k_dt<StoreD><<<(unsigned)nb, kThreads, 0, s>>>(G, st(B, cur), B.S)));
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    TIMED(KS_DT, s, (k_prim_dt<StoreD><<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, st(B, cur), (double *)B.Q, B.S)));
     TIMED(KS_DT, s, (k_dt_final<<<1, 1, 0, s>>>(G, B.S)));
     return 3;
+}
+
+// the rotation half-kick of primitive(dt) on Q = primitive(0), as prim_cell applies it
+// (scheme.f90:78-85): one thread per element of the velocity planes
+__global__ void __launch_bounds__(kThreads) k_kick64(Geo G, double *__restrict__ Q, const Scalars *S) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= G.sv) return;
+    const double half = 0.5, two = 2.0, dt = S->dt;
+    const double u = Q[G.sv * IU + c], v = Q[G.sv * IV + c];
+    const double dvx = two * G.omega0 * v;
+    const double dvy = -(half * G.omega0 * u);
+    Q[G.sv * IU + c] = u + dvx * dt * half;
+    Q[G.sv * IV + c] = v + dvy * dt * half;
 }
 
 int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
@@ -242,7 +254,14 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     double *fx = (double *)B.flx[0], *fy = (double *)B.flx[1], *fz = (double *)B.flx[2];
     double *ex = (double *)B.emf[0], *ey = (double *)B.emf[1], *ez = (double *)B.emf[2];
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
-    TIMED(KS_PRIM, s, (k_prim<double, StoreD><<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+    int n = 4 + (G.shearing ? 1 : 0);
+    if (!B.q_fresh) {
+        TIMED(KS_PRIM, s, (k_prim<double, StoreD><<<nblocks((long long)ni * nj * nk, kThreads), kThreads, 0, s>>>(G, U, Q, B.S)));
+        n++;
+    } else if (G.omega0 > 0.0) {  // Q = primitive(0) of this state from launch_dt: add the half-kick
+        TIMED(KS_PRIM, s, (k_kick64<<<nblocks(G.sv, kThreads), kThreads, 0, s>>>(G, Q, B.S)));
+        n++;
+    }
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
@@ -259,7 +278,7 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         TIMED(KS_RIEMANN, s, (k_riemann2d<double><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, 1)));
         TIMED(KS_UPDATE, s, (k_update2d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, ez, B.S)));
     }
-    return 5 + (G.shearing ? 1 : 0);
+    return n;
 }
 
 int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {

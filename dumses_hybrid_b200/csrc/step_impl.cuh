@@ -9,7 +9,7 @@
 //                     CFL reduction, FARGO's remap and the history sums.
 //
 // Pipeline of one step (the call order of src/dumses.f90:82-120):
-//   k_dt          compute_dt  (physics.f90:18-132)      primitive + CFL min-reduction
+//   k_prim_dt     compute_dt  (physics.f90:18-132)      primitive(0) into Q + CFL min-reduction
 //   k_prim        primitive   (scheme.f90:20-91)        Q on the ghosted grid
 //   k_efield      edge E of trace3d/trace2d (scheme.f90:1194-1239, 856-872), once per edge
 //   k_trace       slope + trace3d/trace2d (scheme.f90:253-656, 807-1711)
@@ -275,39 +275,51 @@ __device__ __forceinline__ double comp_speed(double gamma, double rho, double p,
     return cf + fabs(v);
 }
 
-// compute_dt reduction over the active cells (physics.f90:42-121), FP64 in both paths
+// compute_dt (physics.f90:42-121) fused with the primitive variables of the next godunov
+// (FP64 path): one pass over the ghosted grid writes Q = primitive(0) (prim_cell with dt = 0,
+// no rotation half-kick) and reduces the CFL time step over the active cells; the
+// half-kick of primitive(dt) (scheme.f90:78-85) is added once dt is known (k_kick64), to the
+// same unkicked values in the same order, so Q ends as primitive(dt) bit for bit
 template <class Store>
-__global__ void __launch_bounds__(kThreads) k_dt(Geo G, Store U, Scalars *S) {
-    const long long n = (long long)G.nx * G.ny * G.nz;
+__global__ void __launch_bounds__(kThreads) k_prim_dt(Geo G, Store U, double *__restrict__ Q, Scalars *S) {
+    const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
+    const long long n = (long long)ni * nj * nk;
     double best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
     int bad = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(t % G.nx) + 1;
-        long long r = t / G.nx;
-        int j = (int)(r % G.ny) + 1;
-        int k = (int)(r / G.ny) + 1;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < n) {
+        const int i = (int)(t % ni) - 2;
+        const long long r = t / ni;
+        const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
+        const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+        const long long c = G.idx(i, j, k);
         double q[8];
-        prim_cell(G, U, G.idx(i, j, k), 0.0, q);
-        double velx = comp_speed(G.gamma, q[IR], q[IP], q[IU], q[IA], q[IB], q[IC]);
-        if (G.nx == 1) velx = 0.0;
-        double vely = comp_speed(G.gamma, q[IR], q[IP], q[IV], q[IB], q[IC], q[IA]);
-        if ((G.omega0 > 0.0) && !G.fargo) vely = vely + 1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5;
-        if (G.ny == 1) vely = 0.0;
-        double c;
-        if (G.ndim == 3) {
-            double velz = comp_speed(G.gamma, q[IR], q[IP], q[IW], q[IC], q[IA], q[IB]);
-            if (G.nz == 1) velz = 0.0;
-            c = 1.0 / (velx / G.dx + vely / G.dy + velz / G.dz);
-        } else {
-            c = 1.0 / (velx / G.dx + vely / G.dy);
+        prim_cell(G, U, c, 0.0, q);
+        if (chk(Q + c, 8) && chk(Q + G.sv * 7 + c, 8)) {
+#pragma unroll
+            for (int v = 0; v < 8; v++) Q[G.sv * v + c] = q[v];
         }
-        if (!(c > 0.0)) bad = 1;  // NaN or non-positive
-        else best = mn(best, c);
+        if (i >= 1 && i <= G.nx && j >= 1 && j <= G.ny && k >= 1 && k <= G.nz) {
+            double velx = comp_speed(G.gamma, q[IR], q[IP], q[IU], q[IA], q[IB], q[IC]);
+            if (G.nx == 1) velx = 0.0;
+            double vely = comp_speed(G.gamma, q[IR], q[IP], q[IV], q[IB], q[IC], q[IA]);
+            if ((G.omega0 > 0.0) && !G.fargo) vely = vely + 1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5;
+            if (G.ny == 1) vely = 0.0;
+            double cdt;
+            if (G.ndim == 3) {
+                double velz = comp_speed(G.gamma, q[IR], q[IP], q[IW], q[IC], q[IA], q[IB]);
+                if (G.nz == 1) velz = 0.0;
+                cdt = 1.0 / (velx / G.dx + vely / G.dy + velz / G.dz);
+            } else {
+                cdt = 1.0 / (velx / G.dx + vely / G.dy);
+            }
+            if (!(cdt > 0.0)) bad = 1;  // NaN or non-positive
+            else best = mn(best, cdt);
+        }
     }
-    // warp then block minimum on the bit patterns (positive doubles order as integers)
     unsigned long long b = (unsigned long long)__double_as_longlong(best);
     for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
         b = ob < b ? ob : b;
     }
     __shared__ unsigned long long sb[kThreads / 32];
@@ -317,7 +329,8 @@ __global__ void __launch_bounds__(kThreads) k_dt(Geo G, Store U, Scalars *S) {
     if (threadIdx.x == 0) {
         unsigned long long m = sb[0];
         for (int w = 1; w < kThreads / 32; w++) m = sb[w] < m ? sb[w] : m;
-        atomicMin(&S->red, m);
+        // one block per 128 cells: skip the atomic when the running minimum is already smaller
+        if (m < *(volatile unsigned long long *)&S->red) atomicMin(&S->red, m);
     }
 }
 
