@@ -213,3 +213,28 @@ def test_field_loop_full_run_to_t2():
         ug = g.download()
     assert t_g == t_o and n > 100
     compare_states(ug, o.uin, p)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_state_reads_between_dt_and_godunov(tmp_path, precision):
+    """compute_dt leaves the primitive variables for godunov; a download or a dump in between
+    (both use that buffer as scratch in FP64) must not change the step's result."""
+    p = Params(**{**MRI_FARGO.__dict__, "precision": precision})
+    u0 = condinit(p, "mri", beta=1000.0, amp=0.1, seed=5)
+    out = []
+    for interleave in (False, True):
+        with Context(p) as g:
+            g.upload(u0)
+            g.boundary(0.0, 0.0)
+            t = 0.0
+            for _ in range(3):
+                dt = g.compute_dt()
+                if interleave:
+                    g.download()
+                    g.dump(tmp_path / "d.bin", t, dt)
+                g.godunov(dt, t)
+                g.fargo_update(dt)
+                g.boundary(t, dt)
+                t += dt
+            out.append(g.download())
+    assert np.array_equal(out[0], out[1])
