@@ -135,94 +135,92 @@ __device__ __forceinline__ float cfast_r(float gamma, float p, float irho, float
     return sqrtf(cfast2_r(gamma, p, irho, a, b, c));
 }
 
+// packed FP32 (sm_100 FADD2 / FMUL2 / FFMA2: two lanes per instruction) for the mirrored
+// left / right arithmetic of the solvers: x = left, y = right
+__device__ __forceinline__ float2 p2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 s2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
 __device__ __forceinline__ void hlld1d_f(const float *ql, const float *qr, float *f, float &pg, float gamma,
                                          float ciso, int iso) {
     const float half = 0.5f, zero = 0.0f;
-    const float rl = ql[0], ul = ql[2], vl = ql[4], bl = ql[5], wl = ql[6], cl = ql[7];
-    const float rr = qr[0], ur = qr[2], vr = qr[4], br = qr[5], wr = qr[6], cr = qr[7];
+    const float2 r = p2(ql[0], qr[0]), u = p2(ql[2], qr[2]), v = p2(ql[4], qr[4]), b = p2(ql[5], qr[5]);
+    const float2 w = p2(ql[6], qr[6]), c = p2(ql[7], qr[7]);
     const float entho = 1.0f / (gamma - 1.0f);
     const float a = half * (ql[3] + qr[3]);
+    const float aa = a * a;
     const float sgnm = copysignf(1.0f, a);
-    float ploc, proc;
-    if (iso) { ploc = rl * (ciso * ciso); proc = rr * (ciso * ciso); }
-    else { ploc = ql[1]; proc = qr[1]; }
-    const float emagl = half * (a * a + bl * bl + cl * cl);
-    const float etotl = ploc * entho + half * (ul * ul + vl * vl + wl * wl) * rl + emagl;
-    const float ptotl = ploc + emagl;
-    const float vdotbl = ul * a + vl * bl + wl * cl;
-    const float emagr = half * (a * a + br * br + cr * cr);
-    const float etotr = proc * entho + half * (ur * ur + vr * vr + wr * wr) * rr + emagr;
-    const float ptotr = proc + emagr;
-    const float vdotbr = ur * a + vr * br + wr * cr;
-    const float cf = sqrtf(fmaxf(cfast2_r(gamma, ploc, 1.0f / rl, a, bl, cl), cfast2_r(gamma, proc, 1.0f / rr, a, br, cr)));
-    const float sl = fminf(ul, ur) - cf;
-    const float sr = fmaxf(ul, ur) + cf;
-    const float rcl = rl * (ul - sl);
-    const float rcr = rr * (sr - ur);
-    const float irc = 1.0f / (rcr + rcl);
-    const float ustar = (rcr * ur + rcl * ul + (ptotl - ptotr)) * irc;
-    const float ptotstar = (rcr * ptotl + rcl * ptotr + rcl * rcr * (ul - ur)) * irc;
-    // left star region
-    const float isl = 1.0f / (sl - ustar);
-    const float rstarl = rl * (sl - ul) * isl;
-    float estar = rl * (sl - ul) * (sl - ustar) - a * a;
-    const float el = rl * (sl - ul) * (sl - ul) - a * a;
-    float vstarl = vl, bstarl = bl, wstarl = wl, cstarl = cl;
-    if (estar != zero) {
-        const float ie = 1.0f / estar;
-        vstarl = vl - a * bl * (ustar - ul) * ie;
-        bstarl = bl * el * ie;
-        wstarl = wl - a * cl * (ustar - ul) * ie;
-        cstarl = cl * el * ie;
-    }
-    const float vdotbstarl = ustar * a + vstarl * bstarl + wstarl * cstarl;
-    const float etotstarl = ((sl - ul) * etotl - ptotl * ul + ptotstar * ustar + a * (vdotbl - vdotbstarl)) * isl;
-    const float rsl = rsqrtf(rstarl);
-    const float sqrrstarl = rstarl * rsl;
-    const float sal = ustar - fabsf(a) * rsl;
-    // right star region
-    const float isr = 1.0f / (sr - ustar);
-    const float rstarr = rr * (sr - ur) * isr;
-    estar = rr * (sr - ur) * (sr - ustar) - a * a;
-    const float er = rr * (sr - ur) * (sr - ur) - a * a;
-    float vstarr = vr, bstarr = br, wstarr = wr, cstarr = cr;
-    if (estar != zero) {
-        const float ie = 1.0f / estar;
-        vstarr = vr - a * br * (ustar - ur) * ie;
-        bstarr = br * er * ie;
-        wstarr = wr - a * cr * (ustar - ur) * ie;
-        cstarr = cr * er * ie;
-    }
-    const float vdotbstarr = ustar * a + vstarr * bstarr + wstarr * cstarr;
-    const float etotstarr = ((sr - ur) * etotr - ptotr * ur + ptotstar * ustar + a * (vdotbr - vdotbstarr)) * isr;
-    const float rsr = rsqrtf(rstarr);
-    const float sqrrstarr = rstarr * rsr;
-    const float sar = ustar + fabsf(a) * rsr;
+    const float2 p = iso ? mul2(r, s2(ciso * ciso)) : p2(ql[1], qr[1]);
+    const float2 bsum = fma2(b, b, fma2(c, c, s2(aa)));  // a^2 + b^2 + c^2
+    const float2 emag = mul2(s2(half), bsum);
+    const float2 ke = fma2(u, u, fma2(v, v, mul2(w, w)));
+    const float2 etot = fma2(p, s2(entho), fma2(mul2(s2(half), ke), r, emag));
+    const float2 ptot = add2(p, emag);
+    const float2 vdotb = fma2(u, s2(a), fma2(v, b, mul2(w, c)));
+    // fast speeds (cfast2_r of each side), one square root of the larger
+    const float2 irho = p2(1.0f / r.x, 1.0f / r.y);
+    const float2 c2 = mul2(mul2(s2(gamma), p), irho);
+    const float2 d2 = mul2(s2(half), fma2(bsum, irho, c2));
+    const float2 disc = fma2(neg2(mul2(c2, s2(aa))), irho, mul2(d2, d2));
+    const float cf = sqrtf(fmaxf(d2.x + sqrtf(fmaxf(disc.x, 0.0f)), d2.y + sqrtf(fmaxf(disc.y, 0.0f))));
+    const float sl = fminf(u.x, u.y) - cf;
+    const float sr = fmaxf(u.x, u.y) + cf;
+    const float2 S = p2(sl, sr);
+    const float2 Su = sub2(S, u);                     // (sl - ul, sr - ur)
+    const float2 rSu = mul2(r, Su);
+    const float2 rc = mul2(rSu, p2(-1.0f, 1.0f));     // (rl (ul - sl), rr (sr - ur))
+    const float irc = 1.0f / (rc.y + rc.x);
+    const float ustar = (rc.y * u.y + rc.x * u.x + (ptot.x - ptot.y)) * irc;
+    const float ptotstar = (rc.y * ptot.x + rc.x * ptot.y + rc.x * rc.y * (u.x - u.y)) * irc;
+    // single-star regions, left (x) and right (y)
+    const float2 Sus = sub2(S, s2(ustar));
+    const float2 is = p2(1.0f / Sus.x, 1.0f / Sus.y);
+    const float2 rstar = mul2(rSu, is);
+    const float2 estar = fma2(rSu, Sus, s2(-aa));
+    const float2 e = fma2(rSu, Su, s2(-aa));
+    const float2 ie = p2(estar.x != zero ? 1.0f / estar.x : zero, estar.y != zero ? 1.0f / estar.y : zero);
+    const float2 adu_ie = mul2(mul2(s2(a), sub2(s2(ustar), u)), ie);
+    const float2 eie = mul2(e, ie);
+    float2 vstar = sub2(v, mul2(b, adu_ie)), wstar = sub2(w, mul2(c, adu_ie));
+    float2 bstar = mul2(b, eie), cstar = mul2(c, eie);
+    if (estar.x == zero) { vstar.x = v.x; bstar.x = b.x; wstar.x = w.x; cstar.x = c.x; }
+    if (estar.y == zero) { vstar.y = v.y; bstar.y = b.y; wstar.y = w.y; cstar.y = c.y; }
+    const float2 vdotbstar = fma2(s2(ustar), s2(a), fma2(vstar, bstar, mul2(wstar, cstar)));
+    const float2 etotstar = mul2(fma2(Su, etot, fma2(neg2(ptot), u, fma2(s2(ptotstar), s2(ustar),
+                                                                            mul2(s2(a), sub2(vdotb, vdotbstar))))), is);
+    const float2 rs = p2(rsqrtf(rstar.x), rsqrtf(rstar.y));
+    const float2 sqrr = mul2(rstar, rs);
+    const float sal = ustar - fabsf(a) * rs.x;
+    const float sar = ustar + fabsf(a) * rs.y;
     // double star region
-    const float isum = 1.0f / (sqrrstarl + sqrrstarr);
-    const float vstarstar = (sqrrstarl * vstarl + sqrrstarr * vstarr + sgnm * (bstarr - bstarl)) * isum;
-    const float wstarstar = (sqrrstarl * wstarl + sqrrstarr * wstarr + sgnm * (cstarr - cstarl)) * isum;
-    const float bstarstar = (sqrrstarl * bstarr + sqrrstarr * bstarl + sgnm * sqrrstarl * sqrrstarr * (vstarr - vstarl)) * isum;
-    const float cstarstar = (sqrrstarl * cstarr + sqrrstarr * cstarl + sgnm * sqrrstarl * sqrrstarr * (wstarr - wstarl)) * isum;
+    const float isum = 1.0f / (sqrr.x + sqrr.y);
+    const float vstarstar = (sqrr.x * vstar.x + sqrr.y * vstar.y + sgnm * (bstar.y - bstar.x)) * isum;
+    const float wstarstar = (sqrr.x * wstar.x + sqrr.y * wstar.y + sgnm * (cstar.y - cstar.x)) * isum;
+    const float bstarstar = (sqrr.x * bstar.y + sqrr.y * bstar.x + sgnm * sqrr.x * sqrr.y * (vstar.y - vstar.x)) * isum;
+    const float cstarstar = (sqrr.x * cstar.y + sqrr.y * cstar.x + sgnm * sqrr.x * sqrr.y * (wstar.y - wstar.x)) * isum;
     const float vdotbstarstar = ustar * a + vstarstar * bstarstar + wstarstar * cstarstar;
     // sample at x/t = 0
     float ro, uo, vo, wo, bo, co, ptoto, etoto, vdotbo;
     if (sl > zero) {
-        ro = rl; uo = ul; vo = vl; wo = wl; bo = bl; co = cl; ptoto = ptotl; etoto = etotl; vdotbo = vdotbl;
+        ro = r.x; uo = u.x; vo = v.x; wo = w.x; bo = b.x; co = c.x; ptoto = ptot.x; etoto = etot.x; vdotbo = vdotb.x;
     } else if (sal > zero) {
-        ro = rstarl; uo = ustar; vo = vstarl; wo = wstarl; bo = bstarl; co = cstarl;
-        ptoto = ptotstar; etoto = etotstarl; vdotbo = vdotbstarl;
+        ro = rstar.x; uo = ustar; vo = vstar.x; wo = wstar.x; bo = bstar.x; co = cstar.x;
+        ptoto = ptotstar; etoto = etotstar.x; vdotbo = vdotbstar.x;
     } else if (ustar > zero) {
-        ro = rstarl; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
-        ptoto = ptotstar; etoto = etotstarl - sgnm * sqrrstarl * (vdotbstarl - vdotbstarstar); vdotbo = vdotbstarstar;
+        ro = rstar.x; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
+        ptoto = ptotstar; etoto = etotstar.x - sgnm * sqrr.x * (vdotbstar.x - vdotbstarstar); vdotbo = vdotbstarstar;
     } else if (sar > zero) {
-        ro = rstarr; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
-        ptoto = ptotstar; etoto = etotstarr + sgnm * sqrrstarr * (vdotbstarr - vdotbstarstar); vdotbo = vdotbstarstar;
+        ro = rstar.y; uo = ustar; vo = vstarstar; wo = wstarstar; bo = bstarstar; co = cstarstar;
+        ptoto = ptotstar; etoto = etotstar.y + sgnm * sqrr.y * (vdotbstar.y - vdotbstarstar); vdotbo = vdotbstarstar;
     } else if (sr > zero) {
-        ro = rstarr; uo = ustar; vo = vstarr; wo = wstarr; bo = bstarr; co = cstarr;
-        ptoto = ptotstar; etoto = etotstarr; vdotbo = vdotbstarr;
+        ro = rstar.y; uo = ustar; vo = vstar.y; wo = wstar.y; bo = bstar.y; co = cstar.y;
+        ptoto = ptotstar; etoto = etotstar.y; vdotbo = vdotbstar.y;
     } else {
-        ro = rr; uo = ur; vo = vr; wo = wr; bo = br; co = cr; ptoto = ptotr; etoto = etotr; vdotbo = vdotbr;
+        ro = r.y; uo = u.y; vo = v.y; wo = w.y; bo = b.y; co = c.y; ptoto = ptot.y; etoto = etot.y; vdotbo = vdotb.y;
     }
     f[0] = ro * uo;
     f[1] = (etoto + ptoto) * uo - a * vdotbo;
