@@ -261,50 +261,10 @@ __global__ void __launch_bounds__(kThreads) k_prim_hl(Geo G, StoreHL U, float *_
     for (int v = 0; v < 8; v++) Q[G.sv * v + c] = q[v];
 }
 
-// compute_dt (physics.f90:42-121): FP32 signal speeds from prim_hl, the minimum of
-// the per-cell time steps taken in FP64 on their bit patterns
-__global__ void __launch_bounds__(kThreads) k_dt_hl(Geo G, StoreHL U, Scalars *S) {
-    const long long n = (long long)G.nx * G.ny * G.nz;
-    const float gamma = (float)G.gamma;
-    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
-    const float vsh = ((G.omega0 > 0.0) && !G.fargo) ? (float)(1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5) : 0.0f;
-    float best = __int_as_float(0x7f800000);  // +inf
-    int bad = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % G.nx) + 1;
-        const long long r = t / G.nx;
-        const int j = (int)(r % G.ny) + 1;
-        const int k = (int)(r / G.ny) + 1;
-        float q[8];
-        prim_hl(G, U, G.idx(i, j, k), q);
-        const float ir = 1.0f / q[IR];
-        float sum = 0.0f;
-        if (G.nx != 1) sum += (cfast_r(gamma, q[IP], ir, q[IA], q[IB], q[IC]) + fabsf(q[IU])) * rdx;
-        if (G.ny != 1) sum += (cfast_r(gamma, q[IP], ir, q[IB], q[IC], q[IA]) + fabsf(q[IV]) + vsh) * rdy;
-        if (G.ndim == 3 && G.nz != 1) sum += (cfast_r(gamma, q[IP], ir, q[IC], q[IA], q[IB]) + fabsf(q[IW])) * rdz;
-        const float cdt = 1.0f / sum;
-        if (!(cdt > 0.0f)) bad = 1;  // NaN or non-positive
-        else best = fminf(best, cdt);
-    }
-    unsigned long long b = (unsigned long long)__double_as_longlong((double)best);
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
-        b = ob < b ? ob : b;
-    }
-    __shared__ unsigned long long sb[kThreads / 32];
-    if ((threadIdx.x & 31) == 0) sb[threadIdx.x >> 5] = b;
-    if (bad) S->err = DG_ERR_STATE;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long m = sb[0];
-        for (int w = 1; w < kThreads / 32; w++) m = sb[w] < m ? sb[w] : m;
-        atomicMin(&S->red, m);
-    }
-}
-
 // compute_dt fused with the primitive variables of the next godunov: one pass over the
 // ghosted grid writes Q without the rotation half-kick (prim_hl) and reduces the CFL time
-// step over the active cells as k_dt_hl does; k_kick adds the half-kick once dt is known
+// step over the active cells (FP32 signal speeds from prim_hl, the minimum of the per-cell
+// time steps taken on their bit patterns); k_kick adds the half-kick once dt is known
 __global__ void __launch_bounds__(kThreads) k_prim_dt_hl(Geo G, StoreHL U, float *__restrict__ Q, Scalars *S) {
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
     const long long n = (long long)ni * nj * nk;
