@@ -168,16 +168,11 @@ __device__ __forceinline__ float smelu(float z) {
     return fmaxf(z, h * h);
 }
 __device__ __forceinline__ float smelu_d(float z) { return smelu_h(z); }
-// two SmeLUs of accumulator + bias packed as BF16x2 (low half = a): the sums as one packed FP32
-// add, then BF16x2 arithmetic (h = min(relu(z/2 + 1/2), 1) in two instructions); the results
-// are BF16 activations, so BF16 accuracy suffices
-__device__ __forceinline__ uint32_t bias_smelu2_bf16(float a, float b, float ba, float bb) {
-    unsigned long long zab;
-    asm("add.rn.f32x2 %0, %1, %2;"
-        : "=l"(zab)
-        : "l"(((unsigned long long)__float_as_uint(b) << 32) | __float_as_uint(a)),
-          "l"(((unsigned long long)__float_as_uint(bb) << 32) | __float_as_uint(ba)));
-    const __nv_bfloat162 z = __floats2bfloat162_rn(__uint_as_float((unsigned)zab), __uint_as_float((unsigned)(zab >> 32)));
+// two SmeLUs of pre-activations (accumulators that already hold the bias) packed as BF16x2
+// (low half = a): one conversion, then BF16x2 arithmetic (h = min(relu(z/2 + 1/2), 1) in two
+// instructions); the results are BF16 activations, so BF16 accuracy suffices
+__device__ __forceinline__ uint32_t smelu2_bf16(float a, float b) {
+    const __nv_bfloat162 z = __floats2bfloat162_rn(a, b);
     const __nv_bfloat162 one = __float2bfloat162_rn(1.0f), half = __float2bfloat162_rn(0.5f);
     const __nv_bfloat162 h = __hmin2(__hfma2_relu(z, half, half), one);
     const __nv_bfloat162 f = __hmax2(z, __hmul2(h, h));
@@ -190,9 +185,21 @@ struct Scaling {
     float xmu[kIn], xsd[kIn], ysd[kOut], xisd[kIn];
 };
 
+// The hidden layers' biases as one extra K = 16 step of their MMAs in the face kernel: a B
+// operand [kHid][kBiasK] (blocked K-major) holding each bias split in two BF16 parts,
+// column 0 = bf16(b), column 1 = bf16(b - column 0), the other columns zero, multiplied by
+// an A operand whose columns 0 and 1 are 1.  The sum of the parts is b to within 2^-17 |b|, and
+// the accumulator gets it with no per-activation add in the epilogue.
+constexpr int kBiasK = 16;
+__host__ __device__ __forceinline__ void bias_split(float b, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn(b);
+    lo = __float2bfloat16_rn(b - __bfloat162float(hi));
+}
+
 // device view of the trained network for inference inside the step
 struct NetView {
     const __nv_bfloat16 *wt[4];  // forward B operands, blocked K-major [N_l][K_l]
+    const __nv_bfloat16 *bt[3];  // hidden-layer bias operands, blocked K-major [kHid][kBiasK]
     const float *b[4];           // biases
     Gates gates;
     Scaling sc;

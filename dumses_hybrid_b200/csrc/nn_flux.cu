@@ -277,7 +277,7 @@ struct AdamArgs {
     float *W[4], *b[4], *mW[4], *vW[4], *mb[4], *vb[4];
     const float *dw[4];  // weight-gradient partials
     const float *db[4];  // bias-gradient partials
-    bf16 *Wt[4], *Wn[4];
+    bf16 *Wt[4], *Wn[4], *Bt[3];
     int splits, tiles;
     float lr, beta1, beta2, eps, c1, c2;  // c1 = 1 - beta1^t, c2 = 1 - beta2^t
     int apply;                             // 1: Adam step; 0: only reduce the gradient; 2: only pack BF16 copies
@@ -299,6 +299,15 @@ __global__ void k_adam(AdamArgs a) {
     const bool is_w = t < (long long)kr * nr;
     float g = 0.0f;
     int k = 0, n = 0;
+    // the face kernel's bias operand of hidden layer l < 3 (its columns 2.. stay zero)
+    auto pack_bias = [&](int nb, float b) {
+        if (l < 3) {
+            bf16 hi, lo;
+            bias_split(b, hi, lo);
+            a.Bt[l][blk_off(nb, 0, kBiasK, kTileRows)] = hi;
+            a.Bt[l][blk_off(nb, 1, kBiasK, kTileRows)] = lo;
+        }
+    };
     if (a.apply == 2) {  // pack only: BF16 copies of the current masters
         if (is_w) {
             k = (int)(t / nr);
@@ -306,6 +315,9 @@ __global__ void k_adam(AdamArgs a) {
             const float w = a.W[l][k * N + n];
             a.Wt[l][blk_off(n, k, K, N < kTileRows ? N : kTileRows)] = __float2bfloat16_rn(w);
             if (l > 0) a.Wn[l][blk_off(k, n, N, kTileRows)] = __float2bfloat16_rn(w);
+        } else {
+            n = (int)(t - (long long)kr * nr);
+            pack_bias(n, a.b[l][n]);
         }
         return;
     }
@@ -334,6 +346,8 @@ __global__ void k_adam(AdamArgs a) {
     if (is_w) {
         a.Wt[l][blk_off(n, k, K, N < kTileRows ? N : kTileRows)] = __float2bfloat16_rn(w);
         if (l > 0) a.Wn[l][blk_off(k, n, N, kTileRows)] = __float2bfloat16_rn(w);
+    } else {
+        pack_bias(n, w);
     }
 }
 
@@ -403,7 +417,7 @@ struct dg_nn {
     cudaStream_t stream = nullptr;
     int *d_err = nullptr;
     float *W[4] = {}, *b[4] = {}, *mW[4] = {}, *vW[4] = {}, *mb[4] = {}, *vb[4] = {};
-    bf16 *Wt[4] = {}, *Wn[4] = {};
+    bf16 *Wt[4] = {}, *Wn[4] = {}, *Bt[3] = {};
     float *xs = nullptr, *ts = nullptr;  // samples
     long long ns = 0, cap = 0;
     // batch scratch
@@ -573,6 +587,7 @@ int adam(dg_nn *n, long long rows, float lr, int apply, float *gout) {
     for (int l = 0; l < 4; l++) {
         a.W[l] = n->W[l]; a.b[l] = n->b[l]; a.mW[l] = n->mW[l]; a.vW[l] = n->vW[l]; a.mb[l] = n->mb[l];
         a.vb[l] = n->vb[l]; a.dw[l] = n->dw[l]; a.db[l] = n->db[l]; a.Wt[l] = n->Wt[l]; a.Wn[l] = n->Wn[l];
+        if (l < 3) a.Bt[l] = n->Bt[l];
     }
     a.splits = (int)(rows / ((rows % 512 == 0) ? 512 : 128));
     a.tiles = (int)(rows / kTileRows);
@@ -689,7 +704,8 @@ int dg_nn_create(int device, unsigned long long seed, dg_nn **out) {
         if ((rc = nn_alloc_t(n, &n->W[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->b[l], N)) ||
             (rc = nn_alloc_t(n, &n->mW[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->vW[l], (size_t)K * N)) ||
             (rc = nn_alloc_t(n, &n->mb[l], N)) || (rc = nn_alloc_t(n, &n->vb[l], N)) ||
-            (rc = nn_alloc_t(n, &n->Wt[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->Wn[l], (size_t)K * N)))
+            (rc = nn_alloc_t(n, &n->Wt[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->Wn[l], (size_t)K * N)) ||
+            (l < 3 && (rc = nn_alloc_t(n, &n->Bt[l], (size_t)kBiasK * kHid))))
             return bail(rc);
         std::vector<float> w((size_t)K * N, 0.0f);
         const double sd = std::sqrt(2.0 / real_k(l)) * (l == 3 ? 0.1 : 1.0);
@@ -959,6 +975,7 @@ int dg_nn_set_gates(dg_nn *n, float jump, float compress) {
 int dg_nn_view(const dg_nn *n, dg::nn::NetView *v) {
     if (!n) return DG_ERR_ARG;
     for (int l = 0; l < 4; l++) { v->wt[l] = n->Wt[l]; v->b[l] = n->b[l]; }
+    for (int l = 0; l < 3; l++) v->bt[l] = n->Bt[l];
     v->gates = n->gates;
     v->sc = n->sc;
     return DG_OK;

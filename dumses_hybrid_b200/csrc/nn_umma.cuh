@@ -163,6 +163,11 @@ __device__ __forceinline__ void mma_tiles(uint32_t d_tmem, const void *a_tile, c
     }
 }
 
+// one more K = 16 step over a second pair of tiles (A [2][128][8], B [2][n][8]), accumulating
+__device__ __forceinline__ void mma_extra_step(uint32_t d_tmem, const void *a_tile, const void *b_tile, int n) {
+    mma_bf16(d_tmem, sdesc(a_tile, kTileRows * 16, 128), sdesc(b_tile, (unsigned)n * 16, 128), idesc_bf16(kTileRows, n), 1);
+}
+
 // blocked K-major element offset of (row r, column c) for a matrix with C reduction columns
 __host__ __device__ __forceinline__ long long blk_off(long long r, int c, int C, int RT) {
     return ((r / RT) * (C / 8) + c / 8) * (long long)RT * 8 + (r % RT) * 8 + (c % 8);

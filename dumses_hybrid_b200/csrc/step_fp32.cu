@@ -531,19 +531,24 @@ __global__ void __launch_bounds__(kThreads) k_nn_harvest(Geo G, const float *__r
         to[n] = (u.jump > nn::kTinyJump) ? (float)((t[n] - b[n]) / ((double)nn::out_scale(u, n) * (double)u.jump)) : 0.0f;
 }
 
-// shared-memory plan of the face-network kernel (bytes): the four weight tiles, then per
-// warpgroup one activation tile (its first 8 KB hold the input tile of layer 1), the
-// biases and the barriers
+// shared-memory plan of the face-network kernel (bytes): the four weight tiles, the three
+// hidden-layer bias operands and the all-ones A operand they are multiplied by, then per
+// warpgroup one activation tile (its first 8 KB hold the input tile of layer 1), the output
+// layer's biases and the barriers
 constexpr int kNWG = 4;  // warpgroups per CTA (4 x 128 TMEM columns)
-constexpr int kNW1 = 0, kNW2 = 8192, kNW3 = 40960, kNW4 = 73728, kNH0 = 77824, kNHsz = 32768,
-              kNBias = kNH0 + kNWG * kNHsz, kNBar = kNBias + 1600, kNSmem = kNBar + 128;
+constexpr int kNBtsz = nn::kBiasK * nn::kHid * 2;
+constexpr int kNW1 = 0, kNW2 = 8192, kNW3 = 40960, kNW4 = 73728, kNBt = 77824, kNOne = kNBt + 3 * kNBtsz,
+              kNH0 = kNOne + nn::kBiasK * 128 * 2, kNHsz = 32768, kNBias = kNH0 + kNWG * kNHsz, kNBar = kNBias + 64,
+              kNSmem = kNBar + 128;
+static_assert(kNSmem <= 232448, "face-network kernel exceeds the shared memory of one CTA");
 
 __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory"); }
 
 // Four warpgroups per CTA, each taking 128-face tiles in turn: the faces' interface states,
 // inputs and gates, the four layers as tcgen05 MMAs (weights resident in shared memory,
-// each warpgroup with its own 128 TMEM columns, activations through TMEM -> SmeLU -> shared
-// memory), then the gated flux or a mark for HLLD.
+// each warpgroup with its own 128 TMEM columns; a hidden layer's bias enters its accumulator
+// as one more K step, activations go through TMEM -> SmeLU -> shared memory), then the gated
+// flux or a mark for HLLD.
 __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *__restrict__ core,
                                                             float *__restrict__ flux, int *__restrict__ fallback,
                                                             int d, nn::NetView nv, const Scalars *S,
@@ -551,9 +556,12 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     extern __shared__ __align__(1024) unsigned char sm[];
     using bf16 = __nv_bfloat16;
     const int tid = threadIdx.x, wg = tid >> 7, wt = tid & 127, warp = tid >> 5, lane = tid & 31;
-    bf16 *W[4] = {(bf16 *)(sm + kNW1), (bf16 *)(sm + kNW2), (bf16 *)(sm + kNW3), (bf16 *)(sm + kNW4)};
+    // weight tile and bias operand of layer l
+    auto W = [&](int l) { return (bf16 *)(sm + (l == 0 ? kNW1 : l == 1 ? kNW2 : l == 2 ? kNW3 : kNW4)); };
+    auto Bt = [&](int l) { return (bf16 *)(sm + kNBt + l * kNBtsz); };
+    bf16 *One = (bf16 *)(sm + kNOne);
     bf16 *Hs = (bf16 *)(sm + kNH0 + wg * kNHsz), *Xs = Hs;
-    float *bias = (float *)(sm + kNBias);  // 3 x 128 + 8
+    float *bias = (float *)(sm + kNBias);  // output layer
     uint64_t *wbar = (uint64_t *)(sm + kNBar);
     uint64_t *mbar = (uint64_t *)(sm + kNBar + 8 + 8 * wg);
     uint32_t *tslot = (uint32_t *)(sm + kNBar + 8 + 8 * kNWG);
@@ -567,10 +575,13 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         }
         nn::mbar_fence_init();
     }
-    for (int q = tid; q < 3 * nn::kHid + nn::kOut; q += 128 * kNWG) {
-        const int l = q / nn::kHid;
-        bias[q] = (l < 3) ? nv.b[l][q % nn::kHid] : nv.b[3][q - 3 * nn::kHid];
+    if (tid < nn::kOut) bias[tid] = nv.b[3][tid];
+    // the A operand of the bias step: columns 0 and 1 of every row are 1
+    for (int q = tid; q < nn::kBiasK * 128; q += 128 * kNWG) {
+        const int r = q / nn::kBiasK, c = q % nn::kBiasK;
+        One[nn::blk_off(r, c, nn::kBiasK, 128)] = __float2bfloat16_rn(c < 2 ? 1.0f : 0.0f);
     }
+    nn::fence_async_smem();
     if (warp == 0) nn::tmem_alloc(tslot, 128 * kNWG);
     nn::tc_fence_before();
     __syncthreads();
@@ -579,8 +590,11 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     if (tid == 0) {
         const unsigned wb[4] = {128 * nn::kInPad * 2, 128 * 128 * 2, 128 * 128 * 2, nn::kOutPad * 128 * 2};
-        nn::mbar_expect_tx(wbar, wb[0] + wb[1] + wb[2] + wb[3]);
-        for (int l = 0; l < 4; l++) nn::bulk_g2s(W[l], nv.wt[l], wb[l], wbar);
+        nn::mbar_expect_tx(wbar, wb[0] + wb[1] + wb[2] + wb[3] + 3 * kNBtsz);
+#pragma unroll
+        for (int l = 0; l < 4; l++) nn::bulk_g2s(W(l), nv.wt[l], wb[l], wbar);
+#pragma unroll
+        for (int l = 0; l < 3; l++) nn::bulk_g2s(Bt(l), nv.bt[l], kNBtsz, wbar);
         if (!nn::mbar_wait(wbar, 0)) {
             nn::mbar_wait(wbar, 0);
             for (int g = 0; g < kNWG; g++) flags[g] = 0;
@@ -637,7 +651,8 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         for (int l = 0; l < 4; l++) {
             if (wt == 0) {
                 nn::tc_fence_after();
-                nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W[l], l == 3 ? nn::kOutPad : nn::kHid, l == 0 ? 2 : 8, 0);
+                nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W(l), l == 3 ? nn::kOutPad : nn::kHid, l == 0 ? 2 : 8, 0);
+                if (l < 3) nn::mma_extra_step(tmem, One, Bt(l), nn::kHid);  // + bias
                 nn::mma_commit(mbar);
             }
             // every thread observes the MMA's completion itself; the warp agrees on the outcome
@@ -652,19 +667,18 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
             nn::tc_fence_after();
             if (l < 3) {
                 if (ok) {
+                    // one 32-column chunk at a time (chunks interleaved by the compiler took the
+                    // kernel to its 128-register limit, with spills, and 2% more time)
+#pragma unroll 1
                     for (int cc = 0; cc < nn::kHid / 32; cc++) {
                         float v[32];
                         nn::tmem_ld32(taddr + cc * 32, v);
-                        const float4 *bq = (const float4 *)(bias + l * nn::kHid + cc * 32);
 #pragma unroll
                         for (int hh = 0; hh < 4; hh++) {
-                            const float4 b0 = bq[2 * hh], b1 = bq[2 * hh + 1];
                             const float *w = v + hh * 8;
-                            const uint32_t h0 = nn::bias_smelu2_bf16(w[0], w[1], b0.x, b0.y);
-                            const uint32_t h1 = nn::bias_smelu2_bf16(w[2], w[3], b0.z, b0.w);
-                            const uint32_t h2 = nn::bias_smelu2_bf16(w[4], w[5], b1.x, b1.y);
-                            const uint32_t h3 = nn::bias_smelu2_bf16(w[6], w[7], b1.z, b1.w);
-                            *(uint4 *)(Hs + ((cc * 4 + hh) * 128 + wt) * 8) = make_uint4(h0, h1, h2, h3);
+                            *(uint4 *)(Hs + ((cc * 4 + hh) * 128 + wt) * 8) =
+                                make_uint4(nn::smelu2_bf16(w[0], w[1]), nn::smelu2_bf16(w[2], w[3]),
+                                           nn::smelu2_bf16(w[4], w[5]), nn::smelu2_bf16(w[6], w[7]));
                         }
                     }
                 }
@@ -677,7 +691,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
                 float v[16];
                 nn::tmem_ld16(taddr, v);
 #pragma unroll
-                for (int q = 0; q < nn::kOut; q++) y[q] = (v[q] + bias[3 * nn::kHid + q]) * nv.sc.ysd[q];
+                for (int q = 0; q < nn::kOut; q++) y[q] = (v[q] + bias[q]) * nv.sc.ysd[q];
             }
         }
         if (!tile_ok || !*flag) valid = false;  // a failed tile writes nothing (the error word reports it)
