@@ -5,7 +5,8 @@ nvcc compiles each CUDA translation unit with
 plus --fmad=false for the FP64 path and the host code (no multiply-add
 contraction: the FP64 path is bit-identical to the CPU reference arithmetic)
 and --use_fast_math for the FP32 mixed path, and links them, with the host-side initial conditions,
-into dumses_hybrid_b200/libdumses_gpu.so against the static CUDA runtime.  A second
+into dumses_hybrid_b200/libdumses_gpu.so against the static CUDA runtime, and builds the
+C++ driver dumses_hybrid_b200/dg_driver (the reference's main program over the C-ABI) against it.  A second
 library, libdumses_gpu_chk.so, is the same with the step kernels compiled with
 -DDG_CHECK_BOUNDS: every array access of the step kernels checked against the registered
 device buffers (a debug stand-in for a memory sanitizer, used by the tests).
@@ -40,6 +41,9 @@ CU_SOURCES = {"step_fp64.cu": EXACT, "step_fp32.cu": FAST, "dg_api.cu": EXACT, "
 CXX_SOURCES = ["condinit.cpp"]
 LIB_CHK = PKG / "libdumses_gpu_chk.so"
 CHECKED_SOURCES = ("step_fp64.cu", "step_fp32.cu")  # compiled again with -DDG_CHECK_BOUNDS
+# the reference's main program over the C-ABI (a C++ executable linked to LIB)
+DRIVER_SOURCE = "dg_driver.cpp"
+DRIVER = PKG / "dg_driver"
 
 
 def _nvcc() -> str:
@@ -74,8 +78,7 @@ def _run(cmd: list[str], verbose: bool) -> None:
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> pathlib.Path:
     newest = _newest_input()
-    if (not force and LIB.exists() and LIB_CHK.exists() and LIB.stat().st_mtime >= newest
-            and LIB_CHK.stat().st_mtime >= newest):
+    if not force and all(f.exists() and f.stat().st_mtime >= newest for f in (LIB, LIB_CHK, DRIVER)):
         return LIB
     BUILD.mkdir(exist_ok=True)
     nvcc, cxx = _nvcc(), _cxx()
@@ -101,6 +104,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         tmp = lib.with_suffix(".so.tmp")
         _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)], verbose)
         tmp.replace(lib)
+    tmp = DRIVER.with_suffix(".tmp")
+    _run([cxx, "-O2", "-std=c++17", "-I", str(INCLUDE), str(CSRC / DRIVER_SOURCE), "-L", str(PKG), "-ldumses_gpu",
+          "-Wl,-rpath,$ORIGIN", "-o", str(tmp)], verbose)
+    tmp.replace(DRIVER)
     return LIB
 
 
