@@ -376,8 +376,15 @@ def main() -> None:
             src = "measured (sustained)" if tpeak else "fallback"
             tpeak = tpeak or 1400.0
             achieved = flops / per_launch_s / 1e12
+            traffic = None
+            tpath = ROOT / "profiles" / f"ncu_traffic_{args.workload}{args.n}_fp32nn.json"
+            if tpath.exists():
+                try:
+                    traffic = json.loads(tpath.read_text()).get(dom)
+                except Exception:
+                    traffic = None
             out = {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": tpeak, "unit": "TFLOP/s",
-                   "frac": achieved / tpeak, "traffic": None, "peak_source": src,
+                   "frac": achieved / tpeak, "traffic": traffic, "peak_source": src,
                    "algorithmic_flops_per_launch": flops,
                    "note": "one launch per face direction; 2 x 35968 flops per face (17-128-128-128-8 MLP)"}
             upath = ROOT / "profiles" / "pipe_util_mri128.json"
