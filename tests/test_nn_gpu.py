@@ -237,3 +237,59 @@ def test_surrogate_in_2d():
         divb = (bx[4:-2, 3:-3, 0] - bx[3:-3, 3:-3, 0]) + (by[3:-3, 4:-2, 0] - by[3:-3, 3:-3, 0])
         # CT keeps div B at the round-off of the FP32 increments (about 1e-8 of |B| per face difference)
         assert np.max(np.abs(divb)) < 1e-6 * max(np.max(np.abs(bx)), 1e-30)
+
+
+def effective_face_fluxes(g, p, dt):
+    """Face records of the last godunov of a 3D context as (faces, 5) effective fluxes: mass,
+    energy and the three momentum fluxes, the normal one with p*_T added back (the 1D
+    solvers that carry p*_T separately leave it out of the normal momentum flux)."""
+    nf = (p.nx + 1) * (p.ny + 1) * (p.nz + 1)
+    dx, dy, dz = (p.xmax - p.xmin) / p.nx, (p.ymax - p.ymin) / p.ny, (p.zmax - p.zmin) / p.nz
+    ds = (dy * dz, dx * dz, dx * dy)
+    k, j, i = np.meshgrid(np.arange(1, p.nz + 2), np.arange(1, p.ny + 2), np.arange(1, p.nx + 2), indexing="ij")
+    valid = ((j <= p.ny) & (k <= p.nz), (i <= p.nx) & (k <= p.nz), (i <= p.nx) & (j <= p.ny))
+    out = []
+    for d in range(3):
+        rec = g.debug_array(d, 6 * nf).reshape(p.nz + 1, p.ny + 1, p.nx + 1, 6)
+        eff = rec[..., :5].copy()
+        eff[..., 2 + d] += rec[..., 5] * ds[d] * dt
+        out.append(eff[valid[d]])
+    return np.concatenate(out)
+
+
+def test_face_network_kernel_against_hlld_and_llf():
+    """The inference kernel of the step (k_nn_faces) on its own: after one godunov from the
+    same state, the faces it accepted (its count agrees with the kernel's own) carry fluxes
+    much closer to HLLD than LLF's, as the held-out test of the network predicts; the faces
+    it sent back carry the HLLD flux.  A wrong weight or bias operand in the kernel would
+    either move the accepted fluxes away from HLLD or get nearly every face sent back."""
+    with FluxNet(seed=2) as net:
+        train_on_ot(net)
+        net.set_gates(jump=0.1, compress=0.1)
+        eff, stats = {}, None
+        for name, riemann, sur in (("hlld", "hlld", False), ("llf", "llf", False), ("nn", "hlld", True)):
+            p = Params(**{**ot_params(32, "fp32", sur).__dict__, "riemann": riemann})
+            with Context(p) as g:
+                if sur:
+                    g.attach_surrogate(net)
+                g.upload(condinit(p, "orszag_tang"))
+                g.boundary(0.0, 0.0)
+                dt = g.compute_dt()
+                g.godunov(dt, 0.0)
+                eff[name] = effective_face_fluxes(g, p, dt)
+                if sur:
+                    stats = g.surrogate_stats()
+        faces, fallback = stats
+        assert faces == eff["nn"].shape[0]
+        dn = np.abs(eff["nn"] - eff["hlld"]).sum(axis=1)
+        dl = np.abs(eff["llf"] - eff["hlld"]).sum(axis=1)
+        accepted = dn > 1e-3 * dl + 1e-30
+        print("faces", faces, "fallback", fallback, "classified accepted", int(accepted.sum()))
+        assert abs(int(accepted.sum()) - (faces - fallback)) <= 0.01 * faces
+        assert faces - fallback >= 0.1 * faces
+        ratio = dn[accepted].sum() / dl[accepted].sum()
+        print("accepted faces: L1(network - HLLD) / L1(LLF - HLLD) =", ratio)
+        assert ratio < 0.5
+        # faces sent back carry HLLD (the same solver in another kernel)
+        back = ~accepted
+        assert np.abs(eff["nn"][back] - eff["hlld"][back]).sum() <= 1e-4 * np.abs(eff["hlld"][back]).sum()
