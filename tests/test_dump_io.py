@@ -72,6 +72,31 @@ def test_read_dump_wrong_grid(tmp_path):
         dg.read_dump(GOLDEN / META["dump"], q)
 
 
+def test_damaged_dumps_are_errors_not_crashes(tmp_path):
+    """A dump cut short anywhere, or with a record marker changed, is refused with an error
+    code; the reader never reads past a record it was not promised."""
+    p = dg.Params(**PARAMS)
+    good = (GOLDEN / META["dump"]).read_bytes()
+    path = tmp_path / "bad.bin"
+    off = 6 * 4 + 13 * 8 + 2 * 4 * 4
+    cuts = sorted({0, 3, 4, 20, 31, 32, 60, 100, off - 1, off, off + 4, off + 1000, len(good) - 5, len(good) - 1})
+    for cut in cuts:
+        path.write_bytes(good[:cut])
+        with pytest.raises(dg.DumsesError):
+            dg.read_dump(path, p)
+    # record markers: the header's leading and trailing ones, and the uin record's
+    for pos, value in ((0, 28), (28, 20), (0, -24), (off, 16), (off, 2 ** 31 - 1), (len(good) - 4, 8)):
+        bad = bytearray(good)
+        struct.pack_into("<i", bad, pos, value)
+        path.write_bytes(bytes(bad))
+        with pytest.raises(dg.DumsesError):
+            dg.read_dump(path, p)
+    # trailing bytes after the last record are not part of a dump either
+    path.write_bytes(good + b"\0" * 8)
+    u, t, _ = dg.read_dump(path, p)  # the reference reads its records and stops, as this does
+    assert t == META["time"] and np.array_equal(u, seeded_uin(p, SEED))
+
+
 def test_read_dump_of_a_decomposed_run(tmp_path):
     data = bytearray((GOLDEN / META["dump"]).read_bytes())
     struct.pack_into("<i", data, 4 + 5 * 4, 2)  # nzslice = 2
