@@ -201,11 +201,29 @@ class Params:
         return (self.nx + 6, self.ny + 6 if self.ndim > 1 else 1, self.nz + 6 if self.ndim == 3 else 1, 11)
 
 
+def _strip_namelist_comments(text: str) -> str:
+    """Drop Fortran comments ('!' to the end of the line, outside quoted strings)."""
+    out = []
+    for line in text.splitlines():
+        quote = None
+        for k, ch in enumerate(line):
+            if quote:
+                if ch == quote:
+                    quote = None
+            elif ch in "'\"":
+                quote = ch
+            elif ch == "!":
+                line = line[:k]
+                break
+        out.append(line)
+    return "\n".join(out)
+
+
 def read_namelist(path: str | pathlib.Path, ndim: int = 3, iso: int = 0) -> Params:
     """Build :class:`Params` from a reference ``input`` namelist file
     (&scheme_params, &model_params; init.f90:153-173), applying the reference
     defaults (init.f90:244-302) for keys the file does not set."""
-    text = pathlib.Path(path).read_text()
+    text = _strip_namelist_comments(pathlib.Path(path).read_text())
     kv = {}
     for m in re.finditer(r"([A-Za-z0-9_]+)\s*=\s*('[^']*'|\"[^\"]*\"|[^,\s/]+)", text):
         kv[m.group(1).lower()] = m.group(2).strip("'\"")

@@ -128,3 +128,32 @@ def test_driver_without_a_device_stops_with_the_library_message(driver, tmp_path
     path.write_text(INPUT)
     res = run(driver, path, "--iso", 1, "--out", tmp_path / "out")
     assert res.returncode == 1 and "dg_init returned -7" in res.stderr, res.stderr
+
+
+def test_driver_and_mirror_agree_on_namelist_details(driver, tmp_path):
+    """Comments, upper-case names, D exponents, T/F logicals, double quotes, several
+    assignments on a line: both readers see the same values."""
+    text = """! a run of the MRI problem
+&START_PARAMS TLIM = 2.5D1, restart = 0 /   ! stop time
+&scheme_params
+   BdTypeX = "shearingbox", bdtypey='periodic' ! riemann = 'llf' is a comment
+   Riemann = 'HLLD', RIEMANN2D = 'upwind', slope_type = 1, Courant = 6.d-1, FARGO = T
+/
+&model_params nx = 24, NY = 40, nz = 8, xmin = -5.D-1, xmax = 5.D-1, ymin = -1.0, ymax = 1.0,
+   zmin = -0.125, zmax = 0.125, omega0 = 1.5d0, CISO = 0.5, eta = 1.e-4 /
+&output_params dthist = 0.5, dtdump = 2., io_type = 'binary' /
+&mpi_params /
+"""
+    path = tmp_path / "input"
+    path.write_text(text)
+    res = run(driver, path, "--iso", 1, "--print-params")
+    assert res.returncode == 0, res.stderr
+    got = printed(res.stdout)
+    c = read_namelist(path, ndim=3, iso=1).to_c()
+    for k in ("nx", "ny", "nz", "slope_type", "iriemann", "iriemann2d", "fargo"):
+        assert int(got[k]) == getattr(c, k), k
+    for k in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "ciso", "omega0", "courant", "eta"):
+        assert float(got[k]) == getattr(c, k), k
+    assert [int(b) for b in got["bc"].split(",")] == list(c.bc)
+    assert (c.iriemann, c.iriemann2d, c.fargo, c.bc[0]) == (4, 5, 1, 2)  # HLLD, upwind, FARGO, shearing box
+    assert (float(got["tlim"]), float(got["dthist"]), float(got["dtdump"])) == (25.0, 0.5, 2.0)
