@@ -51,7 +51,8 @@ def lib() -> ctypes.CDLL:
 
 
 class Oracle:
-    """One oracle state, driven like the reference's module globals."""
+    """One oracle state, driven like the reference's module globals.  `uin` is a view of the
+    oracle's own memory: copy what must outlive the Oracle object."""
 
     def __init__(self, params: Params):
         self.params = params

@@ -76,7 +76,7 @@ def run(riemann: str) -> tuple[np.ndarray, np.ndarray, float]:
     t = 0.0
     while t < 0.2:
         t, _ = o.step(t)
-    rho = o.uin[3:3 + NX, 3:3 + NY, 0, 0]
+    rho = o.uin[3:3 + NX, 3:3 + NY, 0, 0].copy()  # a copy: the view dies with the oracle state
     return xc[3:3 + NX], rho, t
 
 
@@ -100,3 +100,46 @@ def test_sod_dissipation_orders_the_solvers():
         x, rho, t = run(riemann)
         errs[riemann] = float(np.abs(rho[:, 0] - exact_sod(x, t)).mean())
     assert errs["hlld"] <= errs["hll"] < errs["llf"], errs
+
+
+def tube_3d(direction: int) -> np.ndarray:
+    """Density profile of the HLLD shock tube along x, y or z of a 3D grid (256 cells along the
+    tube, 4 across, zero-gradient ends) at t = 0.2 (the last step shortened to end there)."""
+    n = [4, 4, 4]
+    n[direction] = NX
+    ext = [c / NX for c in n]
+    bc = ["periodic"] * 3
+    bc[direction] = "zero_gradient"
+    p = Params(ndim=3, iso=0, nx=n[0], ny=n[1], nz=n[2], xmin=0.0, xmax=ext[0], ymin=0.0, ymax=ext[1], zmin=0.0,
+               zmax=ext[2], gamma=GAMMA, courant=0.8, slope_type=2, riemann="hlld", riemann2d="hlld",
+               bdtypex=bc[0], bdtypey=bc[1], bdtypez=bc[2])
+    u = np.zeros(p.shape, order="F")
+    c = (np.arange(NX + 6) - 2.5) / NX
+    shape = [1, 1, 1]
+    shape[direction] = NX + 6
+    left = (c < 0.5).reshape(shape)
+    u[..., 0] = np.where(left, LEFT[0], RIGHT[0])
+    u[..., 4] = np.where(left, LEFT[2], RIGHT[2]) / (GAMMA - 1.0)
+    o = Oracle(p)
+    o.set_state(u)
+    o.boundary(0.0, 0.0)
+    t = 0.0
+    while t < 0.2:
+        dt = min(o.compute_dt(), 0.2 - t)
+        o.godunov(dt, t)
+        o.boundary(t, dt)
+        t = t + dt
+    rho = np.moveaxis(o.uin[3:-3, 3:-3, 3:-3, 0], direction, 0).copy()
+    return rho[:, 0, 0], rho
+
+
+def test_sod_shock_tube_is_the_same_along_x_y_and_z():
+    """The solvers' direction permutations (solver.f90:116-160) and the trace's per-direction
+    slopes: the tube along y and along z gives the x tube's profile, uniform across."""
+    px, _ = tube_3d(0)
+    x = (np.arange(NX) + 0.5) / NX
+    assert np.abs(px - exact_sod(x, 0.2)).mean() / np.abs(exact_sod(x, 0.2)).mean() < 0.007
+    for d in (1, 2):
+        prof, full = tube_3d(d)
+        assert np.allclose(full, prof[:, None, None], rtol=0, atol=1e-14)
+        assert np.allclose(prof, px, rtol=0, atol=1e-12), (d, np.abs(prof - px).max())
