@@ -50,17 +50,14 @@ def lib() -> ctypes.CDLL:
     return _lib
 
 
-class Oracle:
-    """One oracle state, driven like the reference's module globals.  `uin` is a view of the
-    oracle's own memory: copy what must outlive the Oracle object."""
+class _State:
+    """Owner of one C oracle state: freed when the last holder (the Oracle, or a view of its
+    uin) goes, or by close()."""
 
-    def __init__(self, params: Params):
-        self.params = params
-        self._cp = params.to_c()
-        self.L = lib()
-        self.h = self.L.or_create(ctypes.byref(self._cp))
-        n = self.L.or_uin_size(self.h)
-        self.uin = np.ctypeslib.as_array(self.L.or_uin(self.h), shape=(n,)).reshape(params.shape, order="F")
+    def __init__(self, L, params: Params):
+        self.L = L
+        self.cp = params.to_c()
+        self.h = L.or_create(ctypes.byref(self.cp))
 
     def close(self):
         if self.h:
@@ -69,6 +66,34 @@ class Oracle:
 
     def __del__(self):
         self.close()
+
+
+class _Memory:
+    """n doubles of oracle memory at ptr, exposed to numpy with a reference to their owner."""
+
+    def __init__(self, owner: _State, ptr: int, n: int):
+        self.owner = owner
+        self.__array_interface__ = {"data": (ptr, False), "shape": (n,), "typestr": "<f8", "version": 3}
+
+
+class Oracle:
+    """One oracle state, driven like the reference's module globals.  `uin` is the oracle's
+    own memory; views of it keep the state alive until they go (close() frees it at once)."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        self.L = lib()
+        self._state = _State(self.L, params)
+        n = self.L.or_uin_size(self.h)
+        ptr = ctypes.cast(self.L.or_uin(self.h), ctypes.c_void_p).value
+        self.uin = np.asarray(_Memory(self._state, ptr, n)).reshape(params.shape, order="F")
+
+    @property
+    def h(self):
+        return self._state.h
+
+    def close(self):
+        self._state.close()
 
     def set_state(self, u: np.ndarray) -> None:
         self.uin[...] = u
