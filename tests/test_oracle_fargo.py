@@ -98,3 +98,34 @@ def test_fargo_whole_cell_shift_is_a_translation():
             want = -(ez(i + 1, k) - ez(i, k)) / dx + (ex(i, k + 1) - ex(i, k)) / dz
             got = u1[i + 2, 3:3 + NY, k + 2, 6].mean() - u0[i + 2, 3:3 + NY, k + 2, 6].mean()
             assert abs(got - want) <= 1e-13, (i, k, got, want)
+
+
+def test_fargo_fractional_shift_conserves_every_column():
+    """With fractional shifts the remap interpolates (linear weights plus the parabolic slope
+    correction) but stays conservative: every column keeps its sums of rho, momenta, E, B_x and
+    B_z along y, and div B stays at round-off."""
+    p = params()
+    o = Oracle(p)
+    o.set_state(state(p, seed=5))
+    o.boundary(0.0, 0.0)
+    u0 = o.uin.copy()
+    o.fargo_update(0.137)
+    u1 = o.uin.copy()
+    act_y, act_z = slice(3, 3 + NY), slice(3, 3 + NZ)
+    moved = False
+    for i in range(1, NX + 1):
+        for v in (0, 1, 2, 3, 4, 7):
+            s0 = u0[i + 2, act_y, act_z, v].sum(axis=0)
+            s1 = u1[i + 2, act_y, act_z, v].sum(axis=0)
+            assert np.allclose(s1, s0, rtol=0, atol=1e-13 * np.abs(u0[..., v]).max() * NY), (i, v)
+        moved = moved or not np.allclose(u1[i + 2, act_y, act_z, 0], u0[i + 2, act_y, act_z, 0])
+    for i in range(2, NX + 1):
+        s0, s1 = u0[i + 2, act_y, act_z, 5].sum(axis=0), u1[i + 2, act_y, act_z, 5].sum(axis=0)
+        assert np.allclose(s1, s0, rtol=0, atol=1e-13 * np.abs(u0[..., 5]).max() * NY), i
+    assert moved
+    o.boundary(0.0, 0.137)
+    b = o.uin
+    dx, dy, dz = 1.0 / 8, 1.0 / 16, 1.0 / 16
+    div = ((b[4:-3, 3:-3, 3:-3, 5] - b[3:-4, 3:-3, 3:-3, 5]) / dx + (b[3:-4, 4:-2, 3:-3, 6] - b[3:-4, 3:-3, 3:-3, 6]) / dy
+           + (b[3:-4, 3:-3, 4:-2, 7] - b[3:-4, 3:-3, 3:-3, 7]) / dz)
+    assert np.max(np.abs(div)) <= 1e-12 * np.max(np.abs(b[..., 5:8])) / dx
