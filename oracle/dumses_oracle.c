@@ -9,6 +9,7 @@
  */
 #include "dumses_oracle.h"
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
@@ -2118,4 +2119,112 @@ int or_run_history(or_state *s, double tlim, double dthist, double *rows, int ma
         if ((time - dt) > tlim) break;
     }
     return n;
+}
+
+/* ------------------------------------------------------------------------- */
+/* initial conditions (the problem plug-ins src/problem/<p>/condinit.f90)     */
+/* ------------------------------------------------------------------------- */
+/* Counter-based uniform variates in [0,1): splitmix64 of (seed, stream, cell).  The
+ * reference seeds random_number from the wall clock (mri/condinit.f90:52-61), which no
+ * two runs share; a counter-based generator gives every cell the same kick on any
+ * thread count, and the same value as the library's own initial-condition generator. */
+static uint64_t or_mix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+static double or_uniform01(uint64_t seed, uint64_t stream, uint64_t counter)
+{
+    const uint64_t h = or_mix64(seed ^ or_mix64(stream * 0x100000001B3ull + counter));
+    return (double)(h >> 11) * (1.0 / 9007199254740992.0);
+}
+
+int or_condinit(or_state *s, int ic, double beta, double amp, unsigned long long seed)
+{
+    const double twopi = 4.0 * asin(1.0), pi = 2.0 * asin(1.0); /* commons.f90:47 */
+    memset(s->uin.d, 0, sizeof(double) * s->uin.size);
+    if (ic == DG_IC_MRI || ic == DG_IC_MRI_TEST) {
+        /* mri/condinit.f90:30-105: rho = 1, p0 = rho ciso^2, B0 = sqrt(2 p0 / beta) */
+        if (s->ndim != 3) return DG_ERR_ARG;
+        const double d0 = 1.0, p0 = d0 * s->p.ciso * s->p.ciso, B0 = sqrt(2.0 * p0 / beta);
+#pragma omp parallel for collapse(2)
+        for (int k = s->ku1; k <= s->ku2; k++)
+            for (int j = s->ju1; j <= s->ju2; j++)
+                for (int i = s->iu1; i <= s->iu2; i++) {
+                    /* the kick stream's counter: the cell's offset in the uin array */
+                    const uint64_t cell = (uint64_t)(&A4(s->uin, i, j, k, 1) - s->uin.d);
+                    A4(s->uin, i, j, k, ir) = d0;
+                    if (ic == DG_IC_MRI_TEST) {
+                        /* the regression set-up ('Test', amp = 0): one vx mode, B_z = B0 sin(2 pi x) */
+                        A4(s->uin, i, j, k, iu) = 1.e-2 * 1.e-3 * cos(twopi * 10.0 * ZC(k)) * cos(twopi * 5.0 * XC(i));
+                        A4(s->uin, i, j, k, iC) = B0 * sin(twopi * XC(i));
+                        A4(s->uin, i, j, k, 11) = B0 * sin(twopi * XC(i));
+                    } else {
+                        /* 'fluxZ' with uniform kicks amp (r - 1/2) sqrt(p0) per component */
+                        for (int c = 0; c < 3; c++)
+                            A4(s->uin, i, j, k, iu + c) =
+                                A4(s->uin, i, j, k, ir) * amp * (or_uniform01(seed, (uint64_t)(c + 1), cell) - 0.5) * sqrt(p0);
+                        A4(s->uin, i, j, k, iC) = B0;
+                        A4(s->uin, i, j, k, 11) = B0;
+                    }
+                }
+        return DG_OK;
+    }
+    if (ic == DG_IC_ORSZAG_TANG) {
+        /* the 3D form of orszag_tang/condinit.f90:33-56: rho = 25/(36 pi), P = 5/(12 pi),
+         * v = (-sin 2 pi y, sin 2 pi x, 0.2 sin 2 pi z), B = (-sin 2 pi y, sin 4 pi x, 0)/sqrt(4 pi) */
+        if (s->ndim != 3) return DG_ERR_ARG;
+        const double rho = 25.0 / (36.0 * pi), pres = 5.0 / (12.0 * pi), b0 = 1.0 / sqrt(4.0 * pi);
+        const double gamma = s->p.gamma;
+#pragma omp parallel for collapse(2)
+        for (int k = s->ku1; k <= s->ku2; k++)
+            for (int j = s->ju1; j <= s->ju2; j++)
+                for (int i = s->iu1; i <= s->iu2; i++) {
+                    const double x = XC(i), y = YC(j), z = ZC(k);
+                    const double vx = -sin(twopi * y), vy = sin(twopi * x), vz = 0.2 * sin(twopi * z);
+                    const double bx = -b0 * sin(twopi * y), by = b0 * sin(2.0 * twopi * x);
+                    A4(s->uin, i, j, k, ir) = rho;
+                    A4(s->uin, i, j, k, iu) = rho * vx;
+                    A4(s->uin, i, j, k, iv) = rho * vy;
+                    A4(s->uin, i, j, k, iw) = rho * vz;
+                    A4(s->uin, i, j, k, iA) = bx; A4(s->uin, i, j, k, 9) = bx;
+                    A4(s->uin, i, j, k, iB) = by; A4(s->uin, i, j, k, 10) = by;
+                    A4(s->uin, i, j, k, ip) = pres / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy + vz * vz)
+                                              + 0.5 * (bx * bx + by * by);
+                }
+        return DG_OK;
+    }
+    if (ic == DG_IC_FIELD_LOOP) {
+        /* magnetic_loop/condinit.f90:40-104 (direction 'x') with A0 = 1e-3, R = 0.3, v = (2, 1):
+         * A_z = A0 (R - r) for r <= R, face B from its differences */
+        if (s->ndim != 2) return DG_ERR_ARG;
+        const double A0 = 1.e-3, R = 0.3, rho = 1.0, pres = 1.0, vx = 2.0, vy = 1.0, gamma = s->p.gamma;
+        const double dx = s->dx, dy = s->dy, xmin = s->p.xmin, ymin = s->p.ymin;
+        const int k = 1;
+        for (int j = s->ju1; j <= s->ju2; j++)
+            for (int i = s->iu1; i <= s->iu2; i++) {
+                /* A_z at the cell's lower-left corner, from the centre formula of init_grid */
+                double az[2][2];
+                for (int a = 0; a < 2; a++)
+                    for (int b = 0; b < 2; b++) {
+                        const double x = xmin + dx / 2 + (i + a - 1) * dx, y = ymin + dy / 2 + (j + b - 1) * dy;
+                        const double dist = sqrt(x * x + y * y);
+                        az[a][b] = dist <= R ? A0 * (R - dist) : 0.0;
+                    }
+                const double bxl = (az[0][1] - az[0][0]) / dy, bxr = (az[1][1] - az[1][0]) / dy;
+                const double byl = -(az[1][0] - az[0][0]) / dx, byr = -(az[1][1] - az[0][1]) / dx;
+                A4(s->uin, i, j, k, ir) = rho;
+                A4(s->uin, i, j, k, iu) = rho * vx;
+                A4(s->uin, i, j, k, iv) = rho * vy;
+                A4(s->uin, i, j, k, iA) = bxl; A4(s->uin, i, j, k, 9) = bxr;
+                A4(s->uin, i, j, k, iB) = byl; A4(s->uin, i, j, k, 10) = byr;
+                const double bcx = 0.5 * (bxl + bxr), bcy = 0.5 * (byl + byr);
+                A4(s->uin, i, j, k, ip) = pres / (gamma - 1.0) + 0.5 * rho * (vx * vx + vy * vy)
+                                          + 0.5 * (bcx * bcx + bcy * bcy);
+            }
+        return DG_OK;
+    }
+    return DG_ERR_ARG;
 }

@@ -57,6 +57,12 @@ int or_run_history(or_state *s, double tlim, double dthist, double *rows, int ma
  * (iu1:iu2,...), 4 fgodunov_pre (iu1:iu2,...,1:ndim), 5 qin (iu1:iu2,...,1:8). */
 double *or_array(or_state *s, int which, long long *count);
 
+/* Initial state of one of the library's problems (DG_IC_* of dumses_gpu.h) written into
+ * uin, ghosts included: the same values, bit for bit, as the library's dg_condinit, so that
+ * the CPU baseline builds its workload without loading the library.  Returns DG_OK or
+ * DG_ERR_ARG (unknown problem, or one that needs another ndim). */
+int or_condinit(or_state *s, int ic, double beta, double amp, unsigned long long seed);
+
 /* threads used by OpenMP loops (0 = leave the runtime default) */
 void or_set_threads(int n);
 

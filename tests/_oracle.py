@@ -46,6 +46,8 @@ def lib() -> ctypes.CDLL:
         L.or_run_history.argtypes = [vp, ctypes.c_double, ctypes.c_double, dp, ctypes.c_int]
         L.or_array.restype, L.or_array.argtypes = dp, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
         L.or_set_threads.restype, L.or_set_threads.argtypes = None, [ctypes.c_int]
+        L.or_condinit.restype = ctypes.c_int
+        L.or_condinit.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong]
         _lib = L
     return _lib
 
@@ -97,6 +99,14 @@ class Oracle:
 
     def set_state(self, u: np.ndarray) -> None:
         self.uin[...] = u
+
+    def condinit(self, ic: str, beta: float = 1000.0, amp: float = 0.0, seed: int = 0) -> None:
+        """Write one of the library's initial conditions into uin (the oracle's own copy of
+        the problem set-up, equal bit for bit to dumses_hybrid_b200.condinit)."""
+        from dumses_hybrid_b200 import IC
+        rc = self.L.or_condinit(self.h, IC[ic], beta, amp, seed)
+        if rc != 0:
+            raise ValueError(f"or_condinit({ic!r}) returned {rc}")
 
     def compute_dt(self) -> float:
         return self.L.or_compute_dt(self.h)

@@ -57,3 +57,22 @@ def test_reference_arm_is_rank0_only(capsys):
 def test_single_process_max_is_identity():
     import bench
     assert bench.replica_max(3.5, None) == 3.5
+
+
+def test_reference_arm_loads_no_product_library():
+    """The reference arm runs the oracle alone: its initial state comes from the oracle's own
+    problem set-up, so libdumses_gpu.so is never mapped into the process."""
+    import json
+    import pathlib
+    import subprocess
+    import sys
+    root = pathlib.Path(__file__).resolve().parents[1]
+    code = ("import argparse, bench; bench.run_reference(argparse.Namespace(steps=1, warmup=1, workload='mri', gpus=1, "
+            "n=16, nu=0.0, eta=0.0), 0); print('MAPS', open('/proc/self/maps').read().count('libdumses_gpu'), "
+            "open('/proc/self/maps').read().count('liboracle'))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    line = json.loads(out.stdout.splitlines()[0])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["config"]["grid"] == [16, 16, 16]
+    maps = out.stdout.splitlines()[-1].split()
+    assert maps[0] == "MAPS" and int(maps[1]) == 0 and int(maps[2]) > 0
