@@ -246,6 +246,12 @@ __global__ void __launch_bounds__(kThreads) k_kick64(Geo G, double *__restrict__
     Q[G.sv * IV + c] = v + dvy * dt * half;
 }
 
+// 3D Riemann work as two kernels (faces, then edges) instead of one
+#ifndef DG_RIEMANN_SPLIT64
+#define DG_RIEMANN_SPLIT64 1
+#endif
+constexpr bool kRiemannSplit64 = DG_RIEMANN_SPLIT64 != 0;
+
 int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     const StoreD U = st(B, cur);
     double *Un = (double *)B.U[cur ^ 1];
@@ -266,11 +272,22 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
         TIMED(KS_TRACE, s, (k_trace3d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
-        // HLLD/HLLD (the reference's default and every benchmark) runs a kernel without the other solvers
-        if (G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD)
-            TIMED(KS_RIEMANN, s, (k_riemann3d<double, true><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, 1)));
-        else
-            TIMED(KS_RIEMANN, s, (k_riemann3d<double, false><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, 1)));
+        // HLLD/HLLD (the reference's default and every benchmark) runs kernels without the other solvers
+        const unsigned nb = nblocks(G.fsz, kThreads);
+        if (kRiemannSplit64) {
+            if (G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD) {
+                TIMED(KS_RIEMANN, s, (k_faces3d<double, true><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, B.S)));
+                TIMED(KS_RIEMANN, s, (k_edges3d<double, true><<<nb, kThreads, 0, s>>>(G, core, ex, ey, ez, B.S)));
+            } else {
+                TIMED(KS_RIEMANN, s, (k_faces3d<double, false><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, B.S)));
+                TIMED(KS_RIEMANN, s, (k_edges3d<double, false><<<nb, kThreads, 0, s>>>(G, core, ex, ey, ez, B.S)));
+            }
+            n++;
+        } else if (G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD) {
+            TIMED(KS_RIEMANN, s, (k_riemann3d<double, true><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, 1)));
+        } else {
+            TIMED(KS_RIEMANN, s, (k_riemann3d<double, false><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, 1)));
+        }
         TIMED(KS_UPDATE, s, (k_update3d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, fz, ex, ey, ez, B.S)));
     } else {
         TIMED(KS_EFIELD, s, (k_efield2d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2)));

@@ -1034,6 +1034,62 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 
         ex[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
 }
 
+// The same work split in two passes over the face index space: the face fluxes (1D solves)
+// and the edge EMFs (2D solves), each compiled for its own register budget.  A thread
+// holds the live values of one kind of solve only, so more warps fit an SM; the trace core
+// is read twice (once per pass).  Every solve is the same function of the same core values
+// as in k_riemann3d, so the results are identical.
+#ifndef DG_RFACE_MINB64
+#define DG_RFACE_MINB64 5
+#endif
+#ifndef DG_REDGE_MINB64
+#define DG_REDGE_MINB64 4
+#endif
+#ifndef DG_RFACE_MINB32
+#define DG_RFACE_MINB32 8
+#endif
+#ifndef DG_REDGE_MINB32
+#define DG_REDGE_MINB32 8
+#endif
+template <typename T, bool kHLLD>
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RFACE_MINB64 : DG_RFACE_MINB32))
+k_faces3d(Geo G, const T *__restrict__ core, T *__restrict__ fx, T *__restrict__ fy, T *__restrict__ fz,
+          const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const double dt = S->dt;
+    const CoreView<T> cv{core, kCore3};
+    const long long c = G.cidx(i, j, k);
+    if (j <= G.ny && k <= G.nz) face_flux<T, kHLLD>(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
+    if (i <= G.nx && k <= G.nz) face_flux<T, kHLLD>(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
+    if (i <= G.nx && j <= G.ny) face_flux<T, kHLLD>(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
+}
+
+template <typename T, bool kHLLD>
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_REDGE_MINB64 : DG_REDGE_MINB32))
+k_edges3d(Geo G, const T *__restrict__ core, T *__restrict__ ex, T *__restrict__ ey, T *__restrict__ ez,
+          const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.fsz) return;
+    const int i = (int)(t % G.FX) + 1;
+    const long long r = t / G.FX;
+    const int j = (int)(r % G.FY) + 1;
+    const int k = (int)(r / G.FY) + 1;
+    const double dt = S->dt;
+    const CoreView<T> cv{core, kCore3};
+    const long long c = G.cidx(i, j, k);
+    if (k <= G.nz)
+        ez[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
+    if (j <= G.ny)
+        ey[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
+    if (i <= G.nx)
+        ex[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                         T *__restrict__ fy, T *__restrict__ ez, const Scalars *S,
