@@ -176,12 +176,22 @@ int  dg_history(dg_ctx *ctx, double out[9]);
  *            (only variables 1-8 are read), on the calling thread's current device
  *   out_dev  9 device doubles, the same quantities as dg_history
  *   stream   cudaStream_t to enqueue on (NULL: the legacy default stream)
- * Needs ndim = 3 and nx <= DG_HISTORY_NOALLOC_MAX_NX (DG_ERR_ARG otherwise).
- * The reduction scratch is one file-scope device array per GPU, held until the
- * process exits; its address is looked up the first time the call runs on a
- * device, so make that first call before any stream capture.  All calls share
- * the array: calls that overlap on the GPU (different streams, no ordering)
- * race.  The call is asynchronous; out_dev is valid once the stream reaches it. */
+ * Needs ndim = 3, a non-empty domain and nx <= DG_HISTORY_NOALLOC_MAX_NX
+ * (DG_ERR_ARG otherwise).  uin_dev and out_dev must be device or managed memory
+ * of the current device: a host array (e.g. uin without `host_data use_device`)
+ * or another device's memory is refused with DG_ERR_ARG before any launch.  A
+ * CUDA error already pending in the calling thread is reported (DG_ERR_CUDA) and
+ * left pending for the caller.
+ * The reduction scratch is one file-scope device array per GPU (about 280 KB),
+ * held until the process exits; its address is looked up the first time the
+ * call runs on a device, so make that first call before any stream capture.
+ * With lazy module loading (the CUDA default) the driver places that array in
+ * device memory when the library's kernels are first used on a device, so make
+ * the first call at start-up, or run with CUDA_MODULE_LOADING=EAGER, if device
+ * memory must not grow later.  All calls share the array: calls that overlap on
+ * the GPU (different streams, no ordering) race.  The call is asynchronous;
+ * out_dev is valid once the stream reaches it (in the bounds-checked debug
+ * library the call waits for its kernels). */
 #define DG_HISTORY_NOALLOC_MAX_NX 16384
 int  dg_history_noalloc(const dg_params *p, const double *uin_dev, double *out_dev, void *stream);
 
@@ -234,9 +244,10 @@ const char *dg_last_error(void);
 
 /* ---- learned face-flux surrogate --------------------------------------------
  * No counterpart in the reference, whose face solver is always an exact one
- * (src/modules/solvers/solver.f90:163-187).  A 17 -> 128 -> 128 -> 128 -> 8 GELU
- * MLP with BF16 weights and FP32 accumulation on the tensor cores, trained on the
- * device by the library's own forward, backward and Adam kernels.  Per interface
+ * (src/modules/solvers/solver.f90:163-187).  A 17 -> 128 -> 128 -> 128 -> 8 MLP
+ * with SmeLU hidden activations (the smooth ReLU: 0, (z+1)^2/4 or z), BF16
+ * weights and FP32 accumulation on the tensor cores, trained on the device by
+ * the library's own forward, backward and Adam kernels.  Per interface
  * it predicts HLLD minus LLF of the same states.  States are scaled by the
  * interface's density rho0 = (rhoL+rhoR)/2, a speed a0 >= both fast speeds and the
  * field unit sqrt(rho0) a0 (rho / rho0, velocities / a0, P / (rho0 a0^2), fields
