@@ -32,8 +32,13 @@ state after the same steps.
 
 --impl reference times that CPU implementation alone (the reference itself is
 Fortran and no Fortran compiler exists on this image).
-With torchrun and N > 1 every rank runs an independent replica of the
-workload (the step is not decomposed across GPUs in this build).
+With torchrun and N > 1 the box is decomposed in z over the N processes (one GPU
+each, dumses_hybrid_b200.slabs): every GPU owns an n^3 slab of an n x n x (n N)
+box (weak scaling), the slabs exchange their 3-deep halos after every boundary
+call with NCCL point-to-point operations and take the CFL minimum with an NCCL
+all-reduce, as the reference's MPI ranks do (parallel.f90, physics.f90:123-129).
+--slabs S puts S slabs on each process (S > 1 on one GPU runs the same
+decomposed step with device copies for the halos).
 """
 from __future__ import annotations
 
@@ -153,8 +158,8 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def replica_barrier(dist, cuda: bool = True) -> None:
-    """All ranks (independent replicas) meet before and after a timed region."""
+def rank_barrier(dist, cuda: bool = True) -> None:
+    """All ranks meet before and after a timed region."""
     if dist is not None:
         dist.barrier()
     if cuda:
@@ -162,8 +167,8 @@ def replica_barrier(dist, cuda: bool = True) -> None:
         torch.cuda.synchronize()
 
 
-def replica_max(x: float, dist, device: str = "cuda") -> float:
-    """The largest value of x over the ranks (a timed region ends when its slowest replica does)."""
+def rank_max(x: float, dist, device: str = "cuda") -> float:
+    """The largest value of x over the ranks (a timed region ends when its slowest rank does)."""
     if dist is None:
         return x
     import torch
@@ -234,6 +239,9 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="mri")
     ap.add_argument("--nu", type=float, default=0.0, help="viscosity: adds the dissipation step (default off)")
     ap.add_argument("--eta", type=float, default=0.0, help="resistivity: adds the dissipation step (default off)")
+    ap.add_argument("--slabs", type=int, default=1,
+                    help="z slabs per process: with N processes the box is n x n x (n N slabs), one n^3 slab "
+                         "per slab (weak scaling); 1 with one process: the undecomposed n^3 box")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -269,14 +277,17 @@ def main() -> None:
         pass
 
     def barrier():
-        replica_barrier(dist, cuda=True)
+        rank_barrier(dist, cuda=True)
 
     def max_over_ranks(x: float) -> float:
-        return replica_max(x, dist, device="cuda")
+        return rank_max(x, dist, device="cuda")
 
     ncell = args.n ** 3
+    nzslice = world * args.slabs
 
     def measure(precision: str, with_e2e: bool) -> dict:
+        if nzslice > 1:
+            return measure_slabs(precision, with_e2e)
         surrogate = precision == "fp32nn"
         P = workload_params(args.n, device=local_rank, precision="fp32" if surrogate else precision,
                             kind=args.workload, nu=args.nu, eta=args.eta)
@@ -335,6 +346,7 @@ def main() -> None:
                 if P.fargo:
                     ctx.fargo_update(dt)
                 ctx.boundary(te, dt)
+                ctx.dissipation(te, dt)
                 te = te + dt
             ctx.download_into(host)
             e1.record(stream)
@@ -347,6 +359,112 @@ def main() -> None:
                           "finite": bool(np.isfinite(host[..., :8]).all())}
         ctx.close()
         if surrogate:
+            net.close()
+        return out
+
+    def measure_slabs(precision: str, with_e2e: bool) -> dict:
+        """The box cut into nzslice z slabs of n^3 (args.slabs per process, one process per GPU):
+        the reference's loop body over the slabs with the halo exchange (NCCL point-to-point
+        between processes, device copies within one) and the CFL minimum over all slabs."""
+        from dataclasses import replace as dc_replace
+
+        from dumses_hybrid_b200.slabs import SlabSet, slab_params
+        surrogate = precision == "fp32nn"
+        P = workload_params(args.n, device=local_rank, precision="fp32" if surrogate else precision,
+                            kind=args.workload, nu=args.nu, eta=args.eta)
+        zlo, zhi = (-0.5 * nzslice, 0.5 * nzslice) if args.workload == "mri" else (0.0, float(nzslice))
+        box = dc_replace(P, nz=args.n * nzslice, zmin=zlo, zmax=zhi)
+        S = SlabSet(box, nzslice, dist=dist, device=local_rank)
+        # each slab's own initial state: the workload's set-up on the slab's cells (velocity
+        # kicks seeded per slab)
+        u0s = []
+        for sp in S.params:
+            if args.workload == "mri":
+                u0s.append(dg.condinit(sp, "mri", beta=1000.0, amp=0.1, seed=2024 + 7919 * sp.zposition))
+            else:
+                u0s.append(dg.condinit(sp, "orszag_tang"))
+        nets = []
+        if surrogate:
+            for c, u in zip(S.ctxs, u0s):
+                c.close()
+            one = dc_replace(P, surrogate=False)
+            S.ctxs = []
+            for sp, u in zip(S.params, u0s):
+                torch.cuda.synchronize()
+                net, nn_info = train_flux_net(one, u, snapshots=args.nn_snapshots, every=args.nn_every,
+                                              stride=args.nn_stride, epochs=args.nn_epochs, batch=args.nn_batch)
+                nets.append(net)
+                c = dg.Context(dc_replace(sp, surrogate=True))
+                c.attach_surrogate(net)
+                S.ctxs.append(c)
+            S.params = [dc_replace(sp, surrogate=True) for sp in S.params]
+            S.rebuild_exchange()
+        stream = torch.cuda.ExternalStream(S.ctxs[0].stream)
+        S.upload(u0s)
+        S.boundary(0.0, 0.0)
+        t_sim = 0.0
+        for _ in range(args.warmup):
+            t_sim, _ = S.step(t_sim)
+        S.sync()
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        S.ctxs[0].profile(True)
+        S.ctxs[0].profile_read()
+        launches0 = sum(c.kernel_launches for c in S.ctxs)
+        with ClockSampler(uuid) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                t_sim, _ = S.step(t_sim)
+            S.sync()
+            ev1.record(stream)
+            ev1.synchronize()
+        barrier()
+        out = {"launches": sum(c.kernel_launches for c in S.ctxs) - launches0, "prof": S.ctxs[0].profile_read(),
+               "clocks": clk.summary()}
+        if surrogate:
+            faces = fallback = 0
+            for c in S.ctxs:
+                a, b = c.surrogate_stats()
+                faces, fallback = faces + a, fallback + b
+            nn_info["faces_timed"] = faces
+            nn_info["fallback_fraction"] = fallback / max(faces, 1)
+            out["nn"] = nn_info
+        S.ctxs[0].profile(False)
+        out["ms"] = max_over_ranks(ev0.elapsed_time(ev1))
+        out["value"] = nzslice * ncell * args.steps / (out["ms"] / 1e3)
+        out["state"] = S.ctxs[0].download() if rank == 0 else None
+        out["sim_time"] = t_sim
+        if with_e2e:
+            # end-to-end through the public API: every slab's state uploaded from pinned host
+            # memory, the loop with the host-side CFL minimum and the exchange, the states downloaded
+            nt = (args.n + 6) ** 3
+            hosts = []
+            for u in u0s:
+                pinned = torch.empty((11, args.n + 6, args.n + 6, args.n + 6), dtype=torch.float64, pin_memory=True)
+                h = pinned.numpy().T
+                h[...] = u
+                hosts.append(h)
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            S.upload(hosts)
+            S.boundary(0.0, 0.0)
+            te = 0.0
+            for _ in range(args.steps):
+                te, _ = S.step(te)
+            for c, h in zip(S.ctxs, hosts):
+                c.download_into(h)
+            S.sync()
+            e1.record(stream)
+            e1.synchronize()
+            barrier()
+            ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+            out["e2e"] = {"value": nzslice * ncell * args.steps / (ms_e2e / 1e3), "unit": "zone-cycles/s",
+                          "h2d_bytes_per_step": len(hosts) * 8 * nt * 8 / args.steps,
+                          "d2h_bytes_per_step": len(hosts) * ((11 * nt * 8) / args.steps + 8),
+                          "finite": bool(all(np.isfinite(h[..., :8]).all() for h in hosts))}
+        S.close()
+        for net in nets:
             net.close()
         return out
 
@@ -439,7 +557,9 @@ def main() -> None:
             "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32", "data": "synthetic",
             "config": {"workload": f"{WORKLOADS[args.workload]}_{args.n}^3", "grid": [args.n] * 3,
                        "arithmetic": arith[head], "solver": "hlld/hlld", "slope": "mc", "courant": 0.8,
-                       "parallelism": f"replicas x{world}",
+                       "parallelism": (f"z slabs x{nzslice} ({world} processes, NCCL halo exchange)" if nzslice > 1
+                                       else "one GPU"),
+                       **({"box": [args.n, args.n, args.n * nzslice]} if nzslice > 1 else {}),
                        "l2": "working set 8-13 GB per step >> 126 MB L2, no flush needed",
                        **({"nu": args.nu, "eta": args.eta} if args.nu > 0 or args.eta > 0 else {})},
             "e2e": h["e2e"], "gpu_launches": h["launches"], "roofline": roofline(h, head if head != "fp32nn" else "fp32"),

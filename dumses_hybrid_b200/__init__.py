@@ -55,7 +55,7 @@ class DgParams(ctypes.Structure):
                 ("iriemann", ctypes.c_int), ("iriemann2d", ctypes.c_int), ("bc", ctypes.c_int * 3),
                 ("fargo", ctypes.c_int), ("precision", ctypes.c_int), ("surrogate", ctypes.c_int),
                 ("device", ctypes.c_int), ("nu", ctypes.c_double), ("eta", ctypes.c_double),
-                ("reserved", ctypes.c_int * 6)]
+                ("nzslice", ctypes.c_int), ("zposition", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 class DgDumpInfo(ctypes.Structure):
@@ -114,6 +114,11 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_stream": (vp, [vp]),
         "dg_last_error": (ctypes.c_char_p, []),
         "dg_history_noalloc": (ctypes.c_int, [c_p, vp, vp, vp]),
+        "dg_halo_count": (ctypes.c_longlong, [vp]),
+        "dg_halo_pack": (ctypes.c_int, [vp, ctypes.c_int, vp]),
+        "dg_halo_unpack": (ctypes.c_int, [vp, ctypes.c_int, vp]),
+        "dg_history_columns": (ctypes.c_int, [vp, dp]),
+        "dg_history_share": (ctypes.c_int, [vp, dp, dp]),
         "dg_profile": (ctypes.c_int, [vp, ctypes.c_int]),
         "dg_profile_read": (ctypes.c_int, [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
         "dg_profile_slot_name": (ctypes.c_char_p, [ctypes.c_int]),
@@ -183,6 +188,8 @@ class Params:
     device: int = 0
     nu: float = 0.0
     eta: float = 0.0
+    nzslice: int = 1      # z slabs of a decomposed box (nz = this slab's share)
+    zposition: int = 0    # this slab's place, 0 .. nzslice-1
 
     def to_c(self) -> DgParams:
         p = DgParams()
@@ -194,6 +201,7 @@ class Params:
         p.bc[0], p.bc[1], p.bc[2] = BC[self.bdtypex], BC[self.bdtypey], BC[self.bdtypez]
         p.fargo, p.precision, p.surrogate, p.device = int(self.fargo), PREC[self.precision], int(self.surrogate), self.device
         p.nu, p.eta = self.nu, self.eta
+        p.nzslice, p.zposition = self.nzslice, self.zposition
         return p
 
     @property
@@ -441,6 +449,33 @@ class Context:
         cnt = (ctypes.c_longlong * n)()
         _check(self.lib.dg_profile_read(self.h, self._ptr(ms), cnt, n))
         return {self.lib.dg_profile_slot_name(k).decode(): (float(ms[k]), int(cnt[k])) for k in range(n) if cnt[k]}
+
+    # ---- z-slab decomposition (see dumses_hybrid_b200.slabs) ----
+    @property
+    def halo_count(self) -> int:
+        """Doubles in one z halo of this context (3 planes of every stored state plane)."""
+        return int(self.lib.dg_halo_count(self.h))
+
+    def halo_pack(self, side: int, dev_ptr: int) -> None:
+        """Copy the slab's 3 lowest (side 0) or highest (side 1) active planes to a device buffer."""
+        _check(self.lib.dg_halo_pack(self.h, side, ctypes.c_void_p(dev_ptr)))
+
+    def halo_unpack(self, side: int, dev_ptr: int) -> None:
+        """Copy a neighbour's halo into the 3 ghost planes below (side 0) or above (side 1)."""
+        _check(self.lib.dg_halo_unpack(self.h, side, ctypes.c_void_p(dev_ptr)))
+
+    def history_columns(self) -> np.ndarray:
+        """This slab's per-x-column sums of v_x and v_y, shape (nx, 2)."""
+        col = np.zeros(2 * self.params.nx)
+        _check(self.lib.dg_history_columns(self.h, self._ptr(col)))
+        return col.reshape(self.params.nx, 2)
+
+    def history_share(self, colmean: np.ndarray) -> np.ndarray:
+        """This slab's share of the 9 history values, given the box's column means (nx, 2)."""
+        cm = np.ascontiguousarray(colmean, dtype=np.float64).reshape(-1)
+        out = np.zeros(9)
+        _check(self.lib.dg_history_share(self.h, self._ptr(cm), self._ptr(out)))
+        return out
 
     @property
     def stream(self) -> int:

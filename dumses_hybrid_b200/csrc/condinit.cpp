@@ -21,6 +21,7 @@ struct Grid {
     int iu1, iu2, ju1, ju2, ku1, ku2;
     long n0, n1, n2;
     double dx, dy, dz;
+    double zoff;  // a z slab's offset dz * nz * zposition (init.f90:491), 0 for one domain
     explicit Grid(const dg_params &p) {
         ndim = p.ndim; nx = p.nx; ny = p.ny; nz = p.nz;
         iu1 = -2; iu2 = nx + 3;
@@ -30,7 +31,9 @@ struct Grid {
         n0 = iu2 - iu1 + 1; n1 = ju2 - ju1 + 1; n2 = ku2 - ku1 + 1;
         dx = (p.xmax - p.xmin) / nx;
         dy = (p.ymax - p.ymin) / ny;
-        dz = (p.zmax - p.zmin) / nz;
+        const int nzslice = p.nzslice > 1 ? p.nzslice : 1;
+        dz = (p.zmax - p.zmin) / (nz * nzslice);
+        zoff = nzslice > 1 ? dz * nz * p.zposition : 0.0;
     }
     long idx(int i, int j, int k, int v) const {
         return (i - iu1) + n0 * ((j - ju1) + n1 * ((k - ku1) + n2 * (long)(v - 1)));
@@ -38,7 +41,9 @@ struct Grid {
     // cell centres as init_grid computes them (init.f90:461-501)
     double x(const dg_params &p, int i) const { return p.xmin + dx / 2 + (i - 1) * dx; }
     double y(const dg_params &p, int j) const { return p.ymin + dy / 2 + (j - 1) * dy; }
-    double z(const dg_params &p, int k) const { return p.zmin + dz / 2 + (k - 1) * dz; }
+    double z(const dg_params &p, int k) const {
+        return zoff != 0.0 ? p.zmin + zoff + dz / 2 + (k - 1) * dz : p.zmin + dz / 2 + (k - 1) * dz;
+    }
 };
 
 uint64_t splitmix64(uint64_t x) {

@@ -59,6 +59,8 @@ struct Launches {
     int (*fargo)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*boundary)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*history)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*history_columns)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*history_share)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*dissipation)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*right_faces)(const dg::Geo &, const dg::Bufs &, int, double *, cudaStream_t);
     int (*to_f64)(const dg::Geo &, const dg::Bufs &, int, double *, cudaStream_t);
@@ -66,7 +68,8 @@ struct Launches {
 };
 #define DG_LAUNCH_TABLE(ns)                                                                                  \
     Launches{ns::launch_set_scalars, ns::launch_advance_time, ns::launch_dt, ns::launch_godunov, ns::launch_fargo, \
-             ns::launch_boundary, ns::launch_history, ns::launch_dissipation, ns::launch_right_faces,        \
+             ns::launch_boundary, ns::launch_history, ns::launch_history_columns, ns::launch_history_share,   \
+             ns::launch_dissipation, ns::launch_right_faces,                                                 \
              ns::launch_state_to_f64, ns::launch_f64_to_state}
 const Launches kLaunchF64 = DG_LAUNCH_TABLE(dg::f64);
 const Launches kLaunchF32 = DG_LAUNCH_TABLE(dg::f32);
@@ -197,6 +200,15 @@ int validate(const dg_params *p) {
     if (!(p->nu >= 0.0) || !(p->eta >= 0.0)) return fail(DG_ERR_ARG, "nu and eta must be >= 0");
     if (p->surrogate && p->iriemann != DG_RIEMANN_HLLD)
         return fail(DG_ERR_UNSUPPORTED, "the flux surrogate stands in for HLLD (iriemann = hlld)");
+    if (p->nzslice < 0) return fail(DG_ERR_ARG, "nzslice must be >= 0");
+    if (p->nzslice > 1) {
+        if (p->ndim != 3) return fail(DG_ERR_UNSUPPORTED, "a z-slab decomposition needs ndim = 3");
+        if (p->zposition < 0 || p->zposition >= p->nzslice) return fail(DG_ERR_ARG, "zposition must be in [0, nzslice)");
+        if (p->bc[2] != DG_BC_PERIODIC && p->bc[2] != DG_BC_ZERO_GRADIENT)
+            return fail(DG_ERR_UNSUPPORTED, "z slabs need a periodic or zero-gradient z boundary");
+    } else if (p->zposition != 0) {
+        return fail(DG_ERR_ARG, "zposition must be 0 without a z-slab decomposition");
+    }
     return DG_OK;
 }
 
@@ -227,7 +239,10 @@ dg::Geo dg::make_geo(const dg_params &p) {
     // init_grid (init.f90:447-449), single rank
     G.dx = (p.xmax - p.xmin) / p.nx;
     G.dy = (p.ymax - p.ymin) / p.ny;
-    G.dz = (p.zmax - p.zmin) / p.nz;
+    // a z slab's dz is that of the whole box, (zmax - zmin) / nzglob (init.f90:447-449)
+    G.nzslice = p.nzslice > 1 ? p.nzslice : 1;
+    G.zposition = p.nzslice > 1 ? p.zposition : 0;
+    G.dz = (p.zmax - p.zmin) / (p.nz * G.nzslice);
     G.xmin = p.xmin; G.xmax = p.xmax; G.ymin = p.ymin; G.ymax = p.ymax; G.zmin = p.zmin; G.zmax = p.zmax;
     G.gamma = p.gamma; G.ciso = p.ciso; G.omega0 = p.omega0; G.courant = p.courant;
     G.nu = p.nu; G.eta = p.eta;
@@ -235,6 +250,12 @@ dg::Geo dg::make_geo(const dg_params &p) {
     G.fargo = p.fargo;
     G.shearing = (p.bc[0] == DG_BC_SHEARINGBOX);
     for (int d = 0; d < 3; d++) G.bc[d] = p.bc[d];
+    // slab sides: a neighbour's halo, except a zero-gradient box edge, which the slab fills itself
+    G.bcz_lo = G.bcz_hi = p.bc[2];
+    if (G.nzslice > 1) {
+        G.bcz_lo = (p.bc[2] == DG_BC_ZERO_GRADIENT && G.zposition == 0) ? DG_BC_ZERO_GRADIENT : dg::kBcHalo;
+        G.bcz_hi = (p.bc[2] == DG_BC_ZERO_GRADIENT && G.zposition == G.nzslice - 1) ? DG_BC_ZERO_GRADIENT : dg::kBcHalo;
+    }
     // ndim_act, init.f90:203-213
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     if ((nx == 1 && ny == 1) || (nx == 1 && nz == 1) || (ny == 1 && nz == 1)) G.ndim_act = 1;
@@ -449,7 +470,8 @@ dg::dump::Header make_header(const dg_params &p, double time, double dt) {
     const dg::Geo G = dg::make_geo(p);
     dg::dump::Header h{};
     h.nx = p.nx; h.ny = p.ny; h.nz = p.nz;
-    h.nxslice = h.nyslice = h.nzslice = 1;  // one rank
+    h.nxslice = h.nyslice = 1;
+    h.nzslice = G.nzslice;  // a z slab writes its own rank's file, as each MPI rank does
     h.time = time; h.dt = dt; h.dx = G.dx; h.dy = G.dy; h.dz = G.dz;
     h.xmin = p.xmin; h.xmax = p.xmax; h.ymin = p.ymin; h.ymax = p.ymax; h.zmin = p.zmin; h.zmax = p.zmax;
     h.gamma = p.gamma; h.ciso = p.ciso;
@@ -458,8 +480,11 @@ dg::dump::Header make_header(const dg_params &p, double time, double dt) {
 
 // a dump read into a context (or a host array of its grid) must hold the same grid and constants
 int check_header(const dg::dump::Header &h, const dg_params &p, const char *path) {
-    if (h.nxslice != 1 || h.nyslice != 1 || h.nzslice != 1)
-        return fail(DG_ERR_UNSUPPORTED, std::string(path) + ": a dump of one rank of a decomposed run");
+    const int nzslice = p.nzslice > 1 ? p.nzslice : 1;
+    if (h.nxslice != 1 || h.nyslice != 1 || h.nzslice != nzslice)
+        return fail(DG_ERR_UNSUPPORTED, std::string(path) + ": a dump of another decomposition (slices " +
+                                            std::to_string(h.nxslice) + "x" + std::to_string(h.nyslice) + "x" +
+                                            std::to_string(h.nzslice) + ")");
     if (h.nx != p.nx || h.ny != p.ny || h.nz != p.nz)
         return fail(DG_ERR_ARG, std::string(path) + ": grid " + std::to_string(h.nx) + "x" + std::to_string(h.ny) +
                                     "x" + std::to_string(h.nz) + " differs from the context's");
@@ -716,6 +741,9 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
     TimerScope ts_(c);
     if (!c || !time) return fail(DG_ERR_ARG, "null argument");
     if (nsteps < 0) return fail(DG_ERR_ARG, "nsteps < 0");
+    if (c->G.nzslice > 1)
+        return fail(DG_ERR_UNSUPPORTED, "a z slab needs its halos exchanged every step: drive it with dg_compute_dt, "
+                                        "dg_godunov, dg_fargo_update, dg_boundary and dg_halo_pack/unpack");
     c->launches += c->L->set_scalars(c->B, 0.0, *time, 0, 1, c->stream);
     for (int n = 0; n < nsteps; n++) {
         c->launches += c->L->dt(c->G, c->B, c->cur, c->stream);
@@ -750,6 +778,85 @@ int dg_history(dg_ctx *c, double out[9]) {
     if (rc) return rc;
     DG_CUDA(cudaMemcpyAsync(c->h_hist, c->B.hist, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if ((rc = bounded_sync(c->stream))) return rc;
+    std::memcpy(out, c->h_hist, 9 * sizeof(double));
+    return DG_OK;
+}
+
+// ---- z-slab halos: 3 planes of every stored state plane (FP64: nv double planes;
+// FP32: 2 nv float planes, hi then lo), one strided copy per side
+namespace {
+struct HaloGeom {
+    size_t width;   // bytes of 3 planes of one stored plane
+    size_t pitch;   // bytes between stored planes
+    size_t planes;  // stored planes
+    size_t es;      // bytes per element of the state
+};
+HaloGeom halo_geom(const dg_ctx *c) {
+    const bool f64 = c->p.precision == DG_PREC_FP64;
+    HaloGeom h;
+    h.es = f64 ? 8 : 4;
+    h.planes = f64 ? (size_t)c->nv : 2 * (size_t)c->nv;
+    h.width = 3 * (size_t)c->G.sz * h.es;
+    h.pitch = (size_t)c->G.sv * h.es;
+    return h;
+}
+int halo_check(const dg_ctx *c, int side, const void *buf) {
+    if (!c || !buf) return fail(DG_ERR_ARG, "null argument");
+    if (side != 0 && side != 1) return fail(DG_ERR_ARG, "side must be 0 (lower) or 1 (upper)");
+    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "z halos exist for ndim = 3");
+    return DG_OK;
+}
+}  // namespace
+
+long long dg_halo_count(const dg_ctx *c) {
+    if (!c || c->p.ndim != 3) return 0;
+    return 3LL * c->G.sz * c->nv;
+}
+
+int dg_halo_pack(dg_ctx *c, int side, double *buf) {
+    if (int rc = halo_check(c, side, buf)) return rc;
+    DG_CUDA(cudaSetDevice(c->p.device));
+    const HaloGeom h = halo_geom(c);
+    // active planes k = 1..3 (side 0) or nz-2..nz (side 1): plane k starts at (k + 2) * sz
+    const size_t k0 = side == 0 ? 3 : (size_t)c->G.nz;
+    const char *src = (const char *)c->B.U[c->cur] + k0 * (size_t)c->G.sz * h.es;
+    DG_CUDA(cudaMemcpy2DAsync(buf, h.width, src, h.pitch, h.width, h.planes, cudaMemcpyDefault, c->stream));
+    return DG_OK;
+}
+
+int dg_halo_unpack(dg_ctx *c, int side, const double *buf) {
+    if (int rc = halo_check(c, side, buf)) return rc;
+    DG_CUDA(cudaSetDevice(c->p.device));
+    const HaloGeom h = halo_geom(c);
+    // ghost planes k = -2..0 (side 0, from 0) or nz+1..nz+3 (side 1, from (nz + 3) * sz)
+    const size_t k0 = side == 0 ? 0 : (size_t)c->G.nz + 3;
+    char *dst = (char *)c->B.U[c->cur] + k0 * (size_t)c->G.sz * h.es;
+    DG_CUDA(cudaMemcpy2DAsync(dst, h.pitch, buf, h.width, h.width, h.planes, cudaMemcpyDefault, c->stream));
+    c->version++;
+    return DG_OK;
+}
+
+int dg_history_columns(dg_ctx *c, double *col) {
+    TimerScope ts_(c);
+    if (!c || !col) return fail(DG_ERR_ARG, "null argument");
+    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the MRI history is defined for ndim = 3");
+    DG_CUDA(cudaSetDevice(c->p.device));
+    c->launches += c->L->history_columns(c->G, c->B, c->cur, c->stream);
+    if (int rc = check_launch()) return rc;
+    DG_CUDA(cudaMemcpyAsync(col, c->B.part, 2 * (size_t)c->G.nx * sizeof(double), cudaMemcpyDefault, c->stream));
+    return bounded_sync(c->stream);
+}
+
+int dg_history_share(dg_ctx *c, const double *colmean, double out[9]) {
+    TimerScope ts_(c);
+    if (!c || !colmean || !out) return fail(DG_ERR_ARG, "null argument");
+    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the MRI history is defined for ndim = 3");
+    DG_CUDA(cudaSetDevice(c->p.device));
+    DG_CUDA(cudaMemcpyAsync(c->B.part, colmean, 2 * (size_t)c->G.nx * sizeof(double), cudaMemcpyDefault, c->stream));
+    c->launches += c->L->history_share(c->G, c->B, c->cur, c->stream);
+    if (int rc = check_launch()) return rc;
+    DG_CUDA(cudaMemcpyAsync(c->h_hist, c->B.hist, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (int rc = bounded_sync(c->stream)) return rc;
     std::memcpy(out, c->h_hist, 9 * sizeof(double));
     return DG_OK;
 }

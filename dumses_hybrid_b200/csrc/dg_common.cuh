@@ -51,6 +51,10 @@ struct Geo {
     int iso, slope_type, iriemann, iriemann2d, fargo, shearing;
     int bc[3];
     int ndim_act;
+    // z-slab decomposition: slabs, this slab's position, and the boundary of its lower and
+    // upper z sides (bc[2], or kBcHalo where the neighbour's halo fills the ghost planes)
+    int nzslice, zposition;
+    int bcz_lo, bcz_hi;
 
     __host__ __device__ __forceinline__ long long idx(int i, int j, int k) const {
         return (long long)(i + 2) + sy * (long long)(j + gy - 1) + sz * (long long)(k + gz - 1);
@@ -67,6 +71,9 @@ struct Geo {
     // cell centre x(i) = xmin + dx/2 + (i-1) dx (init.f90:461-468)
     __host__ __device__ __forceinline__ double xc(int i) const { return xmin + dx / 2 + (i - 1) * dx; }
 };
+
+// z side of a slab whose ghost planes are filled from the neighbour slab's halo
+constexpr int kBcHalo = 3;
 
 // Scalars that stay on the device across steps (dt, time, CFL reduction).
 struct Scalars {

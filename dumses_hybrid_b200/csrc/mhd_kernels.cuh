@@ -57,6 +57,10 @@ extern thread_local KernelTimer *g_timer;  // set by the context that enqueues (
     int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t st);     /* U[cur] -> U[cur^1] */ \
     int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t st);  /* in place on U[cur] */ \
     int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st);                       \
+    /* z slabs: per-column sums of v_x, v_y into B.part (2 nx doubles); then this slab's share of */ \
+    /* the history with the box's column means read from B.part, into B.hist */                      \
+    int launch_history_columns(const Geo &G, const Bufs &B, int cur, cudaStream_t st);               \
+    int launch_history_share(const Geo &G, const Bufs &B, int cur, cudaStream_t st);                 \
     int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t st); /* in place, then boundary */ \
     int launch_right_faces(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t st);      \
     int launch_state_to_f64(const Geo &G, const Bufs &B, int cur, double *out, cudaStream_t st);     \

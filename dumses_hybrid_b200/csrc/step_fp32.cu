@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kThreads) k_fargo_emf_hl(Geo G, StoreHL U, flo
     const double dt = S->dt;
     const float dy = (float)G.dy;
     const int ny = G.ny, ist = mn(G.slope_type, 2);
-    const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
+    const int kw = fargo_zplane(G, k);
     // the sum over the shifted-through cells and the fractional donor (get_emfx / get_emfz)
     auto line = [&](int v, float sgn, const FargoShift &f, float *out) {
         auto A = [&](int jj) { return hl_at(G, U, v, G.idx(i, jj, kw)); };
@@ -788,6 +788,12 @@ int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     return 3;
 }
 
+// 3D Riemann work as two kernels (faces, then edges) instead of one
+#ifndef DG_RIEMANN_SPLIT32
+#define DG_RIEMANN_SPLIT32 0
+#endif
+constexpr bool kRiemannSplit32 = DG_RIEMANN_SPLIT32 != 0;
+
 int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     const StoreHL U = st(B, cur), Un = st(B, cur ^ 1);
     float *Q = (float *)B.Q, *core = (float *)B.core;
@@ -825,11 +831,22 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         faces = 0;
     }
     if (G.ndim == 3) {
-        // HLLD/HLLD (the reference's default and every benchmark) runs a kernel without the other solvers
-        if (G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD)
-            TIMED(KS_RIEMANN, s, (k_riemann3d<float, true><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
-        else
-            TIMED(KS_RIEMANN, s, (k_riemann3d<float, false><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
+        // HLLD/HLLD (the reference's default and every benchmark) runs kernels without the other solvers
+        const bool hlld = G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD;
+        const unsigned nb = nblocks(G.fsz, kThreads);
+        if (kRiemannSplit32) {
+            if (faces) {
+                if (hlld) TIMED(KS_RIEMANN, s, (k_faces3d<float, true><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, B.S)));
+                else TIMED(KS_RIEMANN, s, (k_faces3d<float, false><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, B.S)));
+                n++;
+            }
+            if (hlld) TIMED(KS_RIEMANN, s, (k_edges3d<float, true><<<nb, kThreads, 0, s>>>(G, core, ex, ey, ez, B.S)));
+            else TIMED(KS_RIEMANN, s, (k_edges3d<float, false><<<nb, kThreads, 0, s>>>(G, core, ex, ey, ez, B.S)));
+        } else if (hlld) {
+            TIMED(KS_RIEMANN, s, (k_riemann3d<float, true><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
+        } else {
+            TIMED(KS_RIEMANN, s, (k_riemann3d<float, false><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, faces)));
+        }
     } else {
         TIMED(KS_RIEMANN, s, (k_riemann2d<float><<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, core, fx, fy, ez, B.S, faces)));
     }
@@ -942,6 +959,18 @@ int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     TIMED(KS_HISTORY, s, (k_hist_sums<StoreHL><<<nb, 256, 0, s>>>(G, st(B, cur), B.part, B.part + 2 * G.nx)));
     TIMED(KS_HISTORY, s, (k_hist_final<<<1, 32, 0, s>>>(G, B.part + 2 * G.nx, nb, B.hist)));
     return 3;
+}
+
+int launch_history_columns(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    TIMED(KS_HISTORY, s, (k_hist_yzmean<StoreHL><<<G.nx, 256, 0, s>>>(G, st(B, cur), B.part, 1)));
+    return 1;
+}
+
+int launch_history_share(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+    const int nb = 296;
+    TIMED(KS_HISTORY, s, (k_hist_sums<StoreHL><<<nb, 256, 0, s>>>(G, st(B, cur), B.part, B.part + 2 * G.nx)));
+    TIMED(KS_HISTORY, s, (k_hist_final<<<1, 32, 0, s>>>(G, B.part + 2 * G.nx, nb, B.hist)));
+    return 2;
 }
 
 #include "debug_bounds.cuh"

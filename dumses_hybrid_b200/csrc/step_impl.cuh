@@ -229,8 +229,10 @@ __global__ void k_dt_reset(Geo G, Scalars *S) {
 __global__ void k_dt_final(Geo G, Scalars *S) {
     double m = __longlong_as_double((long long)S->red);
     double dt = G.courant * m;
-    S->dt = dt;
     if (!(dt > 0.0) || !isfinite(dt)) S->err = DG_ERR_DT;
+    // after a failed CFL pass (a non-finite state, or no valid step) the steps that dg_run has
+    // already enqueued behind it run with dt = 0 and change nothing; the host reports the error
+    S->dt = S->err ? 0.0 : dt;
 }
 
 // primitive variables of one cell in FP64 (scheme.f90:44-86); the right faces are the
@@ -1040,7 +1042,7 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 
 // is read twice (once per pass).  Every solve is the same function of the same core values
 // as in k_riemann3d, so the results are identical.
 #ifndef DG_RFACE_MINB64
-#define DG_RFACE_MINB64 5
+#define DG_RFACE_MINB64 4
 #endif
 #ifndef DG_REDGE_MINB64
 #define DG_REDGE_MINB64 4
@@ -1051,7 +1053,8 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 
 #ifndef DG_REDGE_MINB32
 #define DG_REDGE_MINB32 8
 #endif
-template <typename T, bool kHLLD>
+// kDir: the one direction this launch solves (0, 1, 2), or -1 for all three
+template <typename T, bool kHLLD, int kDir = -1>
 __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RFACE_MINB64 : DG_RFACE_MINB32))
 k_faces3d(Geo G, const T *__restrict__ core, T *__restrict__ fx, T *__restrict__ fy, T *__restrict__ fz,
           const Scalars *S) {
@@ -1064,12 +1067,12 @@ k_faces3d(Geo G, const T *__restrict__ core, T *__restrict__ fx, T *__restrict__
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore3};
     const long long c = G.cidx(i, j, k);
-    if (j <= G.ny && k <= G.nz) face_flux<T, kHLLD>(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
-    if (i <= G.nx && k <= G.nz) face_flux<T, kHLLD>(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
-    if (i <= G.nx && j <= G.ny) face_flux<T, kHLLD>(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
+    if ((kDir < 0 || kDir == 0) && j <= G.ny && k <= G.nz) face_flux<T, kHLLD>(G, cv, G.cidx(i - 1, j, k), c, 0, i, dt, fx, t);
+    if ((kDir < 0 || kDir == 1) && i <= G.nx && k <= G.nz) face_flux<T, kHLLD>(G, cv, G.cidx(i, j - 1, k), c, 1, i, dt, fy, t);
+    if ((kDir < 0 || kDir == 2) && i <= G.nx && j <= G.ny) face_flux<T, kHLLD>(G, cv, G.cidx(i, j, k - 1), c, 2, i, dt, fz, t);
 }
 
-template <typename T, bool kHLLD>
+template <typename T, bool kHLLD, int kDir = -1>
 __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_REDGE_MINB64 : DG_REDGE_MINB32))
 k_edges3d(Geo G, const T *__restrict__ core, T *__restrict__ ex, T *__restrict__ ey, T *__restrict__ ez,
           const Scalars *S) {
@@ -1082,11 +1085,11 @@ k_edges3d(Geo G, const T *__restrict__ core, T *__restrict__ ex, T *__restrict__
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore3};
     const long long c = G.cidx(i, j, k);
-    if (k <= G.nz)
+    if ((kDir < 0 || kDir == 2) && k <= G.nz)
         ez[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i - 1, j - 1, k), G.cidx(i, j - 1, k), G.cidx(i - 1, j, k), c, 2, i, dt);
-    if (j <= G.ny)
+    if ((kDir < 0 || kDir == 1) && j <= G.ny)
         ey[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i - 1, j, k - 1), G.cidx(i - 1, j, k), G.cidx(i, j, k - 1), c, 1, i, dt);
-    if (i <= G.nx)
+    if ((kDir < 0 || kDir == 0) && i <= G.nx)
         ex[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
 }
 
@@ -1205,6 +1208,8 @@ __global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, c
         const unsigned r = u0 / NX;
         j = (int)(r % NY) - 2;
         k = ghost((int)(r / NY), G.nz);
+        // a z slab's ghost planes on a neighbour's side come from its halo (dg_halo_unpack)
+        if ((k < 1 ? G.bcz_lo : G.bcz_hi) == kBcHalo) return;
     } else if (u0 - nA < nB) {
         const unsigned u = u0 - nA;
         i = (int)(u % NX) - 2;
@@ -1220,7 +1225,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, c
     }
     const bool gx = (i < 1 || i > G.nx);
     const int jj = (G.ndim > 1) ? map_bc(G.bc[1], j, G.ny) : 1;
-    const int kk = (G.ndim == 3) ? map_bc(G.bc[2], k, G.nz) : 1;
+    const int kk = (G.ndim == 3) ? map_bc(k < 1 ? G.bcz_lo : G.bcz_hi, k, G.nz) : 1;
     const long long c = G.idx(i, j, k);
     // every value is read (from active cells, or the outer x face that no thread writes)
     // before the first store, so the loads of all variables are in flight together
@@ -1331,7 +1336,10 @@ struct FargoShift {
 __device__ __forceinline__ FargoShift fargo_shift(const Geo &G, double xpos, double dt) {
     FargoShift f;
     f.vK = -1.5 * G.omega0 * xpos;
-    f.nshft = (int)(fabs(f.vK * dt) / G.dy);
+    // whole cells of the shift; a shift of a box length or more (a step far beyond the CFL
+    // limit, or a non-finite dt) is held at ny, so the loops over the shifted cells stay bounded
+    const double cells = fabs(f.vK * dt) / G.dy;
+    f.nshft = cells < (double)G.ny ? (int)cells : G.ny;
     f.eps = fmod(fabs(f.vK * dt), G.dy);
     f.eps = f.eps / G.dy;
     return f;
@@ -1384,6 +1392,15 @@ __device__ __forceinline__ int fargo_src(const FargoShift &f, int j, int ny) {
     return wrap1(js, ny);
 }
 __device__ __forceinline__ int next_row(int j, int ny) { return j + 1 > ny ? j + 1 - ny : j + 1; }
+// The z plane that FARGO's EMFs read for face plane k (1..nz+1).  The reference refreshes the
+// z ghosts first (fargo.f90:36-49), so plane nz+1 holds its boundary copy: plane 1 when
+// periodic, plane nz when zero-gradient.  In a z slab the reference exchanges that plane with
+// the upper neighbour (boundary_z); the top face plane this slab's godunov updated holds the
+// same values (its EMFs come from the neighbour's halo cells), so the slab reads it directly.
+__device__ __forceinline__ int fargo_zplane(const Geo &G, int k) {
+    if (k > G.nz && G.bcz_hi == kBcHalo) return k;
+    return map_bc(G.bc[2], k, G.nz);
+}
 
 // emfx (i in 1..nx, k in 1..nz+1) and emfz (i in 1..nx+1, k in 1..nz) over j in 1..ny+1,
 // along y lines (fargo_line): per column the shift is computed once and the donor field and
@@ -1396,7 +1413,7 @@ __global__ void __launch_bounds__(kThreads) k_fargo_emf(Geo G, Store U, double *
     const int i = L.i, k = L.k;
     const double dt = S->dt, dy = G.dy, half = 0.5, one = 1.0;
     const int ny = G.ny, st = mn(G.slope_type, 2);
-    const int kw = map_bc(G.bc[2], k, G.nz);  // z ghosts hold their boundary copy here
+    const int kw = fargo_zplane(G, k);
     auto lim = [&](double m, double c, double p) { return st == 0 ? 0.0 : limit1<double>((double)st, m, c, p); };
     // one component: get_emfx (v = IC, sign +1, fargo.f90:146-177) or get_emfz (v = IA, sign -1, :204-235)
     auto line = [&](int v, double sgn, const FargoShift &f, double *out) {
@@ -1730,7 +1747,8 @@ __global__ void __launch_bounds__(kThreads) k_visc_update(Geo G, Store U, const 
 // ---------------------------------------------------------------------------
 // pass 1: per-x-column yz sums of vx and vy (compute_yz_mean)
 template <class Store>
-__global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m) {
+// raw = 1: the column sums themselves (a z slab's share, summed over the slabs by the caller)
+__global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m, int raw = 0) {
     const int i = blockIdx.x + 1;
     double a = 0.0, b = 0.0;
     const long long n = (long long)G.ny * G.nz;
@@ -1749,8 +1767,8 @@ __global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m) {
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        m[2 * (i - 1)] = sa[0] / G.ny / G.nz;
-        m[2 * (i - 1) + 1] = sb[0] / G.ny / G.nz;
+        m[2 * (i - 1)] = raw ? sa[0] : sa[0] / G.ny / G.nz;
+        m[2 * (i - 1) + 1] = raw ? sb[0] : sb[0] / G.ny / G.nz;
     }
 }
 

@@ -41,24 +41,41 @@ def box_params(precision: str, nx: int = 128, ny: int = 256, nz: int = 128):
                   riemann2d="hlld", bdtypex="shearingbox", fargo=True, precision=precision)
 
 
-def run(precision: str, u0: np.ndarray, tend: float, every: int, grid, max_s: float = 0.0) -> dict:
-    """One arm to time tend, or until max_s seconds of wall time have passed (0: no limit)."""
-    from dumses_hybrid_b200 import Context
+def run(precision: str, u0: np.ndarray, tend: float, every: int, grid, max_s: float = 0.0,
+        progress_s: float = 30.0) -> dict:
+    """One arm to time tend, or until max_s seconds of wall time have passed (0: no limit).
+    Prints a progress line (time, steps, last dt, alpha, magnetic pressure) every progress_s
+    seconds, and ends the arm at the first non-finite history value or library error."""
+    from dumses_hybrid_b200 import Context, DumsesError
     p = box_params(precision, *grid)
-    rows, steps, t = [], 0, 0.0
-    w0 = time.time()
+    rows, steps, t, dt = [], 0, 0.0, 0.0
+    w0 = wlast = time.time()
+    error = None
     with Context(p) as g:
         g.upload(u0)
         g.boundary(0.0, 0.0)
         rows.append([t, *g.history()])
         while t < tend and not (max_s > 0 and time.time() - w0 > max_s):
-            t, _ = g.run(every, t)
+            try:
+                t, dt = g.run(every, t)
+            except DumsesError as e:
+                error = str(e)
+                break
             steps += every
-            rows.append([t, *g.history()])
+            h = g.history()
+            rows.append([t, *h])
+            if not np.all(np.isfinite(h)):
+                error = "non-finite history values"
+                break
+            if time.time() - wlast > progress_s:
+                wlast = time.time()
+                print(json.dumps({"arm": precision, "t": t, "orbits": t / (2 * math.pi), "steps": steps, "dt": dt,
+                                  "alpha": float(h[3]), "magp": float(h[4]), "wall_s": wlast - w0}), flush=True)
         u = g.download()
-    out = {"rows": np.array(rows), "steps": steps, "wall_s": time.time() - w0, "state": u, "stopped_early": t < tend}
+    out = {"rows": np.array(rows), "steps": steps, "wall_s": time.time() - w0, "state": u, "stopped_early": t < tend,
+           "error": error}
     print(json.dumps({"arm": precision, "steps": steps, "t_end": t, "wall_s": out["wall_s"],
-                      "stopped_early": out["stopped_early"]}), flush=True)
+                      "stopped_early": out["stopped_early"], "error": error}), flush=True)
     return out
 
 

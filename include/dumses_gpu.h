@@ -87,7 +87,14 @@ typedef struct dg_params {
     int    device;           /* CUDA device ordinal                                    */
     double nu;               /* kinematic viscosity (physics.f90:459-664); 0 = off     */
     double eta;              /* Ohmic resistivity (physics.f90:295-455); 0 = off       */
-    int    reserved[6];
+    /* z-slab decomposition (the reference's &mpi_params nzslice and the rank's
+     * zposition, init.f90:159,190-197, parallel.f90:197-257), z only: nz is this
+     * slab's share (nzglob = nz * nzslice), zmin/zmax bound the whole box, and the
+     * slab's z ghost planes come from its neighbours (dg_halo_pack/unpack).
+     * nzslice = 0 or 1: one domain. */
+    int    nzslice;
+    int    zposition;        /* 0 .. nzslice-1, from the bottom of the box             */
+    int    reserved[4];
 } dg_params;
 
 typedef struct dg_ctx dg_ctx;
@@ -194,6 +201,41 @@ int  dg_history(dg_ctx *ctx, double out[9]);
  * library the call waits for its kernels). */
 #define DG_HISTORY_NOALLOC_MAX_NX 16384
 int  dg_history_noalloc(const dg_params *p, const double *uin_dev, double *out_dev, void *stream);
+
+/* ---- z-slab decomposition ----------------------------------------------------
+ * The reference decomposes the box over MPI ranks (parallel.f90:197-697) and
+ * exchanges 3-deep ghost slabs of uin after each boundary call, with
+ * MPI_Sendrecv or ncclSend/ncclRecv (boundary_z, parallel.f90:480-590).  Here
+ * the box is split in z only (x keeps the shear-periodic boundary local and
+ * FARGO needs whole y lines); each slab is one context (one per GPU, or several
+ * on one GPU), and the caller moves the halos between them with any transport
+ * (NCCL, MPI, a device copy): after dg_boundary (and after dg_dissipation) of
+ * every slab, pack both sides of every slab, send side 0 to the lower
+ * neighbour and side 1 to the upper one (periodic in zposition), and unpack
+ * what arrives: from the lower neighbour into side 0, from the upper into side 1.
+ * The CFL step is the minimum of every slab's dg_compute_dt (the reference's
+ * MPI_Allreduce(MIN), physics.f90:123-129).  A zero-gradient z boundary is
+ * applied by the bottom and top slabs themselves; their outer sides need no
+ * halo.  dg_run refuses slab contexts (the exchange is the caller's).
+ * Halo layout: 3 planes (the x and y ghosts included) of every stored state
+ * plane, plane by plane: dg_halo_count doubles. */
+long long dg_halo_count(const dg_ctx *ctx);
+/* side 0: the slab's 3 lowest active planes; side 1: its 3 highest, into the
+ * device buffer dev_buf (dg_halo_count doubles, any device that can read the
+ * context's memory); enqueued on the context's stream */
+int  dg_halo_pack(dg_ctx *ctx, int side, double *dev_buf);
+/* side 0: dev_buf into the 3 ghost planes below the slab; side 1: above it */
+int  dg_halo_unpack(dg_ctx *ctx, int side, const double *dev_buf);
+/* MRI history of a decomposed box in two phases, as compute_yz_mean and
+ * vol_average do it with MPI (src/problem/mri/history.f90:176-245):
+ *   phase 1: col[2(i-1)], col[2(i-1)+1] = this slab's sums of v_x and v_y over
+ *            the cells of x column i (2 nx doubles, host);
+ *   the caller sums col over the slabs and divides by ny * nz * nzslice;
+ *   phase 2: this slab's share of the 9 history values (dg_history's order,
+ *            volume-normalised by the whole box) with those column means;
+ *            the box's values are the sums of the shares. */
+int  dg_history_columns(dg_ctx *ctx, double *col);
+int  dg_history_share(dg_ctx *ctx, const double *colmean, double out[9]);
 
 /* wait for all work of the context (bounded) */
 int  dg_sync(dg_ctx *ctx);

@@ -11,7 +11,7 @@ reads both back with dumpy, checks every field, and records the result next to t
 
 dumpy imports h5py, netCDF4, tables and pylab at module level; none of them is used by the
 binary or history readers, so they are replaced by empty modules here.  Run it where the
-reference tree is present (python tests/golden/make_dump_golden.py [reference root]); the
+reference tree is present (python tests/golden/make_dump_golden.py <reference root>); the
 tests only read the committed fixtures.
 """
 from __future__ import annotations
@@ -115,4 +115,6 @@ def main(root: pathlib.Path) -> None:
 
 
 if __name__ == "__main__":
-    main(pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_dump_golden.py <reference project root>")
+    main(pathlib.Path(sys.argv[1]))

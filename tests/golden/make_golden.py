@@ -8,17 +8,19 @@ launchProblem, test.py:123-133): pro=mri, iso=1, 32x64x32 cells on
 shearing-box x boundary, periodic y and z, HLLD/HLLD, MC slopes, FARGO off,
 type='Test', beta=1000, amp=0, tlim=60000, dthist=100.
 
-This script is run once in a checkout that has the reference next to it; the
-copied file is committed so the tests never read the reference at run time.
+Run it once with the reference project's root as its argument
+(python tests/golden/make_golden.py <reference root>); the copied file is
+committed so the tests never read the reference at run time.
 """
 import pathlib
 import shutil
 import sys
 
-SRC = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / \
-    "utils/test/fig/reference/shearing/mri/history.txt"
 DST = pathlib.Path(__file__).with_name("mri_history_ref.txt")
 
 if __name__ == "__main__":
-    shutil.copyfile(SRC, DST)
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference project root>")
+    src = pathlib.Path(sys.argv[1]) / "utils/test/fig/reference/shearing/mri/history.txt"
+    shutil.copyfile(src, DST)
     print(f"wrote {DST} ({sum(1 for _ in open(DST)) - 1} rows)")

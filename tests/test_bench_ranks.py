@@ -1,5 +1,5 @@
 """The multi-rank plumbing of bench.py on CPU: two gloo ranks on 127.0.0.1 run the
-replica barrier and the max-over-ranks reduction the timed region uses, and the
+rank barrier and the max-over-ranks reduction the timed region uses, and the
 reference arm does no work on ranks other than 0."""
 import os
 import socket
@@ -22,10 +22,10 @@ def _rank_main(rank, world, port, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        bench.replica_barrier(dist, cuda=False)
-        ms = 10.0 * (rank + 1)  # each replica's own elapsed time
-        worst = bench.replica_max(ms, dist, device="cpu")
-        bench.replica_barrier(dist, cuda=False)
+        bench.rank_barrier(dist, cuda=False)
+        ms = 10.0 * (rank + 1)  # each rank's own elapsed time
+        worst = bench.rank_max(ms, dist, device="cpu")
+        bench.rank_barrier(dist, cuda=False)
         q.put((rank, worst))
     finally:
         dist.destroy_process_group()
@@ -56,7 +56,7 @@ def test_reference_arm_is_rank0_only(capsys):
 
 def test_single_process_max_is_identity():
     import bench
-    assert bench.replica_max(3.5, None) == 3.5
+    assert bench.rank_max(3.5, None) == 3.5
 
 
 def test_reference_arm_loads_no_product_library():

@@ -127,6 +127,14 @@ def test_zero_gradient_boundaries():
     run_pair(p, "orszag_tang", 4)
 
 
+def test_mri_fargo_zero_gradient_z():
+    # FARGO's EMFs on the top z faces read the face field there (fargo.f90:146-177), which
+    # the preceding godunov updated; with a zero-gradient z boundary it differs from the
+    # field of the last active plane
+    p = Params(**{**MRI_FARGO.__dict__, "bdtypez": "zero_gradient"})
+    run_pair(p, "mri", 5, beta=1000.0, amp=0.1, seed=29)
+
+
 def test_isothermal_rotating_periodic():
     # Coriolis + shear source terms without the shearing boundary
     p = Params(**{**MRI_TEST.__dict__, "bdtypex": "periodic", "ciso": 1.0, "omega0": 1.0, "gamma": 5 / 3,
