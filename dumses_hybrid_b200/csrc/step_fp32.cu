@@ -788,6 +788,12 @@ int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     return 3;
 }
 
+// 3D trace as two kernels: cell fields, then face fields
+#ifndef DG_TRACE_SPLIT32
+#define DG_TRACE_SPLIT32 0
+#endif
+constexpr bool kTraceSplit32 = DG_TRACE_SPLIT32 != 0;
+
 // 3D Riemann work as two kernels (faces, then edges) instead of one
 #ifndef DG_RIEMANN_SPLIT32
 #define DG_RIEMANN_SPLIT32 0
@@ -813,7 +819,13 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     int faces = 1;
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
-        TIMED(KS_TRACE, s, (k_trace3d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
+        if (kTraceSplit32) {
+            TIMED(KS_TRACE, s, (k_trace3d<float, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
+            TIMED(KS_TRACE, s, (k_trace3d<float, 2><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
+            n++;
+        } else {
+            TIMED(KS_TRACE, s, (k_trace3d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
+        }
     } else {
         TIMED(KS_EFIELD, s, (k_efield2d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2)));
         TIMED(KS_TRACE, s, (k_trace2d<float><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E2, core, B.S)));

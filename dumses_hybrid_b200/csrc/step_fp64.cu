@@ -246,6 +246,13 @@ __global__ void __launch_bounds__(kThreads) k_kick64(Geo G, double *__restrict__
     Q[G.sv * IV + c] = v + dvy * dt * half;
 }
 
+// 3D trace as two kernels: cell fields (5 blocks per SM, 96 registers), then face fields
+// (6 blocks per SM); 3.03 against 3.68 ms at 256^3 for the single kernel, which spills at 128
+#ifndef DG_TRACE_SPLIT64
+#define DG_TRACE_SPLIT64 1
+#endif
+constexpr bool kTraceSplit64 = DG_TRACE_SPLIT64 != 0;
+
 // 3D Riemann work as two kernels (faces, then edges) instead of one
 #ifndef DG_RIEMANN_SPLIT64
 #define DG_RIEMANN_SPLIT64 1
@@ -277,7 +284,13 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
-        TIMED(KS_TRACE, s, (k_trace3d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
+        if (kTraceSplit64) {
+            TIMED(KS_TRACE, s, (k_trace3d<double, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
+            TIMED(KS_TRACE, s, (k_trace3d<double, 2><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
+            n++;
+        } else {
+            TIMED(KS_TRACE, s, (k_trace3d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
+        }
         // HLLD/HLLD (the reference's default and every benchmark) runs kernels without the other solvers
         const unsigned nb = nblocks(G.fsz, kThreads);
         if (kRiemannPerDir64 && G.iriemann == DG_RIEMANN_HLLD && G.iriemann2d == DG_RIEMANN_HLLD) {

@@ -529,7 +529,6 @@ __device__ __forceinline__ T face_slope(const QV<T> &a, int c, int dir, int i, i
     return limit1(s, a.bf(c, i - di, j - dj, k - dk), a.bf(c, i, j, k), a.bf(c, i + di, j + dj, k + dk));
 }
 
-template <typename T>
 // resident blocks of 128 threads per SM that the trace and Riemann kernels are compiled
 // for (register caps 128/80 for the trace, 128/64 for the Riemann kernel, FP64/FP32),
 // chosen by timing the variants at 256^3
@@ -545,7 +544,29 @@ template <typename T>
 #ifndef DG_RIEMANN_MINB32
 #define DG_RIEMANN_MINB32 8
 #endif
-__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_TRACE_MINB64 : DG_TRACE_MINB32))
+// kPart selects the core fields a launch writes: 0 all 47; 1 the predicted cell state and the
+// cell slopes (fields 0-28); 2 the predicted face fields and their transverse slopes (29-46).
+// The values a part does not write are not computed (their expressions are dead code), and
+// every written value is the same expression of the same inputs in all forms.
+#ifndef DG_TRACEC_MINB64
+#define DG_TRACEC_MINB64 5
+#endif
+#ifndef DG_TRACEF_MINB64
+#define DG_TRACEF_MINB64 6
+#endif
+#ifndef DG_TRACEC_MINB32
+#define DG_TRACEC_MINB32 6
+#endif
+#ifndef DG_TRACEF_MINB32
+#define DG_TRACEF_MINB32 8
+#endif
+template <typename T, int kPart>
+constexpr int trace_minb() {
+    return sizeof(T) == 8 ? (kPart == 0 ? DG_TRACE_MINB64 : kPart == 1 ? DG_TRACEC_MINB64 : DG_TRACEF_MINB64)
+                          : (kPart == 0 ? DG_TRACE_MINB32 : kPart == 1 ? DG_TRACEC_MINB32 : DG_TRACEF_MINB32);
+}
+template <typename T, int kPart = 0>
+__global__ void __launch_bounds__(kThreads, (trace_minb<T, kPart>()))
 k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
           const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -627,16 +648,20 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
     T *o = core + core_base(t, kCore3);
     const int cs = kCoreLane;
     if (!chk(o, ((kCore3 - 1) * cs + 1) * sizeof(T))) return;
-    o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
-    o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
-    o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
-    o[15 * cs] = dry; o[16 * cs] = duy; o[17 * cs] = dvy; o[18 * cs] = dwy; o[19 * cs] = dpy; o[20 * cs] = dAy; o[21 * cs] = dCy;
-    o[22 * cs] = drz; o[23 * cs] = duz; o[24 * cs] = dvz; o[25 * cs] = dwz; o[26 * cs] = dpz; o[27 * cs] = dAz; o[28 * cs] = dBz;
-    o[29 * cs] = AL + sAL0; o[30 * cs] = AR + sAR0; o[31 * cs] = BL + sBL0; o[32 * cs] = BR + sBR0;
-    o[33 * cs] = CL + sCL0; o[34 * cs] = CR + sCR0;
-    o[35 * cs] = dALy; o[36 * cs] = dARy; o[37 * cs] = dALz; o[38 * cs] = dARz;
-    o[39 * cs] = dBLx; o[40 * cs] = dBRx; o[41 * cs] = dBLz; o[42 * cs] = dBRz;
-    o[43 * cs] = dCLx; o[44 * cs] = dCRx; o[45 * cs] = dCLy; o[46 * cs] = dCRy;
+    if constexpr (kPart != 2) {
+        o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
+        o[4 * cs] = p + sp0; o[5 * cs] = A + sA0; o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
+        o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx; o[13 * cs] = dBx; o[14 * cs] = dCx;
+        o[15 * cs] = dry; o[16 * cs] = duy; o[17 * cs] = dvy; o[18 * cs] = dwy; o[19 * cs] = dpy; o[20 * cs] = dAy; o[21 * cs] = dCy;
+        o[22 * cs] = drz; o[23 * cs] = duz; o[24 * cs] = dvz; o[25 * cs] = dwz; o[26 * cs] = dpz; o[27 * cs] = dAz; o[28 * cs] = dBz;
+    }
+    if constexpr (kPart != 1) {
+        o[29 * cs] = AL + sAL0; o[30 * cs] = AR + sAR0; o[31 * cs] = BL + sBL0; o[32 * cs] = BR + sBR0;
+        o[33 * cs] = CL + sCL0; o[34 * cs] = CR + sCR0;
+        o[35 * cs] = dALy; o[36 * cs] = dARy; o[37 * cs] = dALz; o[38 * cs] = dARz;
+        o[39 * cs] = dBLx; o[40 * cs] = dBRx; o[41 * cs] = dBLz; o[42 * cs] = dBRz;
+        o[43 * cs] = dCLx; o[44 * cs] = dCRx; o[45 * cs] = dCLy; o[46 * cs] = dCRy;
+    }
 }
 
 template <typename T>
