@@ -793,6 +793,11 @@ int launch_dt(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
 #define DG_TRACE_SPLIT32 0
 #endif
 constexpr bool kTraceSplit32 = DG_TRACE_SPLIT32 != 0;
+// 3D trace with its stencil staged in shared memory (k_trace3d_tile)
+#ifndef DG_TRACE_TILE32
+#define DG_TRACE_TILE32 1
+#endif
+constexpr bool kTraceTile32 = DG_TRACE_TILE32 != 0;
 
 // 3D Riemann work as two kernels (faces, then edges) instead of one
 #ifndef DG_RIEMANN_SPLIT32
@@ -819,7 +824,9 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     int faces = 1;
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
-        if (kTraceSplit32) {
+        if (kTraceTile32) {
+            TIMED(KS_TRACE, s, (launch_trace_tile<float>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
+        } else if (kTraceSplit32) {
             TIMED(KS_TRACE, s, (k_trace3d<float, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
             TIMED(KS_TRACE, s, (k_trace3d<float, 2><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
             n++;

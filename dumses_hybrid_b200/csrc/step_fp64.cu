@@ -252,6 +252,11 @@ __global__ void __launch_bounds__(kThreads) k_kick64(Geo G, double *__restrict__
 #define DG_TRACE_SPLIT64 1
 #endif
 constexpr bool kTraceSplit64 = DG_TRACE_SPLIT64 != 0;
+// 3D trace with its stencil staged in shared memory (k_trace3d_tile)
+#ifndef DG_TRACE_TILE64
+#define DG_TRACE_TILE64 1
+#endif
+constexpr bool kTraceTile64 = DG_TRACE_TILE64 != 0;
 
 // 3D Riemann work as two kernels (faces, then edges) instead of one
 #ifndef DG_RIEMANN_SPLIT64
@@ -284,7 +289,9 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
-        if (kTraceSplit64) {
+        if (kTraceTile64) {
+            TIMED(KS_TRACE, s, (launch_trace_tile<double>(G, Q, U.p, E0, E1, E2, core, B.S, s)));
+        } else if (kTraceSplit64) {
             TIMED(KS_TRACE, s, (k_trace3d<double, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
             TIMED(KS_TRACE, s, (k_trace3d<double, 2><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
             n++;

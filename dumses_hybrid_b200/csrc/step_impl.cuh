@@ -461,38 +461,6 @@ __global__ void __launch_bounds__(kThreads) k_efield2d(Geo G, const T *__restric
     Ez[t] = Ez2_at(a, i, j);
 }
 
-// limited cell slopes of one variable in the three directions (slope_type 1..3)
-template <typename T>
-__device__ __forceinline__ void cell_slopes3(const QV<T> &a, int v, int i, int j, int k, T d[3]) {
-    const int st = a.G.slope_type;
-    if (st == 0) { d[0] = d[1] = d[2] = T(0); return; }
-    const T c = a.q(v, i, j, k);
-    if (st < 3) {
-        const T s = (T)st;
-        d[0] = limit1(s, a.q(v, i - 1, j, k), c, a.q(v, i + 1, j, k));
-        d[1] = limit1(s, a.q(v, i, j - 1, k), c, a.q(v, i, j + 1, k));
-        d[2] = limit1(s, a.q(v, i, j, k - 1), c, a.q(v, i, j, k + 1));
-        return;
-    }
-    // multidimensional limiter, scheme.f90:484-557
-    const T half = T(0.5), one = T(1);
-    T vmin = T(0), vmax = T(0);
-    bool first = true;
-    for (int dk = -1; dk <= 1; dk++)
-        for (int di = -1; di <= 1; di++)
-            for (int dj = -1; dj <= 1; dj++) {
-                T e = a.q(v, i + di, j + dj, k + dk) - c;
-                if (first) { vmin = e; vmax = e; first = false; }
-                else { vmin = mn(vmin, e); vmax = mx(vmax, e); }
-            }
-    T dfx = half * (a.q(v, i + 1, j, k) - a.q(v, i - 1, j, k));
-    T dfy = half * (a.q(v, i, j + 1, k) - a.q(v, i, j - 1, k));
-    T dfz = half * (a.q(v, i, j, k + 1) - a.q(v, i, j, k - 1));
-    T dff = half * (fab(dfx) + fab(dfy) + fab(dfz));
-    T slop = (dff > T(0)) ? mn(one, mn(fab(vmin), fab(vmax)) / dff) : one;
-    d[0] = slop * dfx; d[1] = slop * dfy; d[2] = slop * dfz;
-}
-
 template <typename T>
 __device__ __forceinline__ void cell_slopes2(const QV<T> &a, int v, int i, int j, T d[2]) {
     const int st = a.G.slope_type, k = 1;
@@ -565,53 +533,104 @@ constexpr int trace_minb() {
     return sizeof(T) == 8 ? (kPart == 0 ? DG_TRACE_MINB64 : kPart == 1 ? DG_TRACEC_MINB64 : DG_TRACEF_MINB64)
                           : (kPart == 0 ? DG_TRACE_MINB32 : kPart == 1 ? DG_TRACEC_MINB32 : DG_TRACEF_MINB32);
 }
-template <typename T, int kPart = 0>
-__global__ void __launch_bounds__(kThreads, (trace_minb<T, kPart>()))
-k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
-          const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
-    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= G.csz) return;
-    const int i = (int)(t % G.CX);
-    const long long rr = t / G.CX;
-    const int j = (int)(rr % G.CY);
-    const int k = (int)(rr / G.CY) + G.kc0;
-    const QV<T> a{Q, Bf, G};
-    const double dtd = S->dt;
-    const T dt = (T)dtd;
+// The 3D trace of one cell (slope + trace3d, scheme.f90:253-656, 1149-1711) written once over a
+// stencil accessor that reads, relative to the cell (i, j, k):
+//   a.q(v, di, dj, dk)   primitive variable v of cell (i+di, j+dj, k+dk)
+//   a.bf(c, di, dj, dk)  left-face field component c of that cell
+//   a.ex(dj, dk), a.ey(di, dk), a.ez(di, dj)   the trace's edge fields at (i, j+dj, k+dk),
+//                        (i+di, j, k+dk) and (i+di, j+dj, k)
+// k_trace3d reads through global memory, k_trace3d_tile through shared-memory planes; both
+// evaluate the same expressions of the same values.
+template <typename T>
+struct GStencil {
+    QV<T> a;
+    const T *Ex, *Ey, *Ez;
+    int i, j, k;
+    __device__ __forceinline__ T q(int v, int di, int dj, int dk) const { return a.q(v, i + di, j + dj, k + dk); }
+    __device__ __forceinline__ T bf(int c, int di, int dj, int dk) const { return a.bf(c, i + di, j + dj, k + dk); }
+    __device__ __forceinline__ T ex(int dj, int dk) const { return ld(Ex + a.G.eidx(i, j + dj, k + dk)); }
+    __device__ __forceinline__ T ey(int di, int dk) const { return ld(Ey + a.G.eidx(i + di, j, k + dk)); }
+    __device__ __forceinline__ T ez(int di, int dj) const { return ld(Ez + a.G.eidx(i + di, j + dj, k)); }
+};
+
+// limited cell slopes of variable v in the three directions (slope_type st = 1..3)
+template <typename T, class Sten>
+__device__ __forceinline__ void cell_slopes3s(const Sten &a, int v, int st, T d[3]) {
+    if (st == 0) { d[0] = d[1] = d[2] = T(0); return; }
+    const T c = a.q(v, 0, 0, 0);
+    if (st < 3) {
+        const T s = (T)st;
+        d[0] = limit1(s, a.q(v, -1, 0, 0), c, a.q(v, 1, 0, 0));
+        d[1] = limit1(s, a.q(v, 0, -1, 0), c, a.q(v, 0, 1, 0));
+        d[2] = limit1(s, a.q(v, 0, 0, -1), c, a.q(v, 0, 0, 1));
+        return;
+    }
+    // multidimensional limiter, scheme.f90:484-557
+    const T half = T(0.5), one = T(1);
+    T vmin = T(0), vmax = T(0);
+#pragma unroll
+    for (int dk = -1; dk <= 1; dk++)
+#pragma unroll
+        for (int di = -1; di <= 1; di++)
+#pragma unroll
+            for (int dj = -1; dj <= 1; dj++) {
+                T e = a.q(v, di, dj, dk) - c;
+                if (dk == -1 && di == -1 && dj == -1) { vmin = e; vmax = e; }
+                else { vmin = mn(vmin, e); vmax = mx(vmax, e); }
+            }
+    T dfx = half * (a.q(v, 1, 0, 0) - a.q(v, -1, 0, 0));
+    T dfy = half * (a.q(v, 0, 1, 0) - a.q(v, 0, -1, 0));
+    T dfz = half * (a.q(v, 0, 0, 1) - a.q(v, 0, 0, -1));
+    T dff = half * (fab(dfx) + fab(dfy) + fab(dfz));
+    T slop = (dff > T(0)) ? mn(one, mn(fab(vmin), fab(vmax)) / dff) : one;
+    d[0] = slop * dfx; d[1] = slop * dfy; d[2] = slop * dfz;
+}
+
+// transverse slope of face-B component c of the face at offset (di, dj, dk) along direction dir
+template <typename T, class Sten>
+__device__ __forceinline__ T face_slope_s(const Sten &a, int c, int dir, int di, int dj, int dk, int st) {
+    if (st == 0) return T(0);
+    const T s = (T)mn(st, 2);
+    const int ei = dir == 0, ej = dir == 1, ek = dir == 2;
+    return limit1(s, a.bf(c, di - ei, dj - ej, dk - ek), a.bf(c, di, dj, dk), a.bf(c, di + ei, dj + ej, dk + ek));
+}
+
+// the trace core of cell (i, ., .) from its stencil, stored at o (field f at o[f * kCoreLane]);
+// kPart: 0 all 47 fields, 1 the predicted cell state and cell slopes (0-28), 2 the predicted
+// face fields and their transverse slopes (29-46)
+template <typename T, int kPart, class Sten>
+__device__ __forceinline__ void trace3_cell(const Sten &a, const Geo &G, int i, double dtd, T *o) {
+    const int st = G.slope_type;
     const T half = T(0.5), gamma = (T)G.gamma;
     const T dtdx = (T)(dtd / G.dx), dtdy = (T)(dtd / G.dy), dtdz = (T)(dtd / G.dz), dx = (T)G.dx;
-    (void)dt;
 
-    const T r = a.q(IR, i, j, k), u = a.q(IU, i, j, k), v = a.q(IV, i, j, k), w = a.q(IW, i, j, k);
-    const T p = a.q(IP, i, j, k), A = a.q(IA, i, j, k), B = a.q(IB, i, j, k), C = a.q(IC, i, j, k);
+    const T r = a.q(IR, 0, 0, 0), u = a.q(IU, 0, 0, 0), v = a.q(IV, 0, 0, 0), w = a.q(IW, 0, 0, 0);
+    const T p = a.q(IP, 0, 0, 0), A = a.q(IA, 0, 0, 0), B = a.q(IB, 0, 0, 0), C = a.q(IC, 0, 0, 0);
     T d3[3];
-    cell_slopes3(a, IR, i, j, k, d3); const T drx = half * d3[0], dry = half * d3[1], drz = half * d3[2];
-    cell_slopes3(a, IU, i, j, k, d3); const T dux = half * d3[0], duy = half * d3[1], duz = half * d3[2];
-    cell_slopes3(a, IV, i, j, k, d3); const T dvx = half * d3[0], dvy = half * d3[1], dvz = half * d3[2];
-    cell_slopes3(a, IW, i, j, k, d3); const T dwx = half * d3[0], dwy = half * d3[1], dwz = half * d3[2];
-    cell_slopes3(a, IP, i, j, k, d3); const T dpx = half * d3[0], dpy = half * d3[1], dpz = half * d3[2];
-    cell_slopes3(a, IA, i, j, k, d3); const T dAy = half * d3[1], dAz = half * d3[2];
-    cell_slopes3(a, IB, i, j, k, d3); const T dBx = half * d3[0], dBz = half * d3[2];
-    cell_slopes3(a, IC, i, j, k, d3); const T dCx = half * d3[0], dCy = half * d3[1];
+    cell_slopes3s<T>(a, IR, st, d3); const T drx = half * d3[0], dry = half * d3[1], drz = half * d3[2];
+    cell_slopes3s<T>(a, IU, st, d3); const T dux = half * d3[0], duy = half * d3[1], duz = half * d3[2];
+    cell_slopes3s<T>(a, IV, st, d3); const T dvx = half * d3[0], dvy = half * d3[1], dvz = half * d3[2];
+    cell_slopes3s<T>(a, IW, st, d3); const T dwx = half * d3[0], dwy = half * d3[1], dwz = half * d3[2];
+    cell_slopes3s<T>(a, IP, st, d3); const T dpx = half * d3[0], dpy = half * d3[1], dpz = half * d3[2];
+    cell_slopes3s<T>(a, IA, st, d3); const T dAy = half * d3[1], dAz = half * d3[2];
+    cell_slopes3s<T>(a, IB, st, d3); const T dBx = half * d3[0], dBz = half * d3[2];
+    cell_slopes3s<T>(a, IC, st, d3); const T dCx = half * d3[0], dCy = half * d3[1];
 
-    const T AL = a.bf(0, i, j, k), AR = a.bf(0, i + 1, j, k);
-    const T BL = a.bf(1, i, j, k), BR = a.bf(1, i, j + 1, k);
-    const T CL = a.bf(2, i, j, k), CR = a.bf(2, i, j, k + 1);
+    const T AL = a.bf(0, 0, 0, 0), AR = a.bf(0, 1, 0, 0);
+    const T BL = a.bf(1, 0, 0, 0), BR = a.bf(1, 0, 1, 0);
+    const T CL = a.bf(2, 0, 0, 0), CR = a.bf(2, 0, 0, 1);
     const T dAx = half * (AR - AL), dBy = half * (BR - BL), dCz = half * (CR - CL);
 
-    const T dALy = half * face_slope(a, 0, 1, i, j, k), dARy = half * face_slope(a, 0, 1, i + 1, j, k);
-    const T dALz = half * face_slope(a, 0, 2, i, j, k), dARz = half * face_slope(a, 0, 2, i + 1, j, k);
-    const T dBLx = half * face_slope(a, 1, 0, i, j, k), dBRx = half * face_slope(a, 1, 0, i, j + 1, k);
-    const T dBLz = half * face_slope(a, 1, 2, i, j, k), dBRz = half * face_slope(a, 1, 2, i, j + 1, k);
-    const T dCLx = half * face_slope(a, 2, 0, i, j, k), dCRx = half * face_slope(a, 2, 0, i, j, k + 1);
-    const T dCLy = half * face_slope(a, 2, 1, i, j, k), dCRy = half * face_slope(a, 2, 1, i, j, k + 1);
+    const T dALy = half * face_slope_s<T>(a, 0, 1, 0, 0, 0, st), dARy = half * face_slope_s<T>(a, 0, 1, 1, 0, 0, st);
+    const T dALz = half * face_slope_s<T>(a, 0, 2, 0, 0, 0, st), dARz = half * face_slope_s<T>(a, 0, 2, 1, 0, 0, st);
+    const T dBLx = half * face_slope_s<T>(a, 1, 0, 0, 0, 0, st), dBRx = half * face_slope_s<T>(a, 1, 0, 0, 1, 0, st);
+    const T dBLz = half * face_slope_s<T>(a, 1, 2, 0, 0, 0, st), dBRz = half * face_slope_s<T>(a, 1, 2, 0, 1, 0, st);
+    const T dCLx = half * face_slope_s<T>(a, 2, 0, 0, 0, 0, st), dCRx = half * face_slope_s<T>(a, 2, 0, 0, 0, 1, st);
+    const T dCLy = half * face_slope_s<T>(a, 2, 1, 0, 0, 0, st), dCRy = half * face_slope_s<T>(a, 2, 1, 0, 0, 1, st);
 
-    const T ELL = ld(Exa + G.eidx(i, j, k)), ELR = ld(Exa + G.eidx(i, j, k + 1));
-    const T ERL = ld(Exa + G.eidx(i, j + 1, k)), ERR = ld(Exa + G.eidx(i, j + 1, k + 1));
-    const T FLL = ld(Eya + G.eidx(i, j, k)), FLR = ld(Eya + G.eidx(i, j, k + 1));
-    const T FRL = ld(Eya + G.eidx(i + 1, j, k)), FRR = ld(Eya + G.eidx(i + 1, j, k + 1));
-    const T GLL = ld(Eza + G.eidx(i, j, k)), GLR = ld(Eza + G.eidx(i, j + 1, k));
-    const T GRL = ld(Eza + G.eidx(i + 1, j, k)), GRR = ld(Eza + G.eidx(i + 1, j + 1, k));
+    const T ELL = a.ex(0, 0), ELR = a.ex(0, 1), ERL = a.ex(1, 0), ERR = a.ex(1, 1);
+    const T FLL = a.ey(0, 0), FLR = a.ey(0, 1), FRL = a.ey(1, 0), FRR = a.ey(1, 1);
+    const T GLL = a.ez(0, 0), GLR = a.ez(0, 1), GRL = a.ez(1, 0), GRR = a.ez(1, 1);
 
     // source terms, scheme.f90:1351-1389
     T sr0 = (-u * drx - dux * r) * dtdx + (-v * dry - dvy * r) * dtdy + (-w * drz - dwz * r) * dtdz;
@@ -645,7 +664,6 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
     const T sCL0 = +(FRL - FLL) * dtdx * half - (ERL - ELL) * dtdy * half;
     const T sCR0 = +(FRR - FLR) * dtdx * half - (ERR - ELR) * dtdy * half;
 
-    T *o = core + core_base(t, kCore3);
     const int cs = kCoreLane;
     if (!chk(o, ((kCore3 - 1) * cs + 1) * sizeof(T))) return;
     if constexpr (kPart != 2) {
@@ -662,6 +680,173 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
         o[39 * cs] = dBLx; o[40 * cs] = dBRx; o[41 * cs] = dBLz; o[42 * cs] = dBRz;
         o[43 * cs] = dCLx; o[44 * cs] = dCRx; o[45 * cs] = dCLy; o[46 * cs] = dCRy;
     }
+}
+
+template <typename T, int kPart = 0>
+__global__ void __launch_bounds__(kThreads, (trace_minb<T, kPart>()))
+k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
+          const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.csz) return;
+    const int i = (int)(t % G.CX);
+    const long long rr = t / G.CX;
+    const int j = (int)(rr % G.CY);
+    const int k = (int)(rr / G.CY) + G.kc0;
+    const GStencil<T> a{QV<T>{Q, Bf, G}, Exa, Eya, Eza, i, j, k};
+    trace3_cell<T, kPart>(a, G, i, S->dt, core + core_base(t, kCore3));
+}
+
+// ---------------------------------------------------------------------------
+// The 3D trace with its stencil staged in shared memory.  A block of kThreads threads owns a
+// tile of kTX x kTY cells in (x, y) and marches along z through kTZ planes of the core index
+// space.  Shared memory holds a ring of z planes of the tile plus a one-cell halo in x and y:
+// the 8 primitive variables and the 3 left-face field components (kRingQ planes: k-1, k, k+1
+// and the one being fetched) and the 3 edge-field components of the trace (kRingE planes: k,
+// k+1 and the one being fetched).  Planes arrive by cp.async (element copies, so no alignment
+// rule applies to the ghosted rows); plane k+2 is fetched while plane k is computed, and one
+// block barrier per plane orders the ring.  Each stencil read is then a shared-memory load at
+// a fixed offset from the thread's cell.
+// ---------------------------------------------------------------------------
+constexpr int kTX = 32, kTY = kThreads / kTX;
+constexpr int kTR = kTX + 2;              // row of a staged plane (halo of one cell each side)
+constexpr int kTP = kTR * (kTY + 2);      // one field of a staged plane
+constexpr int kTQF = NVAR + 3;            // fields of a Q plane: 8 primitives, 3 face-B components
+constexpr int kRingQ = 4, kRingE = 3;
+#ifndef DG_TRACE_KZ
+#define DG_TRACE_KZ 16
+#endif
+constexpr int kTZ = DG_TRACE_KZ;
+template <typename T>
+constexpr int trace_tile_smem() { return (kRingQ * kTQF + kRingE * 3) * kTP * (int)sizeof(T); }
+
+template <typename T>
+struct TStencil {
+    const T *p0, *p1, *p2;  // this cell in the staged Q planes k-1, k, k+1
+    const T *e0, *e1;       // this cell in the staged edge planes k, k+1
+    __device__ __forceinline__ const T *pl(int dk) const { return dk < 0 ? p0 : (dk > 0 ? p2 : p1); }
+    __device__ __forceinline__ T q(int v, int di, int dj, int dk) const { return pl(dk)[v * kTP + dj * kTR + di]; }
+    __device__ __forceinline__ T bf(int c, int di, int dj, int dk) const {
+        return pl(dk)[(NVAR + c) * kTP + dj * kTR + di];
+    }
+    __device__ __forceinline__ T ex(int dj, int dk) const { return (dk ? e1 : e0)[dj * kTR]; }
+    __device__ __forceinline__ T ey(int di, int dk) const { return (dk ? e1 : e0)[kTP + di]; }
+    __device__ __forceinline__ T ez(int di, int dj) const { return e0[2 * kTP + dj * kTR + di]; }
+};
+
+// one element copy global -> shared, zero-filled when the source is outside its array
+template <typename T>
+__device__ __forceinline__ void cp_elem(T *dst, const T *src, bool ok) {
+    ok = ok && chk(src, sizeof(T));
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = ok ? (int)sizeof(T) : 0;
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(ok ? src : nullptr), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(ok ? src : nullptr), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// fetch Q plane k (8 primitives and the 3 face-B components, tile + halo) into slot s
+template <typename T>
+__device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *Bf, T *s, int i0, int j0, int k) {
+    const bool kok = k + G.gz - 1 >= 0 && k + G.gz - 1 < G.NZ;
+    for (int q = threadIdx.x; q < kTP; q += kThreads) {
+        const int ii = q % kTR, jj = q / kTR;
+        const int i = i0 - 1 + ii, j = j0 - 1 + jj;
+        const bool ok = kok && i + 2 >= 0 && i + 2 < G.NX && j + G.gy - 1 >= 0 && j + G.gy - 1 < G.NY;
+        const long long c = ok ? G.idx(i, j, k) : 0;
+#pragma unroll
+        for (int v = 0; v < NVAR; v++) cp_elem(s + v * kTP + q, Q + G.sv * v + c, ok);
+#pragma unroll
+        for (int f = 0; f < 3; f++) cp_elem(s + (NVAR + f) * kTP + q, Bf + G.sv * (IA + f) + c, ok);
+    }
+}
+// fetch the trace's edge fields of plane k (edges i0..i0+kTX, j0..j0+kTY) into slot s
+template <typename T>
+__device__ __forceinline__ void fetch_eplane(const Geo &G, const T *Ex, const T *Ey, const T *Ez, T *s, int i0, int j0,
+                                             int k) {
+    const bool kok = k - G.ke0 >= 0 && k - G.ke0 < G.EZ;
+    for (int q = threadIdx.x; q < (kTX + 1) * (kTY + 1); q += kThreads) {
+        const int ii = 1 + q % (kTX + 1), jj = 1 + q / (kTX + 1);
+        const int i = i0 - 1 + ii, j = j0 - 1 + jj;
+        const bool ok = kok && i < G.EX && j < G.EY;
+        const long long e = ok ? G.eidx(i, j, k) : 0;
+        const int o = jj * kTR + ii;
+        cp_elem(s + o, Ex + e, ok);
+        cp_elem(s + kTP + o, Ey + e, ok);
+        cp_elem(s + 2 * kTP + o, Ez + e, ok);
+    }
+}
+
+#ifndef DG_TRACET_MINB32
+#define DG_TRACET_MINB32 5
+#endif
+#ifndef DG_TRACET_MINB64
+#define DG_TRACET_MINB64 2
+#endif
+template <typename T, int kPart = 0>
+__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_TRACET_MINB64 : DG_TRACET_MINB32))
+k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
+               const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
+    extern __shared__ __align__(16) unsigned char tsm[];
+    T *ringQ = (T *)tsm;
+    T *ringE = ringQ + kRingQ * kTQF * kTP;
+    const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
+    const int kb = G.kc0 + blockIdx.z * kTZ;
+    const int ke = min(kb + kTZ, G.kc0 + G.CZ);  // core planes [kb, ke)
+    const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool mine = i < G.CX && j < G.CY;
+    const int own = (ty + 1) * kTR + (tx + 1);  // this cell in a staged plane
+    auto qslot = [&](int k) { return ringQ + ((k - kb + 1) % kRingQ) * (kTQF * kTP); };
+    auto eslot = [&](int k) { return ringE + ((k - kb) % kRingE) * (3 * kTP); };
+    const double dtd = S->dt;
+    // planes k-1, k and edge plane k of the first core plane, then plane k+1
+    fetch_qplane(G, Q, Bf, qslot(kb - 1), i0, j0, kb - 1);
+    fetch_qplane(G, Q, Bf, qslot(kb), i0, j0, kb);
+    fetch_eplane(G, Exa, Eya, Eza, eslot(kb), i0, j0, kb);
+    cp_commit();
+    fetch_qplane(G, Q, Bf, qslot(kb + 1), i0, j0, kb + 1);
+    fetch_eplane(G, Exa, Eya, Eza, eslot(kb + 1), i0, j0, kb + 1);
+    cp_commit();
+    for (int k = kb; k < ke; k++) {
+        cp_wait_all();
+        __syncthreads();  // plane k+1 is in; every thread is done with plane k-1
+        if (k + 2 <= ke) {
+            fetch_qplane(G, Q, Bf, qslot(k + 2), i0, j0, k + 2);
+            fetch_eplane(G, Exa, Eya, Eza, eslot(k + 2), i0, j0, k + 2);
+        }
+        cp_commit();
+        if (mine) {
+            const TStencil<T> a{qslot(k - 1) + own, qslot(k) + own, qslot(k + 1) + own, eslot(k) + own,
+                                eslot(k + 1) + own};
+            const long long t = (long long)i + (long long)G.CX * ((long long)j + (long long)G.CY * (k - G.kc0));
+            trace3_cell<T, kPart>(a, G, i, dtd, core + core_base(t, kCore3));
+        }
+    }
+    cp_wait_all();
+}
+
+// launch k_trace3d_tile over the core index space (its dynamic shared memory is above the
+// default 48 KB limit in FP64: the attribute is set once per device)
+template <typename T, int kPart = 0>
+cudaError_t launch_trace_tile(const Geo &G, const T *Q, const T *Bf, const T *E0, const T *E1, const T *E2, T *core,
+                              const Scalars *S, cudaStream_t s) {
+    const int smem = trace_tile_smem<T>();
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        e = cudaFuncSetAttribute(k_trace3d_tile<T, kPart>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    const dim3 grid((unsigned)((G.CX + kTX - 1) / kTX), (unsigned)((G.CY + kTY - 1) / kTY),
+                    (unsigned)((G.CZ + kTZ - 1) / kTZ));
+    k_trace3d_tile<T, kPart><<<grid, kThreads, smem, s>>>(G, Q, Bf, E0, E1, E2, core, S);
+    return cudaSuccess;
 }
 
 template <typename T>
