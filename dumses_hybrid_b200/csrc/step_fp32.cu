@@ -824,7 +824,11 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     int faces = 1;
     if (G.ndim == 3) {
         TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
-        if (kTraceTile32) {
+        if (kTraceTile32 && kTraceSplit32) {
+            TIMED(KS_TRACE, s, (launch_trace_tile<float, 1>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<float, 2>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
+            n++;
+        } else if (kTraceTile32) {
             TIMED(KS_TRACE, s, (launch_trace_tile<float>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
         } else if (kTraceSplit32) {
             TIMED(KS_TRACE, s, (k_trace3d<float, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));

@@ -700,37 +700,60 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
 // The 3D trace with its stencil staged in shared memory.  A block of kThreads threads owns a
 // tile of kTX x kTY cells in (x, y) and marches along z through kTZ planes of the core index
 // space.  Shared memory holds a ring of z planes of the tile plus a one-cell halo in x and y:
-// the 8 primitive variables and the 3 left-face field components (kRingQ planes: k-1, k, k+1
-// and the one being fetched) and the 3 edge-field components of the trace (kRingE planes: k,
-// k+1 and the one being fetched).  Planes arrive by cp.async (element copies, so no alignment
-// rule applies to the ghosted rows); plane k+2 is fetched while plane k is computed, and one
-// block barrier per plane orders the ring.  Each stencil read is then a shared-memory load at
-// a fixed offset from the thread's cell.
+// the primitive variables and left-face field components the part needs (kRingQ planes: k-1,
+// k, k+1 and the one being fetched) and the 3 edge-field components of the trace (kRingE
+// planes: k, k+1 and the one being fetched).  Planes arrive by cp.async (element copies, so no
+// alignment rule applies to the ghosted rows); plane k+2 is fetched while plane k is computed,
+// and one block barrier per plane orders the ring.  Each stencil read is then a shared-memory
+// load at a fixed offset from the thread's cell.  The parts (kPart as in trace3_cell) stage
+// only what they read: part 1 the 8 primitives (its four face-B values come from global
+// memory), part 2 the face-B components and the edge fields, part 0 all of them.
 // ---------------------------------------------------------------------------
 constexpr int kTX = 32, kTY = kThreads / kTX;
 constexpr int kTR = kTX + 2;              // row of a staged plane (halo of one cell each side)
 constexpr int kTP = kTR * (kTY + 2);      // one field of a staged plane
-constexpr int kTQF = NVAR + 3;            // fields of a Q plane: 8 primitives, 3 face-B components
 constexpr int kRingQ = 4, kRingE = 3;
 #ifndef DG_TRACE_KZ
 #define DG_TRACE_KZ 16
 #endif
 constexpr int kTZ = DG_TRACE_KZ;
-template <typename T>
-constexpr int trace_tile_smem() { return (kRingQ * kTQF + kRingE * 3) * kTP * (int)sizeof(T); }
+// staged fields of a Q plane: [tq_first, tq_first + tq_count) of the 8 primitives (0-7) and
+// the 3 left-face field components (8-10)
+template <int kPart> __host__ __device__ constexpr int tq_first() { return kPart == 2 ? NVAR : 0; }
+template <int kPart> __host__ __device__ constexpr int tq_count() { return kPart == 1 ? NVAR : (kPart == 2 ? 3 : NVAR + 3); }
+template <int kPart> __host__ __device__ constexpr bool t_edges() { return kPart != 1; }
+template <typename T, int kPart>
+constexpr int trace_tile_smem() {
+    return (kRingQ * tq_count<kPart>() + (t_edges<kPart>() ? kRingE * 3 : 0)) * kTP * (int)sizeof(T);
+}
 
-template <typename T>
+template <typename T, int kPart>
 struct TStencil {
     const T *p0, *p1, *p2;  // this cell in the staged Q planes k-1, k, k+1
     const T *e0, *e1;       // this cell in the staged edge planes k, k+1
+    const T *bg;            // part 1: this cell's left-face component 0 in global memory ...
+    long long sv, sy, sz;   // ... and the strides from it
     __device__ __forceinline__ const T *pl(int dk) const { return dk < 0 ? p0 : (dk > 0 ? p2 : p1); }
-    __device__ __forceinline__ T q(int v, int di, int dj, int dk) const { return pl(dk)[v * kTP + dj * kTR + di]; }
-    __device__ __forceinline__ T bf(int c, int di, int dj, int dk) const {
-        return pl(dk)[(NVAR + c) * kTP + dj * kTR + di];
+    __device__ __forceinline__ T q(int v, int di, int dj, int dk) const {
+        if constexpr (kPart == 2) return T(0);  // part 2 reads no primitive
+        else return pl(dk)[(v - tq_first<kPart>()) * kTP + dj * kTR + di];
     }
-    __device__ __forceinline__ T ex(int dj, int dk) const { return (dk ? e1 : e0)[dj * kTR]; }
-    __device__ __forceinline__ T ey(int di, int dk) const { return (dk ? e1 : e0)[kTP + di]; }
-    __device__ __forceinline__ T ez(int di, int dj) const { return e0[2 * kTP + dj * kTR + di]; }
+    __device__ __forceinline__ T bf(int c, int di, int dj, int dk) const {
+        if constexpr (kPart == 1) return ld(bg + sv * c + sy * dj + sz * dk + di);
+        else return pl(dk)[(NVAR + c - tq_first<kPart>()) * kTP + dj * kTR + di];
+    }
+    __device__ __forceinline__ T ex(int dj, int dk) const {
+        if constexpr (kPart == 1) return T(0);  // part 1 reads no edge field
+        else return (dk ? e1 : e0)[dj * kTR];
+    }
+    __device__ __forceinline__ T ey(int di, int dk) const {
+        if constexpr (kPart == 1) return T(0);
+        else return (dk ? e1 : e0)[kTP + di];
+    }
+    __device__ __forceinline__ T ez(int di, int dj) const {
+        if constexpr (kPart == 1) return T(0);
+        else return e0[2 * kTP + dj * kTR + di];
+    }
 };
 
 // one element copy global -> shared, zero-filled when the source is outside its array
@@ -747,8 +770,8 @@ __device__ __forceinline__ void cp_elem(T *dst, const T *src, bool ok) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// fetch Q plane k (8 primitives and the 3 face-B components, tile + halo) into slot s
-template <typename T>
+// fetch the staged fields of Q plane k (tile + halo) into slot s
+template <typename T, int kPart>
 __device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *Bf, T *s, int i0, int j0, int k) {
     const bool kok = k + G.gz - 1 >= 0 && k + G.gz - 1 < G.NZ;
     for (int q = threadIdx.x; q < kTP; q += kThreads) {
@@ -757,9 +780,10 @@ __device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *
         const bool ok = kok && i + 2 >= 0 && i + 2 < G.NX && j + G.gy - 1 >= 0 && j + G.gy - 1 < G.NY;
         const long long c = ok ? G.idx(i, j, k) : 0;
 #pragma unroll
-        for (int v = 0; v < NVAR; v++) cp_elem(s + v * kTP + q, Q + G.sv * v + c, ok);
-#pragma unroll
-        for (int f = 0; f < 3; f++) cp_elem(s + (NVAR + f) * kTP + q, Bf + G.sv * (IA + f) + c, ok);
+        for (int f = 0; f < tq_count<kPart>(); f++) {
+            const int v = tq_first<kPart>() + f;
+            cp_elem(s + f * kTP + q, (v < NVAR ? Q + G.sv * v : Bf + G.sv * (IA + v - NVAR)) + c, ok);
+        }
     }
 }
 // fetch the trace's edge fields of plane k (edges i0..i0+kTX, j0..j0+kTY) into slot s
@@ -779,19 +803,39 @@ __device__ __forceinline__ void fetch_eplane(const Geo &G, const T *Ex, const T 
     }
 }
 
-#ifndef DG_TRACET_MINB32
-#define DG_TRACET_MINB32 5
-#endif
+// resident blocks per SM the tiled trace is compiled for, by arithmetic and part (bounded by
+// its shared memory: FP64 86/52/34 KB, FP32 43/26/17 KB per block for parts 0/1/2)
 #ifndef DG_TRACET_MINB64
 #define DG_TRACET_MINB64 2
 #endif
+#ifndef DG_TRACET1_MINB64
+#define DG_TRACET1_MINB64 4
+#endif
+#ifndef DG_TRACET2_MINB64
+#define DG_TRACET2_MINB64 6
+#endif
+#ifndef DG_TRACET_MINB32
+#define DG_TRACET_MINB32 5
+#endif
+#ifndef DG_TRACET1_MINB32
+#define DG_TRACET1_MINB32 6
+#endif
+#ifndef DG_TRACET2_MINB32
+#define DG_TRACET2_MINB32 8
+#endif
+template <typename T, int kPart>
+constexpr int trace_tile_minb() {
+    return sizeof(T) == 8 ? (kPart == 0 ? DG_TRACET_MINB64 : kPart == 1 ? DG_TRACET1_MINB64 : DG_TRACET2_MINB64)
+                          : (kPart == 0 ? DG_TRACET_MINB32 : kPart == 1 ? DG_TRACET1_MINB32 : DG_TRACET2_MINB32);
+}
 template <typename T, int kPart = 0>
-__global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_TRACET_MINB64 : DG_TRACET_MINB32))
+__global__ void __launch_bounds__(kThreads, (trace_tile_minb<T, kPart>()))
 k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
                const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
     extern __shared__ __align__(16) unsigned char tsm[];
+    constexpr int kQS = tq_count<kPart>() * kTP;  // one Q slot
     T *ringQ = (T *)tsm;
-    T *ringE = ringQ + kRingQ * kTQF * kTP;
+    T *ringE = ringQ + kRingQ * kQS;
     const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
     const int kb = G.kc0 + blockIdx.z * kTZ;
     const int ke = min(kb + kTZ, G.kc0 + G.CZ);  // core planes [kb, ke)
@@ -799,28 +843,33 @@ k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T
     const int i = i0 + tx, j = j0 + ty;
     const bool mine = i < G.CX && j < G.CY;
     const int own = (ty + 1) * kTR + (tx + 1);  // this cell in a staged plane
-    auto qslot = [&](int k) { return ringQ + ((k - kb + 1) % kRingQ) * (kTQF * kTP); };
+    auto qslot = [&](int k) { return ringQ + ((k - kb + 1) % kRingQ) * kQS; };
     auto eslot = [&](int k) { return ringE + ((k - kb) % kRingE) * (3 * kTP); };
     const double dtd = S->dt;
     // planes k-1, k and edge plane k of the first core plane, then plane k+1
-    fetch_qplane(G, Q, Bf, qslot(kb - 1), i0, j0, kb - 1);
-    fetch_qplane(G, Q, Bf, qslot(kb), i0, j0, kb);
-    fetch_eplane(G, Exa, Eya, Eza, eslot(kb), i0, j0, kb);
+    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb - 1), i0, j0, kb - 1);
+    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb), i0, j0, kb);
+    if constexpr (t_edges<kPart>()) fetch_eplane(G, Exa, Eya, Eza, eslot(kb), i0, j0, kb);
     cp_commit();
-    fetch_qplane(G, Q, Bf, qslot(kb + 1), i0, j0, kb + 1);
-    fetch_eplane(G, Exa, Eya, Eza, eslot(kb + 1), i0, j0, kb + 1);
+    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb + 1), i0, j0, kb + 1);
+    if constexpr (t_edges<kPart>()) fetch_eplane(G, Exa, Eya, Eza, eslot(kb + 1), i0, j0, kb + 1);
     cp_commit();
     for (int k = kb; k < ke; k++) {
         cp_wait_all();
         __syncthreads();  // plane k+1 is in; every thread is done with plane k-1
         if (k + 2 <= ke) {
-            fetch_qplane(G, Q, Bf, qslot(k + 2), i0, j0, k + 2);
-            fetch_eplane(G, Exa, Eya, Eza, eslot(k + 2), i0, j0, k + 2);
+            fetch_qplane<T, kPart>(G, Q, Bf, qslot(k + 2), i0, j0, k + 2);
+            if constexpr (t_edges<kPart>()) fetch_eplane(G, Exa, Eya, Eza, eslot(k + 2), i0, j0, k + 2);
         }
         cp_commit();
         if (mine) {
-            const TStencil<T> a{qslot(k - 1) + own, qslot(k) + own, qslot(k + 1) + own, eslot(k) + own,
-                                eslot(k + 1) + own};
+            TStencil<T, kPart> a{qslot(k - 1) + own, qslot(k) + own, qslot(k + 1) + own, nullptr, nullptr,
+                                 nullptr, G.sv, G.sy, G.sz};
+            if constexpr (t_edges<kPart>()) {
+                a.e0 = eslot(k) + own;
+                a.e1 = eslot(k + 1) + own;
+            }
+            if constexpr (kPart == 1) a.bg = Bf + G.sv * IA + G.idx(i, j, k);
             const long long t = (long long)i + (long long)G.CX * ((long long)j + (long long)G.CY * (k - G.kc0));
             trace3_cell<T, kPart>(a, G, i, dtd, core + core_base(t, kCore3));
         }
@@ -833,7 +882,7 @@ k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T
 template <typename T, int kPart = 0>
 cudaError_t launch_trace_tile(const Geo &G, const T *Q, const T *Bf, const T *E0, const T *E1, const T *E2, T *core,
                               const Scalars *S, cudaStream_t s) {
-    const int smem = trace_tile_smem<T>();
+    const int smem = trace_tile_smem<T, kPart>();
     static bool attr_set[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
