@@ -823,13 +823,15 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     int faces = 1;
     if (G.ndim == 3) {
-        TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
+        // the tiled trace computes its edge fields itself
+        if (kTraceTile32) n--;
+        else TIMED(KS_EFIELD, s, (k_efield3d<float><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2)));
         if (kTraceTile32 && kTraceSplit32) {
-            TIMED(KS_TRACE, s, (launch_trace_tile<float, 1>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
-            TIMED(KS_TRACE, s, (launch_trace_tile<float, 2>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<float, 1>(G, Q, U.hi, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<float, 2>(G, Q, U.hi, core, B.S, s)));
             n++;
         } else if (kTraceTile32) {
-            TIMED(KS_TRACE, s, (launch_trace_tile<float>(G, Q, U.hi, E0, E1, E2, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<float>(G, Q, U.hi, core, B.S, s)));
         } else if (kTraceSplit32) {
             TIMED(KS_TRACE, s, (k_trace3d<float, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));
             TIMED(KS_TRACE, s, (k_trace3d<float, 2><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.hi, E0, E1, E2, core, B.S)));

@@ -288,13 +288,15 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     }
     if (G.shearing) TIMED(KS_SCALARS, s, (k_shear_offset<<<1, 1, 0, s>>>(G, B.S, 0.5)));
     if (G.ndim == 3) {
-        TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
+        // the tiled trace computes its edge fields itself
+        if (kTraceTile64) n--;
+        else TIMED(KS_EFIELD, s, (k_efield3d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2)));
         if (kTraceTile64 && kTraceSplit64) {
-            TIMED(KS_TRACE, s, (launch_trace_tile<double, 1>(G, Q, U.p, E0, E1, E2, core, B.S, s)));
-            TIMED(KS_TRACE, s, (launch_trace_tile<double, 2>(G, Q, U.p, E0, E1, E2, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<double, 1>(G, Q, U.p, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<double, 2>(G, Q, U.p, core, B.S, s)));
             n++;
         } else if (kTraceTile64) {
-            TIMED(KS_TRACE, s, (launch_trace_tile<double>(G, Q, U.p, E0, E1, E2, core, B.S, s)));
+            TIMED(KS_TRACE, s, (launch_trace_tile<double>(G, Q, U.p, core, B.S, s)));
         } else if (kTraceSplit64) {
             TIMED(KS_TRACE, s, (k_trace3d<double, 1><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));
             TIMED(KS_TRACE, s, (k_trace3d<double, 2><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E0, E1, E2, core, B.S)));

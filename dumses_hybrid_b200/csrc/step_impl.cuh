@@ -699,28 +699,32 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
 // ---------------------------------------------------------------------------
 // The 3D trace with its stencil staged in shared memory.  A block of kThreads threads owns a
 // tile of kTX x kTY cells in (x, y) and marches along z through kTZ planes of the core index
-// space.  Shared memory holds a ring of z planes of the tile plus a one-cell halo in x and y:
-// the primitive variables and left-face field components the part needs (kRingQ planes: k-1,
-// k, k+1 and the one being fetched) and the 3 edge-field components of the trace (kRingE
-// planes: k, k+1 and the one being fetched).  Planes arrive by cp.async (element copies, so no
-// alignment rule applies to the ghosted rows); plane k+2 is fetched while plane k is computed,
-// and one block barrier per plane orders the ring.  Each stencil read is then a shared-memory
-// load at a fixed offset from the thread's cell.  The parts (kPart as in trace3_cell) stage
-// only what they read: part 1 the 8 primitives (its four face-B values come from global
-// memory), part 2 the face-B components and the edge fields, part 0 all of them.
+// space.  Shared memory holds a ring of kRingQ z planes (k-1, k, k+1 and the one being
+// fetched) of the tile plus a one-cell halo in x and y, with the primitive variables and
+// left-face field components the part reads, and a ring of kRingE planes of the trace's edge
+// fields (scheme.f90:1194-1239), which the block computes from the staged planes: edge plane
+// k+1 needs the cell planes k and k+1 only.  Planes arrive by cp.async (element copies, so no
+// alignment rule applies to the ghosted rows); cell plane k+2 is fetched while plane k is
+// computed.  Each stencil read is a shared-memory load at a fixed offset from the thread's
+// cell.  The parts (kPart as in trace3_cell) stage only what they read: part 1 the 8
+// primitives (its four face-B values come from global memory) and no edge fields, part 2 the
+// velocities and the face-B components (for the edge fields), part 0 all of them.
 // ---------------------------------------------------------------------------
 constexpr int kTX = 32, kTY = kThreads / kTX;
 constexpr int kTR = kTX + 2;              // row of a staged plane (halo of one cell each side)
 constexpr int kTP = kTR * (kTY + 2);      // one field of a staged plane
-constexpr int kRingQ = 4, kRingE = 3;
+constexpr int kRingQ = 4, kRingE = 2;
 #ifndef DG_TRACE_KZ
 #define DG_TRACE_KZ 16
 #endif
 constexpr int kTZ = DG_TRACE_KZ;
-// staged fields of a Q plane: [tq_first, tq_first + tq_count) of the 8 primitives (0-7) and
-// the 3 left-face field components (8-10)
-template <int kPart> __host__ __device__ constexpr int tq_first() { return kPart == 2 ? NVAR : 0; }
-template <int kPart> __host__ __device__ constexpr int tq_count() { return kPart == 1 ? NVAR : (kPart == 2 ? 3 : NVAR + 3); }
+// staged fields of a cell plane; field v (0-7 primitives, 8-10 face-B components) sits at
+// slot position tq_pos(v): part 0 all 11, part 1 the 8 primitives, part 2 u, v, w and the face B
+template <int kPart> __host__ __device__ constexpr int tq_count() { return kPart == 0 ? NVAR + 3 : kPart == 1 ? NVAR : 6; }
+template <int kPart> __host__ __device__ constexpr int tq_field(int f) {  // the field at slot position f
+    return kPart == 2 ? (f < 3 ? IU + f : NVAR + f - 3) : f;
+}
+template <int kPart> __host__ __device__ constexpr int tq_pos(int v) { return kPart == 2 ? (v < NVAR ? v - IU : v - NVAR + 3) : v; }
 template <int kPart> __host__ __device__ constexpr bool t_edges() { return kPart != 1; }
 template <typename T, int kPart>
 constexpr int trace_tile_smem() {
@@ -729,18 +733,18 @@ constexpr int trace_tile_smem() {
 
 template <typename T, int kPart>
 struct TStencil {
-    const T *p0, *p1, *p2;  // this cell in the staged Q planes k-1, k, k+1
-    const T *e0, *e1;       // this cell in the staged edge planes k, k+1
+    const T *p0, *p1, *p2;  // this cell in the staged cell planes k-1, k, k+1
+    const T *e0, *e1;       // this cell in the edge planes k, k+1
     const T *bg;            // part 1: this cell's left-face component 0 in global memory ...
     long long sv, sy, sz;   // ... and the strides from it
     __device__ __forceinline__ const T *pl(int dk) const { return dk < 0 ? p0 : (dk > 0 ? p2 : p1); }
     __device__ __forceinline__ T q(int v, int di, int dj, int dk) const {
-        if constexpr (kPart == 2) return T(0);  // part 2 reads no primitive
-        else return pl(dk)[(v - tq_first<kPart>()) * kTP + dj * kTR + di];
+        if constexpr (kPart == 2) return T(0);  // part 2 evaluates no primitive
+        else return pl(dk)[tq_pos<kPart>(v) * kTP + dj * kTR + di];
     }
     __device__ __forceinline__ T bf(int c, int di, int dj, int dk) const {
         if constexpr (kPart == 1) return ld(bg + sv * c + sy * dj + sz * dk + di);
-        else return pl(dk)[(NVAR + c - tq_first<kPart>()) * kTP + dj * kTR + di];
+        else return pl(dk)[tq_pos<kPart>(NVAR + c) * kTP + dj * kTR + di];
     }
     __device__ __forceinline__ T ex(int dj, int dk) const {
         if constexpr (kPart == 1) return T(0);  // part 1 reads no edge field
@@ -770,7 +774,7 @@ __device__ __forceinline__ void cp_elem(T *dst, const T *src, bool ok) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// fetch the staged fields of Q plane k (tile + halo) into slot s
+// fetch the staged fields of cell plane k (tile + halo) into slot s
 template <typename T, int kPart>
 __device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *Bf, T *s, int i0, int j0, int k) {
     const bool kok = k + G.gz - 1 >= 0 && k + G.gz - 1 < G.NZ;
@@ -781,30 +785,64 @@ __device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *
         const long long c = ok ? G.idx(i, j, k) : 0;
 #pragma unroll
         for (int f = 0; f < tq_count<kPart>(); f++) {
-            const int v = tq_first<kPart>() + f;
+            const int v = tq_field<kPart>(f);
             cp_elem(s + f * kTP + q, (v < NVAR ? Q + G.sv * v : Bf + G.sv * (IA + v - NVAR)) + c, ok);
         }
     }
 }
-// fetch the trace's edge fields of plane k (edges i0..i0+kTX, j0..j0+kTY) into slot s
-template <typename T>
-__device__ __forceinline__ void fetch_eplane(const Geo &G, const T *Ex, const T *Ey, const T *Ez, T *s, int i0, int j0,
-                                             int k) {
-    const bool kok = k - G.ke0 >= 0 && k - G.ke0 < G.EZ;
+
+// the trace's edge fields of plane k (Ex_at, Ey_at, Ez_at on the staged cell planes lo = k-1
+// and hi = k) for the edges i0..i0+kTX, j0..j0+kTY, into slot s at the cells' positions
+template <typename T, int kPart>
+__device__ __forceinline__ void edge_plane(const Geo &G, const T *lo, const T *hi, T *s, int i0) {
+    constexpr int pU = tq_pos<kPart>(IU) * kTP, pV = tq_pos<kPart>(IV) * kTP, pW = tq_pos<kPart>(IW) * kTP;
+    constexpr int pA = tq_pos<kPart>(NVAR) * kTP, pB = tq_pos<kPart>(NVAR + 1) * kTP, pC = tq_pos<kPart>(NVAR + 2) * kTP;
+    const T forth = T(0.25), half = T(0.5);
+    const bool shear = (G.omega0 > 0.0) && !G.fargo;
     for (int q = threadIdx.x; q < (kTX + 1) * (kTY + 1); q += kThreads) {
         const int ii = 1 + q % (kTX + 1), jj = 1 + q / (kTX + 1);
-        const int i = i0 - 1 + ii, j = j0 - 1 + jj;
-        const bool ok = kok && i < G.EX && j < G.EY;
-        const long long e = ok ? G.eidx(i, j, k) : 0;
-        const int o = jj * kTR + ii;
-        cp_elem(s + o, Ex + e, ok);
-        cp_elem(s + kTP + o, Ey + e, ok);
-        cp_elem(s + 2 * kTP + o, Ez + e, ok);
+        const int o = jj * kTR + ii;                    // edge (i, j) sits at cell (i, j)
+        const int ojm = o - kTR, oim = o - 1, oimjm = o - kTR - 1;
+        const int i = i0 - 1 + ii;
+        // Ex(i, j, k): cells (i, j-1..j, k-1..k)
+        {
+            T v = forth * (lo[pV + ojm] + hi[pV + ojm] + lo[pV + o] + hi[pV + o]);
+            T w = forth * (lo[pW + ojm] + hi[pW + ojm] + lo[pW + o] + hi[pW + o]);
+            T B = half * (lo[pB + o] + hi[pB + o]);
+            T C = half * (hi[pC + ojm] + hi[pC + o]);
+            T e = v * C - w * B;
+            if (shear) {
+                T sh = (T)(-1.5 * G.omega0 * G.xc(i));
+                e = e + sh * C;
+            }
+            s[o] = e;
+        }
+        // Ey(i, j, k): cells (i-1..i, j, k-1..k)
+        {
+            T u = forth * (lo[pU + oim] + hi[pU + oim] + lo[pU + o] + hi[pU + o]);
+            T w = forth * (lo[pW + oim] + hi[pW + oim] + lo[pW + o] + hi[pW + o]);
+            T A = half * (lo[pA + o] + hi[pA + o]);
+            T C = half * (hi[pC + oim] + hi[pC + o]);
+            s[kTP + o] = w * A - u * C;
+        }
+        // Ez(i, j, k): cells (i-1..i, j-1..j, k)
+        {
+            T u = forth * (hi[pU + oimjm] + hi[pU + oim] + hi[pU + ojm] + hi[pU + o]);
+            T v = forth * (hi[pV + oimjm] + hi[pV + oim] + hi[pV + ojm] + hi[pV + o]);
+            T A = half * (hi[pA + ojm] + hi[pA + o]);
+            T B = half * (hi[pB + oim] + hi[pB + o]);
+            T e = u * B - v * A;
+            if (shear) {
+                T sh = (T)(-1.5 * G.omega0 * 0.5 * (G.xc(i) + G.xc(i - 1)));
+                e = e - sh * A;
+            }
+            s[2 * kTP + o] = e;
+        }
     }
 }
 
 // resident blocks per SM the tiled trace is compiled for, by arithmetic and part (bounded by
-// its shared memory: FP64 86/52/34 KB, FP32 43/26/17 KB per block for parts 0/1/2)
+// its shared memory: FP64 82/52/49 KB, FP32 41/26/24 KB per block for parts 0/1/2)
 #ifndef DG_TRACET_MINB64
 #define DG_TRACET_MINB64 2
 #endif
@@ -812,7 +850,7 @@ __device__ __forceinline__ void fetch_eplane(const Geo &G, const T *Ex, const T 
 #define DG_TRACET1_MINB64 4
 #endif
 #ifndef DG_TRACET2_MINB64
-#define DG_TRACET2_MINB64 6
+#define DG_TRACET2_MINB64 4
 #endif
 #ifndef DG_TRACET_MINB32
 #define DG_TRACET_MINB32 5
@@ -830,10 +868,9 @@ constexpr int trace_tile_minb() {
 }
 template <typename T, int kPart = 0>
 __global__ void __launch_bounds__(kThreads, (trace_tile_minb<T, kPart>()))
-k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__restrict__ Exa,
-               const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
+k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, T *__restrict__ core, const Scalars *S) {
     extern __shared__ __align__(16) unsigned char tsm[];
-    constexpr int kQS = tq_count<kPart>() * kTP;  // one Q slot
+    constexpr int kQS = tq_count<kPart>() * kTP;  // one cell-plane slot
     T *ringQ = (T *)tsm;
     T *ringE = ringQ + kRingQ * kQS;
     const int i0 = blockIdx.x * kTX, j0 = blockIdx.y * kTY;
@@ -846,22 +883,23 @@ k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T
     auto qslot = [&](int k) { return ringQ + ((k - kb + 1) % kRingQ) * kQS; };
     auto eslot = [&](int k) { return ringE + ((k - kb) % kRingE) * (3 * kTP); };
     const double dtd = S->dt;
-    // planes k-1, k and edge plane k of the first core plane, then plane k+1
     fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb - 1), i0, j0, kb - 1);
     fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb), i0, j0, kb);
-    if constexpr (t_edges<kPart>()) fetch_eplane(G, Exa, Eya, Eza, eslot(kb), i0, j0, kb);
     cp_commit();
     fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb + 1), i0, j0, kb + 1);
-    if constexpr (t_edges<kPart>()) fetch_eplane(G, Exa, Eya, Eza, eslot(kb + 1), i0, j0, kb + 1);
     cp_commit();
+    cp_wait_all();
+    __syncthreads();
+    if constexpr (t_edges<kPart>()) edge_plane<T, kPart>(G, qslot(kb - 1), qslot(kb), eslot(kb), i0);
     for (int k = kb; k < ke; k++) {
-        cp_wait_all();
-        __syncthreads();  // plane k+1 is in; every thread is done with plane k-1
-        if (k + 2 <= ke) {
-            fetch_qplane<T, kPart>(G, Q, Bf, qslot(k + 2), i0, j0, k + 2);
-            if constexpr (t_edges<kPart>()) fetch_eplane(G, Exa, Eya, Eza, eslot(k + 2), i0, j0, k + 2);
-        }
+        // cell planes k-1 .. k+1 are in, edge plane k is written; fetch cell plane k+2 into the
+        // slot of plane k-2 (read last by the trace of plane k-1, before the barrier ending it)
+        if (k + 2 <= ke) fetch_qplane<T, kPart>(G, Q, Bf, qslot(k + 2), i0, j0, k + 2);
         cp_commit();
+        if constexpr (t_edges<kPart>()) {
+            edge_plane<T, kPart>(G, qslot(k), qslot(k + 1), eslot(k + 1), i0);  // into the slot of plane k-1
+            __syncthreads();
+        }
         if (mine) {
             TStencil<T, kPart> a{qslot(k - 1) + own, qslot(k) + own, qslot(k + 1) + own, nullptr, nullptr,
                                  nullptr, G.sv, G.sy, G.sz};
@@ -873,15 +911,15 @@ k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T
             const long long t = (long long)i + (long long)G.CX * ((long long)j + (long long)G.CY * (k - G.kc0));
             trace3_cell<T, kPart>(a, G, i, dtd, core + core_base(t, kCore3));
         }
+        cp_wait_all();
+        __syncthreads();  // cell plane k+2 is in; every thread is done with planes k-1 (cells, edges)
     }
-    cp_wait_all();
 }
 
 // launch k_trace3d_tile over the core index space (its dynamic shared memory is above the
 // default 48 KB limit in FP64: the attribute is set once per device)
 template <typename T, int kPart = 0>
-cudaError_t launch_trace_tile(const Geo &G, const T *Q, const T *Bf, const T *E0, const T *E1, const T *E2, T *core,
-                              const Scalars *S, cudaStream_t s) {
+cudaError_t launch_trace_tile(const Geo &G, const T *Q, const T *Bf, T *core, const Scalars *S, cudaStream_t s) {
     const int smem = trace_tile_smem<T, kPart>();
     static bool attr_set[64] = {};
     int dev = 0;
@@ -894,7 +932,7 @@ cudaError_t launch_trace_tile(const Geo &G, const T *Q, const T *Bf, const T *E0
     }
     const dim3 grid((unsigned)((G.CX + kTX - 1) / kTX), (unsigned)((G.CY + kTY - 1) / kTY),
                     (unsigned)((G.CZ + kTZ - 1) / kTZ));
-    k_trace3d_tile<T, kPart><<<grid, kThreads, smem, s>>>(G, Q, Bf, E0, E1, E2, core, S);
+    k_trace3d_tile<T, kPart><<<grid, kThreads, smem, s>>>(G, Q, Bf, core, S);
     return cudaSuccess;
 }
 
