@@ -200,6 +200,9 @@ int validate(const dg_params *p) {
     if (!(p->nu >= 0.0) || !(p->eta >= 0.0)) return fail(DG_ERR_ARG, "nu and eta must be >= 0");
     if (p->surrogate && p->iriemann != DG_RIEMANN_HLLD)
         return fail(DG_ERR_UNSUPPORTED, "the flux surrogate stands in for HLLD (iriemann = hlld)");
+    // the kernels index cells, faces and edges with 32-bit linear indices
+    if ((double)(p->nx + 6) * (p->ndim > 1 ? p->ny + 6 : 1) * (p->ndim == 3 ? p->nz + 6 : 1) >= 2147483647.0)
+        return fail(DG_ERR_UNSUPPORTED, "grid too large: (nx+6)(ny+6)(nz+6) must stay below 2^31 cells");
     if (p->nzslice < 0) return fail(DG_ERR_ARG, "nzslice must be >= 0");
     if (p->nzslice > 1) {
         if (p->ndim != 3) return fail(DG_ERR_UNSUPPORTED, "a z-slab decomposition needs ndim = 3");
@@ -256,6 +259,16 @@ dg::Geo dg::make_geo(const dg_params &p) {
         G.bcz_lo = (p.bc[2] == DG_BC_ZERO_GRADIENT && G.zposition == 0) ? DG_BC_ZERO_GRADIENT : dg::kBcHalo;
         G.bcz_hi = (p.bc[2] == DG_BC_ZERO_GRADIENT && G.zposition == G.nzslice - 1) ? DG_BC_ZERO_GRADIENT : dg::kBcHalo;
     }
+    // dividers of the linear index spaces (every space has fewer than 2^31 points: validate)
+    G.dFX = dg::make_fastdiv((unsigned)G.FX); G.dFY = dg::make_fastdiv((unsigned)G.FY);
+    G.dFZ = dg::make_fastdiv((unsigned)G.FZ);
+    G.dCX = dg::make_fastdiv((unsigned)G.CX); G.dCY = dg::make_fastdiv((unsigned)G.CY);
+    G.dEX = dg::make_fastdiv((unsigned)G.EX); G.dEY = dg::make_fastdiv((unsigned)G.EY);
+    G.dPX = dg::make_fastdiv((unsigned)(p.nx + 5)); G.dPY = dg::make_fastdiv((unsigned)(p.ndim > 1 ? p.ny + 5 : 1));
+    // smallp = smallr smallc^2 / gamma, as the trace and the solvers form it (trace3d, solver.f90)
+    G.smallp = dg::kSmallr * (dg::kSmallc * dg::kSmallc) / p.gamma;
+    G.dvloc = 1.0 / (G.dx * G.dy * G.dz);
+    G.rdx = 1.0 / G.dx; G.rdy = 1.0 / G.dy; G.rdz = 1.0 / G.dz;
     // ndim_act, init.f90:203-213
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     if ((nx == 1 && ny == 1) || (nx == 1 && nz == 1) || (ny == 1 && nz == 1)) G.ndim_act = 1;

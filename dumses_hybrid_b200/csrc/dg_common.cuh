@@ -29,6 +29,40 @@ __device__ __forceinline__ float fab(float x) { return fabsf(x); }
 __device__ __forceinline__ double sqr(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqr(float x) { return sqrtf(x); }
 
+// Unsigned division by a divisor fixed for the context, by a multiply-high and a shift
+// (Granlund and Montgomery, "Division by invariant integers using multiplication", PLDI 1994,
+// theorem 4.2 with N = 32): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// n / d = (mulhi(m, n) + n) >> l for every n < 2^31 (the sum then stays below 2^32).  The
+// kernels split their linear cell, face and edge indices (all below 2^31, checked when a
+// context is made) into (i, j, k) with it instead of 64-bit divisions.
+struct FastDiv {
+    unsigned d, m;
+    int l;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d;
+    f.l = 0;
+    while ((1ull << f.l) < d) f.l++;
+    f.m = (unsigned)(((1ull << 32) * ((1ull << f.l) - d)) / d + 1);
+    return f;
+}
+__host__ __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv &f) {
+#ifdef __CUDA_ARCH__
+    return (__umulhi(f.m, n) + n) >> f.l;
+#else
+    return (unsigned)((((unsigned long long)f.m * n >> 32) + n) >> f.l);
+#endif
+}
+// a + X (b + Y c) = t  ->  (a, b, c)
+__host__ __device__ __forceinline__ void split3(unsigned t, const FastDiv &X, const FastDiv &Y, int &a, int &b, int &c) {
+    const unsigned r = fdiv(t, X);
+    a = (int)(t - r * X.d);
+    const unsigned q = fdiv(r, Y);
+    b = (int)(r - q * Y.d);
+    c = (int)q;
+}
+
 // Geometry of one context, passed to every kernel by value.
 struct Geo {
     int ndim, nx, ny, nz;
@@ -55,6 +89,12 @@ struct Geo {
     // upper z sides (bc[2], or kBcHalo where the neighbour's halo fills the ghost planes)
     int nzslice, zposition;
     int bcz_lo, bcz_hi;
+    // dividers of the index spaces: face (FX, FY, FZ), core (CX, CY), edge (EX, EY), and the
+    // ghosted cells of the primitive variables (nx+5, ny+5)
+    FastDiv dFX, dFY, dFZ, dCX, dCY, dEX, dEY, dPX, dPY;
+    double smallp;            // pressure floor smallr smallc^2 / gamma of the trace and solvers
+    double dvloc;             // 1 / (dx dy dz), as update forms it (scheme.f90:1778-1779)
+    double rdx, rdy, rdz;     // 1 / dx, 1 / dy, 1 / dz (FP32 constrained transport)
 
     __host__ __device__ __forceinline__ long long idx(int i, int j, int k) const {
         return (long long)(i + 2) + sy * (long long)(j + gy - 1) + sz * (long long)(k + gz - 1);

@@ -42,10 +42,10 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
                                                           const float *__restrict__ ez, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    int i, j, k;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
+    const long long fxy = (long long)G.FX * G.FY;  // face index steps: +1 (x), +FX (y), +fxy (z)
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const double dtd = S->dt;
     const float dt = (float)dtd;
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
     }
 
     if (i <= nx && j <= ny && k <= nz) {
-        const float dvloc = (float)(1.0 / (G.dx * G.dy * G.dz));
+        const float dvloc = (float)G.dvloc;
         const float Om = (float)G.omega0;
         float dr = 0.f, du = 0.f, dv = 0.f, dw = 0.f, dp = 0.f;
         float opl = 1.f;
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
             du += uu * rm1 + 2.f * Om * dt * uv / opl;
             dv += uv * rm1 - 0.5f * Om * dt * uu / opl;
         }
-        const long long FR[3] = {G.fidx(i + 1, j, k), G.fidx(i, j + 1, k), G.fidx(i, j, k + 1)};
+        const long long FR[3] = {(t + 1), (t + G.FX), (t + fxy)};
         const float *FA[3] = {fx, fy, fz};
         const float ds[3] = {(float)(G.dy * G.dz), (float)(G.dx * G.dz), (float)(G.dx * G.dy)};
         float pre[3];
@@ -120,21 +120,21 @@ __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo 
             return shear_avg(G, sr, ey, 1, ii == 1 ? 0 : 1, jj, kk);
         return ld(ey + G.fidx(ii, jj, kk));
     };
-    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
+    const float rdx = (float)G.rdx, rdy = (float)G.rdy, rdz = (float)G.rdz;
     const bool ct = G.ndim_act > 1;
     if (j <= ny && k <= nz) {
         float inc = 0.f;
-        if (ct) inc = (ld(ez + G.fidx(i, j + 1, k)) - ld(ez + t)) * rdy - (EYc(i, j, k + 1) - EYc(i, j, k)) * rdz;
+        if (ct) inc = (ld(ez + (t + G.FX)) - ld(ez + t)) * rdy - (EYc(i, j, k + 1) - EYc(i, j, k)) * rdz;
         put(Un, G, IA, c, uh[IA], ul[IA], inc);
     }
     if (i <= nx && k <= nz) {
         float inc = 0.f;
-        if (ct) inc = -(ld(ez + G.fidx(i + 1, j, k)) - ld(ez + t)) * rdx + (ld(ex + G.fidx(i, j, k + 1)) - ld(ex + t)) * rdz;
+        if (ct) inc = -(ld(ez + (t + 1)) - ld(ez + t)) * rdx + (ld(ex + (t + fxy)) - ld(ex + t)) * rdz;
         put(Un, G, IB, c, uh[IB], ul[IB], inc);
     }
     if (i <= nx && j <= ny) {
         float inc = 0.f;
-        if (ct) inc = (EYc(i + 1, j, k) - EYc(i, j, k)) * rdx - (ld(ex + G.fidx(i, j + 1, k)) - ld(ex + t)) * rdy;
+        if (ct) inc = (EYc(i + 1, j, k) - EYc(i, j, k)) * rdx - (ld(ex + (t + G.FX)) - ld(ex + t)) * rdy;
         put(Un, G, IC, c, uh[IC], ul[IC], inc);
     }
 }
@@ -144,8 +144,8 @@ __global__ void __launch_bounds__(kThreads) k_update2d_hl(Geo G, StoreHL U, Stor
                                                           const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const int j = (int)(t / G.FX) + 1;
+    const int j = (int)fdiv((unsigned)t, G.dFX) + 1;
+    const int i = (int)((unsigned)t - (unsigned)(j - 1) * G.dFX.d) + 1;
     const int k = 1;
     const int nx = G.nx, ny = G.ny;
     const double dtd = S->dt;
@@ -235,7 +235,7 @@ __device__ __forceinline__ void prim_hl(const Geo &G, const StoreHL &U, long lon
         const double eken = 0.5 * ((double)q[IU] * q[IU] + (double)q[IV] * q[IV] + (double)q[IW] * q[IW]);
         double pe = (G.gamma - 1.0) * (E - emag - d * eken);
         if (d < kSmallr) pe = pe * (kSmallr / d);
-        q[IP] = (float)mx(pe, kSmallr * (kSmallc * kSmallc) / G.gamma);
+        q[IP] = (float)mx(pe, G.smallp);
     }
 }
 
@@ -244,10 +244,11 @@ __global__ void __launch_bounds__(kThreads) k_prim_hl(Geo G, StoreHL U, float *_
     const long long n = (long long)ni * nj * nk;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int i = (int)(t % ni) - 2;
-    const long long r = t / ni;
-    const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
-    const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+    int i, j, k;
+    split3((unsigned)t, G.dPX, G.dPY, i, j, k);
+    i -= 2;
+    j = (G.ndim > 1) ? j - 2 : 1;
+    k = (G.ndim == 3) ? k - 2 : 1;
     const long long c = G.idx(i, j, k);
     float q[8];
     prim_hl(G, U, c, q);
@@ -269,16 +270,17 @@ __global__ void __launch_bounds__(kThreads) k_prim_dt_hl(Geo G, StoreHL U, float
     const int ni = G.nx + 5, nj = (G.ndim > 1) ? G.ny + 5 : 1, nk = (G.ndim == 3) ? G.nz + 5 : 1;
     const long long n = (long long)ni * nj * nk;
     const float gamma = (float)G.gamma;
-    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
+    const float rdx = (float)G.rdx, rdy = (float)G.rdy, rdz = (float)G.rdz;
     const float vsh = ((G.omega0 > 0.0) && !G.fargo) ? (float)(1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5) : 0.0f;
     float best = __int_as_float(0x7f800000);  // +inf
     int bad = 0;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t < n) {
-        const int i = (int)(t % ni) - 2;
-        const long long r = t / ni;
-        const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
-        const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+        int i, j, k;
+        split3((unsigned)t, G.dPX, G.dPY, i, j, k);
+        i -= 2;
+        j = (G.ndim > 1) ? j - 2 : 1;
+        k = (G.ndim == 3) ? k - 2 : 1;
         const long long c = G.idx(i, j, k);
         float q[8];
         prim_hl(G, U, c, q);
@@ -448,7 +450,7 @@ __global__ void __launch_bounds__(kThreads, DG_FARGO_MINB32) k_fargo_update_hl(G
             }
         }
     }
-    const float rdx = (float)(1.0 / G.dx), rdy = (float)(1.0 / G.dy), rdz = (float)(1.0 / G.dz);
+    const float rdx = (float)G.rdx, rdy = (float)G.rdy, rdz = (float)G.rdz;
     // face indices clamped into the EMF arrays; a clamped value is never used
     auto EX = [&](int ii, int jj, int kk) { return ld(fex + G.fidx(ii, mn(jj, G.FY), mn(kk, G.FZ))); };
     auto EZ = [&](int ii, int jj, int kk) { return (ii <= nx + 1) ? ld(fez + G.fidx(ii, mn(jj, G.FY), kk)) : 0.0f; };
@@ -613,10 +615,8 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         int i = 0, j = 0, k = 1;
         bool valid = t < G.fsz;
         if (valid) {
-            i = (int)(t % G.FX) + 1;
-            const long long r = t / G.FX;
-            j = (int)(r % G.FY) + 1;
-            k = (int)(r / G.FY) + 1;
+            split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+            i++; j++; k++;
             valid = (d == 0) ? (j <= G.ny && (G.ndim == 2 || k <= G.nz))
                   : (d == 1) ? (i <= G.nx && (G.ndim == 2 || k <= G.nz)) : (i <= G.nx && j <= G.ny);
         }
@@ -746,9 +746,9 @@ __global__ void __launch_bounds__(kThreads) k_nn_fallback(Geo G, const float *__
     for (unsigned long long q = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; q < n;
          q += (unsigned long long)gridDim.x * blockDim.x) {
         const long long t = list[q];
-        const int i = (int)(t % G.FX) + 1;
-        const long long r = t / G.FX;
-        const int j = (int)(r % G.FY) + 1, k = (int)(r / G.FY) + 1;
+        int i, j, k;
+        split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+        i++; j++; k++;
         long long cl, cr;
         face_cells(G, d, i, j, k, cl, cr);
         face_flux(G, cv, cl, cr, d, i, dt, flux, t);

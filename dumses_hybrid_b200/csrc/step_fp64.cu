@@ -26,10 +26,10 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
                                                        const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    int i, j, k;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
+    const long long fxy = (long long)G.FX * G.FY;  // face index steps: +1 (x), +FX (y), +fxy (z)
     const int nx = G.nx, ny = G.ny, nz = G.nz;
     const double dt = S->dt;
     const double one = 1.0, two = 2.0, half = 0.5;
@@ -48,8 +48,7 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
             lambda = Omega0 * dt; lambda = 2.5e-1 * lambda * lambda;
             ratio = (one - lambda) / (one + lambda);
         }
-        const double dv = G.dx * G.dy * G.dz;
-        const double dvloc = one / dv;
+        const double dvloc = G.dvloc;  // one / (dx dy dz)
         double ur = ld(U + c), uu = ld(U + sv * IU + c), uv = ld(U + sv * IV + c), uw = ld(U + sv * IW + c);
         double up = ld(U + sv * IP + c);
         if (Omega0 > 0.0) {
@@ -59,7 +58,7 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
             uv = uv * ratio + dsy;
         }
         const long long f0 = t;
-        const long long fxr = G.fidx(i + 1, j, k), fyr = G.fidx(i, j + 1, k), fzr = G.fidx(i, j, k + 1);
+        const long long fxr = (t + 1), fyr = (t + G.FX), fzr = (t + fxy);
         const double *FA[3] = {fx, fy, fz};
         const long long FR[3] = {fxr, fyr, fzr};
         double pre[3];
@@ -107,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
     if (j <= ny && k <= nz) {  // B_x at face i (i = 1..nx+1)
         double b = ld(U + sv * IA + c);
         if (ct) {
-            b = b + (ld(ez + G.fidx(i, j + 1, k)) - ld(ez + t)) / dy;
+            b = b + (ld(ez + (t + G.FX)) - ld(ez + t)) / dy;
             b = b - (EYc(i, j, k + 1) - EYc(i, j, k)) / dz;
         }
         Un[sv * IA + c] = b;
@@ -115,14 +114,14 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
     if (i <= nx && k <= nz) {  // B_y at face j
         double b = ld(U + sv * IB + c);
         if (ct) {
-            b = b - (ld(ez + G.fidx(i + 1, j, k)) - ld(ez + t)) / dx;
-            b = b + (ld(ex + G.fidx(i, j, k + 1)) - ld(ex + t)) / dz;
+            b = b - (ld(ez + (t + 1)) - ld(ez + t)) / dx;
+            b = b + (ld(ex + (t + fxy)) - ld(ex + t)) / dz;
         }
         Un[sv * IB + c] = b;
     }
     if (i <= nx && j <= ny) {  // B_z at face k
         double b = ld(U + sv * IC + c);
-        if (ct) b = b + (EYc(i + 1, j, k) - EYc(i, j, k)) / dx - (ld(ex + G.fidx(i, j + 1, k)) - ld(ex + t)) / dy;
+        if (ct) b = b + (EYc(i + 1, j, k) - EYc(i, j, k)) / dx - (ld(ex + (t + G.FX)) - ld(ex + t)) / dy;
         Un[sv * IC + c] = b;
     }
 }
@@ -132,8 +131,8 @@ __global__ void __launch_bounds__(kThreads) k_update2d(Geo G, const double *__re
                                                        const double *__restrict__ ez, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const int j = (int)(t / G.FX) + 1;
+    const int j = (int)fdiv((unsigned)t, G.dFX) + 1;
+    const int i = (int)((unsigned)t - (unsigned)(j - 1) * G.dFX.d) + 1;
     const int k = 1;
     const int nx = G.nx, ny = G.ny;
     const double dt = S->dt;

@@ -252,7 +252,7 @@ __device__ __forceinline__ void prim_cell(const Geo &G, const Store &U, long lon
     if (G.iso) {
         q[IP] = d * (G.ciso * G.ciso);
     } else {
-        const double smallp = kSmallr * (kSmallc * kSmallc) / G.gamma;
+        const double smallp = G.smallp;
         double eken = half * (q[IU] * q[IU] + q[IV] * q[IV] + q[IW] * q[IW]);
         double emag = half * (q[IA] * q[IA] + q[IB] * q[IB] + q[IC] * q[IC]);
         double eint = (U.getr(G, IP, c) - emag) / d - eken;
@@ -290,10 +290,11 @@ __global__ void __launch_bounds__(kThreads) k_prim_dt(Geo G, Store U, double *__
     int bad = 0;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t < n) {
-        const int i = (int)(t % ni) - 2;
-        const long long r = t / ni;
-        const int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
-        const int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+        int i, j, k;
+        split3((unsigned)t, G.dPX, G.dPY, i, j, k);
+        i -= 2;
+        j = (G.ndim > 1) ? j - 2 : 1;
+        k = (G.ndim == 3) ? k - 2 : 1;
         const long long c = G.idx(i, j, k);
         double q[8];
         prim_cell(G, U, c, 0.0, q);
@@ -345,10 +346,11 @@ __global__ void __launch_bounds__(kThreads) k_prim(Geo G, Store U, T *__restrict
     const long long n = (long long)ni * nj * nk;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= n) return;
-    int i = (int)(t % ni) - 2;
-    long long r = t / ni;
-    int j = (G.ndim > 1) ? (int)(r % nj) - 2 : 1;
-    int k = (G.ndim == 3) ? (int)(r / nj) - 2 : 1;
+    int i, j, k;
+    split3((unsigned)t, G.dPX, G.dPY, i, j, k);
+    i -= 2;
+    j = (G.ndim > 1) ? j - 2 : 1;
+    k = (G.ndim == 3) ? k - 2 : 1;
     const long long c = G.idx(i, j, k);
     double q[8];
     prim_cell(G, U, c, S->dt, q);
@@ -440,10 +442,9 @@ __global__ void __launch_bounds__(kThreads) k_efield3d(Geo G, const T *__restric
                                                        T *__restrict__ Ex, T *__restrict__ Ey, T *__restrict__ Ez) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.esz) return;
-    const int i = (int)(t % G.EX);
-    const long long rr = t / G.EX;
-    const int j = (int)(rr % G.EY);
-    const int k = (int)(rr / G.EY) + G.ke0;
+    int i, j, k;
+    split3((unsigned)t, G.dEX, G.dEY, i, j, k);
+    k += G.ke0;
     const QV<T> a{Q, Bf, G};
     Ex[t] = Ex_at(a, i, j, k);
     Ey[t] = Ey_at(a, i, j, k);
@@ -455,8 +456,8 @@ __global__ void __launch_bounds__(kThreads) k_efield2d(Geo G, const T *__restric
                                                        T *__restrict__ Ez) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.esz) return;
-    const int i = (int)(t % G.EX);
-    const int j = (int)(t / G.EX);
+    const int j = (int)fdiv((unsigned)t, G.dEX);
+    const int i = (int)((unsigned)t - (unsigned)j * G.dEX.d);
     const QV<T> a{Q, Bf, G};
     Ez[t] = Ez2_at(a, i, j);
 }
@@ -688,10 +689,9 @@ k_trace3d(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, const T *__r
           const T *__restrict__ Eya, const T *__restrict__ Eza, T *__restrict__ core, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.csz) return;
-    const int i = (int)(t % G.CX);
-    const long long rr = t / G.CX;
-    const int j = (int)(rr % G.CY);
-    const int k = (int)(rr / G.CY) + G.kc0;
+    int i, j, k;
+    split3((unsigned)t, G.dCX, G.dCY, i, j, k);
+    k += G.kc0;
     const GStencil<T> a{QV<T>{Q, Bf, G}, Exa, Eya, Eza, i, j, k};
     trace3_cell<T, kPart>(a, G, i, S->dt, core + core_base(t, kCore3));
 }
@@ -760,33 +760,56 @@ struct TStencil {
     }
 };
 
-// one element copy global -> shared, zero-filled when the source is outside its array
-template <typename T>
-__device__ __forceinline__ void cp_elem(T *dst, const T *src, bool ok) {
-    ok = ok && chk(src, sizeof(T));
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    const int n = ok ? (int)sizeof(T) : 0;
-    if constexpr (sizeof(T) == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(ok ? src : nullptr), "r"(n) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(ok ? src : nullptr), "r"(n) : "memory");
-}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// fetch the staged fields of cell plane k (tile + halo) into slot s
-template <typename T, int kPart>
-__device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *Bf, T *s, int i0, int j0, int k) {
-    const bool kok = k + G.gz - 1 >= 0 && k + G.gz - 1 < G.NZ;
-    for (int q = threadIdx.x; q < kTP; q += kThreads) {
+// The positions of a staged plane a thread fetches (kTP <= 2 kThreads: at most two), fixed for
+// the whole z march: the cell of position n of plane k is c[n] + (k - k0) sz.
+struct FetchPos {
+    long long c[2];  // cell index at plane k0
+    int q[2];        // position in the plane, or -1
+    bool in[2];      // inside the ghosted grid in x and y
+    int k0;
+};
+__device__ __forceinline__ FetchPos fetch_positions(const Geo &G, int i0, int j0, int k0) {
+    FetchPos P;
+    P.k0 = k0;
+#pragma unroll
+    for (int n = 0; n < 2; n++) {
+        const int q = threadIdx.x + n * kThreads;
         const int ii = q % kTR, jj = q / kTR;
         const int i = i0 - 1 + ii, j = j0 - 1 + jj;
-        const bool ok = kok && i + 2 >= 0 && i + 2 < G.NX && j + G.gy - 1 >= 0 && j + G.gy - 1 < G.NY;
-        const long long c = ok ? G.idx(i, j, k) : 0;
+        P.q[n] = q < kTP ? q : -1;
+        P.in[n] = q < kTP && i + 2 >= 0 && i + 2 < G.NX && j + G.gy - 1 >= 0 && j + G.gy - 1 < G.NY;
+        P.c[n] = P.in[n] ? G.idx(i, j, k0) : 0;
+    }
+    return P;
+}
+
+// fetch the staged fields of cell plane k (tile + halo) into slot s: cp.async element copies,
+// or zeros where the cell is outside the ghosted grid
+template <typename T, int kPart>
+__device__ __forceinline__ void fetch_qplane(const Geo &G, const T *Q, const T *Bf, T *s, const FetchPos &P, int k) {
+    const bool kok = k + G.gz - 1 >= 0 && k + G.gz - 1 < G.NZ;
+    const long long dk = (long long)(k - P.k0) * G.sz;
+#pragma unroll
+    for (int n = 0; n < 2; n++) {
+        if (P.q[n] < 0) continue;
+        T *d = s + P.q[n];
+        const long long c = P.c[n] + dk;
 #pragma unroll
         for (int f = 0; f < tq_count<kPart>(); f++) {
             const int v = tq_field<kPart>(f);
-            cp_elem(s + f * kTP + q, (v < NVAR ? Q + G.sv * v : Bf + G.sv * (IA + v - NVAR)) + c, ok);
+            const T *src = (v < NVAR ? Q + G.sv * v : Bf + G.sv * (IA + v - NVAR)) + c;
+            if (kok && P.in[n] && chk(src, sizeof(T))) {
+                const unsigned a = (unsigned)__cvta_generic_to_shared(d + f * kTP);
+                if constexpr (sizeof(T) == 4)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(src) : "memory");
+                else
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(a), "l"(src) : "memory");
+            } else {
+                d[f * kTP] = T(0);
+            }
         }
     }
 }
@@ -883,10 +906,11 @@ k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, T *__re
     auto qslot = [&](int k) { return ringQ + ((k - kb + 1) % kRingQ) * kQS; };
     auto eslot = [&](int k) { return ringE + ((k - kb) % kRingE) * (3 * kTP); };
     const double dtd = S->dt;
-    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb - 1), i0, j0, kb - 1);
-    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb), i0, j0, kb);
+    const FetchPos P = fetch_positions(G, i0, j0, kb - 1);
+    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb - 1), P, kb - 1);
+    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb), P, kb);
     cp_commit();
-    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb + 1), i0, j0, kb + 1);
+    fetch_qplane<T, kPart>(G, Q, Bf, qslot(kb + 1), P, kb + 1);
     cp_commit();
     cp_wait_all();
     __syncthreads();
@@ -894,7 +918,7 @@ k_trace3d_tile(Geo G, const T *__restrict__ Q, const T *__restrict__ Bf, T *__re
     for (int k = kb; k < ke; k++) {
         // cell planes k-1 .. k+1 are in, edge plane k is written; fetch cell plane k+2 into the
         // slot of plane k-2 (read last by the trace of plane k-1, before the barrier ending it)
-        if (k + 2 <= ke) fetch_qplane<T, kPart>(G, Q, Bf, qslot(k + 2), i0, j0, k + 2);
+        if (k + 2 <= ke) fetch_qplane<T, kPart>(G, Q, Bf, qslot(k + 2), P, k + 2);
         cp_commit();
         if constexpr (t_edges<kPart>()) {
             edge_plane<T, kPart>(G, qslot(k), qslot(k + 1), eslot(k + 1), i0);  // into the slot of plane k-1
@@ -942,8 +966,8 @@ __global__ void __launch_bounds__(kThreads) k_trace2d(Geo G, const T *__restrict
                                                       const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.csz) return;
-    const int i = (int)(t % G.CX);
-    const int j = (int)(t / G.CX);
+    const int j = (int)fdiv((unsigned)t, G.dCX);
+    const int i = (int)((unsigned)t - (unsigned)j * G.dCX.d);
     const int k = 1;
     const QV<T> a{Q, Bf, G};
     const double dtd = S->dt;
@@ -1142,7 +1166,7 @@ template <typename T>
 __device__ __forceinline__ void face_io(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d,
                                         T ql[8], T qr[8]) {
     const T half = T(0.5);
-    const T smallp = (T)(kSmallr * (kSmallc * kSmallc) / G.gamma);
+    const T smallp = (T)G.smallp;
     T sm[8], sp[8];
     face_state(cv, cl, d, +1, G.ndim, smallp, sm);
     face_state(cv, cr, d, -1, G.ndim, smallp, sp);
@@ -1224,7 +1248,7 @@ template <typename T, bool kHLLD = false>
 __device__ T edge_emf(const Geo &G, const CoreView<T> &cv, long long cLL, long long cRL, long long cLR, long long cRR,
                       int e, int i, double dtd) {
     const T half = T(0.5);
-    const T smallp = (T)(kSmallr * (kSmallc * kSmallc) / G.gamma);
+    const T smallp = (T)G.smallp;
     T sLL[8], sRL[8], sLR[8], sRR[8];
     int lt1, lt2, bn, bt1, bt2;
     if (e == 0) {
@@ -1312,10 +1336,9 @@ __global__ void __launch_bounds__(kThreads, (sizeof(T) == 8 ? DG_RIEMANN_MINB64 
                                                            int faces) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    int i, j, k;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore3};
     const int nx = G.nx, ny = G.ny, nz = G.nz;
@@ -1357,10 +1380,9 @@ k_faces3d(Geo G, const T *__restrict__ core, T *__restrict__ fx, T *__restrict__
           const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    int i, j, k;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore3};
     const long long c = G.cidx(i, j, k);
@@ -1375,10 +1397,9 @@ k_edges3d(Geo G, const T *__restrict__ core, T *__restrict__ ex, T *__restrict__
           const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    const int j = (int)(r % G.FY) + 1;
-    const int k = (int)(r / G.FY) + 1;
+    int i, j, k;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore3};
     const long long c = G.cidx(i, j, k);
@@ -1396,8 +1417,8 @@ __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restri
                                                         int faces) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= G.fsz) return;
-    const int i = (int)(t % G.FX) + 1;
-    const int j = (int)(t / G.FX) + 1;
+    const int j = (int)fdiv((unsigned)t, G.dFX) + 1;
+    const int i = (int)((unsigned)t - (unsigned)(j - 1) * G.dFX.d) + 1;
     const double dt = S->dt;
     const CoreView<T> cv{core, kCore2};
     const long long c = G.cidx(i, j, 1);
@@ -1667,10 +1688,10 @@ struct FargoLine {
 };
 __device__ __forceinline__ bool fargo_line(const Geo &G, long long t, FargoLine &L) {
     const int nseg = (G.FY + kFargoSeg - 1) / kFargoSeg;
-    L.i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    L.k = (int)(r % G.FZ) + 1;
-    const long long sg = r / G.FZ;
+    if (t >= 2147483647LL) return false;
+    int sg;
+    split3((unsigned)t, G.dFX, G.dFZ, L.i, L.k, sg);
+    L.i++; L.k++;
     if (sg >= nseg) return false;
     L.jb = (int)sg * kFargoSeg + 1;
     L.je = mn(L.jb + kFargoSeg - 1, G.FY);
@@ -1840,10 +1861,8 @@ __global__ void __launch_bounds__(kThreads, DG_FARGO_MINB64) k_fargo_update(Geo 
 // one thread per point of the face index space [1, nx+1] x [1, ny+1] x [1, nz+1]
 __device__ __forceinline__ bool face_point(const Geo &G, long long t, int &i, int &j, int &k) {
     if (t >= G.fsz) return false;
-    i = (int)(t % G.FX) + 1;
-    const long long r = t / G.FX;
-    j = (int)(r % G.FY) + 1;
-    k = (int)(r / G.FY) + 1;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
     return true;
 }
 
