@@ -32,9 +32,9 @@ __device__ __forceinline__ void put(const StoreHL &Un, const Geo &G, int v, long
 }
 
 // update + constrained_transport (scheme.f90:1764-1993) as FP32 increments on the compensated state
-// 12 resident blocks (40 registers): faster than the uncapped allocation at 256^3 despite a few spills
+// 10 resident blocks (48 registers): timed best at 256^3 against 12 (40, with spills), 8 and 6
 #ifndef DG_UPDATE_MINB32
-#define DG_UPDATE_MINB32 12
+#define DG_UPDATE_MINB32 10
 #endif
 __global__ void __launch_bounds__(kThreads, DG_UPDATE_MINB32) k_update3d_hl(Geo G, StoreHL U, StoreHL Un, const float *__restrict__ fx,
                                                           const float *__restrict__ fy, const float *__restrict__ fz,
