@@ -268,6 +268,7 @@ dg::Geo dg::make_geo(const dg_params &p) {
     // smallp = smallr smallc^2 / gamma, as the trace and the solvers form it (trace3d, solver.f90)
     G.smallp = dg::kSmallr * (dg::kSmallc * dg::kSmallc) / p.gamma;
     G.dvloc = 1.0 / (G.dx * G.dy * G.dz);
+    G.entho = 1.0 / (p.gamma - 1.0);
     G.rdx = 1.0 / G.dx; G.rdy = 1.0 / G.dy; G.rdz = 1.0 / G.dz;
     // ndim_act, init.f90:203-213
     const int nx = p.nx, ny = p.ny, nz = p.nz;

@@ -94,6 +94,7 @@ struct Geo {
     FastDiv dFX, dFY, dFZ, dCX, dCY, dEX, dEY, dPX, dPY;
     double smallp;            // pressure floor smallr smallc^2 / gamma of the trace and solvers
     double dvloc;             // 1 / (dx dy dz), as update forms it (scheme.f90:1778-1779)
+    double entho;             // 1 / (gamma - 1) of the HLLD solver (solver.f90:646)
     double rdx, rdy, rdz;     // 1 / dx, 1 / dy, 1 / dz (FP32 constrained transport)
 
     __host__ __device__ __forceinline__ long long idx(int i, int j, int k) const {

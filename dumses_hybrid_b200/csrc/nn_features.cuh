@@ -126,7 +126,7 @@ __device__ __forceinline__ bool gate_dissipation(const float y[kOut], const floa
 __device__ __forceinline__ void hlld_targets(const double *ql, const double *qr, double gamma, double ciso, int iso,
                                              double t[kOut]) {
     double f[8], pg;
-    hlld1d<double>(ql, qr, f, pg, gamma, ciso, iso);
+    hlld1d<double>(ql, qr, f, pg, gamma, ciso, iso, 1.0 / (gamma - 1.0));
     t[0] = f[0]; t[1] = f[1]; t[2] = f[2] + pg; t[3] = f[4]; t[4] = f[5]; t[5] = f[6]; t[6] = f[7]; t[7] = pg;
 }
 

@@ -233,17 +233,17 @@ __device__ __forceinline__ void hlld1d_f(const float *ql, const float *qr, float
     pg = ptoto;
 }
 
-// HLLD; returns p*_T in pg
+// HLLD; returns p*_T in pg.  entho = 1 / (gamma - 1), the same for every interface of a run
+// (formed once per context by the caller; the FP32 form takes its own reciprocal)
 template <typename T>
-__device__ void hlld1d(const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso, int iso) {
+__device__ void hlld1d(const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso, int iso, T entho) {
     if constexpr (sizeof(T) == 4) {
         hlld1d_f(ql, qr, f, pg, gamma, ciso, iso);
         return;
     }
-    const T one = T(1), half = T(0.5), zero = T(0);
+    const T half = T(0.5), zero = T(0);
     const T rl = ql[0], ul = ql[2], vl = ql[4], bl = ql[5], wl = ql[6], cl = ql[7];
     const T rr = qr[0], ur = qr[2], vr = qr[4], br = qr[5], wr = qr[6], cr = qr[7];
-    const T entho = one / (gamma - one);
     const T a = half * (ql[3] + qr[3]);
     const T sgnm = sgn1(a);
     T ploc, proc;

@@ -1146,13 +1146,13 @@ __device__ __forceinline__ void corner_state(const CoreView<T> &cv, long long c,
 // a kernel for the HLLD/HLLD configuration carries no code of the other solvers
 template <typename T, bool kHLLD = false>
 __device__ __forceinline__ void solve1d(int iriemann, const T *ql, const T *qr, T *f, T &pg, T gamma, T ciso,
-                                        int iso) {
+                                        int iso, T entho) {
     if constexpr (kHLLD) {
-        hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso);
+        hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso, entho);
         return;
     }
     switch (iriemann) {
-        case DG_RIEMANN_HLLD: hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso); break;
+        case DG_RIEMANN_HLLD: hlld1d<T>(ql, qr, f, pg, gamma, ciso, iso, entho); break;
         case DG_RIEMANN_HLL: hll1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
         case DG_RIEMANN_LLF: llf1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
         default: upwind1d<T>(ql, qr, f, gamma, ciso, iso); pg = T(0); break;
@@ -1239,7 +1239,7 @@ __device__ void face_flux(const Geo &G, const CoreView<T> &cv, long long cl, lon
     T ql[8], qr[8];
     face_io(G, cv, cl, cr, d, ql, qr);
     T f[8], pg = T(0);
-    solve1d<T, kHLLD>(G.iriemann, ql, qr, f, pg, (T)G.gamma, (T)G.ciso, G.iso);
+    solve1d<T, kHLLD>(G.iriemann, ql, qr, f, pg, (T)G.gamma, (T)G.ciso, G.iso, (T)G.entho);
     flux_store(G, ql, qr, f, pg, d, i, dtd, out, fo);
 }
 
