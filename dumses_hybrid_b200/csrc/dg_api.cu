@@ -270,6 +270,8 @@ dg::Geo dg::make_geo(const dg_params &p) {
     G.dvloc = 1.0 / (G.dx * G.dy * G.dz);
     G.entho = 1.0 / (p.gamma - 1.0);
     G.rdx = 1.0 / G.dx; G.rdy = 1.0 / G.dy; G.rdz = 1.0 / G.dz;
+    auto pow2 = [](double d) { int e; return d > 0.0 && std::frexp(d, &e) == 0.5 && e > -1000 && e < 1000; };
+    G.p2x = pow2(G.dx); G.p2y = pow2(G.dy); G.p2z = pow2(G.dz);
     // ndim_act, init.f90:203-213
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     if ((nx == 1 && ny == 1) || (nx == 1 && nz == 1) || (ny == 1 && nz == 1)) G.ndim_act = 1;

@@ -95,7 +95,13 @@ struct Geo {
     double smallp;            // pressure floor smallr smallc^2 / gamma of the trace and solvers
     double dvloc;             // 1 / (dx dy dz), as update forms it (scheme.f90:1778-1779)
     double entho;             // 1 / (gamma - 1) of the HLLD solver (solver.f90:646)
-    double rdx, rdy, rdz;     // 1 / dx, 1 / dy, 1 / dz (FP32 constrained transport)
+    double rdx, rdy, rdz;     // 1 / dx, 1 / dy, 1 / dz
+    // 1 where dx (dy, dz) is a power of two: then x / dx and x * (1 / dx) are the same real number
+    // correctly rounded, so the FP64 kernels multiply instead of dividing (bit for bit the same)
+    int p2x, p2y, p2z;
+    __host__ __device__ __forceinline__ double per_dx(double x) const { return p2x ? x * rdx : x / dx; }
+    __host__ __device__ __forceinline__ double per_dy(double x) const { return p2y ? x * rdy : x / dy; }
+    __host__ __device__ __forceinline__ double per_dz(double x) const { return p2z ? x * rdz : x / dz; }
 
     __host__ __device__ __forceinline__ long long idx(int i, int j, int k) const {
         return (long long)(i + 2) + sy * (long long)(j + gy - 1) + sz * (long long)(k + gz - 1);

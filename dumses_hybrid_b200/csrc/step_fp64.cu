@@ -101,27 +101,26 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
             return shear_avg(G, sr, ey, 1, ii == 1 ? 0 : 1, jj, kk);
         return ld(ey + G.fidx(ii, jj, kk));
     };
-    const double dx = G.dx, dy = G.dy, dz = G.dz;
     const bool ct = G.ndim_act > 1;
     if (j <= ny && k <= nz) {  // B_x at face i (i = 1..nx+1)
         double b = ld(U + sv * IA + c);
         if (ct) {
-            b = b + (ld(ez + (t + G.FX)) - ld(ez + t)) / dy;
-            b = b - (EYc(i, j, k + 1) - EYc(i, j, k)) / dz;
+            b = b + G.per_dy(ld(ez + (t + G.FX)) - ld(ez + t));
+            b = b - G.per_dz(EYc(i, j, k + 1) - EYc(i, j, k));
         }
         Un[sv * IA + c] = b;
     }
     if (i <= nx && k <= nz) {  // B_y at face j
         double b = ld(U + sv * IB + c);
         if (ct) {
-            b = b - (ld(ez + (t + 1)) - ld(ez + t)) / dx;
-            b = b + (ld(ex + (t + fxy)) - ld(ex + t)) / dz;
+            b = b - G.per_dx(ld(ez + (t + 1)) - ld(ez + t));
+            b = b + G.per_dz(ld(ex + (t + fxy)) - ld(ex + t));
         }
         Un[sv * IB + c] = b;
     }
     if (i <= nx && j <= ny) {  // B_z at face k
         double b = ld(U + sv * IC + c);
-        if (ct) b = b + (EYc(i + 1, j, k) - EYc(i, j, k)) / dx - (ld(ex + (t + G.FX)) - ld(ex + t)) / dy;
+        if (ct) b = b + G.per_dx(EYc(i + 1, j, k) - EYc(i, j, k)) - G.per_dy(ld(ex + (t + G.FX)) - ld(ex + t));
         Un[sv * IC + c] = b;
     }
 }

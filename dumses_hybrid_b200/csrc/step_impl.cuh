@@ -312,9 +312,9 @@ __global__ void __launch_bounds__(kThreads) k_prim_dt(Geo G, Store U, double *__
             if (G.ndim == 3) {
                 double velz = comp_speed(G.gamma, q[IR], q[IP], q[IW], q[IC], q[IA], q[IB]);
                 if (G.nz == 1) velz = 0.0;
-                cdt = 1.0 / (velx / G.dx + vely / G.dy + velz / G.dz);
+                cdt = 1.0 / (G.per_dx(velx) + G.per_dy(vely) + G.per_dz(velz));
             } else {
-                cdt = 1.0 / (velx / G.dx + vely / G.dy);
+                cdt = 1.0 / (G.per_dx(velx) + G.per_dy(vely));
             }
             if (!(cdt > 0.0)) bad = 1;  // NaN or non-positive
             else best = mn(best, cdt);
