@@ -40,6 +40,7 @@ DG_OK = 0
 ERRORS = {-1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_NOMEM", -4: "DG_ERR_TIMEOUT", -5: "DG_ERR_STATE",
           -6: "DG_ERR_DT", -7: "DG_ERR_NODEVICE", -8: "DG_ERR_UNSUPPORTED"}
 RIEMANN = {"llf": 2, "hll": 3, "hlld": 4, "upwind": 5, "hlla": 8}
+HISTORY_VARIANTS = {"mri": 0, "default": 1}  # DG_HISTORY_MRI, DG_HISTORY_DEFAULT
 BC = {"periodic": 0, "zero_gradient": 1, "shearingbox": 2}
 IC = {"field_loop": 1, "orszag_tang": 2, "mri": 3, "mri_test": 4}
 PREC = {"fp64": 0, "fp32": 1}
@@ -104,6 +105,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_dissipation": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_double]),
         "dg_step": (ctypes.c_int, [vp, dp, dp]),
         "dg_history": (ctypes.c_int, [vp, dp]),
+        "dg_history_variant": (ctypes.c_int, [vp, ctypes.c_int, dp]),
         "dg_dump_header": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(DgDumpInfo)]),
         "dg_dump_write": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_double]),
         "dg_dump_read": (ctypes.c_int, [vp, ctypes.c_char_p, dp, dp]),
@@ -413,9 +415,15 @@ class Context:
         _check(self.lib.dg_run(self.h, nsteps, ctypes.byref(t), ctypes.byref(dt)))
         return t.value, dt.value
 
-    def history(self) -> np.ndarray:
+    def history(self, variant: str = "mri") -> np.ndarray:
+        """The 9 history sums of the current state: variant "mri" (src/problem/mri/history.f90,
+        dg_history) or "default" (src/subroutines/history.f90, the problems without their own
+        history routine)."""
         out = np.zeros(9)
-        _check(self.lib.dg_history(self.h, self._ptr(out)))
+        if variant == "mri":
+            _check(self.lib.dg_history(self.h, self._ptr(out)))
+        else:
+            _check(self.lib.dg_history_variant(self.h, HISTORY_VARIANTS[variant], self._ptr(out)))
         return out
 
     def sync(self) -> None:

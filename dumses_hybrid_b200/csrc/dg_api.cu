@@ -58,7 +58,7 @@ struct Launches {
     int (*godunov)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*fargo)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*boundary)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
-    int (*history)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
+    int (*history)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t, int);
     int (*history_columns)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*history_share)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
     int (*dissipation)(const dg::Geo &, const dg::Bufs &, int, cudaStream_t);
@@ -785,11 +785,12 @@ int dg_run(dg_ctx *c, int nsteps, double *time, double *dt) {
 
 int dg_step(dg_ctx *c, double *time, double *dt) { return dg_run(c, 1, time, dt); }
 
-int dg_history(dg_ctx *c, double out[9]) {
+int dg_history_variant(dg_ctx *c, int variant, double out[9]) {
     TimerScope ts_(c);
     if (!c || !out) return fail(DG_ERR_ARG, "null argument");
-    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the MRI history is defined for ndim = 3");
-    c->launches += c->L->history(c->G, c->B, c->cur, c->stream);
+    if (variant != DG_HISTORY_MRI && variant != DG_HISTORY_DEFAULT) return fail(DG_ERR_ARG, "unknown history variant");
+    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the history sums are defined for ndim = 3");
+    c->launches += c->L->history(c->G, c->B, c->cur, c->stream, variant);
     int rc = check_launch();
     if (rc) return rc;
     DG_CUDA(cudaMemcpyAsync(c->h_hist, c->B.hist, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -797,6 +798,8 @@ int dg_history(dg_ctx *c, double out[9]) {
     std::memcpy(out, c->h_hist, 9 * sizeof(double));
     return DG_OK;
 }
+
+int dg_history(dg_ctx *c, double out[9]) { return dg_history_variant(c, DG_HISTORY_MRI, out); }
 
 // ---- z-slab halos: 3 planes of every stored state plane (FP64: nv double planes;
 // FP32: 2 nv float planes, hi then lo), one strided copy per side

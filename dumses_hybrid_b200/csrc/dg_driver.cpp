@@ -195,8 +195,8 @@ std::string fortran_1pe(double x, int w) {
     return s;
 }
 
-// MRI history file (src/problem/mri/history.f90:146-170): a header when the run starts
-// at time 0, then one line per call
+// history file (src/problem/mri/history.f90:146-170; src/subroutines/history.f90:146-167 writes the
+// same header and format): a header when the run starts at time 0, then one line per call
 void write_history(const std::string &path, double time, double dt, const double s[9]) {
     const bool fresh = time == 0.0;
     FILE *f = std::fopen(path.c_str(), fresh ? "w" : "a");
@@ -297,12 +297,15 @@ int main(int argc, char **argv) {
         check(dg_upload(ctx, uin.data()), "dg_upload");
         check(dg_boundary(ctx, 0.0, 0.0), "dg_boundary");
     }
-    const bool history_on = r.p.ndim == 3;  // the MRI history sums (history.f90) are 3D
+    // the history sums are 3D (history.f90 writes nothing in 2D); the MRI problem has its own
+    // routine (src/problem/mri/history.f90), the others use src/subroutines/history.f90
+    const bool history_on = r.p.ndim == 3;
+    const int hist_variant = ic == "mri" ? DG_HISTORY_MRI : DG_HISTORY_DEFAULT;
     const std::string hist_file = out + "/history.txt";
     auto history = [&]() {
         if (!history_on) return;
         double s[9];
-        check(dg_history(ctx, s), "dg_history");
+        check(dg_history_variant(ctx, hist_variant, s), "dg_history_variant");
         write_history(hist_file, time, dt, s);
     };
     if (r.restart == 0) {  // dumses.f90:62-67

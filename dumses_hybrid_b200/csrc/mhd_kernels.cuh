@@ -56,7 +56,7 @@ extern thread_local KernelTimer *g_timer;  // set by the context that enqueues (
     int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t st);   /* U[cur] -> U[cur^1] */ \
     int launch_fargo(const Geo &G, const Bufs &B, int cur, cudaStream_t st);     /* U[cur] -> U[cur^1] */ \
     int launch_boundary(const Geo &G, const Bufs &B, int cur, cudaStream_t st);  /* in place on U[cur] */ \
-    int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st);                       \
+    int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t st, int variant);          \
     /* z slabs: per-column sums of v_x, v_y into B.part (2 nx doubles); then this slab's share of */ \
     /* the history with the box's column means read from B.part, into B.hist */                      \
     int launch_history_columns(const Geo &G, const Bufs &B, int cur, cudaStream_t st);               \
@@ -73,7 +73,8 @@ namespace f64 {
 DG_DECLARE_LAUNCHES
 // history of any FP64 state array U with explicit scratch (>= history_scratch_doubles(G)
 // doubles) and a 9-double output, all device pointers
-int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t st);
+int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t st,
+                        int variant = DG_HISTORY_MRI);
 long long history_scratch_doubles(const Geo &G);
 }  // namespace f64
 

@@ -978,10 +978,11 @@ int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     return n + launch_boundary(G, B, cur, s);
 }
 
-int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
+int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s, int variant) {
     const int nb = 296;
-    TIMED(KS_HISTORY, s, (k_hist_yzmean<StoreHL><<<G.nx, 256, 0, s>>>(G, st(B, cur), B.part)));
-    TIMED(KS_HISTORY, s, (k_hist_sums<StoreHL><<<nb, 256, 0, s>>>(G, st(B, cur), B.part, B.part + 2 * G.nx)));
+    const int iv2 = variant == DG_HISTORY_DEFAULT ? IW : IV, ib2 = variant == DG_HISTORY_DEFAULT ? IC : IB;
+    TIMED(KS_HISTORY, s, (k_hist_yzmean<StoreHL><<<G.nx, 256, 0, s>>>(G, st(B, cur), B.part, 0, iv2)));
+    TIMED(KS_HISTORY, s, (k_hist_sums<StoreHL><<<nb, 256, 0, s>>>(G, st(B, cur), B.part, B.part + 2 * G.nx, iv2, ib2)));
     TIMED(KS_HISTORY, s, (k_hist_final<<<1, 32, 0, s>>>(G, B.part + 2 * G.nx, nb, B.hist)));
     return 3;
 }

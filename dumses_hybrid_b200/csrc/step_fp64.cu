@@ -372,11 +372,12 @@ constexpr int kHistBlocks = 296;
 
 long long history_scratch_doubles(const Geo &G) { return 2LL * G.nx + 8LL * kHistBlocks; }
 
-int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t s) {
+int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t s, int variant) {
     // every scratch entry read below is written earlier in the same launch sequence
     const StoreD S{(double *)U};
-    TIMED(KS_HISTORY, s, (k_hist_yzmean<StoreD><<<G.nx, 256, 0, s>>>(G, S, scratch)));
-    TIMED(KS_HISTORY, s, (k_hist_sums<StoreD><<<kHistBlocks, 256, 0, s>>>(G, S, scratch, scratch + 2 * G.nx)));
+    const int iv2 = variant == DG_HISTORY_DEFAULT ? IW : IV, ib2 = variant == DG_HISTORY_DEFAULT ? IC : IB;
+    TIMED(KS_HISTORY, s, (k_hist_yzmean<StoreD><<<G.nx, 256, 0, s>>>(G, S, scratch, 0, iv2)));
+    TIMED(KS_HISTORY, s, (k_hist_sums<StoreD><<<kHistBlocks, 256, 0, s>>>(G, S, scratch, scratch + 2 * G.nx, iv2, ib2)));
     TIMED(KS_HISTORY, s, (k_hist_final<<<1, 32, 0, s>>>(G, scratch + 2 * G.nx, kHistBlocks, out)));
     return 3;
 }
@@ -406,8 +407,8 @@ int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     return n + launch_boundary(G, B, cur, s);
 }
 
-int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
-    return launch_history_ptrs(G, (const double *)B.U[cur], B.part, B.hist, s);
+int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s, int variant) {
+    return launch_history_ptrs(G, (const double *)B.U[cur], B.part, B.hist, s, variant);
 }
 
 int launch_history_columns(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {

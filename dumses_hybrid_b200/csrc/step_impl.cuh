@@ -2059,12 +2059,15 @@ __global__ void __launch_bounds__(kThreads) k_visc_update(Geo G, Store U, const 
 }
 
 // ---------------------------------------------------------------------------
-// MRI history sums (src/problem/mri/history.f90:60-125), FP64
+// History sums, FP64: the MRI problem's (src/problem/mri/history.f90:60-125) and the default
+// routine's of the other problems (src/subroutines/history.f90:57-125); they differ in the
+// second velocity of the Reynolds stress (iv2: v_y, v_z) and the second face component of the
+// Maxwell stress (ib2: B_y, B_z)
 // ---------------------------------------------------------------------------
-// pass 1: per-x-column yz sums of vx and vy (compute_yz_mean)
+// pass 1: per-x-column yz sums of vx and the second velocity (compute_yz_mean)
 template <class Store>
 // raw = 1: the column sums themselves (a z slab's share, summed over the slabs by the caller)
-__global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m, int raw = 0) {
+__global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m, int raw = 0, int iv2 = IV) {
     const int i = blockIdx.x + 1;
     double a = 0.0, b = 0.0;
     const long long n = (long long)G.ny * G.nz;
@@ -2073,7 +2076,7 @@ __global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m, int raw = 
         const long long c = G.idx(i, j, k);
         const double d = U.get(G, IR, c);
         a += U.get(G, IU, c) / d;
-        b += U.get(G, IV, c) / d;
+        b += U.get(G, iv2, c) / d;
     }
     __shared__ double sa[256], sb[256];
     sa[threadIdx.x] = a; sb[threadIdx.x] = b;
@@ -2090,7 +2093,8 @@ __global__ void k_hist_yzmean(Geo G, Store U, double *__restrict__ m, int raw = 
 
 // pass 2: per-block partial sums of the 9 quantities
 template <class Store>
-__global__ void k_hist_sums(Geo G, Store U, const double *__restrict__ m, double *__restrict__ part) {
+__global__ void k_hist_sums(Geo G, Store U, const double *__restrict__ m, double *__restrict__ part, int iv2 = IV,
+                            int ib2 = IB) {
     const long long n = (long long)G.nx * G.ny * G.nz;
     const double forth = 0.25;
     const double dtau = G.dx * G.dy * G.dz / (G.xmax - G.xmin) / (G.ymax - G.ymin) / (G.zmax - G.zmin);
@@ -2107,9 +2111,9 @@ __global__ void k_hist_sums(Geo G, Store U, const double *__restrict__ m, double
         const double d = U.get(G, IR, c);
         acc[0] += d;
         acc[1] += forth * (bxc * bxc) + forth * (byc * byc) + forth * (bzc * bzc);
-        acc[2] += -(forth * bxc * byc);
+        acc[2] += -(forth * bxc * (ib2 == IB ? byc : bzc));
         acc[3] += bxl; acc[4] += byl; acc[5] += bzl;
-        acc[6] += d * dtau * (U.get(G, IU, c) / d - m[2 * (i - 1)]) * (U.get(G, IV, c) / d - m[2 * (i - 1) + 1]);
+        acc[6] += d * dtau * (U.get(G, IU, c) / d - m[2 * (i - 1)]) * (U.get(G, iv2, c) / d - m[2 * (i - 1) + 1]);
         acc[7] += (bxr - bxl) / G.dx + (byr - byl) / G.dy + (bzr - bzl) / G.dz;
     }
     __shared__ double sh[8][256];

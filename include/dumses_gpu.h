@@ -16,6 +16,7 @@
  *   dg_boundary      <- boundary                        src/subroutines/boundary.f90:18-92
  *   dg_dissipation   <- dissipation                     src/subroutines/physics.f90:272-664
  *   dg_history       <- history (MRI problem variant)   src/problem/mri/history.f90:19-174
+ *   dg_history_variant <- history of the other problems  src/subroutines/history.f90:19-171 (NDIM 3)
  *   dg_step          <- one pass of the loop body       src/dumses.f90:82-120
  *   dg_finalize      <- deallocate_workspace            src/subroutines/finalize.f90
  *
@@ -173,6 +174,15 @@ int  dg_dump_read_host(const char *path, const dg_params *p, double *time, doubl
  * out[0] mass, out[1] maxwell, out[2] reynolds, out[3] maxwell+reynolds,
  * out[4] magp, out[5..7] <B>, out[8] divB.  FP64 sums in a fixed tree order. */
 int  dg_history(dg_ctx *ctx, double out[9]);
+
+/* The history sums of either history routine of the reference (the history.f90 of a
+ * problem directory replaces the default one at link time): DG_HISTORY_MRI is dg_history;
+ * DG_HISTORY_DEFAULT is src/subroutines/history.f90:57-125 (NDIM 3), used by the problems
+ * without their own history, which takes the Maxwell stress of B_x and B_z and the Reynolds
+ * stress of v_x and v_z about their y-z means.  Same output order and file format. */
+#define DG_HISTORY_MRI     0
+#define DG_HISTORY_DEFAULT 1
+int  dg_history_variant(dg_ctx *ctx, int variant, double out[9]);
 
 /* MRI history sums of a state that the caller keeps on the device, with no
  * device allocation.  No counterpart in the reference: it is for callers that

@@ -1819,12 +1819,16 @@ void or_fargo_update(or_state *s, double dt)
 /* ------------------------------------------------------------------------- */
 /* MRI history, src/problem/mri/history.f90:60-125                            */
 /* ------------------------------------------------------------------------- */
-void or_history_mri(or_state *s, double out[9])
+/* The history sums of the MRI problem (src/problem/mri/history.f90:19-174) and of the default
+ * routine of the other problems (src/subroutines/history.f90:57-125, NDIM = 3): the same loop,
+ * with the Maxwell stress of B_x and face component ib2 and the Reynolds stress of v_x and
+ * velocity iv2 about their y-z means (MRI: B_y and v_y; default: B_z and v_z). */
+static void history_sums(or_state *s, int iv2, int ib2, double out[9])
 {
     const dg_params *p = &s->p;
     const int nx = s->nx, ny = s->ny, nz = s->nz;
     double dtau = s->dx * s->dy * s->dz / (p->xmax - p->xmin) / (p->ymax - p->ymin) / (p->zmax - p->zmin);
-    /* compute_yz_mean of vx and vy (history.f90:247-288, single rank) */
+    /* compute_yz_mean of v_x and the second velocity (history.f90:247-288, single rank) */
     int ni = s->iu2 - s->iu1 + 1;
     double *mvx = (double *)calloc((size_t)ni, sizeof(double)), *mvy = (double *)calloc((size_t)ni, sizeof(double));
     for (int i = s->iu1; i <= s->iu2; i++) {
@@ -1832,7 +1836,7 @@ void or_history_mri(or_state *s, double out[9])
         for (int k = 1; k <= nz; k++)
             for (int j = 1; j <= ny; j++) {
                 a = a + A4(s->uin, i, j, k, iu) / A4(s->uin, i, j, k, ir);
-                b = b + A4(s->uin, i, j, k, iv) / A4(s->uin, i, j, k, ir);
+                b = b + A4(s->uin, i, j, k, iv2) / A4(s->uin, i, j, k, ir);
             }
         mvx[i - s->iu1] = a / ny / nz;
         mvy[i - s->iu1] = b / ny / nz;
@@ -1847,13 +1851,13 @@ void or_history_mri(or_state *s, double out[9])
                 double bzc = A4(s->uin, i, j, k, iC) + A4(s->uin, i, j, k + 1, iC);
                 mass = mass + A4(s->uin, i, j, k, ir);
                 magp = magp + forth * (bxc * bxc) + forth * (byc * byc) + forth * (bzc * bzc);
-                maxwell = maxwell - forth * bxc * byc;
+                maxwell = maxwell - forth * bxc * (ib2 == iB ? byc : bzc);
                 mB[0] = mB[0] + A4(s->uin, i, j, k, iA);
                 mB[1] = mB[1] + A4(s->uin, i, j, k, iB);
                 mB[2] = mB[2] + A4(s->uin, i, j, k, iC);
                 reynolds = reynolds + A4(s->uin, i, j, k, ir) * dtau
                          * (A4(s->uin, i, j, k, iu) / A4(s->uin, i, j, k, ir) - mvx[i - s->iu1])
-                         * (A4(s->uin, i, j, k, iv) / A4(s->uin, i, j, k, ir) - mvy[i - s->iu1]);
+                         * (A4(s->uin, i, j, k, iv2) / A4(s->uin, i, j, k, ir) - mvy[i - s->iu1]);
                 divB = divB + (A4(s->uin, i + 1, j, k, iA) - A4(s->uin, i, j, k, iA)) / s->dx
                             + (A4(s->uin, i, j + 1, k, iB) - A4(s->uin, i, j, k, iB)) / s->dy
                             + (A4(s->uin, i, j, k + 1, iC) - A4(s->uin, i, j, k, iC)) / s->dz;
@@ -1865,6 +1869,9 @@ void or_history_mri(or_state *s, double out[9])
     out[0] = mass; out[1] = maxwell; out[2] = reynolds; out[3] = maxwell + reynolds; out[4] = magp;
     out[5] = mB[0] * dtau; out[6] = mB[1] * dtau; out[7] = mB[2] * dtau; out[8] = divB;
 }
+
+void or_history_mri(or_state *s, double out[9]) { history_sums(s, iv, iB, out); }
+void or_history_default(or_state *s, double out[9]) { history_sums(s, iw, iC, out); }
 
 /* ------------------------------------------------------------------------- */
 /* dissipation, src/subroutines/physics.f90:272-664                           */

@@ -40,6 +40,7 @@ def lib() -> ctypes.CDLL:
         L.or_fargo_update.restype, L.or_fargo_update.argtypes = None, [vp, ctypes.c_double]
         L.or_boundary.restype, L.or_boundary.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
         L.or_history_mri.restype, L.or_history_mri.argtypes = None, [vp, dp]
+        L.or_history_default.restype, L.or_history_default.argtypes = None, [vp, dp]
         L.or_step.restype, L.or_step.argtypes = ctypes.c_double, [vp, dp]
         L.or_dissipation.restype, L.or_dissipation.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
         L.or_run_history.restype = ctypes.c_int
@@ -128,9 +129,12 @@ class Oracle:
         dt = self.L.or_step(self.h, ctypes.byref(t))
         return t.value, dt
 
-    def history(self) -> np.ndarray:
+    def history(self, variant: str = "mri") -> np.ndarray:
+        """The 9 history sums: variant "mri" (src/problem/mri/history.f90) or "default"
+        (src/subroutines/history.f90)."""
         out = np.zeros(9)
-        self.L.or_history_mri(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        f = self.L.or_history_mri if variant == "mri" else self.L.or_history_default
+        f(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         return out
 
     def run_history(self, tlim: float, dthist: float, max_rows: int) -> np.ndarray:

@@ -202,6 +202,36 @@ def test_history_sums_match_oracle():
     assert abs(h_g[8]) < 1e-9 and abs(h_o[8]) < 1e-9
 
 
+def test_default_history_sums_match_oracle():
+    """The default history routine of the problems without their own (src/subroutines/history.f90,
+    Maxwell stress of B_x B_z, Reynolds stress of v_x v_z), on a 3D Orszag-Tang state after 3 steps,
+    FP64 and FP32, against the oracle's restatement; the MRI variant on the same state differs."""
+    p = Params(ndim=3, nx=16, ny=24, nz=12, xmin=0, xmax=1, ymin=0, ymax=1, zmin=0, zmax=1, gamma=5 / 3,
+               courant=0.8)
+    u0 = condinit(p, "orszag_tang")
+    o = Oracle(p)
+    o.set_state(u0)
+    o.boundary(0.0, 0.0)
+    t_o = 0.0
+    for _ in range(3):
+        t_o, _ = o.step(t_o)
+    h_o = o.history("default")
+    scale = np.maximum(np.abs(h_o), 1e-300)
+    # FP64: the same sums in another (tree) order, 1e-12; FP32: the state is within ~1e-5 of FP64
+    for prec, tol in (("fp64", 1e-12), ("fp32", 1e-3)):
+        with Context(Params(**{**p.__dict__, "precision": prec})) as g:
+            g.upload(u0)
+            g.boundary(0.0, 0.0)
+            g.run(3, 0.0)
+            h_g = g.history("default")
+            h_m = g.history("mri")
+        for q in (0, 1, 2, 3, 4, 5, 6, 7):
+            assert abs(h_g[q] - h_o[q]) <= tol * scale[q] + (1e-15 if prec == "fp64" else 1e-6 * h_o[4]), \
+                (prec, q, h_g[q], h_o[q])
+        assert abs(h_g[8]) < 1e-9 and abs(h_o[8]) < 1e-9
+        assert not np.isclose(h_m[1], h_g[1])
+
+
 def test_field_loop_full_run_to_t2():
     """The 2D field-loop configuration as specified (128x64 on [-1,1]x[-0.5,0.5], HLLD + CT, MC, CFL 0.7,
     v = (2, 1), A_z = 1e-3 (0.3 - r)) run to t = 2: every step's dt and the final state bit-identical."""
