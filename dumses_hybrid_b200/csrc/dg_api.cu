@@ -77,7 +77,9 @@ const Launches kLaunchF32 = DG_LAUNCH_TABLE(dg::f32);
 
 namespace dg {
 thread_local KernelTimer *g_timer = nullptr;
-int nstate_vars(const Geo &G) { return G.ndim == 2 ? 9 : 8; }
+// stored state planes: the 8 variables, plus the right-face B copies the reference never
+// refreshes (z in 2D; y and z in 1D), frozen at their initial values
+int nstate_vars(const Geo &G) { return G.ndim == 3 ? 8 : G.ndim == 2 ? 9 : 10; }
 }  // namespace dg
 
 struct dg_ctx {
@@ -170,8 +172,15 @@ int check_launch() {
 
 int validate(const dg_params *p) {
     if (!p) return fail(DG_ERR_ARG, "null parameters");
-    if (p->ndim != 2 && p->ndim != 3) return fail(DG_ERR_UNSUPPORTED, "ndim must be 2 or 3");
-    if (p->nx < 3 || p->ny < 3) return fail(DG_ERR_ARG, "nx and ny must be >= 3 (three ghost layers are copied)");
+    if (p->ndim < 1 || p->ndim > 3) return fail(DG_ERR_UNSUPPORTED, "ndim must be 1, 2 or 3");
+    if (p->ndim == 1) {
+        if (p->ny != 1 || p->nz != 1) return fail(DG_ERR_ARG, "ny and nz must be 1 when ndim = 1");
+        if (p->precision != DG_PREC_FP64) return fail(DG_ERR_UNSUPPORTED, "ndim = 1 runs the FP64 path only");
+        if (p->slope_type > 2) return fail(DG_ERR_UNSUPPORTED, "ndim = 1 takes slope_type 0, 1 or 2 (scheme.f90:313-315)");
+        if (p->nu > 0.0 || p->eta > 0.0) return fail(DG_ERR_UNSUPPORTED, "dissipation with ndim = 1 is not built");
+    }
+    if (p->nx < 3 || (p->ndim > 1 && p->ny < 3))
+        return fail(DG_ERR_ARG, "nx (and ny with ndim > 1) must be >= 3 (three ghost layers are copied)");
     if (p->ndim == 3 && p->nz < 3) return fail(DG_ERR_ARG, "nz must be >= 3 when ndim = 3");
     if (p->ndim == 2 && p->nz != 1) return fail(DG_ERR_ARG, "nz must be 1 when ndim = 2");
     if (!(p->xmax > p->xmin) || !(p->ymax > p->ymin) || !(p->zmax > p->zmin)) return fail(DG_ERR_ARG, "empty domain");
@@ -228,14 +237,14 @@ dg::Geo dg::make_geo(const dg_params &p) {
     G.sy = G.NX;
     G.sz = (long long)G.NX * G.NY;
     G.sv = G.sz * G.NZ;
-    G.CX = p.nx + 2; G.CY = p.ny + 2;
+    G.CX = p.nx + 2; G.CY = p.ndim > 1 ? p.ny + 2 : 1;
     G.CZ = p.ndim == 3 ? p.nz + 2 : 1;
     G.kc0 = p.ndim == 3 ? 0 : 1;
     G.csz = (long long)G.CX * G.CY * G.CZ;
-    G.FX = p.nx + 1; G.FY = p.ny + 1;
+    G.FX = p.nx + 1; G.FY = p.ndim > 1 ? p.ny + 1 : 1;
     G.FZ = p.ndim == 3 ? p.nz + 1 : 1;
     G.fsz = (long long)G.FX * G.FY * G.FZ;
-    G.EX = p.nx + 3; G.EY = p.ny + 3;
+    G.EX = p.nx + 3; G.EY = p.ndim > 1 ? p.ny + 3 : 1;
     G.EZ = p.ndim == 3 ? p.nz + 3 : 1;
     G.ke0 = p.ndim == 3 ? 0 : 1;
     G.esz = (long long)G.EX * G.EY * G.EZ;
@@ -367,13 +376,14 @@ int dg_init(const dg_params *p, dg_ctx **out) {
     const int ncore = p->ndim == 3 ? dg::kCore3 : dg::kCore2;
     if ((rc = alloc_w(c, &c->B.core, (size_t)dg::core_elems(G.csz, ncore)))) return bail(rc);
     for (int d = 0; d < p->ndim; d++)
-        if ((rc = alloc_w(c, &c->B.flx[d], (size_t)G.fsz * dg::kFluxComp))) return bail(rc);
+        if ((rc = alloc_w(c, &c->B.flx[d], (size_t)G.fsz * (p->ndim == 1 ? dg::kFluxRec1 : dg::kFluxComp))))
+            return bail(rc);
     for (int d = 0; d < 3; d++) {
-        if (p->ndim == 2 && d < 2) continue;
+        if (p->ndim == 1 || (p->ndim == 2 && d < 2)) continue;
         if ((rc = alloc_w(c, &c->B.emf[d], (size_t)G.fsz))) return bail(rc);
     }
     for (int d = 0; d < 3; d++) {
-        if (p->ndim == 2 && d < 2) continue;
+        if (p->ndim == 1 || (p->ndim == 2 && d < 2)) continue;
         if ((rc = alloc_w(c, &c->B.E[d], (size_t)G.esz))) return bail(rc);
     }
     if (p->fargo)
@@ -434,20 +444,20 @@ int dg_upload(dg_ctx *c, const double *uin) {
     if (c->p.precision == DG_PREC_FP64) {
         // uin(:,:,:,1:8) is contiguous in the reference layout
         DG_CUDA(cudaMemcpyAsync(c->B.U[c->cur], uin, nt * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        if (c->nv == 9) {
-            // ndim = 2: the right z-face B (uin var 11) is never refreshed by the reference and
-            // stays at its initial value; both state buffers carry it
-            for (int b = 0; b < 2; b++)
-                DG_CUDA(cudaMemcpyAsync((double *)c->B.U[b] + nt * 8, uin + nt * 10, nt * sizeof(double),
-                                        cudaMemcpyHostToDevice, c->stream));
-        }
+        // the right-face B that the reference never refreshes (uin var 11 in 2D, vars 10-11 in
+        // 1D) stays at its initial value; both state buffers carry it (planes 8..nv-1)
+        const size_t nf = (size_t)c->nv - 8;
+        for (int b = 0; b < 2 && nf > 0; b++)
+            DG_CUDA(cudaMemcpyAsync((double *)c->B.U[b] + nt * 8, uin + nt * (11 - nf), nf * nt * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
     } else {
+        const size_t nf = (size_t)c->nv - 8;
         DG_CUDA(cudaMemcpyAsync(c->B.stage, uin, nt * 8 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        if (c->nv == 9)
-            DG_CUDA(cudaMemcpyAsync(c->B.stage + nt * 8, uin + nt * 10, nt * sizeof(double), cudaMemcpyHostToDevice,
-                                    c->stream));
+        if (nf > 0)
+            DG_CUDA(cudaMemcpyAsync(c->B.stage + nt * 8, uin + nt * (11 - nf), nf * nt * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
         c->launches += c->L->from_f64(c->G, c->B, c->cur, c->B.stage, c->nv, c->stream);
-        if (c->nv == 9) c->launches += c->L->from_f64(c->G, c->B, c->cur ^ 1, c->B.stage, c->nv, c->stream);
+        if (nf > 0) c->launches += c->L->from_f64(c->G, c->B, c->cur ^ 1, c->B.stage, c->nv, c->stream);
         int rc = check_launch();
         if (rc) return rc;
     }
@@ -664,8 +674,9 @@ int dg_dump_read(dg_ctx *c, const char *path, double *time, double *dt) {
     if (int rc = bounded_sync(c->stream)) return rc;  // no step may still read the state
     const bool f64 = c->p.precision == DG_PREC_FP64;
     dg::dump::RecordReader r(fc.f);
-    // plane v is read from the file while plane v-1 is copied; vars 9-10 (right faces) are
-    // derived from the left faces and skipped; var 11 is stored only in 2D (frozen, both buffers)
+    // plane v is read from the file while plane v-1 is copied; the right faces are derived from
+    // the left faces and skipped, except the frozen copies: var 11 in 2D, vars 10-11 in 1D
+    // (stored planes 8..nv-1, both buffers)
     for (int v = 0; v < 11; v++) {
         if (v >= 2)
             if (int rc = bounded_event(pb.ev[v & 1])) return rc;  // the copy of plane v-2 is done
@@ -674,12 +685,13 @@ int dg_dump_read(dg_ctx *c, const char *path, double *time, double *dt) {
         double *dst[2] = {nullptr, nullptr};
         if (v < 8) {
             dst[0] = f64 ? (double *)c->B.U[c->cur] + (size_t)v * nt : c->B.stage + (size_t)v * nt;
-        } else if (v == 10 && c->nv == 9) {
+        } else if (v >= 11 - (c->nv - 8)) {
+            const size_t pl = (size_t)(v - (11 - (c->nv - 8)) + 8);
             if (f64) {
-                dst[0] = (double *)c->B.U[0] + nt * 8;
-                dst[1] = (double *)c->B.U[1] + nt * 8;
+                dst[0] = (double *)c->B.U[0] + nt * pl;
+                dst[1] = (double *)c->B.U[1] + nt * pl;
             } else {
-                dst[0] = c->B.stage + nt * 8;
+                dst[0] = c->B.stage + nt * pl;
             }
         }
         for (double *d : dst)
@@ -689,7 +701,7 @@ int dg_dump_read(dg_ctx *c, const char *path, double *time, double *dt) {
     if (!r.close()) return fail(DG_ERR_ARG, std::string(path) + ": the uin record does not hold this grid");
     if (!f64) {
         c->launches += c->L->from_f64(c->G, c->B, c->cur, c->B.stage, c->nv, c->stream);
-        if (c->nv == 9) c->launches += c->L->from_f64(c->G, c->B, c->cur ^ 1, c->B.stage, c->nv, c->stream);
+        if (c->nv > 8) c->launches += c->L->from_f64(c->G, c->B, c->cur ^ 1, c->B.stage, c->nv, c->stream);
         if (int rc = check_launch()) return rc;
     }
     c->version++;
@@ -789,8 +801,14 @@ int dg_history_variant(dg_ctx *c, int variant, double out[9]) {
     TimerScope ts_(c);
     if (!c || !out) return fail(DG_ERR_ARG, "null argument");
     if (variant != DG_HISTORY_MRI && variant != DG_HISTORY_DEFAULT) return fail(DG_ERR_ARG, "unknown history variant");
-    if (c->p.ndim != 3) return fail(DG_ERR_UNSUPPORTED, "the history sums are defined for ndim = 3");
-    c->launches += c->L->history(c->G, c->B, c->cur, c->stream, variant);
+    if (c->p.ndim == 1 && variant == DG_HISTORY_DEFAULT) {
+        // the one-dimensional line (history.f90:37-59): rho, rho u_x and E at x = 1/2
+        c->launches += dg::f64::launch_history_1d(c->G, (const double *)c->B.U[c->cur], c->B.hist, c->stream);
+    } else if (c->p.ndim != 3) {
+        return fail(DG_ERR_UNSUPPORTED, "the history sums are defined for ndim = 3 (and the line of ndim = 1)");
+    } else {
+        c->launches += c->L->history(c->G, c->B, c->cur, c->stream, variant);
+    }
     int rc = check_launch();
     if (rc) return rc;
     DG_CUDA(cudaMemcpyAsync(c->h_hist, c->B.hist, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

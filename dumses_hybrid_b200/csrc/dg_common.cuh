@@ -146,9 +146,11 @@ __host__ __device__ __forceinline__ long long core_elems(long long csz, int nf) 
 
 // face flux records, face-major: rho, E, rho u, rho v, rho w (scaled by area*dt as
 // compflux does), p*_tot, then in 2D the B_z flux and a pad (6 values per face in 3D,
-// 8 in 2D)
+// 8 in 2D, 9 in 1D)
 constexpr int kFluxComp = 8;  // the larger record (allocation)
 constexpr int kFluxRec3 = 6, kFluxRec2 = 8;
-__host__ __device__ __forceinline__ int flux_rec(int ndim) { return ndim == 3 ? kFluxRec3 : kFluxRec2; }
+// ndim = 1: rho, E, rho u, rho v, rho w, p*_tot, B_x, B_y, B_z (every field has an x flux)
+constexpr int kFluxRec1 = 9;
+__host__ __device__ __forceinline__ int flux_rec(int ndim) { return ndim == 3 ? kFluxRec3 : ndim == 2 ? kFluxRec2 : kFluxRec1; }
 
 }  // namespace dg

@@ -76,6 +76,8 @@ DG_DECLARE_LAUNCHES
 int launch_history_ptrs(const Geo &G, const double *U, double *scratch, double *out, cudaStream_t st,
                         int variant = DG_HISTORY_MRI);
 long long history_scratch_doubles(const Geo &G);
+// the ndim = 1 history line: out[0..2] = rho, rho u_x, E of the first cell at x >= 1/2, out[3..8] = 0
+int launch_history_1d(const Geo &G, const double *U, double *out, cudaStream_t st);
 }  // namespace f64
 
 namespace f32 {

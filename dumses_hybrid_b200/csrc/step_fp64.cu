@@ -125,6 +125,56 @@ __global__ void __launch_bounds__(kThreads) k_update3d(
     }
 }
 
+// update of the FP64 state with ndim = 1 (scheme.f90:1764-1936): every field from its x fluxes,
+// no constrained transport (ndim_act = 1), in the reference's statement order
+__global__ void __launch_bounds__(kThreads) k_update1d(Geo G, const double *__restrict__ U, double *__restrict__ Un,
+                                                       const double *__restrict__ fx, const Scalars *S) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.nx) return;
+    const int i = (int)t + 1;
+    const double dt = S->dt;
+    const double one = 1.0, two = 2.0, half = 0.5;
+    const long long sv = G.sv, c = G.idx(i, 1, 1);
+    if (!chk(Un + c, 8) || !chk(Un + sv * IC + c, 8)) return;
+    const double Omega0 = G.omega0;
+    double lambda = 0.0, ratio = 0.0;
+    if (Omega0 > 0.0) {
+        lambda = Omega0 * dt; lambda = 2.5e-1 * lambda * lambda;
+        ratio = (one - lambda) / (one + lambda);
+    }
+    const double dvloc = G.dvloc;  // one / dv
+    double ur = ld(U + c), uu = ld(U + sv * IU + c), uv = ld(U + sv * IV + c), uw = ld(U + sv * IW + c);
+    double up = ld(U + sv * IP + c), ua = ld(U + sv * IA + c), ub = ld(U + sv * IB + c), uc = ld(U + sv * IC + c);
+    if (Omega0 > 0.0) {
+        const double dsx = two * Omega0 * dt * uv / (one + lambda);
+        const double dsy = -(half * Omega0 * dt * uu) / (one + lambda);
+        uu = uu * ratio + dsx;
+        uv = uv * ratio + dsy;
+    }
+    const double *L = fx + t * kFluxRec1, *R = fx + (t + 1) * kFluxRec1;  // faces i and i+1
+    const double ds = G.dy * G.dz;
+    const double pre = -(ld(R + 5) * ds - ld(L + 5) * ds) * dt;  // fgodunov_pre, solver.f90:246-262
+    ur = ur + (ld(L) - ld(R)) * dvloc;
+    uw = uw + (ld(L + 4) * one - ld(R + 4) * one) * dvloc / one;
+    up = up + (ld(L + 1) - ld(R + 1)) * dvloc;
+    ua = ua + (ld(L + 6) - ld(R + 6)) * dvloc;
+    ub = ub + (ld(L + 7) - ld(R + 7)) * dvloc;
+    uc = uc + (ld(L + 8) - ld(R + 8)) * dvloc;
+    if (Omega0 > 0.0) {
+        double dfn2 = (ld(L + 2) - ld(R + 2)) * dvloc;
+        dfn2 = dfn2 + pre * dvloc;
+        const double dfn3 = (ld(L + 3) - ld(R + 3)) * dvloc;
+        uu = uu + dfn2 / (one + lambda) + Omega0 * dt / (one + lambda) * dfn3;
+        uv = uv + dfn3 / (one + lambda) - 2.5e-1 * Omega0 * dt / (one + lambda) * dfn2;
+    } else {
+        uu = uu + (ld(L + 2) * one - ld(R + 2) * one) * dvloc / one;
+        uv = uv + (ld(L + 3) * one - ld(R + 3) * one) * dvloc / one;
+        uu = uu + pre * dvloc;
+    }
+    Un[c] = ur; Un[sv * IU + c] = uu; Un[sv * IV + c] = uv; Un[sv * IW + c] = uw; Un[sv * IP + c] = up;
+    Un[sv * IA + c] = ua; Un[sv * IB + c] = ub; Un[sv * IC + c] = uc;
+}
+
 __global__ void __launch_bounds__(kThreads) k_update2d(Geo G, const double *__restrict__ U, double *__restrict__ Un,
                                                        const double *__restrict__ fx, const double *__restrict__ fy,
                                                        const double *__restrict__ ez, const Scalars *S) {
@@ -327,6 +377,14 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
             TIMED(KS_RIEMANN, s, (k_riemann3d<double, false><<<nb, kThreads, 0, s>>>(G, core, fx, fy, fz, ex, ey, ez, B.S, 1)));
         }
         TIMED(KS_UPDATE, s, (k_update3d<<<nblocks(G.fsz, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, fy, fz, ex, ey, ez, B.S)));
+    } else if (G.ndim == 1) {
+        // trace1d, the x solves, update: no edge fields and no EMFs
+        const bool hlld = G.iriemann == DG_RIEMANN_HLLD;
+        TIMED(KS_TRACE, s, (k_trace1d<double><<<nblocks(G.CX, kThreads), kThreads, 0, s>>>(G, Q, core, B.S)));
+        if (hlld) TIMED(KS_RIEMANN, s, (k_riemann1d<double, true><<<nblocks(G.FX, kThreads), kThreads, 0, s>>>(G, core, fx, B.S)));
+        else TIMED(KS_RIEMANN, s, (k_riemann1d<double, false><<<nblocks(G.FX, kThreads), kThreads, 0, s>>>(G, core, fx, B.S)));
+        TIMED(KS_UPDATE, s, (k_update1d<<<nblocks(G.nx, kThreads), kThreads, 0, s>>>(G, U.p, Un, fx, B.S)));
+        n--;
     } else {
         TIMED(KS_EFIELD, s, (k_efield2d<double><<<nblocks(G.esz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2)));
         TIMED(KS_TRACE, s, (k_trace2d<double><<<nblocks(G.csz, kThreads), kThreads, 0, s>>>(G, Q, U.p, E2, core, B.S)));
@@ -405,6 +463,23 @@ int launch_dissipation(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
         n += 3;
     }
     return n + launch_boundary(G, B, cur, s);
+}
+
+__global__ void k_history_1d(Geo G, const double *__restrict__ U, double *__restrict__ out) {
+    // do ipos = 1, nx: exit at the first x(ipos) >= 1/2 (the loop's exit value nx+1 if none)
+    int ipos = 1;
+    for (ipos = 1; ipos <= G.nx; ipos++)
+        if (G.xc(ipos) >= 0.5) break;
+    const long long c = G.idx(ipos, 1, 1);
+    out[0] = ld(U + c);
+    out[1] = ld(U + G.sv * IU + c);
+    out[2] = ld(U + G.sv * IP + c);
+    for (int q = 3; q < 9; q++) out[q] = 0.0;
+}
+
+int launch_history_1d(const Geo &G, const double *U, double *out, cudaStream_t s) {
+    TIMED(KS_HISTORY, s, (k_history_1d<<<1, 1, 0, s>>>(G, U, out)));
+    return 1;
 }
 
 int launch_history(const Geo &G, const Bufs &B, int cur, cudaStream_t s, int variant) {

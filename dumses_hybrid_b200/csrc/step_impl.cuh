@@ -246,9 +246,12 @@ __device__ __forceinline__ void prim_cell(const Geo &G, const Store &U, long lon
     q[IV] = U.getr(G, IV, c) / d;
     q[IW] = U.getr(G, IW, c) / d;
     q[IA] = half * (U.getr(G, IA, c) + U.getr(G, IA, c + 1));
-    q[IB] = half * (U.getr(G, IB, c) + U.getr(G, IB, c + G.sy));
+    // the right faces: the neighbour's left face, or the stored frozen copy (B_y, B_z in 1D,
+    // B_z in 2D: the reference never refreshes those)
+    if (G.ndim > 1) q[IB] = half * (U.getr(G, IB, c) + U.getr(G, IB, c + G.sy));
+    else q[IB] = half * (U.getr(G, IB, c) + U.getr(G, 8, c));
     if (G.ndim == 3) q[IC] = half * (U.getr(G, IC, c) + U.getr(G, IC, c + G.sz));
-    else q[IC] = half * (U.getr(G, IC, c) + U.getr(G, 8, c));
+    else q[IC] = half * (U.getr(G, IC, c) + U.getr(G, G.ndim == 1 ? 9 : 8, c));
     if (G.iso) {
         q[IP] = d * (G.ciso * G.ciso);
     } else {
@@ -309,7 +312,9 @@ __global__ void __launch_bounds__(kThreads) k_prim_dt(Geo G, Store U, double *__
             if ((G.omega0 > 0.0) && !G.fargo) vely = vely + 1.5 * G.omega0 * (G.xmax - G.xmin) * 0.5;
             if (G.ny == 1) vely = 0.0;
             double cdt;
-            if (G.ndim == 3) {
+            if (G.ndim == 1) {
+                cdt = G.dx / velx;  // physics.f90:101-103
+            } else if (G.ndim == 3) {
                 double velz = comp_speed(G.gamma, q[IR], q[IP], q[IW], q[IC], q[IA], q[IB]);
                 if (G.nz == 1) velz = 0.0;
                 cdt = 1.0 / (G.per_dx(velx) + G.per_dy(vely) + G.per_dz(velz));
@@ -1411,6 +1416,94 @@ k_edges3d(Geo G, const T *__restrict__ core, T *__restrict__ ex, T *__restrict__
         ex[t] = edge_emf<T, kHLLD>(G, cv, G.cidx(i, j - 1, k - 1), G.cidx(i, j, k - 1), G.cidx(i, j - 1, k), c, 0, i, dt);
 }
 
+// ---------------------------------------------------------------------------
+// NDIM = 1: slope, trace1d, riemann_solver and update along x only (scheme.f90:289-316,
+// 661-805; solver.f90:116-262; scheme.f90:1764-1936).  The core of a cell is its predicted
+// state (8: rho, u, v, w, P, B_x cell-centred and unchanged, B_y, B_z) and its 7 half slopes
+// (rho, u, v, w, P, B_y, B_z), at core index i (cells 0 .. nx+1).
+// ---------------------------------------------------------------------------
+constexpr int kCore1 = 15;
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_trace1d(Geo G, const T *__restrict__ Q, T *__restrict__ core,
+                                                      const Scalars *S) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.CX) return;
+    const int i = (int)t;
+    const long long c = G.idx(i, 1, 1);
+    const double dtd = S->dt;
+    const T half = T(0.5), gamma = (T)G.gamma, dtdx = (T)(dtd / G.dx);
+    const T st = (T)G.slope_type;  // 1 or 2 (dg_init refuses 3 with ndim = 1)
+    T qv[8], d[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        qv[v] = ld(Q + G.sv * v + c);
+        d[v] = G.slope_type == 0 ? T(0) : limit1(st, ld(Q + G.sv * v + c - 1), qv[v], ld(Q + G.sv * v + c + 1));
+    }
+    const T r = qv[IR], u = qv[IU], v = qv[IV], w = qv[IW], p = qv[IP], A = qv[IA], B = qv[IB], C = qv[IC];
+    const T drx = half * d[IR], dux = half * d[IU], dvx = half * d[IV], dwx = half * d[IW], dpx = half * d[IP];
+    const T dBx = half * d[IB], dCx = half * d[IC];
+    // source terms, scheme.f90:717-727 (the rotation term of :777-781 changes only the local
+    // sC0 after its last use)
+    T sr0 = -u * drx - r * dux;                   sr0 = sr0 * dtdx;
+    T su0 = -u * dux - (dpx + B * dBx + C * dCx) / r; su0 = su0 * dtdx;
+    T sv0 = -u * dvx + (A * dBx) / r;              sv0 = sv0 * dtdx;
+    T sw0 = -u * dwx + (A * dCx) / r;              sw0 = sw0 * dtdx;
+    T sp0 = -u * dpx - gamma * p * dux;            sp0 = sp0 * dtdx;
+    T sB0 = -u * dBx + A * dvx - B * dux;          sB0 = sB0 * dtdx;
+    T sC0 = -u * dCx + A * dwx - C * dux;          sC0 = sC0 * dtdx;
+    T *o = core + core_base(t, kCore1);
+    const int cs = kCoreLane;
+    if (!chk(o, ((kCore1 - 1) * cs + 1) * sizeof(T))) return;
+    o[0 * cs] = r + sr0; o[1 * cs] = u + su0; o[2 * cs] = v + sv0; o[3 * cs] = w + sw0;
+    o[4 * cs] = p + sp0; o[5 * cs] = A;       o[6 * cs] = B + sB0; o[7 * cs] = C + sC0;
+    o[8 * cs] = drx; o[9 * cs] = dux; o[10 * cs] = dvx; o[11 * cs] = dwx; o[12 * cs] = dpx;
+    o[13 * cs] = dBx; o[14 * cs] = dCx;
+}
+
+// the x faces i = 1 .. nx+1: qm of cell i-1 (state + slope) against qp of cell i (state - slope),
+// the density floored, the pressure not (trace1d, scheme.f90:783-801); record per face: the
+// compflux-scaled fluxes of rho, E, rho u, rho v, rho w, then p*_T, then those of B_x, B_y, B_z
+template <typename T, bool kHLLD>
+__global__ void __launch_bounds__(kThreads) k_riemann1d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
+                                                        const Scalars *S) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= G.FX) return;
+    const int i = (int)t + 1;
+    const T half = T(0.5), smallr = T(kSmallr);
+    auto side = [&](long long cc, int sgn, T s[8]) {
+        const CoreView<T> cv{core, kCore1};
+        const T pr = cv.f(0, cc), pu = cv.f(1, cc), pv = cv.f(2, cc), pw = cv.f(3, cc), pp = cv.f(4, cc);
+        const T pA = cv.f(5, cc), pB = cv.f(6, cc), pC = cv.f(7, cc);
+        const T dr = cv.f(8, cc), du = cv.f(9, cc), dv = cv.f(10, cc), dw = cv.f(11, cc), dp = cv.f(12, cc);
+        const T dB = cv.f(13, cc), dC = cv.f(14, cc);
+        if (sgn > 0) {
+            s[IR] = mx(smallr, pr + dr); s[IU] = pu + du; s[IV] = pv + dv; s[IW] = pw + dw; s[IP] = pp + dp;
+            s[IA] = pA; s[IB] = pB + dB; s[IC] = pC + dC;
+        } else {
+            s[IR] = mx(smallr, pr - dr); s[IU] = pu - du; s[IV] = pv - dv; s[IW] = pw - dw; s[IP] = pp - dp;
+            s[IA] = pA; s[IB] = pB - dB; s[IC] = pC - dC;
+        }
+    };
+    T sm[8], sp[8];
+    side(i - 1, +1, sm);
+    side(i, -1, sp);
+    const T bn_mean = half * (sm[IA] + sp[IA]);
+    T ql[8] = {sm[IR], sm[IP], sm[IU], bn_mean, sm[IV], sm[IB], sm[IW], sm[IC]};
+    T qr[8] = {sp[IR], sp[IP], sp[IU], bn_mean, sp[IV], sp[IB], sp[IW], sp[IC]};
+    T f[8], pg = T(0);
+    solve1d<T, kHLLD>(G.iriemann, ql, qr, f, pg, (T)G.gamma, (T)G.ciso, G.iso, (T)G.entho);
+    if (G.omega0 > 0.0) {  // solver.f90:201-207
+        const T shear = (T)(-1.5 * G.omega0 * (G.xc(i) + G.xc(i - 1)));
+        f[7] = f[7] + shear * bn_mean;
+    }
+    // compflux, scheme.f90:1740-1753: ds = dy dz
+    const T ds = (T)(G.dy * G.dz), dt = (T)S->dt;
+    T *o = fx + t * kFluxRec1;
+    if (!chk(o, kFluxRec1 * sizeof(T))) return;
+    o[0] = f[0] * ds * dt; o[1] = f[1] * ds * dt; o[2] = f[2] * ds * dt; o[3] = f[4] * ds * dt;
+    o[4] = f[6] * ds * dt; o[5] = pg; o[6] = f[3] * ds * dt; o[7] = f[5] * ds * dt; o[8] = f[7] * ds * dt;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_riemann2d(Geo G, const T *__restrict__ core, T *__restrict__ fx,
                                                         T *__restrict__ fy, T *__restrict__ ez, const Scalars *S,
@@ -1504,12 +1597,12 @@ __device__ __forceinline__ int map_bc(int type, int i, int n) {
 // the x-ghost cells of the active rows
 __host__ __device__ __forceinline__ long long ghost_cells(const Geo &G) {
     const long long nA = (G.ndim == 3) ? 6LL * G.NX * G.NY : 0;
-    const long long nB = 6LL * G.NX * (G.ndim == 3 ? G.nz : 1);
+    const long long nB = (G.ndim > 1) ? 6LL * G.NX * (G.ndim == 3 ? G.nz : 1) : 0;
     const long long nC = 6LL * G.ny * (G.ndim == 3 ? G.nz : 1);
     return nA + nB + nC;
 }
 
-constexpr int kMaxVars = 9;  // stored state variables: 8, plus the frozen right z-face B in 2D
+constexpr int kMaxVars = 10;  // stored state variables: 8, plus the frozen right-face B (z in 2D, y and z in 1D)
 template <class Store>
 __global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, const Scalars *S) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1517,7 +1610,7 @@ __global__ void __launch_bounds__(kThreads) k_boundary(Geo G, Store U, int nv, c
     // the ghost counts of any grid that fits a GPU are far below 2^32: 32-bit index arithmetic
     const unsigned NX = G.NX, NY = G.NY;
     const unsigned nA = (G.ndim == 3) ? 6u * NX * NY : 0u;
-    const unsigned nB = 6u * NX * (G.ndim == 3 ? (unsigned)G.nz : 1u);
+    const unsigned nB = (G.ndim > 1) ? 6u * NX * (G.ndim == 3 ? (unsigned)G.nz : 1u) : 0u;
     auto ghost = [](int g, int n) { return g < 3 ? g - 2 : n + g - 2; };  // 0..5 -> -2,-1,0,n+1,n+2,n+3
     int i, j, k;
     const unsigned u0 = (unsigned)t;
@@ -1623,9 +1716,12 @@ __global__ void k_right_faces(Geo G, Store U, double *__restrict__ out) {
     const int k = (int)(r / G.NY);
     // last layer of each direction: no neighbour, keep the left-face value
     out[t] = (i + 1 < G.NX) ? U.get(G, IA, t + 1) : U.get(G, IA, t);
-    out[n + t] = (G.ndim > 1 && j + 1 < G.NY) ? U.get(G, IB, t + G.sy) : U.get(G, IB, t);
+    // ndim = 1: the right y and z faces are never refreshed by the reference (stored planes 8, 9);
+    // ndim = 2: the right z face (plane 8)
+    if (G.ndim == 1) out[n + t] = U.get(G, 8, t);
+    else out[n + t] = (j + 1 < G.NY) ? U.get(G, IB, t + G.sy) : U.get(G, IB, t);
     if (G.ndim == 3) out[2 * n + t] = (k + 1 < G.NZ) ? U.get(G, IC, t + G.sz) : U.get(G, IC, t);
-    else out[2 * n + t] = U.get(G, 8, t);
+    else out[2 * n + t] = U.get(G, G.ndim == 1 ? 9 : 8, t);
 }
 
 // state <-> FP64 planes (upload/download of the compensated state)

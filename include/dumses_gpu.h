@@ -70,9 +70,10 @@ extern "C" {
 /* POD mirror of the reference's &scheme_params / &model_params namelists
  * (src/subroutines/init.f90:153-173) plus the compile-time switches NDIM/ISO. */
 typedef struct dg_params {
-    int    ndim;             /* 2 or 3 (reference NDIM)                                */
+    int    ndim;             /* 1, 2 or 3 (reference NDIM; 1: FP64, slope_type <= 2,   */
+                             /* no dissipation)                                        */
     int    iso;              /* 1: isothermal EOS (reference ISO=1), 0: adiabatic      */
-    int    nx, ny, nz;       /* active cells (nz = 1 when ndim = 2)                    */
+    int    nx, ny, nz;       /* active cells (nz = 1 when ndim = 2, ny = nz = 1 when 1) */
     double xmin, xmax, ymin, ymax, zmin, zmax;
     double gamma;            /* ratio of specific heats                                */
     double ciso;             /* isothermal sound speed                                 */

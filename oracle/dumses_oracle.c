@@ -291,7 +291,8 @@ double or_compute_dt(or_state *s)
                     if (nz == 1) velz = zero;
                 }
                 double c;
-                if (s->ndim == 2) c = one / (velx / s->dx + vely / s->dy);
+                if (s->ndim == 1) c = s->dx / velx;  /* physics.f90:101-103 */
+                else if (s->ndim == 2) c = one / (velx / s->dx + vely / s->dy);
                 else c = one / (velx / s->dx + vely / s->dy + velz / s->dz);
                 dt = MN(dt, c);
             }
@@ -346,6 +347,17 @@ static void slope(or_state *s)
     const double stl = (double)MN(st, 2);
     const double sd = (double)st;
     const farr q = s->qin;
+    if (s->ndim == 1) {
+        /* scheme.f90:289-316: slope_type 1 or 2 (the reference stops on any other) */
+        if (st >= 3) return;
+#pragma omp parallel for schedule(static)
+        for (int k = klo; k <= khi; k++)
+            for (int j = jlo; j <= jhi; j++)
+                for (int i = ilo; i <= ihi; i++)
+                    for (int ivar = 1; ivar <= nvar; ivar++)
+                        A5(s->dq, i, j, k, ivar, 1) = limit1(sd, A4(q, i - 1, j, k, ivar), A4(q, i, j, k, ivar), A4(q, i + 1, j, k, ivar));
+        return;
+    }
     if (s->ndim == 2) {
         if (st < 3) {
 #pragma omp parallel for schedule(static)
@@ -628,6 +640,57 @@ static void trace3d(or_state *s, double dt)
 }
 
 /* trace2d, scheme.f90:807-1143 (Cartesian branch) */
+/* trace1d, scheme.f90:661-805 (Cartesian): the predicted cell state and its face states in x;
+ * the face B_x is the cell-centred value, the density has a floor, the pressure none, and the
+ * rotation term of :777-781 changes only the local sC0 after its last use (no effect) */
+static void trace1d(or_state *s, double dt)
+{
+    const dg_params *p = &s->p;
+    const double gamma = p->gamma;
+    int ilo = MN(1, s->iu1 + 1), ihi = MX(1, s->iu2 - 1);
+    int jlo = MN(1, s->ju1 + 1), jhi = MX(1, s->ju2 - 1);
+    int klo = MN(1, s->ku1 + 1), khi = MX(1, s->ku2 - 1);
+    const double dtdx = dt / s->dx;
+    const farr q = s->qin;
+#pragma omp parallel for schedule(static)
+    for (int k = klo; k <= khi; k++)
+        for (int j = jlo; j <= jhi; j++)
+            for (int i = ilo; i <= ihi; i++) {
+                double r = A4(q, i, j, k, ir), u = A4(q, i, j, k, iu), v = A4(q, i, j, k, iv), w = A4(q, i, j, k, iw);
+                double pp = A4(q, i, j, k, ip), A = A4(q, i, j, k, iA), B = A4(q, i, j, k, iB), C = A4(q, i, j, k, iC);
+                double drx = half * A5(s->dq, i, j, k, ir, 1), dux = half * A5(s->dq, i, j, k, iu, 1);
+                double dvx = half * A5(s->dq, i, j, k, iv, 1), dwx = half * A5(s->dq, i, j, k, iw, 1);
+                double dpx = half * A5(s->dq, i, j, k, ip, 1), dBx = half * A5(s->dq, i, j, k, iB, 1);
+                double dCx = half * A5(s->dq, i, j, k, iC, 1);
+                double sr0 = -u * drx - r * dux;                   sr0 = sr0 * dtdx;
+                double su0 = -u * dux - (dpx + B * dBx + C * dCx) / r; su0 = su0 * dtdx;
+                double sv0 = -u * dvx + (A * dBx) / r;              sv0 = sv0 * dtdx;
+                double sw0 = -u * dwx + (A * dCx) / r;              sw0 = sw0 * dtdx;
+                double sp0 = -u * dpx - gamma * pp * dux;          sp0 = sp0 * dtdx;
+                double sB0 = -u * dBx + A * dvx - B * dux;          sB0 = sB0 * dtdx;
+                double sC0 = -u * dCx + A * dwx - C * dux;          sC0 = sC0 * dtdx;
+                r = r + sr0; u = u + su0; v = v + sv0; w = w + sw0; pp = pp + sp0; B = B + sB0; C = C + sC0;
+                A5(s->qp, i, j, k, ir, 1) = r - drx;
+                A5(s->qp, i, j, k, iu, 1) = u - dux;
+                A5(s->qp, i, j, k, iv, 1) = v - dvx;
+                A5(s->qp, i, j, k, iw, 1) = w - dwx;
+                A5(s->qp, i, j, k, ip, 1) = pp - dpx;
+                A5(s->qp, i, j, k, iA, 1) = A;
+                A5(s->qp, i, j, k, iB, 1) = B - dBx;
+                A5(s->qp, i, j, k, iC, 1) = C - dCx;
+                A5(s->qp, i, j, k, ir, 1) = MX(smallr, A5(s->qp, i, j, k, ir, 1));
+                A5(s->qm, i, j, k, ir, 1) = r + drx;
+                A5(s->qm, i, j, k, iu, 1) = u + dux;
+                A5(s->qm, i, j, k, iv, 1) = v + dvx;
+                A5(s->qm, i, j, k, iw, 1) = w + dwx;
+                A5(s->qm, i, j, k, ip, 1) = pp + dpx;
+                A5(s->qm, i, j, k, iA, 1) = A;
+                A5(s->qm, i, j, k, iB, 1) = B + dBx;
+                A5(s->qm, i, j, k, iC, 1) = C + dCx;
+                A5(s->qm, i, j, k, ir, 1) = MX(smallr, A5(s->qm, i, j, k, ir, 1));
+            }
+}
+
 static void trace2d(or_state *s, double dt)
 {
     const dg_params *p = &s->p;
@@ -966,7 +1029,12 @@ static void riemann_solver(or_state *s, double dt)
                     if (have)
                         for (int n = 0; n < 8; n++) A5(s->fgodunov, i, j, k, n + 1, idim) = f[n];
                     /* shearing-box upwind terms, solver.f90:199-241 */
-                    if (ndim == 2) {
+                    if (ndim == 1) {
+                        if (Omega0 > zero) {
+                            double shear = -1.5 * Omega0 * (XC(i) + XC(i - 1));
+                            A5(s->fgodunov, i, j, k, 8, idim) = A5(s->fgodunov, i, j, k, 8, idim) + shear * bn_mean;
+                        }
+                    } else if (ndim == 2) {
                         if (Omega0 > zero) {
                             double shear = -1.5 * Omega0 * XC(i);
                             if (idim == 1) shear = -1.5 * Omega0 * (XC(i) + XC(i - 1));
@@ -1457,7 +1525,10 @@ static void update(or_state *s, double dt)
                     A4(s->uin, i, j, k, iw) = A4(s->uin, i, j, k, iw)
                         + (A5(s->flux, i, j, k, iw, idim) * one - A5(s->flux, i + i0, j + j0, k + k0, iw, idim) * one) * dvloc / one;
                     A4(s->uin, i, j, k, ip) = A4(s->uin, i, j, k, ip) + (A5(s->flux, i, j, k, ip, idim) - A5(s->flux, i + i0, j + j0, k + k0, ip, idim)) * dvloc;
-                    if (ndim == 2)
+                    if (ndim == 1) {
+                        for (int b = iA; b <= iC; b++)
+                            A4(s->uin, i, j, k, b) = A4(s->uin, i, j, k, b) + (A5(s->flux, i, j, k, b, idim) - A5(s->flux, i + i0, j + j0, k + k0, b, idim)) * dvloc;
+                    } else if (ndim == 2)
                         A4(s->uin, i, j, k, iC) = A4(s->uin, i, j, k, iC) + (A5(s->flux, i, j, k, iC, idim) - A5(s->flux, i + i0, j + j0, k + k0, iC, idim)) * dvloc;
                     if (Omega0 > zero) {
                         double dfn2 = (A5(s->flux, i, j, k, iu, idim) - A5(s->flux, i + i0, j + j0, k + k0, iu, idim)) * dvloc;
@@ -1475,7 +1546,8 @@ static void update(or_state *s, double dt)
                 }
                 if (Omega0 == 0) {
                     A4(s->uin, i, j, k, iu) = A4(s->uin, i, j, k, iu) + A4(s->fgodunov_pre, i, j, k, 1) * dvloc;
-                    A4(s->uin, i, j, k, iv) = A4(s->uin, i, j, k, iv) + A4(s->fgodunov_pre, i, j, k, 2) * dvloc;
+                    if (ndim > 1)
+                        A4(s->uin, i, j, k, iv) = A4(s->uin, i, j, k, iv) + A4(s->fgodunov_pre, i, j, k, 2) * dvloc;
                 }
                 if (ndim > 2)
                     A4(s->uin, i, j, k, iw) = A4(s->uin, i, j, k, iw) + A4(s->fgodunov_pre, i, j, k, 3) * dvloc;
@@ -1491,7 +1563,8 @@ void or_godunov(or_state *s, double dt, double time)
     or_primitive(s, dt);
     slope(s);
     if (s->ndim == 3) trace3d(s, dt);
-    else trace2d(s, dt);
+    else if (s->ndim == 2) trace2d(s, dt);
+    else trace1d(s, dt);
     riemann_solver(s, dt);
     if (s->ndim > 1) riemann_solver_magnetic(s, &s->qRT, &s->qRB, &s->qLT, &s->qLB, &s->emfz, 3, dt);
     if (s->ndim == 3) {
@@ -1872,6 +1945,18 @@ static void history_sums(or_state *s, int iv2, int ib2, double out[9])
 
 void or_history_mri(or_state *s, double out[9]) { history_sums(s, iv, iB, out); }
 void or_history_default(or_state *s, double out[9]) { history_sums(s, iw, iC, out); }
+
+/* the one-dimensional history line (src/subroutines/history.f90:37-59): rho, rho u_x and E of
+ * the first cell whose centre is at x >= 1/2 (the loop's exit value nx+1, a ghost cell, if none) */
+void or_history_1d(or_state *s, double out[3])
+{
+    int ipos = 1;
+    for (ipos = 1; ipos <= s->nx; ipos++)
+        if (XC(ipos) >= half) break;
+    out[0] = A4(s->uin, ipos, 1, 1, ir);
+    out[1] = A4(s->uin, ipos, 1, 1, iu);
+    out[2] = A4(s->uin, ipos, 1, 1, ip);
+}
 
 /* ------------------------------------------------------------------------- */
 /* dissipation, src/subroutines/physics.f90:272-664                           */

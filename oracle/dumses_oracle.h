@@ -41,6 +41,7 @@ void   or_fargo_update(or_state *s, double dt);       /* fargo.f90:17-124      *
 void   or_boundary(or_state *s, double time, double dt); /* boundary.f90:18-92 */
 void   or_history_mri(or_state *s, double out[9]);    /* mri/history.f90:19-174 */
 void   or_history_default(or_state *s, double out[9]); /* subroutines/history.f90:19-171, NDIM 3 */
+void   or_history_1d(or_state *s, double out[3]);      /* subroutines/history.f90:37-59, NDIM 1 */
 void   or_dissipation(or_state *s, double time, double dt); /* physics.f90:272-664 */
 
 /* loop body dumses.f90:82-120; returns the dt used and advances *time */

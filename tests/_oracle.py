@@ -41,6 +41,7 @@ def lib() -> ctypes.CDLL:
         L.or_boundary.restype, L.or_boundary.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
         L.or_history_mri.restype, L.or_history_mri.argtypes = None, [vp, dp]
         L.or_history_default.restype, L.or_history_default.argtypes = None, [vp, dp]
+        L.or_history_1d.restype, L.or_history_1d.argtypes = None, [vp, dp]
         L.or_step.restype, L.or_step.argtypes = ctypes.c_double, [vp, dp]
         L.or_dissipation.restype, L.or_dissipation.argtypes = None, [vp, ctypes.c_double, ctypes.c_double]
         L.or_run_history.restype = ctypes.c_int
@@ -131,7 +132,12 @@ class Oracle:
 
     def history(self, variant: str = "mri") -> np.ndarray:
         """The 9 history sums: variant "mri" (src/problem/mri/history.f90) or "default"
-        (src/subroutines/history.f90)."""
+        (src/subroutines/history.f90); "1d": the one-dimensional line of the default routine
+        (rho, rho u_x, E at x = 1/2)."""
+        if variant == "1d":
+            out = np.zeros(3)
+            self.L.or_history_1d(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+            return out
         out = np.zeros(9)
         f = self.L.or_history_mri if variant == "mri" else self.L.or_history_default
         f(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))

@@ -78,6 +78,14 @@ def test_invalid_params_rejected_before_device_use():
     assert b"ndim" in lib.dg_last_error()
     bad = dg.Params(ndim=3, nx=8, ny=8, nz=8, bdtypey="shearingbox").to_c()
     assert lib.dg_init(ctypes.byref(bad), ctypes.byref(h)) == -8
+    # ndim = 1: a single row, the FP64 path, slope types up to 2 (scheme.f90:313-315), no dissipation
+    for kw, code in ((dict(ny=4), -1), (dict(precision="fp32"), -8), (dict(slope_type=3), -8), (dict(nu=1e-3), -8)):
+        bad = dg.Params(**{**dict(ndim=1, nx=64, ny=1, nz=1), **kw}).to_c()
+        assert lib.dg_init(ctypes.byref(bad), ctypes.byref(h)) == code, kw
+        assert not h.value
+    if not _has_gpu():  # a valid 1D grid passes validation and stops at the missing device
+        good = dg.Params(ndim=1, nx=64, ny=1, nz=1).to_c()
+        assert lib.dg_init(ctypes.byref(good), ctypes.byref(h)) in (-7, -2)
 
 
 @pytest.mark.skipif(_has_gpu(), reason="checks the no-device path")

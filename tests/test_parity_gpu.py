@@ -26,6 +26,8 @@ def compare_states(ug, uo, params):
     assert np.array_equal(ug[:-1, :, :, 8], uo[:-1, :, :, 8])
     if params.ndim > 1:
         assert np.array_equal(ug[:, :-1, :, 9], uo[:, :-1, :, 9])
+    else:
+        assert np.array_equal(ug[..., 9], uo[..., 9])  # ndim = 1: the frozen right y face
     if params.ndim == 3:
         assert np.array_equal(ug[:, :, :-1, 10], uo[:, :, :-1, 10])
     else:
@@ -230,6 +232,67 @@ def test_default_history_sums_match_oracle():
                 (prec, q, h_g[q], h_o[q])
         assert abs(h_g[8]) < 1e-9 and abs(h_o[8]) < 1e-9
         assert not np.isclose(h_m[1], h_g[1])
+
+
+def tube_1d(nx: int, bdtype: str, omega0: float = 0.0, riemann: str = "hlld") -> tuple[Params, np.ndarray]:
+    """A 1D Riemann problem with field: left rho 1, P 1, B_y 1; right rho 0.125, P 0.1, B_y -1;
+    B_x 0.75 and a transverse velocity and B_z on both sides (the Brio-Wu-like tube), with the
+    right y and z faces (vars 10, 11) set to the left faces, as a problem's condinit sets them."""
+    p = Params(ndim=1, iso=0, nx=nx, ny=1, nz=1, xmin=0.0, xmax=1.0, ymin=0.0, ymax=1.0, zmin=0.0, zmax=1.0,
+               gamma=2.0, courant=0.8, slope_type=2, riemann=riemann, riemann2d="hlld", bdtypex=bdtype,
+               omega0=omega0)
+    u = np.zeros(p.shape, order="F")
+    xc = (np.arange(nx + 6) - 2.5) / nx
+    left = xc < 0.5
+    rho = np.where(left, 1.0, 0.125)
+    pres = np.where(left, 1.0, 0.1)
+    bx, by, bz = 0.75, np.where(left, 1.0, -1.0), 0.3 * np.sin(2 * np.pi * xc)
+    vy = 0.1 * np.cos(2 * np.pi * xc)
+    u[:, 0, 0, 0] = rho
+    u[:, 0, 0, 2] = rho * vy
+    u[:, 0, 0, 4] = pres / (p.gamma - 1.0) + 0.5 * rho * vy ** 2 + 0.5 * (bx * bx + by * by + bz * bz)
+    for v, b in ((5, bx), (6, by), (7, bz), (8, bx), (9, by), (10, bz)):
+        u[:, 0, 0, v] = b
+    return p, u
+
+
+@pytest.mark.parametrize("bdtype,omega0,riemann", [("zero_gradient", 0.0, "hlld"), ("periodic", 0.0, "hlld"),
+                                                   ("zero_gradient", 0.0, "hll"), ("zero_gradient", 0.0, "llf"),
+                                                   ("zero_gradient", 0.0, "upwind"), ("periodic", 1.0, "hlld")])
+def test_one_dimensional_scheme_matches_oracle(bdtype, omega0, riemann):
+    """NDIM = 1 (trace1d, the x solves, every field updated by its x flux, the frozen right y and z
+    faces of the reference): 40 steps of an MHD tube, every dt and the final state bit-identical,
+    the rotation terms and the B_z shear flux included (omega0 > 0), and the history line."""
+    p, u0 = tube_1d(128, bdtype, omega0, riemann)
+    o = Oracle(p)
+    o.set_state(u0)
+    o.boundary(0.0, 0.0)
+    with Context(p) as g:
+        g.upload(u0)
+        g.boundary(0.0, 0.0)
+        t_g = t_o = 0.0
+        for _ in range(40):
+            dt_o = o.compute_dt()
+            dt_g = g.compute_dt()
+            assert dt_g == dt_o
+            o.godunov(dt_o, t_o)
+            o.boundary(t_o, dt_o)
+            g.godunov(dt_g, t_g)
+            g.boundary(t_g, dt_g)
+            t_o = t_o + dt_o
+            t_g = t_g + dt_g
+        ug = g.download()
+        h = g.history("default")
+        t_r, _ = g.run(3, t_g)
+        ur = g.download()
+    compare_states(ug, o.uin, p)
+    assert np.array_equal(h[:3], o.history("1d")) and not np.any(h[3:])
+    for _ in range(3):
+        t_o, _ = o.step(t_o)
+    assert t_r == t_o
+    compare_states(ur, o.uin, p)
+    # the right y and z faces keep their initial values in the active cells (the ghost fill copies them)
+    assert np.array_equal(ur[3:-3, ..., 9:11], u0[3:-3, ..., 9:11])
 
 
 def test_field_loop_full_run_to_t2():
