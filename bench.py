@@ -56,7 +56,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "zone-cycles/s at 256³: plain FP64 vs FP32+NN-flux at stated L1 vs FP64"
 ALGO_BYTES_PER_ZONE = 128  # read + write of 8 conserved FP64 variables per zone-cycle
-NN_MACS_PER_FACE = 17 * 128 + 128 * 128 + 128 * 128 + 128 * 8  # the face network's multiply-adds
+def nn_macs_per_face(width: int, depth: int) -> int:
+    """The face network's multiply-adds per face: 17 -> width (x depth hidden layers) -> 8."""
+    return 17 * width + (depth - 1) * width * width + width * 8
 
 
 WORKLOADS = {"ot": "orszag_tang_3d", "mri": "shearing_box_mri_fargo"}
@@ -492,13 +494,24 @@ def main() -> None:
         dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
         per_launch_s = kernels[dom]["ms_per_launch"] / 1e3
         if dom == "nn_faces":
-            # tensor-core bound: the network's multiply-adds over the faces of one direction
+            # the network's multiply-adds and the face kernel's algorithmic bytes over the faces of one
+            # direction: per face the 16 trace-core values of each of its two cells (each cell's
+            # values serve its two faces of the direction: 64 B per face) and the 6-value flux
+            # record (24 B).  The roof is the one the operational intensity reaches first: the
+            # tensor pipe above the ridge point (peak flop rate / copy bandwidth), HBM below it.
+            from dumses_hybrid_b200 import network_shape
+            width, depth = network_shape()
+            macs = nn_macs_per_face(width, depth)
             faces = (args.n + 1) * args.n * args.n
-            flops = 2.0 * NN_MACS_PER_FACE * faces
+            flops = 2.0 * macs * faces
+            nbytes = (16 * 4 + 6 * 4) * faces
             tpeak = peaks.get("bf16_tflops_sustained")
             src = "measured (sustained)" if tpeak else "fallback"
             tpeak = tpeak or 1400.0
-            achieved = flops / per_launch_s / 1e12
+            t_ach = flops / per_launch_s / 1e12
+            b_ach = nbytes / per_launch_s / 1e9
+            intensity = flops / nbytes
+            ridge = tpeak * 1e12 / (hbm_peak * 1e9)
             traffic = None
             tpath = ROOT / "profiles" / f"ncu_traffic_{args.workload}{args.n}_fp32nn.json"
             if tpath.exists():
@@ -506,10 +519,17 @@ def main() -> None:
                     traffic = json.loads(tpath.read_text()).get(dom)
                 except Exception:
                     traffic = None
-            out = {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": tpeak, "unit": "TFLOP/s",
-                   "frac": achieved / tpeak, "traffic": traffic, "peak_source": src,
-                   "algorithmic_flops_per_launch": flops,
-                   "note": "one launch per face direction; 2 x 35968 flops per face (17-128-128-128-8 MLP)"}
+            shape = f"17-{'-'.join([str(width)] * depth)}-8 MLP"
+            if intensity >= ridge:
+                out = {"bound": "tensor", "kernel": dom, "achieved": t_ach, "peak": tpeak, "unit": "TFLOP/s",
+                       "frac": t_ach / tpeak, "peak_source": src}
+            else:
+                out = {"bound": "hbm", "kernel": dom, "achieved": b_ach, "peak": hbm_peak, "unit": "GB/s",
+                       "frac": b_ach / hbm_peak, "peak_source": peak_src}
+            out.update({"traffic": traffic, "algorithmic_flops_per_launch": flops,
+                        "algorithmic_bytes_per_launch": nbytes, "intensity_flop_per_byte": intensity,
+                        "ridge_flop_per_byte": ridge, "tensor_frac": t_ach / tpeak, "hbm_frac": b_ach / hbm_peak,
+                        "note": f"one launch per face direction; 2 x {macs} flops and 88 bytes per face ({shape})"})
             upath = ROOT / "profiles" / "pipe_util_mri128.json"
             if upath.exists():
                 try:

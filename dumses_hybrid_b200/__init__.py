@@ -127,6 +127,7 @@ def load_library(path: str | pathlib.Path | None = None) -> ctypes.CDLL:
         "dg_debug_copy": (ctypes.c_int, [vp, ctypes.c_int, dp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
         "dg_condinit": (ctypes.c_int, [c_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong, dp]),
         "dg_nn_param_count": (ctypes.c_longlong, []),
+        "dg_nn_shape": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
         "dg_nn_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(vp)]),
         "dg_nn_destroy": (ctypes.c_int, [vp]),
         "dg_nn_set_samples": (ctypes.c_int, [vp, fp, fp, ctypes.c_longlong]),
@@ -507,14 +508,24 @@ class Context:
 N_IN, N_OUT = 17, 8
 
 
+def network_shape(lib=None) -> tuple[int, int]:
+    """(hidden width, hidden layers) of the network the library was built with."""
+    lib = lib or load_library()
+    w, d = ctypes.c_int(), ctypes.c_int()
+    _check(lib.dg_nn_shape(ctypes.byref(w), ctypes.byref(d)))
+    return w.value, d.value
+
+
 def _fptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
 
 
 class FluxNet:
-    """The learned face-flux network (a dg_nn of the C-ABI): 17 -> 128 -> 128 -> 128 -> 8,
-    SmeLU, BF16 weights with FP32 accumulation, trained on the device.  Parameters are a
-    flat float32 vector in the order W1[17][128], b1, W2[128][128], b2, W3, b3, W4[128][8], b4."""
+    """The learned face-flux network (a dg_nn of the C-ABI): 17 inputs, `depth` hidden layers
+    of `width` SmeLU units (the library's build fixes them; 64 x 2 by default), 8 outputs,
+    BF16 weights with FP32 accumulation, trained on the device.  Parameters are a flat
+    float32 vector in the order W1[17][width], b1, the hidden W[width][width], b pairs,
+    then W[width][8], b; `shapes` lists the (inputs, outputs) of each weight layer."""
 
     def __init__(self, device: int = 0, seed: int = 1):
         self.lib = load_library()
@@ -542,6 +553,16 @@ class FluxNet:
     @property
     def param_count(self) -> int:
         return int(self.lib.dg_nn_param_count())
+
+    @property
+    def shape(self) -> tuple[int, int]:
+        """(hidden width, hidden layers) of the library's network."""
+        return network_shape(self.lib)
+
+    @property
+    def shapes(self) -> list[tuple[int, int]]:
+        w, d = self.shape
+        return [(N_IN, w)] + [(w, w)] * (d - 1) + [(w, N_OUT)]
 
     def params(self) -> np.ndarray:
         p = np.zeros(self.param_count, dtype=np.float32)

@@ -29,7 +29,24 @@
 namespace dg {
 namespace nn {
 
-constexpr int kIn = 17, kInPad = 32, kHid = 128, kOut = 8, kOutPad = 16;
+// Network shape: kNHid hidden layers of kHid units (a build option, DG_NN_WIDTH and
+// DG_NN_DEPTH; 64 and 2 by default: of the shapes measured, the fastest that learns every
+// output's correction on small harvests as well as on large ones).  kHid is 32, 64 or 128: one M = 128 tile of faces
+// holds its accumulator in kHid tensor-memory columns, and the transposed hidden operands
+// of the weight-gradient products keep kHidT = 128 rows (rows kHid.. stay zero), so those
+// products stay M = 128 MMAs at every width.
+#ifndef DG_NN_WIDTH
+#define DG_NN_WIDTH 64
+#endif
+#ifndef DG_NN_DEPTH
+#define DG_NN_DEPTH 2
+#endif
+constexpr int kIn = 17, kInPad = 32, kHid = DG_NN_WIDTH, kOut = 8, kOutPad = 16;
+constexpr int kNHid = DG_NN_DEPTH;  // hidden layers
+constexpr int kNL = kNHid + 1;      // weight layers; layer kNHid is the output layer
+constexpr int kHidT = 128;
+static_assert(kHid == 32 || kHid == 64 || kHid == 128, "hidden width must be 32, 64 or 128");
+static_assert(kNHid >= 1 && kNHid <= 3, "one to three hidden layers");
 
 struct FaceUnits {
     float rho0, a0, b0, jump;  // interface units and the jump size J
@@ -198,9 +215,9 @@ __host__ __device__ __forceinline__ void bias_split(float b, __nv_bfloat16 &hi, 
 
 // device view of the trained network for inference inside the step
 struct NetView {
-    const __nv_bfloat16 *wt[4];  // forward B operands, blocked K-major [N_l][K_l]
-    const __nv_bfloat16 *bt[3];  // hidden-layer bias operands, blocked K-major [kHid][kBiasK]
-    const float *b[4];           // biases
+    const __nv_bfloat16 *wt[kNL];   // forward B operands, blocked K-major [N_l][K_l]
+    const __nv_bfloat16 *bt[kNHid]; // hidden-layer bias operands, blocked K-major [kHid][kBiasK]
+    const float *b[kNL];            // biases
     Gates gates;
     Scaling sc;
 };

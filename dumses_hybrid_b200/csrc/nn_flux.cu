@@ -1,5 +1,5 @@
-// Learned face-flux surrogate: a 17 -> 128 -> 128 -> 128 -> 8 SmeLU MLP trained and run
-// on sm_100a.  Every matrix product is a BF16 tcgen05 MMA with an FP32 accumulator in
+// Learned face-flux surrogate: a 17 -> kHid x kNHid -> 8 SmeLU MLP (17-64-64-8 by default)
+// trained and run on sm_100a.  Every matrix product is a BF16 tcgen05 MMA with an FP32 accumulator in
 // tensor memory; operands are staged into shared memory by bulk copies from the blocked
 // K-major layout of nn_umma.cuh.  The forward products write the next layer's operands
 // (normal and transposed) and the activation derivative from their epilogues; the backward
@@ -27,9 +27,12 @@ namespace nn {
 using bf16 = __nv_bfloat16;
 
 __host__ __device__ constexpr int layer_k(int l) { return l == 0 ? kInPad : kHid; }
-__host__ __device__ constexpr int layer_n(int l) { return l == 3 ? kOutPad : kHid; }
+__host__ __device__ constexpr int layer_n(int l) { return l == kNHid ? kOutPad : kHid; }
 __host__ __device__ constexpr int real_k(int l) { return l == 0 ? kIn : kHid; }
-__host__ __device__ constexpr int real_n(int l) { return l == 3 ? kOut : kHid; }
+__host__ __device__ constexpr int real_n(int l) { return l == kNHid ? kOut : kHid; }
+// row length of the weight-gradient partials of hidden layer l: its B operand is the
+// transposed input (kInPad rows) or the transposed, zero-padded activations (kHidT rows)
+__host__ __device__ constexpr int dw_cols(int l) { return l == 0 ? kInPad : kHidT; }
 
 enum { M_FWD_HID = 0, M_FWD_OUT = 1, M_BWD_HID = 2, M_DW = 3 };
 
@@ -39,8 +42,8 @@ struct GemmArgs {
     const bf16 *A, *B;
     int C;             // reduction columns per CTA
     const float *bias; // forward
-    bf16 *Hn, *Ht;     // outputs: blocked normal [rows][128] and transposed [128][rows]
-    float *G;          // activation derivative [rows][128]: written forward, read backward
+    bf16 *Hn, *Ht;     // outputs: blocked normal [rows][kHid] and transposed [kHidT][rows]
+    float *G;          // activation derivative [rows][kHid]: written forward, read backward
     float *Y;          // network output [rows][8]
     float *part;       // weight-gradient partials [split][128][N] or bias partials [tile][128]
     long long rows;    // batch rows (row tiles x 128)
@@ -104,11 +107,11 @@ __device__ __forceinline__ void epilogue(const GemmArgs &g, uint32_t tmem, long 
                     if (lane == 0) atomicAdd(&sred[cc * 16 + q], s);
                 }
             }
-            // normal blocked layout [rows/128][16][128][8]
-            store_bf16x8(g.Hn + ((tile * 16 + cc * 2) * kTileRows + rl) * 8, v);
-            store_bf16x8(g.Hn + ((tile * 16 + cc * 2 + 1) * kTileRows + rl) * 8, v + 8);
-            // transposed blocked layout [rows/8][128][8]
-            bf16 *t = g.Ht + (row >> 3) * (kHid * 8) + (row & 7);
+            // normal blocked layout [rows/128][kHid/8][128][8]
+            store_bf16x8(g.Hn + ((tile * (kHid / 8) + cc * 2) * kTileRows + rl) * 8, v);
+            store_bf16x8(g.Hn + ((tile * (kHid / 8) + cc * 2 + 1) * kTileRows + rl) * 8, v + 8);
+            // transposed blocked layout [rows/8][kHidT][8] (rows kHid.. are never written: zero)
+            bf16 *t = g.Ht + (row >> 3) * (kHidT * 8) + (row & 7);
 #pragma unroll
             for (int q = 0; q < 16; q++) t[(cc * 16 + q) * 8] = __float2bfloat16_rn(v[q]);
         }
@@ -274,10 +277,10 @@ __global__ void __launch_bounds__(128) k_loss(const float *__restrict__ Y, const
 }
 
 struct AdamArgs {
-    float *W[4], *b[4], *mW[4], *vW[4], *mb[4], *vb[4];
-    const float *dw[4];  // weight-gradient partials
-    const float *db[4];  // bias-gradient partials
-    bf16 *Wt[4], *Wn[4], *Bt[3];
+    float *W[kNL], *b[kNL], *mW[kNL], *vW[kNL], *mb[kNL], *vb[kNL];
+    const float *dw[kNL];  // weight-gradient partials
+    const float *db[kNL];  // bias-gradient partials
+    bf16 *Wt[kNL], *Wn[kNL], *Bt[kNHid];
     int splits, tiles;
     float lr, beta1, beta2, eps, c1, c2;  // c1 = 1 - beta1^t, c2 = 1 - beta2^t
     int apply;                             // 1: Adam step; 0: only reduce the gradient; 2: only pack BF16 copies
@@ -291,21 +294,21 @@ __host__ __device__ constexpr long long layer_params(int l) { return (long long)
 __global__ void k_adam(AdamArgs a) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     int l = 0;
-    while (l < 4 && t >= layer_params(l)) { t -= layer_params(l); l++; }
-    if (l >= 4) return;
+    while (l < kNL && t >= layer_params(l)) { t -= layer_params(l); l++; }
+    if (l >= kNL) return;
     long long off = 0;
     for (int q = 0; q < l; q++) off += layer_params(q);
     const int K = layer_k(l), N = layer_n(l), kr = real_k(l), nr = real_n(l);
     const bool is_w = t < (long long)kr * nr;
     float g = 0.0f;
     int k = 0, n = 0;
-    // the face kernel's bias operand of hidden layer l < 3 (its columns 2.. stay zero)
+    // the face kernel's bias operand of hidden layer l < kNHid (its columns 2.. stay zero)
     auto pack_bias = [&](int nb, float b) {
-        if (l < 3) {
+        if (l < kNHid) {
             bf16 hi, lo;
             bias_split(b, hi, lo);
-            a.Bt[l][blk_off(nb, 0, kBiasK, kTileRows)] = hi;
-            a.Bt[l][blk_off(nb, 1, kBiasK, kTileRows)] = lo;
+            a.Bt[l][blk_off(nb, 0, kBiasK, kHid)] = hi;
+            a.Bt[l][blk_off(nb, 1, kBiasK, kHid)] = lo;
         }
     };
     if (a.apply == 2) {  // pack only: BF16 copies of the current masters
@@ -314,7 +317,7 @@ __global__ void k_adam(AdamArgs a) {
             n = (int)(t % nr);
             const float w = a.W[l][k * N + n];
             a.Wt[l][blk_off(n, k, K, N < kTileRows ? N : kTileRows)] = __float2bfloat16_rn(w);
-            if (l > 0) a.Wn[l][blk_off(k, n, N, kTileRows)] = __float2bfloat16_rn(w);
+            if (l > 0) a.Wn[l][blk_off(k, n, N, K < kTileRows ? K : kTileRows)] = __float2bfloat16_rn(w);
         } else {
             n = (int)(t - (long long)kr * nr);
             pack_bias(n, a.b[l][n]);
@@ -324,12 +327,13 @@ __global__ void k_adam(AdamArgs a) {
     if (is_w) {
         k = (int)(t / nr);
         n = (int)(t % nr);
-        // the weight-gradient product is [n][k] for the 128-wide layers and [k][n] for the output layer
+        // the weight-gradient product is [n][k] for the hidden layers and [k][n] for the output layer
         for (int s = 0; s < a.splits; s++)
-            g += (l < 3) ? a.dw[l][((long long)s * kTileRows + n) * K + k] : a.dw[l][((long long)s * kTileRows + k) * N + n];
+            g += (l < kNHid) ? a.dw[l][((long long)s * kTileRows + n) * dw_cols(l) + k]
+                             : a.dw[l][((long long)s * kTileRows + k) * N + n];
     } else {
         n = (int)(t - (long long)kr * nr);
-        const int stride = (l < 3) ? kTileRows : kOut;
+        const int stride = (l < kNHid) ? kTileRows : kOut;
         for (int s = 0; s < a.tiles; s++) g += a.db[l][(long long)s * stride + n];
     }
     if (a.gout) a.gout[off + t] = g;
@@ -345,7 +349,7 @@ __global__ void k_adam(AdamArgs a) {
     *p = w;
     if (is_w) {
         a.Wt[l][blk_off(n, k, K, N < kTileRows ? N : kTileRows)] = __float2bfloat16_rn(w);
-        if (l > 0) a.Wn[l][blk_off(k, n, N, kTileRows)] = __float2bfloat16_rn(w);
+        if (l > 0) a.Wn[l][blk_off(k, n, N, K < kTileRows ? K : kTileRows)] = __float2bfloat16_rn(w);
     } else {
         pack_bias(n, w);
     }
@@ -416,14 +420,15 @@ struct dg_nn {
     int device = 0;
     cudaStream_t stream = nullptr;
     int *d_err = nullptr;
-    float *W[4] = {}, *b[4] = {}, *mW[4] = {}, *vW[4] = {}, *mb[4] = {}, *vb[4] = {};
-    bf16 *Wt[4] = {}, *Wn[4] = {}, *Bt[3] = {};
+    float *W[kNL] = {}, *b[kNL] = {}, *mW[kNL] = {}, *vW[kNL] = {}, *mb[kNL] = {}, *vb[kNL] = {};
+    bf16 *Wt[kNL] = {}, *Wn[kNL] = {}, *Bt[kNHid] = {};
     float *xs = nullptr, *ts = nullptr;  // samples
     long long ns = 0, cap = 0;
     // batch scratch
     long long bcap = 0;
-    bf16 *Xn = nullptr, *Xt = nullptr, *Hn[3] = {}, *Ht[3] = {}, *Dn[2] = {}, *Dt[2] = {}, *D3n = nullptr, *D3t = nullptr;
-    float *Tb = nullptr, *Y = nullptr, *G[3] = {}, *dw[4] = {}, *db[4] = {}, *lpart = nullptr, *gout = nullptr;
+    bf16 *Xn = nullptr, *Xt = nullptr, *Hn[kNHid] = {}, *Ht[kNHid] = {}, *Dn[2] = {}, *Dt[2] = {}, *D3n = nullptr,
+         *D3t = nullptr;
+    float *Tb = nullptr, *Y = nullptr, *G[kNHid] = {}, *dw[kNL] = {}, *db[kNL] = {}, *lpart = nullptr, *gout = nullptr;
     long long step = 0;
     unsigned long long seed = 1;
     float beta1 = 0.9f, beta2 = 0.999f, eps = 1e-8f;
@@ -497,14 +502,14 @@ int ensure_batch(dg_nn *n, long long rows) {
         (rc = scratch_t(n, &n->D3n, R * kOutPad)) || (rc = scratch_t(n, &n->D3t, R * kOutPad)) ||
         (rc = scratch_t(n, &n->lpart, tiles)) || (rc = scratch_t(n, &n->gout, dg_nn_param_count())))
         return rc;
-    for (int l = 0; l < 3; l++)
-        if ((rc = scratch_t(n, &n->Hn[l], R * kHid)) || (rc = scratch_t(n, &n->Ht[l], R * kHid)) ||
+    for (int l = 0; l < kNHid; l++)
+        if ((rc = scratch_t(n, &n->Hn[l], R * kHid)) || (rc = scratch_t(n, &n->Ht[l], R * kHidT)) ||
             (rc = scratch_t(n, &n->G[l], R * kHid)))
             return rc;
     for (int q = 0; q < 2; q++)
-        if ((rc = scratch_t(n, &n->Dn[q], R * kHid)) || (rc = scratch_t(n, &n->Dt[q], R * kHid))) return rc;
-    for (int l = 0; l < 4; l++)
-        if ((rc = scratch_t(n, &n->dw[l], splits * kTileRows * kHid)) || (rc = scratch_t(n, &n->db[l], tiles * kTileRows)))
+        if ((rc = scratch_t(n, &n->Dn[q], R * kHid)) || (rc = scratch_t(n, &n->Dt[q], R * kHidT))) return rc;
+    for (int l = 0; l < kNL; l++)
+        if ((rc = scratch_t(n, &n->dw[l], splits * kTileRows * kHidT)) || (rc = scratch_t(n, &n->db[l], tiles * kTileRows)))
             return rc;
     n->bcap = rows;
     return 0;
@@ -522,7 +527,7 @@ int launch_gemm(dg_nn *n, const GemmArgs &g, long long grid) {
 int forward(dg_nn *n, long long rows) {
     const long long tiles = rows / kTileRows;
     int rc;
-    for (int l = 0; l < 3; l++) {
+    for (int l = 0; l < kNHid; l++) {
         GemmArgs g{};
         g.A = (l == 0) ? n->Xn : n->Hn[l - 1];
         g.B = n->Wt[l];
@@ -536,10 +541,10 @@ int forward(dg_nn *n, long long rows) {
         if ((rc = launch_gemm<M_FWD_HID, kHid>(n, g, tiles))) return rc;
     }
     GemmArgs g{};
-    g.A = n->Hn[2];
-    g.B = n->Wt[3];
+    g.A = n->Hn[kNHid - 1];
+    g.B = n->Wt[kNHid];
     g.C = kHid;
-    g.bias = n->b[3];
+    g.bias = n->b[kNHid];
     g.Y = n->Y;
     g.rows = rows;
     g.err = n->d_err;
@@ -551,17 +556,17 @@ int backward(dg_nn *n, long long rows, long long valid) {
     const long long tiles = rows / kTileRows;
     const int csplit = (rows % 512 == 0) ? 512 : 128;
     const long long splits = rows / csplit;
-    k_loss<<<(unsigned)tiles, 128, 0, n->stream>>>(n->Y, n->Tb, rows, valid, n->D3n, n->D3t, n->lpart, n->db[3]);
+    k_loss<<<(unsigned)tiles, 128, 0, n->stream>>>(n->Y, n->Tb, rows, valid, n->D3n, n->D3t, n->lpart, n->db[kNHid]);
     NN_CUDA(cudaGetLastError());
     int rc;
-    {   // output layer: dW[k][n] = sum_b H2t[k][b] D3t[n][b]
+    {   // output layer: dW[k][n] = sum_b Ht[k][b] Dt[n][b] over the last hidden layer's activations
         GemmArgs g{};
-        g.A = n->Ht[2]; g.B = n->D3t; g.C = csplit; g.part = n->dw[3]; g.rows = rows; g.err = n->d_err;
+        g.A = n->Ht[kNHid - 1]; g.B = n->D3t; g.C = csplit; g.part = n->dw[kNHid]; g.rows = rows; g.err = n->d_err;
         if ((rc = launch_gemm<M_DW, kOutPad>(n, g, splits))) return rc;
     }
     const bf16 *dn = n->D3n;
     int cdn = kOutPad;
-    for (int l = 2; l >= 0; l--) {
+    for (int l = kNHid - 1; l >= 0; l--) {
         bf16 *on = n->Dn[l & 1], *ot = n->Dt[l & 1];
         {   // dZ_l = (dZ_{l+1} W_{l+1}^T) * f'(Z_l), bias partials of layer l
             GemmArgs g{};
@@ -573,7 +578,7 @@ int backward(dg_nn *n, long long rows, long long valid) {
             GemmArgs g{};
             g.A = ot; g.B = (l == 0) ? n->Xt : n->Ht[l - 1]; g.C = csplit; g.part = n->dw[l]; g.rows = rows; g.err = n->d_err;
             if (l == 0) rc = launch_gemm<M_DW, kInPad>(n, g, splits);
-            else rc = launch_gemm<M_DW, kHid>(n, g, splits);
+            else rc = launch_gemm<M_DW, kHidT>(n, g, splits);
             if (rc) return rc;
         }
         dn = on;
@@ -584,10 +589,10 @@ int backward(dg_nn *n, long long rows, long long valid) {
 
 int adam(dg_nn *n, long long rows, float lr, int apply, float *gout) {
     AdamArgs a{};
-    for (int l = 0; l < 4; l++) {
+    for (int l = 0; l < kNL; l++) {
         a.W[l] = n->W[l]; a.b[l] = n->b[l]; a.mW[l] = n->mW[l]; a.vW[l] = n->vW[l]; a.mb[l] = n->mb[l];
         a.vb[l] = n->vb[l]; a.dw[l] = n->dw[l]; a.db[l] = n->db[l]; a.Wt[l] = n->Wt[l]; a.Wn[l] = n->Wn[l];
-        if (l < 3) a.Bt[l] = n->Bt[l];
+        if (l < kNHid) a.Bt[l] = n->Bt[l];
     }
     a.splits = (int)(rows / ((rows % 512 == 0) ? 512 : 128));
     a.tiles = (int)(rows / kTileRows);
@@ -670,8 +675,14 @@ int dg_wait_selftest(int device, int arrive, double *seconds) {
 
 long long dg_nn_param_count(void) {
     long long n = 0;
-    for (int l = 0; l < 4; l++) n += layer_params(l);
+    for (int l = 0; l < kNL; l++) n += layer_params(l);
     return n;
+}
+
+int dg_nn_shape(int *width, int *depth) {
+    if (width) *width = kHid;
+    if (depth) *depth = kNHid;
+    return DG_OK;
 }
 
 int dg_nn_create(int device, unsigned long long seed, dg_nn **out) {
@@ -699,16 +710,16 @@ int dg_nn_create(int device, unsigned long long seed, dg_nn **out) {
         z ^= z >> 31;
         return ((z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
     };
-    for (int l = 0; l < 4; l++) {
+    for (int l = 0; l < kNL; l++) {
         const int K = layer_k(l), N = layer_n(l);
         if ((rc = nn_alloc_t(n, &n->W[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->b[l], N)) ||
             (rc = nn_alloc_t(n, &n->mW[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->vW[l], (size_t)K * N)) ||
             (rc = nn_alloc_t(n, &n->mb[l], N)) || (rc = nn_alloc_t(n, &n->vb[l], N)) ||
             (rc = nn_alloc_t(n, &n->Wt[l], (size_t)K * N)) || (rc = nn_alloc_t(n, &n->Wn[l], (size_t)K * N)) ||
-            (l < 3 && (rc = nn_alloc_t(n, &n->Bt[l], (size_t)kBiasK * kHid))))
+            (l < kNHid && (rc = nn_alloc_t(n, &n->Bt[l], (size_t)kBiasK * kHid))))
             return bail(rc);
         std::vector<float> w((size_t)K * N, 0.0f);
-        const double sd = std::sqrt(2.0 / real_k(l)) * (l == 3 ? 0.1 : 1.0);
+        const double sd = std::sqrt(2.0 / real_k(l)) * (l == kNHid ? 0.1 : 1.0);
         for (int k = 0; k < real_k(l); k++)
             for (int j = 0; j < real_n(l); j++) {
                 const double u1 = next(), u2 = next();
@@ -880,7 +891,7 @@ int dg_nn_get_params(dg_nn *n, float *host, long long count) {
     if (!n || !host || count < dg_nn_param_count()) return nn_fail(DG_ERR_ARG, "bad parameter buffer");
     NN_CUDA(cudaSetDevice(n->device));
     long long off = 0;
-    for (int l = 0; l < 4; l++) {
+    for (int l = 0; l < kNL; l++) {
         const int K = layer_k(l), N = layer_n(l);
         std::vector<float> w((size_t)K * N), b(N);
         NN_CUDA(cudaMemcpyAsync(w.data(), n->W[l], w.size() * sizeof(float), cudaMemcpyDeviceToHost, n->stream));
@@ -897,7 +908,7 @@ int dg_nn_set_params(dg_nn *n, const float *host, long long count) {
     if (!n || !host || count < dg_nn_param_count()) return nn_fail(DG_ERR_ARG, "bad parameter buffer");
     NN_CUDA(cudaSetDevice(n->device));
     long long off = 0;
-    for (int l = 0; l < 4; l++) {
+    for (int l = 0; l < kNL; l++) {
         const int K = layer_k(l), N = layer_n(l);
         std::vector<float> w((size_t)K * N, 0.0f), b(N, 0.0f);
         for (int k = 0; k < real_k(l); k++)
@@ -974,8 +985,8 @@ int dg_nn_set_gates(dg_nn *n, float jump, float compress) {
 // ---- internal accessors for the step kernels (nn_host.h) ---------------------------
 int dg_nn_view(const dg_nn *n, dg::nn::NetView *v) {
     if (!n) return DG_ERR_ARG;
-    for (int l = 0; l < 4; l++) { v->wt[l] = n->Wt[l]; v->b[l] = n->b[l]; }
-    for (int l = 0; l < 3; l++) v->bt[l] = n->Bt[l];
+    for (int l = 0; l < kNL; l++) { v->wt[l] = n->Wt[l]; v->b[l] = n->b[l]; }
+    for (int l = 0; l < kNHid; l++) v->bt[l] = n->Bt[l];
     v->gates = n->gates;
     v->sc = n->sc;
     return DG_OK;

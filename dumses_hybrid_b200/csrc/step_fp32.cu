@@ -533,22 +533,76 @@ __global__ void __launch_bounds__(kThreads) k_nn_harvest(Geo G, const float *__r
         to[n] = (u.jump > nn::kTinyJump) ? (float)((t[n] - b[n]) / ((double)nn::out_scale(u, n) * (double)u.jump)) : 0.0f;
 }
 
-// shared-memory plan of the face-network kernel (bytes): the four weight tiles, the three
+// shared-memory plan of the face-network kernel (bytes): the kNL weight tiles, the kNHid
 // hidden-layer bias operands and the all-ones A operand they are multiplied by, then per
 // warpgroup one activation tile (its first 8 KB hold the input tile of layer 1), the output
 // layer's biases and the barriers
-constexpr int kNWG = 4;  // warpgroups per CTA (4 x 128 TMEM columns)
+// warpgroups per CTA, each with kHid TMEM columns (a build option, DG_NN_WG; the whole
+// register file is shared between them, one CTA per SM): six up to width 64 (80 registers),
+// four at width 128 (the tensor memory's 512 columns)
+#ifndef DG_NN_WG
+#define DG_NN_WG (DG_NN_WIDTH > 64 ? 4 : 6)
+#endif
+constexpr int kNWG = DG_NN_WG;
+constexpr int kNTmemUsed = kNWG * nn::kHid;
+constexpr int kNTmem = kNTmemUsed <= 32 ? 32 : kNTmemUsed <= 64 ? 64 : kNTmemUsed <= 128 ? 128
+                     : kNTmemUsed <= 256 ? 256 : 512;  // an allocation is a power of two from 32 to 512
+static_assert(kNTmemUsed <= 512 && kNWG >= 1 && kNWG <= 8, "warpgroups x width exceeds tensor memory");
 constexpr int kNBtsz = nn::kBiasK * nn::kHid * 2;
-constexpr int kNW1 = 0, kNW2 = 8192, kNW3 = 40960, kNW4 = 73728, kNBt = 77824, kNOne = kNBt + 3 * kNBtsz,
-              kNH0 = kNOne + nn::kBiasK * 128 * 2, kNHsz = 32768, kNBias = kNH0 + kNWG * kNHsz, kNBar = kNBias + 64,
-              kNSmem = kNBar + 128;
+// bytes of the weight tile of layer l: [K_l / 8][N_l][8] BF16
+__host__ __device__ constexpr int net_wbytes(int l) {
+    return (l == 0 ? nn::kInPad : nn::kHid) * (l == nn::kNHid ? nn::kOutPad : nn::kHid) * 2;
+}
+__host__ __device__ constexpr int net_woff(int l) { return l == 0 ? 0 : net_woff(l - 1) + net_wbytes(l - 1); }
+// per warpgroup a staging area for the trace-core values of its next tile (kNStF per face,
+// [value][face] floats), when it fits beside the rest (up to width 64; not in the checked build)
+constexpr int kNStF = 30, kNStsz = kNStF * 128 * 4;
+#ifdef DG_CHECK_BOUNDS
+constexpr bool kNChecked = true;
+#else
+constexpr bool kNChecked = false;
+#endif
+constexpr int kNBt = net_woff(nn::kNL), kNOne = kNBt + nn::kNHid * kNBtsz, kNH0 = kNOne + nn::kBiasK * 128 * 2,
+              kNHsz = 128 * nn::kHid * 2, kNSt0 = kNH0 + kNWG * kNHsz;
+#ifndef DG_NN_STAGE
+#define DG_NN_STAGE 1
+#endif
+constexpr bool kNStage = DG_NN_STAGE && !kNChecked && kNSt0 + kNWG * kNStsz + 192 <= 232448;
+constexpr int kNBias = kNSt0 + (kNStage ? kNWG * kNStsz : 0), kNBar = kNBias + 64, kNSmem = kNBar + 128;
 static_assert(kNSmem <= 232448, "face-network kernel exceeds the shared memory of one CTA");
 
 __device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory"); }
 
+// element copies (cp.async) of the trace-core values face t of direction d is made of into
+// this thread's column of a staging area: the 15 face_fields of its minus-side cell, then
+// those of its plus-side cell.  Invalid faces copy nothing.
+__device__ __forceinline__ void stage_face(const Geo &G, const float *__restrict__ core, int nf, int d, long long t,
+                                           float *st) {
+    if (t >= G.fsz) return;
+    int i, j, k;
+    split3((unsigned)t, G.dFX, G.dFY, i, j, k);
+    i++; j++; k++;
+    const bool valid = (d == 0) ? (j <= G.ny && (G.ndim == 2 || k <= G.nz))
+                     : (d == 1) ? (i <= G.nx && (G.ndim == 2 || k <= G.nz)) : (i <= G.nx && j <= G.ny);
+    if (!valid) return;
+    long long c[2];
+    face_cells(G, d, i, j, k, c[0], c[1]);
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+        int f[15];
+        face_fields(d, side == 0 ? +1 : -1, G.ndim, f);
+        const float *src = core + core_base(c[side], nf);
+#pragma unroll
+        for (int q = 0; q < 15; q++) {
+            const unsigned a = (unsigned)__cvta_generic_to_shared(st + (side * 15 + q) * 128);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(src + f[q] * kCoreLane) : "memory");
+        }
+    }
+}
+
 // Four warpgroups per CTA, each taking 128-face tiles in turn: the faces' interface states,
-// inputs and gates, the four layers as tcgen05 MMAs (weights resident in shared memory,
-// each warpgroup with its own 128 TMEM columns; a hidden layer's bias enters its accumulator
+// inputs and gates, the kNL layers as tcgen05 MMAs (weights resident in shared memory,
+// each warpgroup with its own kHid TMEM columns; a hidden layer's bias enters its accumulator
 // as one more K step, activations go through TMEM -> SmeLU -> shared memory), then the gated
 // flux or a mark for HLLD.
 __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *__restrict__ core,
@@ -559,10 +613,11 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     using bf16 = __nv_bfloat16;
     const int tid = threadIdx.x, wg = tid >> 7, wt = tid & 127, warp = tid >> 5, lane = tid & 31;
     // weight tile and bias operand of layer l
-    auto W = [&](int l) { return (bf16 *)(sm + (l == 0 ? kNW1 : l == 1 ? kNW2 : l == 2 ? kNW3 : kNW4)); };
+    auto W = [&](int l) { return (bf16 *)(sm + net_woff(l)); };
     auto Bt = [&](int l) { return (bf16 *)(sm + kNBt + l * kNBtsz); };
     bf16 *One = (bf16 *)(sm + kNOne);
     bf16 *Hs = (bf16 *)(sm + kNH0 + wg * kNHsz), *Xs = Hs;
+    float *stg = (float *)(sm + kNSt0 + wg * kNStsz) + wt;  // this thread's staging column (kNStage)
     float *bias = (float *)(sm + kNBias);  // output layer
     uint64_t *wbar = (uint64_t *)(sm + kNBar);
     uint64_t *mbar = (uint64_t *)(sm + kNBar + 8 + 8 * wg);
@@ -577,26 +632,25 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         }
         nn::mbar_fence_init();
     }
-    if (tid < nn::kOut) bias[tid] = nv.b[3][tid];
+    if (tid < nn::kOut) bias[tid] = nv.b[nn::kNHid][tid];
     // the A operand of the bias step: columns 0 and 1 of every row are 1
     for (int q = tid; q < nn::kBiasK * 128; q += 128 * kNWG) {
         const int r = q / nn::kBiasK, c = q % nn::kBiasK;
         One[nn::blk_off(r, c, nn::kBiasK, 128)] = __float2bfloat16_rn(c < 2 ? 1.0f : 0.0f);
     }
     nn::fence_async_smem();
-    if (warp == 0) nn::tmem_alloc(tslot, 128 * kNWG);
+    if (warp == 0) nn::tmem_alloc(tslot, kNTmem);
     nn::tc_fence_before();
     __syncthreads();
     nn::tc_fence_after();
-    const uint32_t tmem = *tslot + (uint32_t)(wg * 128);
+    const uint32_t tmem = *tslot + (uint32_t)(wg * nn::kHid);
     const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     if (tid == 0) {
-        const unsigned wb[4] = {128 * nn::kInPad * 2, 128 * 128 * 2, 128 * 128 * 2, nn::kOutPad * 128 * 2};
-        nn::mbar_expect_tx(wbar, wb[0] + wb[1] + wb[2] + wb[3] + 3 * kNBtsz);
+        nn::mbar_expect_tx(wbar, net_woff(nn::kNL) + nn::kNHid * kNBtsz);
 #pragma unroll
-        for (int l = 0; l < 4; l++) nn::bulk_g2s(W(l), nv.wt[l], wb[l], wbar);
+        for (int l = 0; l < nn::kNL; l++) nn::bulk_g2s(W(l), nv.wt[l], net_wbytes(l), wbar);
 #pragma unroll
-        for (int l = 0; l < 3; l++) nn::bulk_g2s(Bt(l), nv.bt[l], kNBtsz, wbar);
+        for (int l = 0; l < nn::kNHid; l++) nn::bulk_g2s(Bt(l), nv.bt[l], kNBtsz, wbar);
         if (!nn::mbar_wait(wbar, 0)) {
             nn::mbar_wait(wbar, 0);
             for (int g = 0; g < kNWG; g++) flags[g] = 0;
@@ -609,8 +663,12 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     unsigned ph = 0;
     unsigned long long nface = 0, nfall = 0;
     const bool weights_ok = *flag != 0;  // set before the block-wide barrier above
-    for (long long tile = (long long)kNWG * blockIdx.x + wg; weights_ok && tile * 128 < G.fsz;
-         tile += (long long)kNWG * gridDim.x) {
+    const long long tstride = (long long)kNWG * gridDim.x;
+    if constexpr (kNStage) {
+        if (weights_ok) stage_face(G, core, cv.nf, d, ((long long)kNWG * blockIdx.x + wg) * 128 + wt, stg);
+        cp_commit();
+    }
+    for (long long tile = (long long)kNWG * blockIdx.x + wg; weights_ok && tile * 128 < G.fsz; tile += tstride) {
         const long long t = tile * 128 + wt;
         int i = 0, j = 0, k = 1;
         bool valid = t < G.fsz;
@@ -625,13 +683,30 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         bool use = false;
 #pragma unroll
         for (int n = 0; n < nn::kInPad; n++) x[n] = 0.0f;
+        if constexpr (kNStage) cp_wait_all();  // this thread's copies of this tile's values
         if (valid) {
-            long long cl, cr;
-            face_cells(G, d, i, j, k, cl, cr);
-            face_io(G, cv, cl, cr, d, ql, qr);
+            if constexpr (kNStage) {
+                const float smallp = (float)G.smallp;
+                float v[15], fm[8], fp[8];
+#pragma unroll
+                for (int q = 0; q < 15; q++) v[q] = stg[q * 128];
+                face_state_v(v, d, +1, smallp, fm);
+#pragma unroll
+                for (int q = 0; q < 15; q++) v[q] = stg[(15 + q) * 128];
+                face_state_v(v, d, -1, smallp, fp);
+                face_pair(fm, fp, d, ql, qr);
+            } else {
+                long long cl, cr;
+                face_cells(G, d, i, j, k, cl, cr);
+                face_io(G, cv, cl, cr, d, ql, qr);
+            }
             u = nn::face_inputs(ql, qr, gamma, ciso, G.iso, x);
             use = nn::gate_inputs(nv.gates, ql, qr, ciso, G.iso, u, x);
             nn::base_fluxes<float>(ql, qr, gamma, ciso, G.iso, base, dis);
+        }
+        if constexpr (kNStage) {  // the next tile's values, in flight while this tile's layers run
+            stage_face(G, core, cv.nf, d, (tile + tstride) * 128 + wt, stg);
+            cp_commit();
         }
 #pragma unroll
         for (int n = 0; n < nn::kIn; n++) x[n] = use ? (x[n] - nv.sc.xmu[n]) * nv.sc.xisd[n] : 0.0f;
@@ -648,11 +723,12 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
         if (!*flag) break;  // read right after a barrier, so the whole warpgroup agrees
         float y[nn::kOut];
         bool tile_ok = true;
-        for (int l = 0; l < 4; l++) {
+        for (int l = 0; l < nn::kNL; l++) {
             if (wt == 0) {
                 nn::tc_fence_after();
-                nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W(l), l == 3 ? nn::kOutPad : nn::kHid, l == 0 ? 2 : 8, 0);
-                if (l < 3) nn::mma_extra_step(tmem, One, Bt(l), nn::kHid);  // + bias
+                nn::mma_tiles(tmem, l == 0 ? Xs : Hs, W(l), l == nn::kNHid ? nn::kOutPad : nn::kHid,
+                              (l == 0 ? nn::kInPad : nn::kHid) / 16, 0);
+                if (l < nn::kNHid) nn::mma_extra_step(tmem, One, Bt(l), nn::kHid);  // + bias
                 nn::mma_commit(mbar);
             }
             // every thread observes the MMA's completion itself; the warp agrees on the outcome
@@ -665,7 +741,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
             tile_ok = tile_ok && ok;
             ph++;
             nn::tc_fence_after();
-            if (l < 3) {
+            if (l < nn::kNHid) {
                 if (ok) {
                     // one 32-column chunk at a time (chunks interleaved by the compiler took the
                     // kernel to its 128-register limit, with spills, and 2% more time)
@@ -717,6 +793,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
             nfall += acc ? 0 : 1;
         }
     }
+    if constexpr (kNStage) cp_wait_all();  // no copy into shared memory outlives the loop
     if (!*flag && wt == 0) atomicOr(err, nn::NN_ERR_WAIT);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -731,7 +808,7 @@ __global__ void __launch_bounds__(128 * kNWG, 1) k_nn_faces(Geo G, const float *
     __syncthreads();
     if (warp == 0) {
         nn::tc_fence_after();
-        nn::tmem_dealloc(*tslot, 128 * kNWG);
+        nn::tmem_dealloc(*tslot, kNTmem);
     }
 }
 

@@ -1060,38 +1060,51 @@ struct CoreView {
     }
 };
 
-// face state (uin order r,u,v,w,p,A,B,C) of a cell on its minus (sgn=-1, "qp")
-// or plus (sgn=+1, "qm") side in direction d (scheme.f90:1489-1553, 1062-1100)
+// the 15 trace-core fields a cell's face state in direction d on side sgn is built from, in
+// the order face_state_v takes them: r u v w p, the 7 slopes of direction d (r u v w p and
+// the two transverse field components), the two transverse cell-centred field components,
+// and the field on the face itself
+__host__ __device__ __forceinline__ void face_fields(int d, int sgn, int ndim, int f[15]) {
+    const int base = (d == 0) ? C_DRX : (ndim == 3 ? (d == 1 ? C_DRY : C_DRZ) : D_DRY);
+    const int fAL = ndim == 3 ? C_AL : D_AL;
+#pragma unroll
+    for (int q = 0; q < 5; q++) f[q] = C_R + q;
+#pragma unroll
+    for (int q = 0; q < 7; q++) f[5 + q] = base + q;
+    if (d == 0) { f[12] = C_B; f[13] = C_C; f[14] = sgn > 0 ? fAL + 1 : fAL; }
+    else if (d == 1) { f[12] = C_A; f[13] = C_C; f[14] = sgn > 0 ? fAL + 3 : fAL + 2; }
+    else { f[12] = C_A; f[13] = C_B; f[14] = sgn > 0 ? C_CR : C_CL; }
+}
+
+// face state (uin order r,u,v,w,p,A,B,C) of a cell on its minus (sgn=-1, "qp") or plus
+// (sgn=+1, "qm") side in direction d from the values of its face_fields (scheme.f90:1489-1553,
+// 1062-1100)
+template <typename T>
+__device__ __forceinline__ void face_state_v(const T v[15], int d, int sgn, T smallp, T s[8]) {
+    const T smallr = T(kSmallr);
+    if (sgn > 0) {
+        s[IR] = mx(smallr, v[0] + v[5]); s[IU] = v[1] + v[6]; s[IV] = v[2] + v[7]; s[IW] = v[3] + v[8];
+        s[IP] = mx(smallp, v[4] + v[9]);
+    } else {
+        s[IR] = mx(smallr, v[0] - v[5]); s[IU] = v[1] - v[6]; s[IV] = v[2] - v[7]; s[IW] = v[3] - v[8];
+        s[IP] = mx(smallp, v[4] - v[9]);
+    }
+    const T t1 = sgn > 0 ? v[12] + v[10] : v[12] - v[10];
+    const T t2 = sgn > 0 ? v[13] + v[11] : v[13] - v[11];
+    if (d == 0) { s[IA] = v[14]; s[IB] = t1; s[IC] = t2; }
+    else if (d == 1) { s[IA] = t1; s[IB] = v[14]; s[IC] = t2; }
+    else { s[IA] = t1; s[IB] = t2; s[IC] = v[14]; }
+}
+
 template <typename T>
 __device__ __forceinline__ void face_state(const CoreView<T> &cv, long long c, int d, int sgn, int ndim, T smallp,
                                            T s[8]) {
-    const T r = cv.f(C_R, c), u = cv.f(C_U, c), v = cv.f(C_V, c), w = cv.f(C_W, c), p = cv.f(C_P, c);
-    const int base = (d == 0) ? C_DRX : (ndim == 3 ? (d == 1 ? C_DRY : C_DRZ) : D_DRY);
-    const T dr = cv.f(base + 0, c), du = cv.f(base + 1, c), dv = cv.f(base + 2, c), dw = cv.f(base + 3, c);
-    const T dp = cv.f(base + 4, c);
-    const T smallr = T(kSmallr);
-    if (sgn > 0) {
-        s[IR] = mx(smallr, r + dr); s[IU] = u + du; s[IV] = v + dv; s[IW] = w + dw; s[IP] = mx(smallp, p + dp);
-    } else {
-        s[IR] = mx(smallr, r - dr); s[IU] = u - du; s[IV] = v - dv; s[IW] = w - dw; s[IP] = mx(smallp, p - dp);
-    }
-    const int fAL = ndim == 3 ? C_AL : D_AL;
-    if (d == 0) {
-        const T B = cv.f(C_B, c), C = cv.f(C_C, c), dB = cv.f(base + 5, c), dC = cv.f(base + 6, c);
-        s[IA] = cv.f(sgn > 0 ? fAL + 1 : fAL, c);
-        s[IB] = sgn > 0 ? B + dB : B - dB;
-        s[IC] = sgn > 0 ? C + dC : C - dC;
-    } else if (d == 1) {
-        const T A = cv.f(C_A, c), C = cv.f(C_C, c), dA = cv.f(base + 5, c), dC = cv.f(base + 6, c);
-        s[IA] = sgn > 0 ? A + dA : A - dA;
-        s[IB] = cv.f(sgn > 0 ? fAL + 3 : fAL + 2, c);
-        s[IC] = sgn > 0 ? C + dC : C - dC;
-    } else {
-        const T A = cv.f(C_A, c), B = cv.f(C_B, c), dA = cv.f(base + 5, c), dB = cv.f(base + 6, c);
-        s[IA] = sgn > 0 ? A + dA : A - dA;
-        s[IB] = sgn > 0 ? B + dB : B - dB;
-        s[IC] = cv.f(sgn > 0 ? C_CR : C_CL, c);
-    }
+    int f[15];
+    face_fields(d, sgn, ndim, f);
+    T v[15];
+#pragma unroll
+    for (int q = 0; q < 15; q++) v[q] = cv.f(f[q], c);
+    face_state_v(v, d, sgn, smallp, s);
 }
 
 // corner state qXY(c, e) of edge direction e (0 x, 1 y, 2 z); sa/sb = +1/-1 are the
@@ -1164,17 +1177,12 @@ __device__ __forceinline__ void solve1d(int iriemann, const T *ql, const T *qr, 
     }
 }
 
-// solver-order interface states of the face in direction d between cells cl (minus side)
-// and cr (plus side): 0 rho, 1 P, 2 u_n, 3 B_n (face mean), 4 v_t1, 5 B_t1, 6 v_t2, 7 B_t2
-// (solver.f90:116-160)
+// the solver-order interface states of a face from the face states of its two cells (cell
+// minus side sm, plus side sp): 0 rho, 1 P, 2 u_n, 3 B_n (face mean), 4 v_t1, 5 B_t1, 6 v_t2,
+// 7 B_t2 (solver.f90:116-160)
 template <typename T>
-__device__ __forceinline__ void face_io(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d,
-                                        T ql[8], T qr[8]) {
+__device__ __forceinline__ void face_pair(const T sm[8], const T sp[8], int d, T ql[8], T qr[8]) {
     const T half = T(0.5);
-    const T smallp = (T)G.smallp;
-    T sm[8], sp[8];
-    face_state(cv, cl, d, +1, G.ndim, smallp, sm);
-    face_state(cv, cr, d, -1, G.ndim, smallp, sp);
     int ln, lt1, lt2, bn, bt1, bt2;
     if (d == 0) { ln = IU; lt1 = IV; lt2 = IW; bn = IA; bt1 = IB; bt2 = IC; }
     else if (d == 1) { ln = IV; lt1 = IU; lt2 = IW; bn = IB; bt1 = IA; bt2 = IC; }
@@ -1182,6 +1190,18 @@ __device__ __forceinline__ void face_io(const Geo &G, const CoreView<T> &cv, lon
     const T bn_mean = half * (sm[bn] + sp[bn]);
     ql[0] = sm[IR]; ql[1] = sm[IP]; ql[2] = sm[ln]; ql[3] = bn_mean; ql[4] = sm[lt1]; ql[5] = sm[bt1]; ql[6] = sm[lt2]; ql[7] = sm[bt2];
     qr[0] = sp[IR]; qr[1] = sp[IP]; qr[2] = sp[ln]; qr[3] = bn_mean; qr[4] = sp[lt1]; qr[5] = sp[bt1]; qr[6] = sp[lt2]; qr[7] = sp[bt2];
+}
+
+// solver-order interface states of the face in direction d between cells cl (minus side)
+// and cr (plus side)
+template <typename T>
+__device__ __forceinline__ void face_io(const Geo &G, const CoreView<T> &cv, long long cl, long long cr, int d,
+                                        T ql[8], T qr[8]) {
+    const T smallp = (T)G.smallp;
+    T sm[8], sp[8];
+    face_state(cv, cl, d, +1, G.ndim, smallp, sm);
+    face_state(cv, cr, d, -1, G.ndim, smallp, sp);
+    face_pair(sm, sp, d, ql, qr);
 }
 
 // shearing-box upwind terms (solver.f90:199-241) and compflux scaling of solver fluxes f

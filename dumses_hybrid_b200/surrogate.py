@@ -56,6 +56,6 @@ def train_flux_net(params: Params, u0: np.ndarray, snapshots: int = 2, every: in
             "held_out_error_ratio": {
                 "definition": "per output, L1 of (LLF + network - HLLD) over L1 of (LLF - HLLD) on held-out faces",
                 "outputs": OUTPUTS, "ratio": [float(r) for r in ratio], "mean": float(np.mean(ratio))},
-            "network": "17-128-128-128-8 SmeLU, bf16 weights, fp32 accumulate (tcgen05), Adam, "
-                       "lr 1e-3 / 3e-4 / 1e-4 in three equal phases, standardised inputs and outputs"}
+            "network": f"17-{'-'.join([str(net.shape[0])] * net.shape[1])}-8 SmeLU, bf16 weights, fp32 accumulate "
+                       "(tcgen05), Adam, lr 1e-3 / 3e-4 / 1e-4 in three equal phases, standardised inputs and outputs"}
     return net, info

@@ -297,7 +297,7 @@ const char *dg_last_error(void);
 
 /* ---- learned face-flux surrogate --------------------------------------------
  * No counterpart in the reference, whose face solver is always an exact one
- * (src/modules/solvers/solver.f90:163-187).  A 17 -> 128 -> 128 -> 128 -> 8 MLP
+ * (src/modules/solvers/solver.f90:163-187).  A 17 -> 64 -> 64 -> 8 MLP (by default)
  * with SmeLU hidden activations (the smooth ReLU: 0, (z+1)^2/4 or z), BF16
  * weights and FP32 accumulation on the tensor cores, trained on the device by
  * the library's own forward, backward and Adam kernels.  Per interface
@@ -312,8 +312,11 @@ const char *dg_last_error(void);
  *                B_t1, t2 momentum and B_t2 fluxes, and p*_T - (ptotL+ptotR)/2,
  *                each divided by J and by its unit (rho0 a0, rho0 a0^3, rho0 a0^2,
  *                sqrt(rho0) a0^2, rho0 a0^2)
- * Parameters, in dg_nn_get_params order: W1[17][128], b1[128], W2[128][128],
- * b2[128], W3[128][128], b3[128], W4[128][8], b4[8] (W[k][n]: input k, output n).
+ * Shape: 17 inputs, dg_nn_shape's depth hidden layers of its width, 8 outputs
+ * (the library's build fixes them; 64 x 2 by default, width 32, 64 or 128, depth
+ * 1 to 3).  Parameters, in dg_nn_get_params order, for width H and depth L:
+ * W1[17][H], b1[H], then L - 1 times W[H][H], b[H], then W[H][8], b[8]
+ * (W[k][n]: input k, output n); 5832 of them at the default shape.
  * Batches are multiples of 128 rows.  On a context with precision FP32 and
  * surrogate = 1, an attached network replaces HLLD on faces that pass its gates
  * (positive states, relative pressure and density jumps and compression below
@@ -323,6 +326,8 @@ typedef struct dg_nn dg_nn;
 #define DG_NN_INPUTS  17
 #define DG_NN_OUTPUTS 8
 long long dg_nn_param_count(void);
+/* hidden width and number of hidden layers of this build's network */
+int  dg_nn_shape(int *width, int *depth);
 int  dg_nn_create(int device, unsigned long long seed, dg_nn **out);
 int  dg_nn_destroy(dg_nn *nn);
 /* training samples: x[count][17], t[count][8] (scaled as above) */

@@ -1,7 +1,8 @@
 """CPU oracle of the learned face-flux network (test infrastructure only).
 
-FP64 numpy forward and backward passes of the 17 -> 128 -> 128 -> 128 -> 8 SmeLU MLP
-that the library trains on the GPU, with the mean-squared-error loss and the Adam
+FP64 numpy forward and backward passes of the SmeLU MLP that the library trains on the
+GPU (17 inputs, hidden layers of one width, 8 outputs; 17 -> 64 -> 64 -> 8 by default, any
+other shape through the ``shp`` argument, e.g. ``shapes(128, 3)``), with the mean-squared-error loss and the Adam
 update.  The GPU stores weights, activations and back-propagated errors in BF16 between
 its tensor-core products; with ``bf16=True`` this oracle rounds the same quantities at
 the same points (round-to-nearest-even of the FP32 value), so the two differ only by
@@ -10,19 +11,25 @@ finite differences by the tests.
 
 The network has no counterpart in the reference (whose face solver,
 src/modules/solvers/solver.f90:163-187, is always exact); HLLD (solver.f90:618-836) is
-its label generator.  Parameter order: W1[17][128], b1[128], W2[128][128], b2,
-W3[128][128], b3, W4[128][8], b4 (W[k][n] maps input k to output n).
+its label generator.  Parameter order: W1[17][64], b1[64], W2[64][64], b2, W3[64][8], b3
+at the default shape; W1, b1, the hidden W[w][w], b pairs, then W[w][8], b in general (W[k][n] maps
+input k to output n).
 """
 from __future__ import annotations
 
 import numpy as np
 
-SHAPES = [(17, 128), (128, 128), (128, 128), (128, 8)]
+def shapes(width: int = 64, depth: int = 2) -> list[tuple[int, int]]:
+    """(inputs, outputs) of each weight layer for `depth` hidden layers of `width` units."""
+    return [(17, width)] + [(width, width)] * (depth - 1) + [(width, 8)]
 
 
-def unpack(p: np.ndarray) -> list[tuple[np.ndarray, np.ndarray]]:
+SHAPES = shapes()
+
+
+def unpack(p: np.ndarray, shp=None) -> list[tuple[np.ndarray, np.ndarray]]:
     out, off = [], 0
-    for k, n in SHAPES:
+    for k, n in (shp or SHAPES):
         w = np.asarray(p[off:off + k * n], dtype=np.float64).reshape(k, n)
         off += k * n
         b = np.asarray(p[off:off + n], dtype=np.float64)
@@ -53,17 +60,17 @@ def smelu_d(z: np.ndarray) -> np.ndarray:
     return np.clip(0.5 * (z + 1.0), 0.0, 1.0)
 
 
-def forward(p: np.ndarray, x: np.ndarray, bf16_rounding: bool = True):
+def forward(p: np.ndarray, x: np.ndarray, bf16_rounding: bool = True, shp=None):
     """Network outputs and the cache needed by ``backward``."""
     r = bf16 if bf16_rounding else (lambda a: np.asarray(a, dtype=np.float64))
-    layers = unpack(p)
+    layers = unpack(p, shp)
     h = r(x)
     cache = {"h": [h], "gd": [], "w": []}
     for l, (w, b) in enumerate(layers):
         wb = r(w)
         cache["w"].append(wb)
         z = h @ wb + b
-        if l < 3:
+        if l < len(layers) - 1:
             cache["gd"].append(smelu_d(z))
             h = r(smelu(z))
             cache["h"].append(h)
@@ -72,15 +79,16 @@ def forward(p: np.ndarray, x: np.ndarray, bf16_rounding: bool = True):
     return y, cache
 
 
-def loss_and_grad(p: np.ndarray, x: np.ndarray, t: np.ndarray, bf16_rounding: bool = True):
+def loss_and_grad(p: np.ndarray, x: np.ndarray, t: np.ndarray, bf16_rounding: bool = True, shp=None):
     """Mean squared error over all outputs and its gradient in parameter order."""
     r = bf16 if bf16_rounding else (lambda a: np.asarray(a, dtype=np.float64))
-    y, c = forward(p, x, bf16_rounding)
+    y, c = forward(p, x, bf16_rounding, shp)
     e = y - t
     loss = float(np.mean(e * e))
     d = 2.0 * e / e.size  # dL/dy
-    grads = [None] * 4
-    for l in range(3, -1, -1):
+    nl = len(c["w"])
+    grads = [None] * nl
+    for l in range(nl - 1, -1, -1):
         db = d.sum(axis=0)
         dr = r(d)
         dw = c["h"][l].T @ dr

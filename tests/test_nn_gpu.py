@@ -21,7 +21,7 @@ def rel(a, b):
 def random_params(net, seed, scale=1.0):
     rng = np.random.default_rng(seed)
     p = []
-    for k, n in mo.SHAPES:
+    for k, n in net.shapes:
         p.append(rng.normal(0, scale * np.sqrt(2.0 / k), k * n))
         p.append(rng.normal(0, 0.1, n))
     p = np.concatenate(p).astype(np.float32)
@@ -29,9 +29,9 @@ def random_params(net, seed, scale=1.0):
     return p.astype(np.float64)
 
 
-def layer_slices():
+def layer_slices(net):
     out, off = [], 0
-    for k, n in mo.SHAPES:
+    for k, n in net.shapes:
         out.append(slice(off, off + k * n))
         off += k * n
         out.append(slice(off, off + n))
@@ -42,7 +42,9 @@ def layer_slices():
 def test_param_roundtrip():
     with FluxNet(seed=7) as net:
         p = net.params()
-        assert p.size == 36360 and np.isfinite(p).all() and np.abs(p).max() > 0
+        assert p.size == sum(k * n + n for k, n in net.shapes) and np.isfinite(p).all() and np.abs(p).max() > 0
+        assert net.shapes == mo.shapes(*net.shape)
+        assert p.size == {(64, 1): 1672, (64, 2): 5832, (128, 3): 36360}.get(net.shape, p.size)
         net.set_params(p * 0.5)
         assert np.array_equal(net.params(), (p * 0.5).astype(np.float32))
 
@@ -54,7 +56,7 @@ def test_forward_matches_oracle(rows):
         p = random_params(net, 11)
         x = rng.normal(0, 1, (rows, 17)).astype(np.float32)
         y = net.forward(x)
-        yo, _ = mo.forward(p, x.astype(np.float64))
+        yo, _ = mo.forward(p, x.astype(np.float64), shp=net.shapes)
         assert rel(y, yo) < 2e-3, rel(y, yo)
 
 
@@ -66,9 +68,9 @@ def test_gradients_match_oracle(batch):
         x = rng.normal(0, 1, (batch, 17)).astype(np.float32)
         t = rng.normal(0, 1, (batch, 8)).astype(np.float32)
         loss, g = net.gradients(x, t)
-        lo, go = mo.loss_and_grad(p, x.astype(np.float64), t.astype(np.float64))
+        lo, go = mo.loss_and_grad(p, x.astype(np.float64), t.astype(np.float64), shp=net.shapes)
         assert abs(loss - lo) <= 1e-3 * lo
-        for s in layer_slices():
+        for s in layer_slices(net):
             assert rel(g[s], go[s]) < 2e-3, (s, rel(g[s], go[s]))
 
 

@@ -2,25 +2,30 @@
 central finite differences of its own forward pass (exact arithmetic), and its BF16
 rounding against torch's conversion."""
 import numpy as np
+import pytest
 import torch
 
 from oracle import mlp_oracle as mo
 
 
-def test_oracle_gradient_matches_finite_differences():
+@pytest.mark.parametrize("width,depth", [(128, 3), (64, 2), (32, 1)])
+def test_oracle_gradient_matches_finite_differences(width, depth):
     rng = np.random.default_rng(3)
-    n = sum(k * m + m for k, m in mo.SHAPES)
+    shp = mo.shapes(width, depth)
+    assert mo.shapes() == mo.SHAPES
+    n = sum(k * m + m for k, m in shp)
     p = rng.normal(0, 0.2, n)
     x = rng.normal(0, 1, (4, 17))
     t = rng.normal(0, 1, (4, 8))
-    loss, g = mo.loss_and_grad(p, x, t, bf16_rounding=False)
+    loss, g = mo.loss_and_grad(p, x, t, bf16_rounding=False, shp=shp)
+    assert g.size == n
     idx = rng.choice(n, 60, replace=False)
     h = 1e-6
     for i in idx:
         pp, pm = p.copy(), p.copy()
         pp[i] += h
         pm[i] -= h
-        fd = (mo.loss_and_grad(pp, x, t, False)[0] - mo.loss_and_grad(pm, x, t, False)[0]) / (2 * h)
+        fd = (mo.loss_and_grad(pp, x, t, False, shp)[0] - mo.loss_and_grad(pm, x, t, False, shp)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, g[i])
 
 
