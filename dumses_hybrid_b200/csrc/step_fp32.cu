@@ -954,7 +954,9 @@ int launch_godunov(const Geo &G, const Bufs &B, int cur, cudaStream_t s) {
     }
     if (B.net) {
         for (int d = 0; d < G.ndim; d++) {
-            TIMED(KS_NN_FALLBACK, s, (k_nn_fallback<<<148 * 4, kThreads, 0, s>>>(G, core, fl[d], B.fb_list[d], B.nn_count, d, B.S)));
+            // the list's length is on the device: a grid-stride grid of 16 blocks per SM, above the ~7
+            // that stay resident, so that every SM has its full share of the scattered gathers in flight
+            TIMED(KS_NN_FALLBACK, s, (k_nn_fallback<<<148 * 16, kThreads, 0, s>>>(G, core, fl[d], B.fb_list[d], B.nn_count, d, B.S)));
             n++;
         }
     }
