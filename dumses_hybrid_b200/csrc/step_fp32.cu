@@ -538,10 +538,11 @@ __global__ void __launch_bounds__(kThreads) k_nn_harvest(Geo G, const float *__r
 // warpgroup one activation tile (its first 8 KB hold the input tile of layer 1), the output
 // layer's biases and the barriers
 // warpgroups per CTA, each with kHid TMEM columns (a build option, DG_NN_WG; the whole
-// register file is shared between them, one CTA per SM): six up to width 64 (80 registers),
-// four at width 128 (the tensor memory's 512 columns)
+// register file is shared between them, one CTA per SM): eight up to width 64 (64 registers,
+// with some spills: still faster than six at 80 or five at 94), four at width 128 (the tensor
+// memory's 512 columns)
 #ifndef DG_NN_WG
-#define DG_NN_WG (DG_NN_WIDTH > 64 ? 4 : 6)
+#define DG_NN_WG (DG_NN_WIDTH > 64 ? 4 : 8)
 #endif
 constexpr int kNWG = DG_NN_WG;
 constexpr int kNTmemUsed = kNWG * nn::kHid;
@@ -555,7 +556,8 @@ __host__ __device__ constexpr int net_wbytes(int l) {
 }
 __host__ __device__ constexpr int net_woff(int l) { return l == 0 ? 0 : net_woff(l - 1) + net_wbytes(l - 1); }
 // per warpgroup a staging area for the trace-core values of its next tile (kNStF per face,
-// [value][face] floats), when it fits beside the rest (up to width 64; not in the checked build)
+// [value][face] floats), when it fits beside the rest (width 64 with up to six warpgroups; not
+// in the checked build)
 constexpr int kNStF = 30, kNStsz = kNStF * 128 * 4;
 #ifdef DG_CHECK_BOUNDS
 constexpr bool kNChecked = true;
