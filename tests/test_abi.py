@@ -107,3 +107,16 @@ def test_namelist_reader(tmp_path):
     assert (p.nx, p.ny, p.nz) == (32, 64, 32)
     assert p.bdtypex == "shearingbox" and p.fargo
     assert p.omega0 == 1e-3 and p.courant == 0.8 and p.ymax == 4.0
+
+
+def test_network_shape_matches_parameter_count_and_oracle():
+    """dg_nn_shape and dg_nn_param_count are host-only calls: the library's network shape,
+    its parameter count and the oracle's layer shapes for that shape agree (17-64-64-8 by
+    default, 5832 parameters)."""
+    from oracle import mlp_oracle as mo
+    lib = dg.load_library()
+    width, depth = dg.network_shape(lib)
+    assert width in (32, 64, 128) and 1 <= depth <= 3
+    shp = mo.shapes(width, depth)
+    assert int(lib.dg_nn_param_count()) == sum(k * n + n for k, n in shp)
+    assert (width, depth) != (64, 2) or int(lib.dg_nn_param_count()) == 5832
